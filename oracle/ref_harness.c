@@ -1,0 +1,408 @@
+/*
+ * ref_harness.c -- drives the UNMODIFIED reference C sources (Tandav) for one
+ * gravity evaluation and dumps every hot-path intermediate to a binary file.
+ *
+ * Test infrastructure only: this program is the oracle's view of the real
+ * reference. It is linked against the reference's own objects (all of its
+ * src/ except main.c) by oracle/Makefile and is never part of the product.
+ *
+ * Sequence (mirrors src/main.c:112-191 preamble, src/init.c:11-76,
+ * src/setup.c:9-32, src/update.c:13-34 and src/accel.c:15-71):
+ *   preamble (threads, Task) -> memory -> particles -> periodic init + Ewald
+ *   table -> Setup_Domain_Decomposition -> Setup_Gravity_Tree ->
+ *   [omp parallel] Domain_Decomposition -> Gravity_Tree_Build ->
+ *   BH pass (Gravity_Tree_Acceleration with Use_BH_Criterion) ->
+ *   |a| into Last_Acc_Mag, Acc = 0 (accel.c:28-43) -> relative pass.
+ * For the periodic build the Ewald-only walks (Gravity_Tree_Periodic) are run
+ * once more on zeroed accumulators so that the correction can be compared on
+ * its own.
+ *
+ * Usage: ref_harness <mode> <input.bin> <output.bin>
+ *   mode "force": the sequence above.
+ *   mode "keys":  Peano_Key / Reversed_Peano_Key for the input positions with
+ *                 the domain taken from the input header (no decomposition).
+ *
+ * Input  (little endian): "TVIN", int32 version(1), int64 n, double box
+ *   (<=0: isolated), double softening, double origin[3], double size,
+ *   int32 flags (bit0 BH pass, bit1 relative pass), int32 pad,
+ *   double pos[3][n], double vel[3][n], double mass[n].
+ * Output: a list of records {char name[16]; int64 nbytes; bytes}.
+ */
+#include "includes.h"
+#include "domain.h"
+#include "peano.h"
+#include "timestep.h"
+#include "Gravity/tree.h"
+#include "Gravity/periodic.h"
+#include "periodic.h"
+#include "vector.h"
+
+void Init_Memory_Management(void);
+void Setup_Leaf_Vectors(void);
+
+struct dump_topnode {
+	uint64_t key;
+	int32_t target, level, first_part, npart;
+	float pos[3], mass, com[3], dp[3];
+};
+
+static FILE *Out = NULL;
+
+static void put(const char *name, const void *data, int64_t nbytes)
+{
+	char tag[16] = { 0 };
+	strncpy(tag, name, 15);
+	fwrite(tag, 1, 16, Out);
+	fwrite(&nbytes, sizeof(nbytes), 1, Out);
+	if (nbytes > 0)
+		fwrite(data, 1, (size_t) nbytes, Out);
+}
+
+static double now(void) { return omp_get_wtime(); }
+
+struct input {
+	int64_t n;
+	double box, soft, origin[3], size;
+	int32_t flags;
+	double *pos, *vel, *mass;
+};
+
+static struct input read_input(const char *fname)
+{
+	struct input in = { 0 };
+	FILE *fp = fopen(fname, "rb");
+	if (!fp) { fprintf(stderr, "cannot open %s\n", fname); exit(2); }
+	char magic[4];
+	int32_t version = 0, pad = 0;
+	if (fread(magic, 1, 4, fp) != 4 || memcmp(magic, "TVIN", 4)) { fprintf(stderr, "bad magic\n"); exit(2); }
+	if (fread(&version, 4, 1, fp) != 1 || version != 1) { fprintf(stderr, "bad version\n"); exit(2); }
+	size_t ok = fread(&in.n, 8, 1, fp);
+	ok += fread(&in.box, 8, 1, fp);
+	ok += fread(&in.soft, 8, 1, fp);
+	ok += fread(in.origin, 8, 3, fp);
+	ok += fread(&in.size, 8, 1, fp);
+	ok += fread(&in.flags, 4, 1, fp);
+	ok += fread(&pad, 4, 1, fp);
+	if (ok != 9) { fprintf(stderr, "short header\n"); exit(2); }
+	in.pos = malloc(3 * in.n * sizeof(double));
+	in.vel = malloc(3 * in.n * sizeof(double));
+	in.mass = malloc(in.n * sizeof(double));
+	if (fread(in.pos, 8, 3 * in.n, fp) != (size_t) (3 * in.n)
+	    || fread(in.vel, 8, 3 * in.n, fp) != (size_t) (3 * in.n)
+	    || fread(in.mass, 8, in.n, fp) != (size_t) in.n) {
+		fprintf(stderr, "short body\n");
+		exit(2);
+	}
+	fclose(fp);
+	return in;
+}
+
+/* Same thread/rank bookkeeping as the reference's preamble (main.c:112-191). */
+static void preamble(void)
+{
+	NRank = 1;
+	#pragma omp parallel
+	{
+		#pragma omp single
+		{
+			NThreads = omp_get_num_threads();
+			NTask = NRank * NThreads;
+		}
+		Task.Rank = 0;
+		Task.Thread_ID = omp_get_thread_num();
+		Task.ID = Task.Thread_ID;
+		Task.Is_Thread_Main = (Task.Thread_ID == 0);
+		Task.Is_Master = (Task.Thread_ID == 0);
+		Task.Is_MPI_Master = true;
+		Task.Seed[2] = 14041981L * Task.Thread_ID;
+		erand48(Task.Seed);
+	}
+}
+
+static void set_particle_counts(int64_t n)
+{
+	Sim.Npart_Total = n;
+	memset(Sim.Npart, 0, sizeof(Sim.Npart));
+	Sim.Npart[1] = n;
+	#pragma omp parallel
+	{
+		Task.Npart_Total = (int) n;
+		memset(Task.Npart, 0, sizeof(Task.Npart));
+		Task.Npart[1] = (int) n;
+	}
+}
+
+static void load_particles(const struct input *in)
+{
+	int64_t n = in->n;
+	for (int64_t i = 0; i < n; i++) {
+		P.Type[i] = 1;
+		P.Time_Bin[i] = 0;
+		P.It_Drift_Pos[i] = P.It_Kick_Pos[i] = 0;
+		P.Key[i] = 0;
+		P.ID[i] = (ID_t) i;
+		P.Cost[i] = 0;
+		for (int k = 0; k < 3; k++) {
+			P.Pos[k][i] = (Float) in->pos[k * n + i];
+			P.Vel[k][i] = (Float) in->vel[k * n + i];
+			P.Acc[k][i] = 0;
+			P.Grav_Acc[k][i] = 0;
+		}
+		P.Mass[i] = (Float) in->mass[i];
+		P.Last_Acc_Mag[i] = 0;
+		P.Tree_Parent[i] = 0;
+	}
+}
+
+static void zero_accumulators(void)
+{
+	#pragma omp for
+	for (int i = 0; i < Task.Npart_Total; i++) {
+		P.Acc[0][i] = P.Acc[1][i] = P.Acc[2][i] = 0;
+		P.Grav_Acc[0][i] = P.Grav_Acc[1][i] = P.Grav_Acc[2][i] = 0;
+		P.Cost[i] = 0;
+	}
+}
+
+/* Dump Acc/Grav_Acc/Cost as doubles under a name prefix. */
+static void dump_forces(const char *prefix, int64_t n)
+{
+	double *buf = malloc(3 * n * sizeof(double));
+	char name[16];
+	for (int k = 0; k < 3; k++)
+		for (int64_t i = 0; i < n; i++)
+			buf[k * n + i] = P.Acc[k][i];
+	snprintf(name, 16, "%s_acc", prefix);
+	put(name, buf, 3 * n * sizeof(double));
+	for (int k = 0; k < 3; k++)
+		for (int64_t i = 0; i < n; i++)
+			buf[k * n + i] = P.Grav_Acc[k][i];
+	snprintf(name, 16, "%s_gacc", prefix);
+	put(name, buf, 3 * n * sizeof(double));
+	for (int64_t i = 0; i < n; i++)
+		buf[i] = P.Cost[i];
+	snprintf(name, 16, "%s_cost", prefix);
+	put(name, buf, n * sizeof(double));
+	free(buf);
+}
+
+static void init_memory(int64_t n)
+{
+	size_t tree_bytes = sizeof(struct Tree_Node);
+	/* per-thread scratch: the PH reorder needs N*8 bytes (peano.c:56-58) and
+	 * a subtree is built in the buffer when it fits (tree_build.c:65-96) */
+	double per_thread = fmax(1.05 * n * 8.0, 2.0 * n * tree_bytes) + (16 << 20);
+	Param.Buffer_Size = (int) ceil(per_thread * NThreads / (1 << 20));
+	double pool = (double) n * 1.3 * (sizeof_P + 64.0 + 16.0) + 1.2 * 0.3 * n * tree_bytes;
+	Param.Max_Mem_Size = Param.Buffer_Size + (int) ceil(pool / (1 << 20)) + 512;
+	Param.Part_Alloc_Factor = 1.1;
+	Init_Memory_Management();
+}
+
+static int run_keys(const struct input *in)
+{
+	int64_t n = in->n;
+	Domain.Size = in->size;
+	for (int k = 0; k < 3; k++) Domain.Origin[k] = in->origin[k];
+	peanoKey *std = malloc(n * sizeof(peanoKey));
+	peanoKey *rev = malloc(n * sizeof(peanoKey));
+	for (int64_t i = 0; i < n; i++) {
+		Float x = (Float) in->pos[i], y = (Float) in->pos[n + i], z = (Float) in->pos[2 * n + i];
+		std[i] = Peano_Key(x, y, z);
+		rev[i] = Reversed_Peano_Key(x, y, z);
+	}
+	put("std_key", std, n * sizeof(peanoKey));
+	put("rev_key", rev, n * sizeof(peanoKey));
+	free(std); free(rev);
+	return 0;
+}
+
+static int run_force(const struct input *in)
+{
+	int64_t n = in->n;
+	bool periodic = in->box > 0;
+#ifdef PERIODIC
+	if (!periodic) { fprintf(stderr, "periodic build needs box > 0\n"); return 3; }
+#else
+	if (periodic) { fprintf(stderr, "isolated build needs box <= 0\n"); return 3; }
+#endif
+	set_particle_counts(n);
+	for (int t = 0; t < NPARTYPE; t++) Param.Grav_Softening[t] = in->soft;
+	/* sizeof_P is set by Allocate_Particle_Structures; size the pool first */
+	sizeof_P = 0;
+	for (int i = 0; i < NP_Fields; i++) sizeof_P += P_Fields[i].Bytes * P_Fields[i].N;
+	init_memory(n);
+	Allocate_Particle_Structures();
+	load_particles(in);
+	Time.Max_Active_Bin = 31;
+	Active_Particle_List = Malloc(Task.Npart_Total_Max * sizeof(*Active_Particle_List), "APL");
+	NActive_Particles = (int) n;
+	for (int64_t i = 0; i < n; i++) Active_Particle_List[i] = (int) i;
+
+	double t0 = now();
+	if (periodic) {
+		Sim.Boxsize[0] = Sim.Boxsize[1] = Sim.Boxsize[2] = in->box;
+		Init_Periodic();
+		#pragma omp parallel
+		Periodic_Constrain_Particles_To_Box();
+		Gravity_Periodic_Init();
+	}
+	double t_ewald_init = now() - t0;
+
+	Setup_Leaf_Vectors();
+	Setup_Domain_Decomposition();
+	Setup_Gravity_Tree();
+
+	double t_dd = 0, t_build = 0, t_bh = 0, t_rel = 0, t_bh_ew = 0, t_rel_ew = 0;
+	int flags = in->flags;
+	double *acc_bh = malloc(3 * n * sizeof(double));
+
+	#pragma omp parallel
+	{
+		#pragma omp master
+		t0 = now();
+		Sig.Prepare_Step = true;
+		Sig.Domain_Update = true;
+		Domain_Decomposition();
+		#pragma omp barrier
+		#pragma omp master
+		{ t_dd = now() - t0; t0 = now(); }
+		Gravity_Tree_Build();
+		#pragma omp barrier
+		#pragma omp master
+		t_build = now() - t0;
+	}
+
+	/* ---- dump decomposition and tree ---- */
+	{
+		put("domain_size", &Domain.Size, sizeof(double));
+		put("domain_origin", Domain.Origin, 3 * sizeof(double));
+		uint32_t *ids = malloc(n * sizeof(uint32_t));
+		for (int64_t i = 0; i < n; i++) ids[i] = (uint32_t) P.ID[i];
+		put("perm", ids, n * sizeof(uint32_t));
+		free(ids);
+		put("rev_key", P.Key, n * sizeof(peanoKey));
+		peanoKey *std = malloc(n * sizeof(peanoKey));
+		for (int64_t i = 0; i < n; i++)
+			std[i] = Peano_Key(P.Pos[0][i], P.Pos[1][i], P.Pos[2][i]);
+		put("std_key", std, n * sizeof(peanoKey));
+		free(std);
+		double *pos = malloc(3 * n * sizeof(double));
+		for (int k = 0; k < 3; k++)
+			for (int64_t i = 0; i < n; i++) pos[k * n + i] = P.Pos[k][i];
+		put("pos", pos, 3 * n * sizeof(double));
+		free(pos);
+		struct dump_topnode *tn = calloc(NTop_Nodes, sizeof(*tn));
+		for (uint32_t j = 0; j < NTop_Nodes; j++) {
+			tn[j].key = D[j].TNode.Key;
+			tn[j].target = D[j].TNode.Target;
+			tn[j].level = D[j].TNode.Level;
+			tn[j].first_part = D[j].TNode.First_Part;
+			tn[j].npart = D[j].TNode.Npart;
+			for (int k = 0; k < 3; k++) {
+				tn[j].pos[k] = D[j].TNode.Pos[k];
+				tn[j].com[k] = D[j].TNode.CoM[k];
+				tn[j].dp[k] = D[j].TNode.Dp[k];
+			}
+			tn[j].mass = D[j].TNode.Mass;
+		}
+		put("topnodes", tn, (int64_t) NTop_Nodes * sizeof(*tn));
+		free(tn);
+		put("tree", Tree, (int64_t) NNodes * sizeof(struct Tree_Node));
+		put("tree_parent", P.Tree_Parent, n * sizeof(*P.Tree_Parent));
+		int32_t fsize = (int32_t) sizeof(Float);
+		put("float_size", &fsize, 4);
+	}
+
+	#pragma omp parallel
+	{
+		if (flags & 1) {
+			zero_accumulators();
+			#pragma omp master
+			t0 = now();
+			Sig.Use_BH_Criterion = true;
+			Gravity_Tree_Acceleration();
+			#pragma omp barrier
+			#pragma omp master
+			{
+				t_bh = now() - t0;
+				dump_forces("bh", n);
+				for (int k = 0; k < 3; k++)
+					for (int64_t i = 0; i < n; i++) acc_bh[k * n + i] = P.Acc[k][i];
+			}
+			#pragma omp barrier
+			if (periodic) {
+				zero_accumulators();
+				#pragma omp master
+				t0 = now();
+				Gravity_Tree_Periodic();
+				#pragma omp barrier
+				#pragma omp master
+				{ t_bh_ew = now() - t0; dump_forces("bhew", n); }
+				#pragma omp barrier
+			}
+			/* accel.c:28-43: |a| of the BH pass becomes Last_Acc_Mag */
+			#pragma omp for
+			for (int i = 0; i < (int) n; i++) {
+				P.Acc[0][i] = (Float) acc_bh[i];
+				P.Acc[1][i] = (Float) acc_bh[n + i];
+				P.Acc[2][i] = (Float) acc_bh[2 * n + i];
+				P.Last_Acc_Mag[i] = SQRT(p2(P.Acc[0][i]) + p2(P.Acc[1][i]) + p2(P.Acc[2][i]));
+			}
+		}
+		if (flags & 2) {
+			zero_accumulators();
+			#pragma omp master
+			t0 = now();
+			Sig.Use_BH_Criterion = false;
+			Gravity_Tree_Acceleration();
+			#pragma omp barrier
+			#pragma omp master
+			{ t_rel = now() - t0; dump_forces("rel", n); }
+			#pragma omp barrier
+			if (periodic) {
+				zero_accumulators();
+				#pragma omp master
+				t0 = now();
+				Gravity_Tree_Periodic();
+				#pragma omp barrier
+				#pragma omp master
+				{ t_rel_ew = now() - t0; dump_forces("relew", n); }
+				#pragma omp barrier
+			}
+		}
+	}
+	{
+		double *lam = malloc(n * sizeof(double));
+		for (int64_t i = 0; i < n; i++) lam[i] = P.Last_Acc_Mag[i];
+		put("last_acc_mag", lam, n * sizeof(double));
+		free(lam);
+	}
+	double timings[8] = { t_ewald_init, t_dd, t_build, t_bh, t_bh_ew, t_rel, t_rel_ew, (double) NThreads };
+	put("timings", timings, sizeof(timings));
+	double gconst = Const.Gravity;
+	put("gravity", &gconst, sizeof(double));
+	double eps[3] = { Epsilon[1], Epsilon2[1], Epsilon3[1] };
+	put("epsilon", eps, sizeof(eps));
+	free(acc_bh);
+	return 0;
+}
+
+int main(int argc, char *argv[])
+{
+	if (argc != 4) {
+		fprintf(stderr, "usage: %s force|keys input.bin output.bin\n", argv[0]);
+		return 1;
+	}
+	preamble();
+	struct input in = read_input(argv[2]);
+	Out = fopen(argv[3], "wb");
+	if (!Out) { fprintf(stderr, "cannot write %s\n", argv[3]); return 2; }
+	int rc = 1;
+	if (!strcmp(argv[1], "keys"))
+		rc = run_keys(&in);
+	else if (!strcmp(argv[1], "force"))
+		rc = run_force(&in);
+	fclose(Out);
+	return rc;
+}
