@@ -1,0 +1,215 @@
+/*
+ * tandav_gpu.h -- C ABI of the B200 (sm_100a) gravity hot path for Tandav.
+ *
+ * Each entry point replaces the body of one reference C entry point (paths
+ * relative to the reference's src/); a reference build with GPU gravity calls
+ * these from the original functions, inside one `#pragma omp single` (the
+ * reference's entry points are orphaned OpenMP worksharing functions run by
+ * every thread of the team, src/main.c:37).
+ *
+ * All pointers in this interface are host pointers to plain arrays; device
+ * memory is owned by the context. "Float" arrays have the width given by
+ * tvg_config.float_bytes (4, or 8 under DOUBLE_PRECISION, src/globals.h:46-54).
+ * Every function returns TVG_OK or an error code; tvg_last_error() gives the
+ * message. Nothing here falls back to the CPU: without a usable GPU the calls
+ * fail with TVG_E_CUDA.
+ */
+#ifndef TANDAV_GPU_H
+#define TANDAV_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the reference's fatal Assert, src/aux.c:49-77, becomes a
+ * return value the host maps to Assert) */
+enum {
+	TVG_OK = 0,
+	TVG_E_CUDA = 1,        /* CUDA runtime error or no device */
+	TVG_E_NOMEM = 2,       /* device allocation failed */
+	TVG_E_TREE_FULL = 3,   /* node capacity exceeded */
+	TVG_E_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+	TVG_E_BADINPUT = 5,    /* invalid argument, NaN/Inf or out-of-domain position */
+	TVG_E_COINCIDENT = 6,  /* particles equal to 41 key levels (tree_build.c:337) */
+	TVG_E_STATE = 7        /* call out of order (e.g. walk before tree build) */
+};
+
+typedef struct tvg_context tvg_context;
+
+/* Compile-time Config and run-time parameters of the reference that the hot
+ * path reads. */
+typedef struct {
+	int32_t float_bytes;   /* sizeof(Float) */
+	int32_t periodic;      /* PERIODIC */
+	double boxsize;        /* Sim.Boxsize[0] (periodic) */
+	double gravity;        /* Const.Gravity (src/constants.c:5) */
+	double softening;      /* Param.Grav_Softening[1]; tree_build.c:134-139 */
+	double open_bh;        /* TREE_OPEN_PARAM_BH (theta^2) */
+	double open_rel;       /* TREE_OPEN_PARAM_REL */
+	int32_t vector_size;   /* VECTOR_SIZE */
+	int32_t flags;         /* TVG_CFG_* */
+	int64_t max_particles; /* device capacity (Task.Npart_Total_Max) */
+} tvg_config;
+
+enum {
+	/* interact_with_topnode_particles indexes particles from the top node's
+	 * Target (tree_accel.c:185, tree_periodic.c:188), which for top nodes with
+	 * <= VECTOR_SIZE particles holds a tree index (tree_build.c:91). Set this
+	 * flag to use First_Part instead. Default: the reference's behaviour. */
+	TVG_CFG_FIX_SMALL_TOPNODES = 1
+};
+
+/* Host view of struct Particle_Data (src/Gravity/../particles.h:17-37). Any
+ * pointer may be NULL when the matching field bit is not requested. */
+typedef struct {
+	int32_t *type;
+	int32_t *time_bin;
+	uint32_t *it_drift_pos;
+	uint32_t *it_kick_pos;
+	void *key;             /* peanoKey, 16 bytes per particle (little endian) */
+	uint32_t *id;
+	void *cost;
+	void *pos[3];
+	void *vel[3];
+	void *acc[3];
+	void *mass;
+	void *grav_acc[3];
+	void *last_acc_mag;
+	int32_t *tree_parent;
+} tvg_particles;
+
+enum {
+	TVG_F_TYPE = 1 << 0, TVG_F_TIME_BIN = 1 << 1, TVG_F_IT_DRIFT = 1 << 2,
+	TVG_F_IT_KICK = 1 << 3, TVG_F_KEY = 1 << 4, TVG_F_ID = 1 << 5, TVG_F_COST = 1 << 6,
+	TVG_F_POS = 1 << 7, TVG_F_VEL = 1 << 8, TVG_F_ACC = 1 << 9, TVG_F_MASS = 1 << 10,
+	TVG_F_GRAV_ACC = 1 << 11, TVG_F_LAST_ACC = 1 << 12, TVG_F_TREE_PARENT = 1 << 13,
+	TVG_F_ALL = (1 << 14) - 1
+};
+
+/* Top node as dumped from union Domain_Node_List (src/domain.h:40-52). */
+typedef struct {
+	uint64_t key;
+	int32_t target, level, first_part, npart;
+	float pos[3], mass, com[3], dp[3];
+} tvg_topnode;
+
+/* ------------------------------------------------------------ lifecycle */
+
+/* Creates a context on `device` and allocates device memory for
+ * cfg->max_particles particles. Replaces the device side of
+ * Allocate_Particle_Structures (src/particles.c:28) and Setup_Gravity_Tree
+ * (src/Gravity/tree_build.c:124-142). */
+int tvg_init(int device, const tvg_config *cfg, tvg_context **ctx);
+void tvg_finalize(tvg_context *ctx);
+const char *tvg_last_error(const tvg_context *ctx);
+/* Library version string. */
+const char *tvg_version(void);
+
+/* Copies host particle fields (bitmask TVG_F_*) of n particles to the
+ * device mirror; n becomes the active particle count (Task.Npart_Total). */
+int tvg_upload(tvg_context *ctx, int64_t n, const tvg_particles *p, uint32_t fields);
+/* Copies device fields back to the host arrays. */
+int tvg_download(tvg_context *ctx, tvg_particles *p, uint32_t fields);
+
+/* ------------------------------------------------ keys, sort, top nodes */
+
+/* Domain.Origin / Domain.Size used by the keys (set_computational_domain,
+ * src/domain.c:732-762). */
+int tvg_set_domain(tvg_context *ctx, const double origin[3], double size);
+
+/* Replaces the Peano_Key loop of Sort_Particles_By_Peano_Key
+ * (src/peano.c:27-30): P.Key = standard 128-bit key of P.Pos. */
+int tvg_peano_keys(tvg_context *ctx);
+
+/* Replaces Qsort_Index + reorder_collisionless_particles
+ * (src/peano.c:32-35, src/sort.c:90-116, src/aux.c:187-301): sorts all
+ * device particle fields by P.Key. Equal 128-bit keys keep input order. If
+ * perm is not NULL it receives the index permutation (new i <- old perm[i]). */
+int tvg_sort_particles(tvg_context *ctx, uint32_t *perm);
+
+/* Replaces Reverse_Peano_Keys (src/peano.c:84-97): P.Key = reversed key. */
+int tvg_reverse_keys(tvg_context *ctx);
+
+/* Top nodes of the single-target decomposition (src/domain.c:67-145,
+ * 220-250 with NTarget = 1): every non-empty level-2 cell, in descending key
+ * order. Particles must be sorted. ntop receives the count (<= 64). */
+int tvg_top_nodes(tvg_context *ctx, int32_t *ntop);
+
+/* ----------------------------------------------------------- tree build */
+
+enum {
+	/* node Mass/CoM summed in particle order in Float, as the reference does
+	 * (tree_build.c:561-572); otherwise in FP64 and rounded once. */
+	TVG_BUILD_EXACT_MOMENTS = 1
+};
+
+/* Replaces Gravity_Tree_Build (src/Gravity/tree_build.c:47-122): builds the
+ * subtree of every top node, the top nodes' Target/Mass/CoM and
+ * P.Tree_Parent, on the device. */
+int tvg_tree_build(tvg_context *ctx, uint32_t flags);
+
+/* Copies the tree in the reference layout (struct Tree_Node, 56 B FP32 /
+ * 96 B FP64, src/Gravity/tree.h:23-32) and the top nodes to the host. */
+int tvg_download_tree(tvg_context *ctx, void *tree, int64_t tree_cap, int64_t *nnodes,
+                      tvg_topnode *top, int32_t top_cap, int32_t *ntop);
+
+/* ----------------------------------------------------------- tree walk */
+
+enum {
+	/* the reference algorithm, one thread per active particle, in Float */
+	TVG_FORM_PLAIN = 0,
+	/* one warp per PH group, FP32 on integer-offset positions */
+	TVG_FORM_GROUP = 1
+};
+enum { TVG_WALK_GRAVITY = 1, TVG_WALK_EWALD = 2 };
+enum { TVG_EWALD_TABLE = 0, TVG_EWALD_MLP = 1 };
+
+/* Replaces Gravity_Periodic_Init (src/Gravity/periodic.c:180-233): the
+ * 65^3 Ewald force (and potential) tables, computed in FP64 on the device and
+ * stored as Float divided by Boxsize^2 (Boxsize). */
+int tvg_ewald_init(tvg_context *ctx);
+/* Copies the four raw (box-unit) Float tables Fx, Fy, Fz, Fp, in the layout of
+ * the reference's ./ewald_tables.dat (Gravity/periodic.c:325-342). */
+int tvg_download_ewald_table(tvg_context *ctx, void *fx, void *fy, void *fz, void *fp);
+
+/* Loads raw (box-unit) Float tables as read from ./ewald_tables.dat
+ * (read_ewald_correction_table, Gravity/periodic.c:303-323) instead of
+ * computing them, then divides by Boxsize^2 / Boxsize as the reference does. */
+int tvg_upload_ewald_table(tvg_context *ctx, const void *fx, const void *fy, const void *fz,
+                           const void *fp);
+
+/* Replaces Gravity_Tree_Acceleration (src/Gravity/tree_accel.c:32-91) and,
+ * with TVG_WALK_EWALD, Gravity_Tree_Periodic (src/Gravity/tree_periodic.c:
+ * 23-72), for the active particles: Acc += walk, Grav_Acc = walk (gravity
+ * part) / Grav_Acc += walk (Ewald part), Cost = / += interaction count. The
+ * criterion is Barnes & Hut when use_bh != 0 (Sig.Use_BH_Criterion), else the
+ * relative criterion with P.Last_Acc_Mag. */
+int tvg_walk(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts, int32_t ewald_kind);
+
+/* accel.c:28-43 (safe_last_accel): Last_Acc_Mag = |Acc|, Acc = 0. */
+int tvg_save_last_accel(tvg_context *ctx);
+
+/* Zero Acc, Grav_Acc and Cost of all particles. */
+int tvg_zero_accel(tvg_context *ctx);
+
+/* ---------------------------------------------------- whole force step */
+
+/* One tree-force evaluation on device-resident particles: keys, sort,
+ * top nodes, tree build and the walk(s) of `parts` (accel.c:51-71 without
+ * the BH prepare pass when use_bh == 0). */
+int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
+                   int32_t ewald_kind);
+
+/* Per-phase device times (ms) of the last calls, CUDA events on the
+ * context stream: [keys, sort, top, build, walk, ewald walk, total]. */
+int tvg_phase_times(tvg_context *ctx, double *ms, int32_t n);
+
+/* Counters of the last walk: total gravity and Ewald interactions. */
+int tvg_walk_counters(tvg_context *ctx, double *grav_interactions, double *ewald_interactions);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

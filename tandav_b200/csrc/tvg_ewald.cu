@@ -1,0 +1,185 @@
+// tvg_ewald.cu -- Ewald correction tables on the GPU (Gravity_Periodic_Init,
+// Gravity/periodic.c:180-300).
+//
+// compute_ewald_force / compute_ewald_potential (Gravity/periodic.c:352-461):
+// the force of the periodic lattice minus the nearest image, after Hernquist,
+// Bouchet & Suto (1991, eqs. 2.14-2.16), alpha = 2, real-space images and
+// k-space vectors with |n|, |h| <= 4 per axis, evaluated in FP64 at the
+// (64+1)^3 points of the folded octant [0, L/2]^3 (box units), one thread per
+// point and axis-sum. Stored as Float, then divided by Boxsize^2 (force) and
+// Boxsize (potential) as the reference does after loading (periodic.c:215-228).
+// The raw FP64 values stay on the device as the training target and max-error
+// judge of the learned correction.
+#include "tvg_internal.cuh"
+
+#define N_EWALD 64
+#define N_EW1 (N_EWALD + 1)
+
+__device__ void ewald_point(const double x[3], double f[3], double *pot)
+{
+	const double alpha = 2.0, pi = 3.14159265358979323846;
+	f[0] = f[1] = f[2] = 0;
+	if (x[0] == 0 && x[1] == 0 && x[2] == 0) {
+		*pot = 2.8372975;                     // periodic.c:419
+		return;
+	}
+	const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+	const double r3 = r * r * r;
+	for (int k = 0; k < 3; k++) f[k] = x[k] / r3;
+	double s1 = 0, s2 = 0;
+	for (int a = -4; a < 5; a++)
+		for (int b = -4; b < 5; b++)
+			for (int c = -4; c < 5; c++) {
+				const double d0 = x[0] - a, d1 = x[1] - b, d2 = x[2] - c;
+				const double rr = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+				const double ar = alpha * rr;
+				const double val = erfc(ar) + 2 * alpha * rr / sqrt(pi) * exp(-(ar * ar));
+				const double q = rr * rr * rr;
+				f[0] -= d0 / q * val;
+				f[1] -= d1 / q * val;
+				f[2] -= d2 / q * val;
+				s1 += erfc(ar) / rr;
+			}
+	for (int a = -4; a < 5; a++)
+		for (int b = -4; b < 5; b++)
+			for (int c = -4; c < 5; c++) {
+				const int h2 = a * a + b * b + c * c;
+				if (h2 == 0) continue;
+				const double hx = x[0] * a + x[1] * b + x[2] * c;
+				const double e = exp(-pi * pi * h2 / (alpha * alpha));
+				const double val = 2.0 / h2 * e * sin(2 * pi * hx);
+				f[0] -= a * val;
+				f[1] -= b * val;
+				f[2] -= c * val;
+				s2 += 1.0 / (pi * h2) * e * cos(2 * pi * hx);
+			}
+	*pot = pi / (alpha * alpha) - s1 - s2 + 1.0 / r;
+}
+
+template <typename F>
+__global__ void k_ewald_table(double box, F *fx, F *fy, F *fz, F *fp, double *raw)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= N_EW1 * N_EW1 * N_EW1) return;
+	const int i = idx / (N_EW1 * N_EW1), j = (idx / N_EW1) % N_EW1, k = idx % N_EW1;
+	const double x[3] = { (0.5 * i) / N_EWALD, (0.5 * j) / N_EWALD, (0.5 * k) / N_EWALD };
+	double f[3], pot;
+	ewald_point(x, f, &pot);
+	raw[4 * idx + 0] = f[0];
+	raw[4 * idx + 1] = f[1];
+	raw[4 * idx + 2] = f[2];
+	raw[4 * idx + 3] = pot;
+	// Float storage, then the division after the load (periodic.c:215-228)
+	fx[idx] = (F) ((double) (F) f[0] / (box * box));
+	fy[idx] = (F) ((double) (F) f[1] / (box * box));
+	fz[idx] = (F) ((double) (F) f[2] / (box * box));
+	fp[idx] = (F) ((double) (F) pot / box);
+}
+
+int tvg_impl_ewald_init(tvg_context *ctx)
+{
+	const size_t npt = (size_t) N_EW1 * N_EW1 * N_EW1;
+	for (int t = 0; t < 4; t++)
+		if (!ctx->ewald_f[t]) TVG_CUDA(ctx, cudaMalloc(&ctx->ewald_f[t], tvg_fsize(ctx) * npt));
+	if (!ctx->ewald_raw) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->ewald_raw, 4 * 8 * npt));
+	const unsigned nb = tvg_blocks((int64_t) npt, 128);
+	if (ctx->cfg.float_bytes == 4)
+		k_ewald_table<float><<<nb, 128, 0, ctx->stream>>>(
+		    ctx->cfg.boxsize, (float *) ctx->ewald_f[0], (float *) ctx->ewald_f[1],
+		    (float *) ctx->ewald_f[2], (float *) ctx->ewald_f[3], ctx->ewald_raw);
+	else
+		k_ewald_table<double><<<nb, 128, 0, ctx->stream>>>(
+		    ctx->cfg.boxsize, (double *) ctx->ewald_f[0], (double *) ctx->ewald_f[1],
+		    (double *) ctx->ewald_f[2], (double *) ctx->ewald_f[3], ctx->ewald_raw);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+	return TVG_OK;
+}
+
+// raw Float tables (box units) -> device tables, as after
+// read_ewald_correction_table + the division at periodic.c:215-228
+template <typename F>
+__global__ void k_ewald_from_raw(double box, const F *rx, const F *ry, const F *rz, const F *rp,
+                                 F *fx, F *fy, F *fz, F *fp, double *raw)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= N_EW1 * N_EW1 * N_EW1) return;
+	raw[4 * idx + 0] = (double) rx[idx];
+	raw[4 * idx + 1] = (double) ry[idx];
+	raw[4 * idx + 2] = (double) rz[idx];
+	raw[4 * idx + 3] = (double) rp[idx];
+	fx[idx] = (F) ((double) rx[idx] / (box * box));
+	fy[idx] = (F) ((double) ry[idx] / (box * box));
+	fz[idx] = (F) ((double) rz[idx] / (box * box));
+	fp[idx] = (F) ((double) rp[idx] / box);
+}
+
+extern "C" int tvg_upload_ewald_table(tvg_context *ctx, const void *fx, const void *fy,
+                                      const void *fz, const void *fp)
+{
+	if (!ctx || !fx || !fy || !fz || !fp) return TVG_E_BADINPUT;
+	if (!ctx->cfg.periodic) return tvg_fail(ctx, TVG_E_STATE, "upload_ewald_table: not periodic");
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	const size_t npt = (size_t) N_EW1 * N_EW1 * N_EW1, b = tvg_fsize(ctx) * npt;
+	for (int t = 0; t < 4; t++)
+		if (!ctx->ewald_f[t]) TVG_CUDA(ctx, cudaMalloc(&ctx->ewald_f[t], b));
+	if (!ctx->ewald_raw) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->ewald_raw, 4 * 8 * npt));
+	void *tmp = nullptr;
+	TVG_CUDA(ctx, cudaMalloc(&tmp, 4 * b));
+	const void *src[4] = { fx, fy, fz, fp };
+	for (int t = 0; t < 4; t++)
+		TVG_CUDA(ctx, cudaMemcpyAsync((char *) tmp + t * b, src[t], b, cudaMemcpyHostToDevice, ctx->stream));
+	const unsigned nb = tvg_blocks((int64_t) npt, 256);
+	if (ctx->cfg.float_bytes == 4) {
+		const float *r = (const float *) tmp;
+		k_ewald_from_raw<float><<<nb, 256, 0, ctx->stream>>>(
+		    ctx->cfg.boxsize, r, r + npt, r + 2 * npt, r + 3 * npt, (float *) ctx->ewald_f[0],
+		    (float *) ctx->ewald_f[1], (float *) ctx->ewald_f[2], (float *) ctx->ewald_f[3], ctx->ewald_raw);
+	} else {
+		const double *r = (const double *) tmp;
+		k_ewald_from_raw<double><<<nb, 256, 0, ctx->stream>>>(
+		    ctx->cfg.boxsize, r, r + npt, r + 2 * npt, r + 3 * npt, (double *) ctx->ewald_f[0],
+		    (double *) ctx->ewald_f[1], (double *) ctx->ewald_f[2], (double *) ctx->ewald_f[3],
+		    ctx->ewald_raw);
+	}
+	cudaError_t e = cudaGetLastError();
+	if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+	cudaFree(tmp);
+	TVG_CUDA(ctx, e);
+	ctx->have_ewald = true;
+	return TVG_OK;
+}
+
+template <typename F>
+__global__ void k_ewald_raw_float(const double *raw, F *out, int comp, int n)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = (F) raw[4 * i + comp];
+}
+
+extern "C" int tvg_download_ewald_table(tvg_context *ctx, void *fx, void *fy, void *fz, void *fp)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!ctx->have_ewald) return tvg_fail(ctx, TVG_E_STATE, "ewald table not initialised");
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	const int npt = N_EW1 * N_EW1 * N_EW1;
+	void *outs[4] = { fx, fy, fz, fp };
+	void *tmp = nullptr;
+	TVG_CUDA(ctx, cudaMalloc(&tmp, tvg_fsize(ctx) * npt));
+	for (int c = 0; c < 4; c++) {
+		if (!outs[c]) continue;
+		if (ctx->cfg.float_bytes == 4)
+			k_ewald_raw_float<float><<<tvg_blocks(npt, 256), 256, 0, ctx->stream>>>(ctx->ewald_raw,
+			                                                                          (float *) tmp, c, npt);
+		else
+			k_ewald_raw_float<double><<<tvg_blocks(npt, 256), 256, 0, ctx->stream>>>(ctx->ewald_raw,
+			                                                                           (double *) tmp, c, npt);
+		cudaError_t e = cudaMemcpyAsync(outs[c], tmp, tvg_fsize(ctx) * npt, cudaMemcpyDeviceToHost,
+		                                ctx->stream);
+		if (e != cudaSuccess) { cudaFree(tmp); TVG_CUDA(ctx, e); }
+	}
+	cudaError_t e = cudaStreamSynchronize(ctx->stream);
+	cudaFree(tmp);
+	TVG_CUDA(ctx, e);
+	return TVG_OK;
+}

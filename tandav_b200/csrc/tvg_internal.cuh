@@ -1,0 +1,199 @@
+// tvg_internal.cuh -- shared definitions of the B200 gravity hot path.
+//
+// Device data layout (HBM, all arrays structure-of-arrays, capacity `cap`):
+//   particle fields mirror struct Particle_Data (particles.h:17-37) in the
+//   host's Float width, each with a second "alt" buffer so that the PH
+//   permutation is a gather into alt followed by a pointer swap;
+//   keys are split into key_hi / key_lo (uint64) for the radix sort;
+//   the tree is kept twice: in the reference layout (struct Tree_Node, for
+//   download and the plain walk) and, for the group walk, as level-ordered
+//   node records with integer (box-fraction) coordinates.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/tandav_gpu.h"
+
+#define TVG_MAX_TOP 64
+#define TVG_MAX_LEVEL 42
+
+// ---------------------------------------------------------------- errors
+
+#define TVG_CUDA(ctx, call)                                                        \
+	do {                                                                           \
+		cudaError_t e_ = (call);                                                   \
+		if (e_ != cudaSuccess)                                                     \
+			return tvg_fail((ctx), TVG_E_CUDA, "%s:%d %s: %s", __FILE__, __LINE__,  \
+			                #call, cudaGetErrorString(e_));                         \
+	} while (0)
+
+#define TVG_CHECK(expr)                                                            \
+	do {                                                                           \
+		int rc_ = (expr);                                                          \
+		if (rc_ != TVG_OK) return rc_;                                             \
+	} while (0)
+
+// device status word bits (written by kernels, read by the host after a phase)
+enum {
+	TVG_ST_COINCIDENT = 1,
+	TVG_ST_BADPOS = 2,
+	TVG_ST_TREE_FULL = 4,
+	TVG_ST_TIMEOUT = 8,
+	TVG_ST_LIST_OVERFLOW = 16
+};
+
+struct tvg_buf {
+	void *p = nullptr;
+	size_t bytes = 0;
+};
+
+// Walk node record of the group walk (level-ordered tree, 48 bytes).
+struct __align__(16) tvg_wnode {
+	uint32_t cx, cy, cz;    // centre of mass, integer box coordinates
+	float mass;
+	uint32_t gx, gy, gz;    // geometric centre (reference Tree.Pos), integer coords
+	float size;             // node size (box units scaled to length)
+	int32_t child;          // first child (walk index) or first particle
+	int32_t nchild;         // > 0: children; < 0: -(number of particles) of a bundle
+	float size2;            // size^2
+	int32_t level;
+};
+
+struct tvg_context {
+	int device = 0;
+	tvg_config cfg{};
+	cudaStream_t stream = nullptr;
+	int64_t cap = 0;          // particle capacity
+	int64_t n = 0;            // active particle count
+	double origin[3] = { 0, 0, 0 };
+	double dsize = 0;         // Domain.Size
+	bool have_domain = false;
+	bool keys_std = false;    // key holds standard keys
+	bool sorted = false;
+	bool have_top = false;
+	bool have_tree = false;
+	bool have_ewald = false;
+	bool have_walktree = false;
+	char err[512] = { 0 };
+
+	// particle fields (two buffers each for the permutation)
+	void *f[TVG_MAX_TOP] = { nullptr };
+	void *falt[TVG_MAX_TOP] = { nullptr };
+	// key split for the sort
+	uint64_t *key_hi = nullptr, *key_lo = nullptr, *key_tmp = nullptr;
+	uint32_t *perm = nullptr, *perm_tmp = nullptr;
+	uint32_t *sort_hist = nullptr;     // per-tile digit histograms
+	uint32_t *sort_off = nullptr;      // scanned
+	uint32_t *digit_count = nullptr;   // 8 x 256 global digit histogram
+	void *scan_tmp = nullptr;
+	size_t scan_tmp_bytes = 0;
+	int *status = nullptr;             // device status word
+	int *h_status = nullptr;           // pinned mirror
+
+	// top nodes
+	int32_t ntop = 0;
+	tvg_topnode *d_top = nullptr;
+	tvg_topnode h_top[TVG_MAX_TOP];
+	int32_t *top_first = nullptr;      // [64] first particle of level-2 cell c
+	int32_t *top_count = nullptr;      // [64]
+
+	// tree build scratch
+	uint8_t *lvl = nullptr;            // LCA level with the previous particle
+	int32_t *ncnt = nullptr;           // nodes starting at each particle; then scan
+	uint8_t *lvl_min64 = nullptr;      // min of lvl over 64-blocks
+	int64_t ucap = 0;                  // capacity of uncollapsed node arrays
+	int32_t *u_start = nullptr, *u_count = nullptr, *u_endu = nullptr, *u_diff = nullptr;
+	int32_t *u_final = nullptr;
+	uint8_t *u_level = nullptr, *u_flag = nullptr;
+	int64_t nu = 0;                    // uncollapsed node count
+	// final tree
+	int64_t tcap = 0;                  // node capacity
+	int64_t nnodes = 0;
+	void *tree = nullptr;              // reference layout
+	int32_t *tree_u = nullptr;         // final node -> uncollapsed index
+	double *pref = nullptr;            // prefix sums of m, m*x, m*y, m*z (FP64)
+	int32_t h_target[TVG_MAX_TOP];
+	int32_t h_nsurv[TVG_MAX_TOP];
+
+	// Ewald tables (Float, divided by box^2) and raw FP64
+	void *ewald_f[4] = { nullptr, nullptr, nullptr, nullptr };
+	double *ewald_raw = nullptr;
+
+	// group walk data
+	uint32_t *ipos[3] = { nullptr, nullptr, nullptr };
+	tvg_wnode *wtree = nullptr;
+	int64_t nw = 0;
+	int32_t *group_first = nullptr;
+	int64_t ngroups = 0;
+	int32_t *work_counter = nullptr;
+	double *counters = nullptr;        // device interaction counters [4]
+
+	// timings
+	cudaEvent_t ev[16];
+	double phase_ms[8] = { 0 };
+	double last_counts[2] = { 0, 0 };
+};
+
+// field slots in ctx->f[]
+enum {
+	FS_TYPE = 0, FS_TIME_BIN, FS_IT_DRIFT, FS_IT_KICK, FS_ID, FS_COST,
+	FS_POS0, FS_POS1, FS_POS2, FS_VEL0, FS_VEL1, FS_VEL2,
+	FS_ACC0, FS_ACC1, FS_ACC2, FS_MASS, FS_GACC0, FS_GACC1, FS_GACC2,
+	FS_LAST_ACC, FS_TREE_PARENT, FS_NFIELDS
+};
+
+int tvg_fail(tvg_context *ctx, int code, const char *fmt, ...);
+int tvg_sync_status(tvg_context *ctx, const char *phase);
+int tvg_device_scan_i32(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n,
+                        int64_t *total);
+
+// phase implementations (one translation unit each)
+int tvg_impl_keys(tvg_context *ctx, bool reversed);
+int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out);
+int tvg_impl_top_nodes(tvg_context *ctx);
+int tvg_impl_tree_build(tvg_context *ctx, uint32_t flags);
+int tvg_impl_download_tree(tvg_context *ctx, void *tree, int64_t cap, int64_t *nnodes);
+int tvg_impl_ewald_init(tvg_context *ctx);
+int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts);
+int tvg_impl_walk_group(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind);
+int tvg_impl_save_last_accel(tvg_context *ctx);
+int tvg_impl_zero_accel(tvg_context *ctx);
+
+static inline size_t tvg_fsize(const tvg_context *ctx) { return (size_t) ctx->cfg.float_bytes; }
+
+// element size of field slot
+static inline size_t tvg_field_bytes(const tvg_context *ctx, int slot)
+{
+	switch (slot) {
+	case FS_TYPE: case FS_TIME_BIN: case FS_IT_DRIFT: case FS_IT_KICK: case FS_ID:
+	case FS_TREE_PARENT:
+		return 4;
+	default:
+		return tvg_fsize(ctx);
+	}
+}
+
+static inline unsigned tvg_blocks(int64_t n, int threads)
+{
+	int64_t b = (n + threads - 1) / threads;
+	return (unsigned) (b < 1 ? 1 : b);
+}
+
+// ------------------------------------------------------- device helpers
+
+__device__ __forceinline__ int tvg_clz128(uint64_t hi, uint64_t lo)
+{
+	return hi ? __clzll(hi) : 64 + (lo ? __clzll(lo) : 64);
+}
+
+// triplet of the standard key at level l (1..42): bits 130-3l .. 128-3l
+__device__ __forceinline__ int tvg_std_triplet(uint64_t hi, uint64_t lo, int l)
+{
+	int sh = 128 - 3 * l;      // lowest bit of the triplet
+	if (sh >= 64) return (int) ((hi >> (sh - 64)) & 7);
+	if (sh >= 62) return (int) (((hi << (64 - sh)) | (lo >> sh)) & 7);
+	return (int) ((lo >> sh) & 7);
+}

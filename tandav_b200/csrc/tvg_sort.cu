@@ -1,0 +1,281 @@
+// tvg_sort.cu -- PH-order sort of all particle fields.
+//
+// Replaces Qsort_Index on the 128-bit keys (sort.c:90-341, cmp_peanoKeys at
+// peano.c:6-12) and reorder_collisionless_particles (peano.c:50-82).
+//  1. LSD radix sort of (key_hi, index) on the 64-bit high key word: 8-bit
+//     digits, digits that are equal for every key are skipped. Each pass is
+//     reduce-then-scan: per-tile (4096 keys) digit histograms, one device
+//     scan of the digit-major histogram, then a scatter in which every tile
+//     ranks its keys stably with warp __match_any_sync and writes them through
+//     a shared-memory staging sort (coalesced runs per digit).
+//  2. Runs of equal high words are ordered by the low word (insertion sort
+//     per run, one thread per run; runs are rare and short unless positions
+//     coincide).
+//  3. Every particle field is gathered through the permutation in one launch.
+// The resulting order is the ascending 128-bit key order, equal keys in
+// input order (the reference's quicksort leaves equal keys in an
+// unspecified order).
+// Roofline: HBM bound; per pass 8 B read (histogram) + 12 B read + 12 B write
+// per key.
+#include "tvg_internal.cuh"
+
+#define RS_THREADS 256
+#define RS_IPT 16
+#define RS_TILE (RS_THREADS * RS_IPT)
+#define RS_WARPS (RS_THREADS / 32)
+
+__global__ void k_iota(int64_t n, uint32_t *p)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i < n) p[i] = (uint32_t) i;
+}
+
+// global histogram of all 8 digits of key_hi (to skip constant digits)
+__global__ void k_digit_counts(int64_t n, const uint64_t *__restrict__ key, uint32_t *count)
+{
+	__shared__ uint32_t h[8 * 256];
+	for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) h[i] = 0;
+	__syncthreads();
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+	     i += (int64_t) gridDim.x * blockDim.x) {
+		uint64_t k = key[i];
+#pragma unroll
+		for (int d = 0; d < 8; d++) atomicAdd(&h[d * 256 + ((k >> (8 * d)) & 0xFF)], 1u);
+	}
+	__syncthreads();
+	for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x)
+		if (h[i]) atomicAdd(&count[i], h[i]);
+}
+
+// per-tile digit histogram, stored digit-major: hist[d * ntiles + tile]
+__global__ void k_tile_hist(int64_t n, int shift, const uint64_t *__restrict__ key,
+                            uint32_t *__restrict__ hist, int64_t ntiles)
+{
+	__shared__ uint32_t h[256];
+	h[threadIdx.x] = 0;
+	__syncthreads();
+	const int64_t base = (int64_t) blockIdx.x * RS_TILE;
+#pragma unroll 4
+	for (int k = 0; k < RS_IPT; k++) {
+		int64_t i = base + (int64_t) k * RS_THREADS + threadIdx.x;
+		if (i < n) {
+			uint32_t d = (uint32_t) (key[i] >> shift) & 0xFF;
+			unsigned peers = __match_any_sync(__activemask(), d);
+			int leader = __ffs(peers) - 1;
+			if ((int) (threadIdx.x & 31) == leader) atomicAdd(&h[d], (uint32_t) __popc(peers));
+		}
+	}
+	__syncthreads();
+	hist[(int64_t) threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_THREADS)
+k_radix_scatter(int64_t n, int shift, const uint64_t *__restrict__ kin,
+                const uint32_t *__restrict__ vin, uint64_t *__restrict__ kout,
+                uint32_t *__restrict__ vout, const uint32_t *__restrict__ off, int64_t ntiles)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	uint64_t *skey = (uint64_t *) smem;                          // RS_TILE
+	uint32_t *sval = (uint32_t *) (skey + RS_TILE);              // RS_TILE
+	uint32_t *whist = sval + RS_TILE;                            // RS_WARPS * 256
+	uint32_t *dstart = whist + RS_WARPS * 256;                   // 256
+	uint32_t *gstart = dstart + 256;                             // 256
+	uint32_t *running = gstart + 256;                            // 256
+	int32_t *s_warp = (int32_t *) (running + 256);               // 33
+
+	const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+	const int64_t base = (int64_t) blockIdx.x * RS_TILE;
+	const int cnt = (int) min((int64_t) RS_TILE, n - base);
+	for (int i = t; i < RS_WARPS * 256; i += RS_THREADS) whist[i] = 0;
+	running[t] = 0;
+	gstart[t] = off[(int64_t) t * ntiles + blockIdx.x];
+	__syncthreads();
+	// tile digit counts -> tile-local exclusive offsets
+	for (int r = 0; r < RS_IPT; r++) {
+		int idx = r * RS_THREADS + t;
+		if (idx < cnt) {
+			uint32_t d = (uint32_t) (kin[base + idx] >> shift) & 0xFF;
+			unsigned peers = __match_any_sync(__activemask(), d);
+			if (lane == __ffs(peers) - 1) atomicAdd(&running[d], (uint32_t) __popc(peers));
+		}
+	}
+	__syncthreads();
+	{
+		int32_t c = (int32_t) running[t], ex;
+		// 256 threads: reuse the generic block scan pattern
+		int32_t inc = c;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			int32_t u = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+			if (lane >= o) inc += u;
+		}
+		if (lane == 31) s_warp[w] = inc;
+		__syncthreads();
+		if (w == 0) {
+			int32_t v = lane < RS_WARPS ? s_warp[lane] : 0;
+			int32_t vi = v;
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				int32_t u = __shfl_up_sync(0xFFFFFFFFu, vi, o);
+				if (lane >= o) vi += u;
+			}
+			if (lane < RS_WARPS) s_warp[lane] = vi - v;
+		}
+		__syncthreads();
+		ex = inc - c + s_warp[w];
+		dstart[t] = (uint32_t) ex;
+		running[t] = 0;
+	}
+	__syncthreads();
+	const unsigned lt_mask = (1u << lane) - 1u;
+	for (int r = 0; r < RS_IPT; r++) {
+		const int idx = r * RS_THREADS + t;
+		const bool valid = idx < cnt;
+		uint64_t k = 0;
+		uint32_t v = 0, d = 256 + lane;      // invalid lanes match nobody
+		if (valid) {
+			k = kin[base + idx];
+			v = vin[base + idx];
+			d = (uint32_t) (k >> shift) & 0xFF;
+		}
+		unsigned peers = __match_any_sync(0xFFFFFFFFu, d);
+		int rank_w = __popc(peers & lt_mask);
+		if (valid && rank_w == 0) whist[w * 256 + d] = (uint32_t) __popc(peers);
+		__syncthreads();
+		{   // per digit: exclusive prefix over warps, continuing the running count
+			uint32_t run = running[t];
+#pragma unroll
+			for (int ww = 0; ww < RS_WARPS; ww++) {
+				uint32_t c = whist[ww * 256 + t];
+				whist[ww * 256 + t] = run;
+				run += c;
+			}
+			running[t] = run;
+		}
+		__syncthreads();
+		if (valid) {
+			uint32_t pos = dstart[d] + whist[w * 256 + d] + (uint32_t) rank_w;
+			skey[pos] = k;
+			sval[pos] = v;
+		}
+		__syncthreads();
+		for (int ww = 0; ww < RS_WARPS; ww++) whist[ww * 256 + t] = 0;
+		__syncthreads();
+	}
+	for (int p = t; p < cnt; p += RS_THREADS) {
+		uint64_t k = skey[p];
+		uint32_t d = (uint32_t) (k >> shift) & 0xFF;
+		int64_t dest = (int64_t) gstart[d] + (p - (int) dstart[d]);
+		kout[dest] = k;
+		vout[dest] = sval[p];
+	}
+}
+
+// order runs of equal key_hi by the low key word (stable)
+__global__ void k_fix_ties(int64_t n, const uint64_t *__restrict__ hi, const uint64_t *__restrict__ lo_orig,
+                           uint32_t *__restrict__ perm)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n - 1) return;
+	if (hi[i] != hi[i + 1]) return;
+	if (i > 0 && hi[i - 1] == hi[i]) return;      // not the first of the run
+	int64_t e = i + 1;
+	while (e < n && hi[e] == hi[i]) e++;
+	for (int64_t a = i + 1; a < e; a++) {
+		uint32_t pv = perm[a];
+		uint64_t kv = lo_orig[pv];
+		int64_t b = a - 1;
+		while (b >= i && lo_orig[perm[b]] > kv) {
+			perm[b + 1] = perm[b];
+			b--;
+		}
+		perm[b + 1] = pv;
+	}
+}
+
+__global__ void k_gather_u64(int64_t n, const uint32_t *__restrict__ perm, const uint64_t *__restrict__ in,
+                             uint64_t *__restrict__ out)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i < n) out[i] = in[perm[i]];
+}
+
+struct GatherList {
+	const void *in[FS_NFIELDS];
+	void *out[FS_NFIELDS];
+	int bytes[FS_NFIELDS];
+	int nf;
+};
+
+// all particle fields through the permutation in one pass (perm read once)
+__global__ void k_gather_fields(int64_t n, const uint32_t *__restrict__ perm, GatherList g)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint32_t src = perm[i];
+	for (int f = 0; f < g.nf; f++) {
+		if (g.bytes[f] == 8)
+			((uint64_t *) g.out[f])[i] = ((const uint64_t *) g.in[f])[src];
+		else
+			((uint32_t *) g.out[f])[i] = ((const uint32_t *) g.in[f])[src];
+	}
+}
+
+int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
+{
+	const int64_t n = ctx->n;
+	if (n == 0) return TVG_OK;
+	cudaStream_t s = ctx->stream;
+	const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
+	k_iota<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->perm);
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->digit_count, 0, 4 * 8 * 256, s));
+	k_digit_counts<<<296, 512, 0, s>>>(n, ctx->key_hi, ctx->digit_count);
+	TVG_CUDA(ctx, cudaGetLastError());
+	uint32_t h_count[8 * 256];
+	TVG_CUDA(ctx, cudaMemcpyAsync(h_count, ctx->digit_count, sizeof(h_count), cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	static bool attr_set = false;
+	const size_t smem = RS_TILE * 12 + (RS_WARPS * 256 + 3 * 256 + 33) * 4;
+	if (!attr_set) {
+		TVG_CUDA(ctx, cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                                   (int) smem));
+		attr_set = true;
+	}
+	uint64_t *kin = ctx->key_hi, *kout = ctx->key_tmp;
+	uint32_t *vin = ctx->perm, *vout = ctx->perm_tmp;
+	for (int d = 0; d < 8; d++) {
+		bool constant = false;
+		for (int b = 0; b < 256; b++)
+			if (h_count[d * 256 + b] == (uint32_t) n) constant = true;
+		if (constant) continue;
+		const int shift = 8 * d;
+		k_tile_hist<<<(unsigned) ntiles, RS_THREADS, 0, s>>>(n, shift, kin, ctx->sort_hist, ntiles);
+		TVG_CUDA(ctx, cudaGetLastError());
+		TVG_CHECK(tvg_device_scan_i32(ctx, (const int32_t *) ctx->sort_hist, (int32_t *) ctx->sort_off,
+		                              256 * ntiles, nullptr));
+		k_radix_scatter<<<(unsigned) ntiles, RS_THREADS, smem, s>>>(n, shift, kin, vin, kout, vout,
+		                                                            ctx->sort_off, ntiles);
+		TVG_CUDA(ctx, cudaGetLastError());
+		uint64_t *kt = kin; kin = kout; kout = kt;
+		uint32_t *vt = vin; vin = vout; vout = vt;
+	}
+	ctx->key_hi = kin; ctx->key_tmp = kout;
+	ctx->perm = vin; ctx->perm_tmp = vout;
+	k_fix_ties<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->perm);
+	k_gather_u64<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->perm, ctx->key_lo, ctx->key_tmp);
+	{ uint64_t *t = ctx->key_lo; ctx->key_lo = ctx->key_tmp; ctx->key_tmp = t; }
+	GatherList g;
+	g.nf = 0;
+	for (int f = 0; f < FS_NFIELDS; f++) {
+		g.in[g.nf] = ctx->f[f];
+		g.out[g.nf] = ctx->falt[f];
+		g.bytes[g.nf] = (int) tvg_field_bytes(ctx, f);
+		g.nf++;
+	}
+	k_gather_fields<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->perm, g);
+	TVG_CUDA(ctx, cudaGetLastError());
+	for (int f = 0; f < FS_NFIELDS; f++) { void *t = ctx->f[f]; ctx->f[f] = ctx->falt[f]; ctx->falt[f] = t; }
+	if (perm_out)
+		TVG_CUDA(ctx, cudaMemcpyAsync(perm_out, ctx->perm, 4 * n, cudaMemcpyDeviceToHost, s));
+	return TVG_OK;
+}

@@ -1,0 +1,641 @@
+// tvg_tree.cu -- top nodes and the octree, built in parallel from PH-sorted
+// keys, bit-exact with Gravity_Tree_Build (src/Gravity/tree_build.c:47-572).
+//
+// The reference inserts particles one by one (build_subtree) and collapses
+// finished branches into bundles of <= VECTOR_SIZE particles
+// (collapse_last_branch). Its result has a closed form, which this file
+// evaluates with one thread per particle / node:
+//
+//   l_i   = level of the deepest common cell of sorted particles i-1 and i
+//           (leading equal key triplets), l = L-1 at a top node's first
+//           particle (L = top level 2).
+//   nodes = the top cell, and every cell whose parent cell holds >= 2
+//           particles. The cells that start at particle i are levels
+//           l_i+1 .. max(l_i, l_{i+1})+1; pre-order = (first particle, level).
+//   event = particle e with l_e < l_{e-1}: the reference sees it as a new
+//           branch. At e the cell A (level l_e+1, holding e-1) becomes a
+//           bundle if it has <= VECTOR_SIZE particles, else the cell B (level
+//           l_{e-1}, holding e-1) if B has <= VECTOR_SIZE particles.
+//           Nothing else collapses (the last branch of a top node stays).
+//   a node survives unless a strict ancestor became a bundle; DNext of an
+//           internal node is the distance to the next surviving node after
+//           its subtree (or to the terminator), of a bundle/leaf -(first)-1.
+// Particles equal to 41 levels ("dumped" by the reference,
+// tree_build.c:337-342) are reported as TVG_E_COINCIDENT.
+//
+// Node centres (Pos) repeat the reference's float arithmetic down the chain
+// of ancestors (tree_build.c:542-550). Mass/CoM: bundles, leaves and, in
+// exact mode, every node are summed sequentially in particle order in Float
+// (tree_build.c:561-572), which reproduces the reference bit for bit; the fast
+// mode sums internal nodes in FP64 with one warp per node.
+// Roofline: HBM/L2 bound (1 B level + 16 B key per particle, ~O(nodes)).
+#include "tvg_internal.cuh"
+
+#define TOP_LEVEL 2
+#define LVL_START 1         // l at a top node's first particle (L - 1)
+#define LVL_SMALL 0xFF      // particle of a top node without subtree
+
+template <typename F> struct TNode {
+	int32_t DNext;
+	uint32_t Bitfield;
+	int32_t DUp;
+	int32_t Npart;
+	F Pos[3];
+	F Mass;
+	F CoM[3];
+	F Dp[3];
+};
+
+// ------------------------------------------------------------ top nodes
+
+__global__ void k_top_first(int64_t n, const uint64_t *__restrict__ key_hi, int32_t *first)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	int c = (int) (key_hi[i] >> 58);
+	if (i == 0 || (int) (key_hi[i - 1] >> 58) != c) first[c] = (int32_t) i;
+}
+
+// one thread: top nodes in descending key order (compare_bunches_by_key,
+// domain.c:678-684), centre from the first particle (domain.c:237-246)
+template <typename F>
+__global__ void k_make_top(int64_t n, const int32_t *first, const F *x, const F *y, const F *z,
+                           double ox, double oy, double oz, double size, tvg_topnode *top,
+                           int32_t *count, int32_t *ntop_out)
+{
+	if (threadIdx.x || blockIdx.x) return;
+	int nt = 0;
+	for (int c = 63; c >= 0; c--) {
+		if (first[c] < 0) { count[c] = 0; continue; }
+		int64_t e = n;
+		for (int d = c + 1; d < 64; d++)
+			if (first[d] >= 0) { e = first[d]; break; }
+		count[c] = (int32_t) (e - first[c]);
+		tvg_topnode t;
+		t.key = ((uint64_t) c << 58) | (0xFFFFFFFFFFFFFFFFULL >> 6);
+		t.target = -1;
+		t.level = TOP_LEVEL;
+		t.first_part = first[c];
+		t.npart = (int32_t) (e - first[c]);
+		int64_t ip = first[c];
+		const double sz = size / (double) (1ULL << TOP_LEVEL);
+		const double px = (double) x[ip] - ox, py = (double) y[ip] - oy, pz = (double) z[ip] - oz;
+		t.pos[0] = (float) __dadd_rn(__dmul_rn(floor(px / sz) + 0.5, sz), ox);
+		t.pos[1] = (float) __dadd_rn(__dmul_rn(floor(py / sz) + 0.5, sz), oy);
+		t.pos[2] = (float) __dadd_rn(__dmul_rn(floor(pz / sz) + 0.5, sz), oz);
+		t.mass = 0;
+		for (int k = 0; k < 3; k++) { t.com[k] = 0; t.dp[k] = 0; }
+		top[nt++] = t;
+	}
+	*ntop_out = nt;
+}
+
+int tvg_impl_top_nodes(tvg_context *ctx)
+{
+	const int64_t n = ctx->n;
+	cudaStream_t s = ctx->stream;
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->top_first, 0xFF, 4 * TVG_MAX_TOP, s));
+	k_top_first<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ctx->top_first);
+	int32_t *d_nt = (int32_t *) ctx->work_counter;
+	if (ctx->cfg.float_bytes == 4)
+		k_make_top<float><<<1, 1, 0, s>>>(n, ctx->top_first, (const float *) ctx->f[FS_POS0],
+		                                  (const float *) ctx->f[FS_POS1], (const float *) ctx->f[FS_POS2],
+		                                  ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
+		                                  ctx->d_top, ctx->top_count, d_nt);
+	else
+		k_make_top<double><<<1, 1, 0, s>>>(n, ctx->top_first, (const double *) ctx->f[FS_POS0],
+		                                   (const double *) ctx->f[FS_POS1], (const double *) ctx->f[FS_POS2],
+		                                   ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
+		                                   ctx->d_top, ctx->top_count, d_nt);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->ntop, d_nt, 4, cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
+	                              cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	return TVG_OK;
+}
+
+// ----------------------------------------------------- build: levels
+
+struct TopInfo {            // per level-2 cell c (0..63)
+	int32_t first[64];      // first particle, -1 if empty
+	int32_t count[64];
+	int32_t tidx[64];       // index in the top node list (D order)
+	int32_t big[64];        // count > VECTOR_SIZE: has a subtree
+};
+
+__device__ __forceinline__ int lca_level(const uint64_t *hi, const uint64_t *lo, int64_t a, int64_t b)
+{
+	int l = tvg_clz128(hi[a] ^ hi[b], lo[a] ^ lo[b]) / 3;
+	return l > TVG_MAX_LEVEL ? TVG_MAX_LEVEL : l;
+}
+
+__global__ void k_levels(int64_t n, const uint64_t *__restrict__ hi, const uint64_t *__restrict__ lo,
+                         TopInfo ti, uint8_t *__restrict__ lvl, int32_t *__restrict__ ncnt,
+                         uint8_t *__restrict__ lvl_min64, int *status)
+{
+	__shared__ uint8_t s_min[256 / 32];
+	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	unsigned my = 0xFF;
+	if (i < n) {
+		const int c = (int) (hi[i] >> 58);
+		const int64_t f = ti.first[c], e = f + ti.count[c];
+		int l, cnt = 0;
+		if (i == f) {
+			l = LVL_START;
+		} else if (!ti.big[c]) {
+			l = LVL_SMALL;
+		} else {
+			l = lca_level(hi, lo, i - 1, i);
+			if (l >= TVG_MAX_LEVEL - 1) atomicOr(status, TVG_ST_COINCIDENT);
+		}
+		if (ti.big[c]) {
+			int lnext = (i + 1 < e) ? lca_level(hi, lo, i, i + 1) : -1;
+			int lo_l = l + 1;
+			int hi_l = (l > lnext ? l : lnext) + 1;
+			cnt = hi_l - lo_l + 1;
+		}
+		lvl[i] = (uint8_t) l;
+		ncnt[i] = cnt;
+		my = (unsigned) l;
+	}
+	// min over each 64-particle block (two warps)
+	unsigned wmin = __reduce_min_sync(0xFFFFFFFFu, my);
+	const int w = threadIdx.x >> 5;
+	if ((threadIdx.x & 31) == 0) s_min[w] = (uint8_t) wmin;
+	__syncthreads();
+	if (threadIdx.x < blockDim.x / 64) {
+		int64_t b = (blockIdx.x * (int64_t) blockDim.x) / 64 + threadIdx.x;
+		if (b * 64 < n) {
+			uint8_t a = s_min[2 * threadIdx.x], bb = s_min[2 * threadIdx.x + 1];
+			lvl_min64[b] = a < bb ? a : bb;
+		}
+	}
+	if (i == n - 1) ncnt[n] = 0;
+}
+
+// first j > s with lvl[j] < l, or n
+__device__ int64_t next_smaller(const uint8_t *__restrict__ lvl, const uint8_t *__restrict__ m64,
+                                int64_t n, int64_t s, int l)
+{
+	int64_t j = s + 1;
+	while (j < n && (j & 63)) {
+		if (lvl[j] < l) return j;
+		j++;
+	}
+	if (j >= n) return n;
+	int64_t b = j >> 6;
+	const int64_t nb = (n + 63) >> 6;
+	while (b < nb && m64[b] >= l) b++;
+	if (b >= nb) return n;
+	j = b << 6;
+	while (j < n && lvl[j] >= l) j++;
+	return j;
+}
+
+// last j < s with lvl[j] < l (exists: a top node's first particle has lvl 1)
+__device__ int64_t prev_smaller(const uint8_t *__restrict__ lvl, const uint8_t *__restrict__ m64,
+                                int64_t s, int l)
+{
+	int64_t j = s - 1;
+	while (j >= 0 && ((j + 1) & 63)) {
+		if (lvl[j] < l) return j;
+		j--;
+	}
+	if (j < 0) return -1;
+	int64_t b = j >> 6;
+	while (b >= 0 && m64[b] >= l) b--;
+	if (b < 0) return -1;
+	j = (b << 6) + 63;
+	while (lvl[j] >= l) j--;
+	return j;
+}
+
+enum { UF_COLLAPSED = 1, UF_LEAF = 2, UF_ROOT = 4 };
+
+// every uncollapsed node: range, collapse decision, removal marks
+__global__ void k_nodes(int64_t n, const uint8_t *__restrict__ lvl, const uint8_t *__restrict__ m64,
+                        const int32_t *__restrict__ base, int vsize, int32_t *__restrict__ u_start,
+                        uint8_t *__restrict__ u_level, int32_t *__restrict__ u_count,
+                        int32_t *__restrict__ u_endu, uint8_t *__restrict__ u_flag,
+                        int32_t *__restrict__ u_diff)
+{
+	const int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (s >= n) return;
+	const int32_t b0 = base[s], nc = base[s + 1] - b0;
+	if (nc == 0) return;
+	const int ls = lvl[s];
+	const int lo_l = ls + 1;
+	for (int k = 0; k < nc; k++) {
+		const int l = lo_l + k;
+		const int64_t u = b0 + k;
+		const int64_t e = next_smaller(lvl, m64, n, s, l);
+		const int32_t cnt = (int32_t) (e - s);
+		uint8_t flag = 0;
+		if (l == TOP_LEVEL) flag |= UF_ROOT;
+		if (cnt == 1) flag |= UF_LEAF;
+		if (cnt <= vsize && e < n && cnt > 1) {
+			const int le = lvl[e], lp = lvl[e - 1];
+			// e is an event: not a top node start and l_e < l_{e-1}
+			if (le != LVL_START && le < lp) {
+				if (l == le + 1) {
+					flag |= UF_COLLAPSED;
+				} else if (l == lp) {
+					// cell A (level l_e+1 holding e-1) must hold > vsize particles
+					int64_t a0 = e - vsize;
+					if (a0 < 0) a0 = 0;
+					bool a_small = false;
+					for (int64_t j = a0; j < e; j++)
+						if (lvl[j] <= le) { a_small = true; break; }
+					if (!a_small) flag |= UF_COLLAPSED;
+				}
+			}
+		}
+		const int32_t endu = base[e];
+		u_start[u] = (int32_t) s;
+		u_level[u] = (uint8_t) l;
+		u_count[u] = cnt;
+		u_endu[u] = endu;
+		u_flag[u] = flag;
+		if (flag & UF_COLLAPSED) {
+			atomicAdd(&u_diff[u + 1], 1);
+			atomicAdd(&u_diff[endu], -1);
+		}
+	}
+}
+
+// survivor flag from the scanned removal marks: surv[u] = (marks(u) == 0)
+__global__ void k_survivors(int64_t nu, const int32_t *__restrict__ excl, int32_t *__restrict__ surv)
+{
+	int64_t u = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (u > nu) return;
+	surv[u] = (u < nu && excl[u + 1] == 0) ? 1 : 0;
+}
+
+// one thread: subtree placement in top-node order (tree_build.c:59-96)
+__global__ void k_place_subtrees(int ntop, tvg_topnode *top, const int32_t *__restrict__ base,
+                                 const int32_t *__restrict__ F, int vsize, int32_t *toff,
+                                 int32_t *nsurv, int64_t *total)
+{
+	if (threadIdx.x || blockIdx.x) return;
+	int64_t run = 0;
+	for (int t = 0; t < ntop; t++) {
+		top[t].target = (int32_t) run;       // also for small top nodes (quirk Q3)
+		if (top[t].npart > vsize) {
+			int64_t f = top[t].first_part, e = f + top[t].npart;
+			int32_t fs = F[base[f]], fe = F[base[e]];
+			nsurv[t] = fe - fs;
+			toff[t] = (int32_t) (run - fs);
+			run += (fe - fs) + 1;             // + terminator
+		} else {
+			nsurv[t] = 0;
+			toff[t] = 0;
+		}
+	}
+	*total = run;
+}
+
+struct TopPlace {
+	int32_t tidx[64];       // by level-2 cell
+	int32_t toff[64];       // by top index: G = toff + F[u]
+	int32_t target[64];
+	int32_t nsurv[64];
+	int32_t end[64];        // by top index: first particle after the node
+};
+
+__device__ __forceinline__ int32_t triplet_at(const uint64_t *hi, const uint64_t *lo, int64_t i, int l)
+{
+	return tvg_std_triplet(hi[i], lo[i], l);
+}
+
+template <typename F>
+__global__ void k_emit_nodes(int64_t nu, int64_t n, const uint8_t *__restrict__ lvl,
+                             const uint8_t *__restrict__ m64, const int32_t *__restrict__ base,
+                             const int32_t *__restrict__ u_start, const uint8_t *__restrict__ u_level,
+                             const int32_t *__restrict__ u_count, const int32_t *__restrict__ u_endu,
+                             const uint8_t *__restrict__ u_flag, const int32_t *__restrict__ surv,
+                             const int32_t *__restrict__ Fidx, const uint64_t *__restrict__ hi,
+                             const uint64_t *__restrict__ lo, TopPlace tp, TNode<F> *tree,
+                             int32_t *__restrict__ tree_u, int32_t *__restrict__ tree_parent,
+                             int64_t tcap, int *status)
+{
+	const int64_t u = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (u >= nu || !surv[u]) return;
+	const int32_t s = u_start[u];
+	const int l = u_level[u];
+	const int32_t cnt = u_count[u];
+	const uint8_t flag = u_flag[u];
+	const int c = (int) (hi[s] >> 58);
+	const int t = tp.tidx[c];
+	const int64_t G = (int64_t) tp.toff[t] + Fidx[u];
+	if (G < 0 || G >= tcap) { atomicOr(status, TVG_ST_TREE_FULL); return; }
+	TNode<F> nd;
+	nd.Npart = cnt;
+	nd.Bitfield = (uint32_t) l | ((uint32_t) triplet_at(hi, lo, s, l) << 6) | (1u << 9)
+	            | ((flag & UF_ROOT) ? (1u << 10) : 0u);
+	if (flag & (UF_COLLAPSED | UF_LEAF)) {
+		nd.DNext = -s - 1;
+	} else {
+		const bool at_end = (int64_t) s + cnt >= tp.end[t];
+		const int64_t nxt = at_end ? (int64_t) tp.target[t] + tp.nsurv[t]
+		                           : (int64_t) tp.toff[t] + Fidx[u_endu[u]];
+		nd.DNext = (int32_t) (nxt - G);
+	}
+	if (flag & UF_ROOT) {
+		nd.DUp = t;
+	} else {
+		int64_t pu;
+		if (u > base[s]) {
+			pu = u - 1;
+		} else {
+			const int ls = lvl[s];
+			const int64_t p = prev_smaller(lvl, m64, s, ls);
+			pu = base[p] + (ls - (lvl[p] + 1));
+		}
+		nd.DUp = (int32_t) (G - ((int64_t) tp.toff[t] + Fidx[pu]));
+	}
+	for (int k = 0; k < 3; k++) { nd.Pos[k] = 0; nd.CoM[k] = 0; nd.Dp[k] = 0; }
+	nd.Mass = 0;
+	tree[G] = nd;
+	tree_u[G] = (int32_t) u;
+	if (flag & (UF_COLLAPSED | UF_LEAF))
+		for (int32_t j = s; j < s + cnt; j++) tree_parent[j] = (int32_t) G;
+}
+
+// particles of top nodes without subtree point to their top node (-t-1),
+// set_tree_parent_pointers, tree_build.c:226-242
+__global__ void k_small_parent(int64_t n, const uint64_t *__restrict__ hi, TopInfo ti,
+                               int32_t *__restrict__ tree_parent)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	int c = (int) (hi[i] >> 58);
+	if (!ti.big[c]) tree_parent[i] = -ti.tidx[c] - 1;
+}
+
+// reference arithmetic for a child centre (tree_build.c:542-550)
+template <typename F>
+__device__ __forceinline__ F child_pos(F ppos, F ppart, double dsize, int l)
+{
+	const int sign = -1 + 2 * (ppart > ppos);
+	const int32_t div = (int32_t) (1u << (l & 31));
+	const F size = (F) (dsize / (double) div);
+	const F ss = (F) sign * size;
+	return (F) __dadd_rn((double) ppos, __dmul_rn((double) ss, 0.5));
+}
+
+template <typename F>
+__global__ void k_node_pos(int64_t nnodes, TNode<F> *tree, const int32_t *__restrict__ tree_u,
+                           const int32_t *__restrict__ u_start, const F *__restrict__ x,
+                           const F *__restrict__ y, const F *__restrict__ z,
+                           const tvg_topnode *__restrict__ top, double dsize)
+{
+	const int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (G >= nnodes) return;
+	const uint32_t bf = tree[G].Bitfield;
+	if (!(bf & (1u << 9))) return;              // terminator
+	int64_t chain[TVG_MAX_LEVEL + 1];
+	int depth = 0;
+	int64_t g = G;
+	while (!(tree[g].Bitfield & (1u << 10))) {  // up to the root (TOP bit)
+		chain[depth++] = g;
+		g = g - tree[g].DUp;
+		if (depth > TVG_MAX_LEVEL) return;
+	}
+	const int t = tree[g].DUp;
+	F p[3] = { (F) top[t].pos[0], (F) top[t].pos[1], (F) top[t].pos[2] };
+	for (int d = depth - 1; d >= 0; d--) {
+		const int64_t gg = chain[d];
+		const int l = (int) (tree[gg].Bitfield & 0x3F);
+		const int32_t s = u_start[tree_u[gg]];
+		p[0] = child_pos<F>(p[0], x[s], dsize, l);
+		p[1] = child_pos<F>(p[1], y[s], dsize, l);
+		p[2] = child_pos<F>(p[2], z[s], dsize, l);
+	}
+	tree[G].Pos[0] = p[0];
+	tree[G].Pos[1] = p[1];
+	tree[G].Pos[2] = p[2];
+}
+
+// Float sums in particle order (add_particle_to_node), then CoM /= Mass
+template <typename F>
+__device__ __forceinline__ void seq_moments(int64_t s, int64_t cnt, const F *__restrict__ x,
+                                            const F *__restrict__ y, const F *__restrict__ z,
+                                            const F *__restrict__ m, F out[4])
+{
+	F cx = 0, cy = 0, cz = 0, mm = 0;
+	for (int64_t j = s; j < s + cnt; j++) {
+		const F mj = m[j];
+		if (sizeof(F) == 4) {
+			cx = __fadd_rn(cx, __fmul_rn(x[j], mj));
+			cy = __fadd_rn(cy, __fmul_rn(y[j], mj));
+			cz = __fadd_rn(cz, __fmul_rn(z[j], mj));
+			mm = __fadd_rn(mm, mj);
+		} else {
+			cx = __dadd_rn(cx, __dmul_rn(x[j], mj));
+			cy = __dadd_rn(cy, __dmul_rn(y[j], mj));
+			cz = __dadd_rn(cz, __dmul_rn(z[j], mj));
+			mm = __dadd_rn(mm, mj);
+		}
+	}
+	out[0] = mm;
+	out[1] = cx / mm;
+	out[2] = cy / mm;
+	out[3] = cz / mm;
+}
+
+template <typename F>
+__global__ void k_moments_seq(int64_t nnodes, TNode<F> *tree, const int32_t *__restrict__ tree_u,
+                              const int32_t *__restrict__ u_start, const F *__restrict__ x,
+                              const F *__restrict__ y, const F *__restrict__ z,
+                              const F *__restrict__ m, int exact)
+{
+	const int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (G >= nnodes) return;
+	const TNode<F> &nd = tree[G];
+	if (!(nd.Bitfield & (1u << 9))) return;
+	if (!exact && nd.DNext > 0) return;         // internal node: fast path
+	F o[4];
+	seq_moments<F>(u_start[tree_u[G]], nd.Npart, x, y, z, m, o);
+	tree[G].Mass = o[0];
+	tree[G].CoM[0] = o[1];
+	tree[G].CoM[1] = o[2];
+	tree[G].CoM[2] = o[3];
+}
+
+// fast mode: one warp per internal node, FP64 sums relative to the node centre
+template <typename F>
+__global__ void k_moments_warp(int64_t nnodes, TNode<F> *tree, const int32_t *__restrict__ tree_u,
+                               const int32_t *__restrict__ u_start, const F *__restrict__ x,
+                               const F *__restrict__ y, const F *__restrict__ z,
+                               const F *__restrict__ m)
+{
+	const int64_t G = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if (G >= nnodes) return;
+	const TNode<F> &nd = tree[G];
+	if (!(nd.Bitfield & (1u << 9)) || nd.DNext <= 0) return;
+	const int64_t s = u_start[tree_u[G]], cnt = nd.Npart;
+	const double c0 = (double) nd.Pos[0], c1 = (double) nd.Pos[1], c2 = (double) nd.Pos[2];
+	double a0 = 0, a1 = 0, a2 = 0, am = 0;
+	for (int64_t j = s + lane; j < s + cnt; j += 32) {
+		const double mj = (double) m[j];
+		am += mj;
+		a0 += mj * ((double) x[j] - c0);
+		a1 += mj * ((double) y[j] - c1);
+		a2 += mj * ((double) z[j] - c2);
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+		am += __shfl_xor_sync(0xFFFFFFFFu, am, o);
+		a0 += __shfl_xor_sync(0xFFFFFFFFu, a0, o);
+		a1 += __shfl_xor_sync(0xFFFFFFFFu, a1, o);
+		a2 += __shfl_xor_sync(0xFFFFFFFFu, a2, o);
+	}
+	if (lane == 0) {
+		tree[G].Mass = (F) am;
+		tree[G].CoM[0] = (F) (c0 + a0 / am);
+		tree[G].CoM[1] = (F) (c1 + a1 / am);
+		tree[G].CoM[2] = (F) (c2 + a2 / am);
+	}
+}
+
+// top node Mass/CoM (finalise_subtree copies the subtree root, as float),
+// terminators (tree_build.c:468-474); small top nodes sum their particles
+template <typename F>
+__global__ void k_finish_top(int ntop, tvg_topnode *top, TNode<F> *tree, const int32_t *nsurv,
+                             const F *__restrict__ x, const F *__restrict__ y,
+                             const F *__restrict__ z, const F *__restrict__ m, int vsize)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= ntop) return;
+	F o[4];
+	if (top[t].npart > vsize) {
+		const TNode<F> &r = tree[top[t].target];
+		o[0] = r.Mass; o[1] = r.CoM[0]; o[2] = r.CoM[1]; o[3] = r.CoM[2];
+		TNode<F> term;
+		term.DNext = 0; term.Bitfield = 1u << 10; term.DUp = 0; term.Npart = 0;
+		for (int k = 0; k < 3; k++) { term.Pos[k] = 0; term.CoM[k] = 0; term.Dp[k] = 0; }
+		term.Mass = 1;
+		tree[(int64_t) top[t].target + nsurv[t]] = term;
+	} else {
+		seq_moments<F>(top[t].first_part, top[t].npart, x, y, z, m, o);
+	}
+	top[t].mass = (float) o[0];
+	top[t].com[0] = (float) o[1];
+	top[t].com[1] = (float) o[2];
+	top[t].com[2] = (float) o[3];
+}
+
+template <typename F>
+static int build_typed(tvg_context *ctx, uint32_t flags)
+{
+	const int64_t n = ctx->n;
+	cudaStream_t s = ctx->stream;
+	const int vsize = ctx->cfg.vector_size;
+	const F *x = (const F *) ctx->f[FS_POS0], *y = (const F *) ctx->f[FS_POS1],
+	        *z = (const F *) ctx->f[FS_POS2], *m = (const F *) ctx->f[FS_MASS];
+	int32_t *tree_parent = (int32_t *) ctx->f[FS_TREE_PARENT];
+
+	TopInfo ti;
+	for (int c = 0; c < 64; c++) { ti.first[c] = -1; ti.count[c] = 0; ti.tidx[c] = -1; ti.big[c] = 0; }
+	for (int t = 0; t < ctx->ntop; t++) {
+		int c = (int) (ctx->h_top[t].key >> 58);
+		ti.first[c] = ctx->h_top[t].first_part;
+		ti.count[c] = ctx->h_top[t].npart;
+		ti.tidx[c] = t;
+		ti.big[c] = ctx->h_top[t].npart > vsize;
+	}
+	k_levels<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ti, ctx->lvl, ctx->ncnt,
+	                                             ctx->lvl_min64, ctx->status);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CHECK(tvg_sync_status(ctx, "tree_build(levels)"));
+	int64_t nu = 0;
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->ncnt, ctx->ncnt, n + 1, &nu));
+	if (nu + 1 > ctx->ucap)
+		return tvg_fail(ctx, TVG_E_TREE_FULL, "tree_build: %lld uncollapsed nodes > capacity %lld",
+		                (long long) nu, (long long) ctx->ucap);
+	ctx->nu = nu;
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->u_diff, 0, 4 * (nu + 1), s));
+	k_nodes<<<tvg_blocks(n, 128), 128, 0, s>>>(n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, vsize,
+	                                            ctx->u_start, ctx->u_level, ctx->u_count, ctx->u_endu,
+	                                            ctx->u_flag, ctx->u_diff);
+	TVG_CUDA(ctx, cudaGetLastError());
+	// removal marks -> survivor flags -> final (per top node) indices
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, nu + 1, nullptr));
+	k_survivors<<<tvg_blocks(nu + 1, 256), 256, 0, s>>>(nu, ctx->u_final, ctx->u_diff);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, nu + 1, nullptr));
+	// placement of the subtrees
+	int32_t *d_toff = (int32_t *) ctx->scan_tmp;     // scan scratch is free here
+	int32_t *d_nsurv = d_toff + 64;
+	int64_t *d_total = (int64_t *) (d_toff + 128);
+	k_place_subtrees<<<1, 1, 0, s>>>(ctx->ntop, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, d_toff,
+	                                  d_nsurv, d_total);
+	TVG_CUDA(ctx, cudaGetLastError());
+	int32_t h_toff[64], h_nsurv[64];
+	int64_t total = 0;
+	TVG_CUDA(ctx, cudaMemcpyAsync(h_toff, d_toff, 4 * 64, cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaMemcpyAsync(h_nsurv, d_nsurv, 4 * 64, cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
+	                              cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	if (total > ctx->tcap)
+		return tvg_fail(ctx, TVG_E_TREE_FULL, "tree_build: %lld nodes > capacity %lld",
+		                (long long) total, (long long) ctx->tcap);
+	ctx->nnodes = total;
+	TopPlace tp;
+	for (int c = 0; c < 64; c++) tp.tidx[c] = ti.tidx[c];
+	for (int t = 0; t < 64; t++) {
+		bool ok = t < ctx->ntop;
+		tp.toff[t] = ok ? h_toff[t] : 0;
+		tp.target[t] = ok ? ctx->h_top[t].target : 0;
+		tp.nsurv[t] = ok ? h_nsurv[t] : 0;
+		tp.end[t] = ok ? ctx->h_top[t].first_part + ctx->h_top[t].npart : 0;
+		ctx->h_target[t] = tp.target[t];
+		ctx->h_nsurv[t] = tp.nsurv[t];
+	}
+	TNode<F> *tree = (TNode<F> *) ctx->tree;
+	k_emit_nodes<F><<<tvg_blocks(nu, 256), 256, 0, s>>>(
+	    nu, n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, ctx->u_start, ctx->u_level, ctx->u_count,
+	    ctx->u_endu, ctx->u_flag, ctx->u_diff, ctx->u_final, ctx->key_hi, ctx->key_lo, tp, tree,
+	    ctx->tree_u, tree_parent, ctx->tcap, ctx->status);
+	TVG_CUDA(ctx, cudaGetLastError());
+	k_small_parent<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ti, tree_parent);
+	TVG_CUDA(ctx, cudaGetLastError());
+	if (total > 0) {
+		k_node_pos<F><<<tvg_blocks(total, 128), 128, 0, s>>>(total, tree, ctx->tree_u, ctx->u_start,
+		                                                       x, y, z, ctx->d_top, ctx->dsize);
+		const int exact = (flags & TVG_BUILD_EXACT_MOMENTS) ? 1 : 0;
+		k_moments_seq<F><<<tvg_blocks(total, 128), 128, 0, s>>>(total, tree, ctx->tree_u,
+		                                                          ctx->u_start, x, y, z, m, exact);
+		if (!exact)
+			k_moments_warp<F><<<tvg_blocks(total * 32, 256), 256, 0, s>>>(total, tree, ctx->tree_u,
+			                                                               ctx->u_start, x, y, z, m);
+		TVG_CUDA(ctx, cudaGetLastError());
+	}
+	k_finish_top<F><<<1, 64, 0, s>>>(ctx->ntop, ctx->d_top, tree, d_nsurv, x, y, z, m, vsize);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
+	                              cudaMemcpyDeviceToHost, s));
+	return tvg_sync_status(ctx, "tree_build");
+}
+
+int tvg_impl_tree_build(tvg_context *ctx, uint32_t flags)
+{
+	if (ctx->cfg.float_bytes == 4) return build_typed<float>(ctx, flags);
+	return build_typed<double>(ctx, flags);
+}
+
+int tvg_impl_download_tree(tvg_context *ctx, void *tree, int64_t cap, int64_t *nnodes)
+{
+	if (cap < ctx->nnodes)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "download_tree: capacity %lld < %lld nodes",
+		                (long long) cap, (long long) ctx->nnodes);
+	const size_t nb = 16 + 10 * tvg_fsize(ctx);
+	TVG_CUDA(ctx, cudaMemcpy(tree, ctx->tree, nb * ctx->nnodes, cudaMemcpyDeviceToHost));
+	if (nnodes) *nnodes = ctx->nnodes;
+	return TVG_OK;
+}

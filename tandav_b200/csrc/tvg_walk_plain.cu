@@ -1,0 +1,423 @@
+// tvg_walk_plain.cu -- the plain GPU form: the reference tree walk, one
+// thread per active particle, in the host's Float width.
+//
+// Gravity part: Gravity_Tree_Acceleration (tree_accel.c:32-394) -- every top
+// node (interact_with_topnode), then the subtree walk with the BH or the
+// relative criterion over the DNext skip pointers; softened monopole
+// interact() with the Dehnen K1 kernel at h = -41/32 eps (tree_build.c:136,
+// kept as in the reference: the sign flip of quirk Q1).
+// Ewald part: Gravity_Tree_Periodic (tree_periodic.c:23-450) with the
+// trilinear table lookup of Ewald_Correction (Gravity/periodic.c:35-113).
+// This file is compiled with -fmad=false: every expression rounds in the
+// reference's order (float/double promotion as in C), so given the same tree
+// the accelerations are the reference's bit for bit.
+// Roofline: FP64/FP32 issue bound with divergent per-thread walks; it is the
+// baseline the group form is measured against.
+#include "tvg_internal.cuh"
+
+template <typename F> struct WNode {
+	int32_t DNext;
+	uint32_t Bitfield;
+	int32_t DUp;
+	int32_t Npart;
+	F Pos[3];
+	F Mass;
+	F CoM[3];
+	F Dp[3];
+};
+
+struct PlainParams {
+	double gravity, domain_size, boxsize, open_bh, open_rel;
+	double eps2, eps3, box2grid;
+	int periodic, use_bh, vsize, ntop, fix_small;
+};
+
+template <typename F> struct PlainCtx {
+	const F *x, *y, *z, *m;
+	const tvg_topnode *top;
+	const WNode<F> *tree;
+	const F *fx, *fy, *fz;
+	F boxhalf;
+	PlainParams p;
+};
+
+template <typename F>
+__device__ __forceinline__ void nearest(const PlainCtx<F> &c, F dr[3])
+{
+	if (!c.p.periodic) return;
+#pragma unroll
+	for (int k = 0; k < 3; k++) {
+		if (dr[k] > c.boxhalf) dr[k] = (F) (dr[k] - c.p.boxsize);
+		else if (dr[k] < -c.boxhalf) dr[k] = (F) (dr[k] + c.p.boxsize);
+	}
+}
+
+template <typename F> __device__ __forceinline__ F fsqrt(F v);
+template <> __device__ __forceinline__ float fsqrt<float>(float v) { return __fsqrt_rn(v); }
+template <> __device__ __forceinline__ double fsqrt<double>(double v) { return __dsqrt_rn(v); }
+
+// interact(), tree_accel.c:362-394
+template <typename F>
+__device__ __forceinline__ void interact(const PlainCtx<F> &c, F mass, const F dr[3], F r2,
+                                         double acc[3], F &cost)
+{
+	F fac = (F) (c.p.gravity * mass);
+	if (r2 < c.p.eps2) {
+		F u2 = (F) (r2 / c.p.eps2);
+		F poly = (F) 175 - u2 * ((F) 294 - u2 * (F) 135);
+		fac = (F) (fac * (poly / (16 * c.p.eps3)));
+	} else {
+		F r_inv = (F) 1 / fsqrt<F>(r2);
+		fac *= r_inv * r_inv * r_inv;
+	}
+	acc[0] += fac * dr[0];
+	acc[1] += fac * dr[1];
+	acc[2] += fac * dr[2];
+	cost += 1;
+}
+
+template <typename F>
+__device__ __forceinline__ F node_size(const PlainCtx<F> &c, int lvl)
+{
+	return (F) (c.p.domain_size / (double) (F) (1ULL << lvl));
+}
+
+template <typename F>
+__device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double acc[3], F &cost)
+{
+	const F fac = (F) (sacc / c.p.gravity * c.p.open_rel);
+	for (int j = 0; j < c.p.ntop; j++) {
+		const tvg_topnode &t = c.top[j];
+		const F nsize = (F) (c.p.domain_size / (double) (F) (1UL << t.level));
+		F dr[3] = { (F) t.pos[0] - sp[0], (F) t.pos[1] - sp[1], (F) t.pos[2] - sp[2] };
+		const bool inside = fabs((double) dr[0]) < 0.6 * nsize && fabs((double) dr[1]) < 0.6 * nsize
+		                 && fabs((double) dr[2]) < 0.6 * nsize;
+		if (!inside) {
+			dr[0] = (F) t.com[0] - sp[0];
+			dr[1] = (F) t.com[1] - sp[1];
+			dr[2] = (F) t.com[2] - sp[2];
+			nearest(c, dr);
+			F r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+			F nmass = (F) t.mass;
+			bool open;
+			if (c.p.use_bh) open = (double) (nsize * nsize) > r2 * c.p.open_bh;
+			else open = nmass * nsize * nsize > r2 * r2 * fac;
+			if (!open) { interact(c, nmass, dr, r2, acc, cost); continue; }
+		}
+		if (t.npart <= c.p.vsize) {
+			const int64_t f0 = c.p.fix_small ? t.first_part : t.target;
+			for (int64_t jp = f0; jp < f0 + t.npart; jp++) {
+				F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
+				nearest(c, d);
+				F r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+				if (r2 != 0) interact(c, c.m[jp], d, r2, acc, cost);
+			}
+			continue;
+		}
+		const int start = t.target;
+		int node = start;
+		while (c.tree[node].DNext != 0 || node == start) {
+			const WNode<F> &nd = c.tree[node];
+			const int32_t dn = nd.DNext;
+			if (dn < 0) {
+				const int64_t f = -(int64_t) dn - 1;
+				const int np = nd.Npart;
+				for (int64_t jp = f; jp < f + np; jp++) {
+					F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
+					nearest(c, d);
+					F r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+					if (r2 != 0) interact(c, c.m[jp], d, r2, acc, cost);
+				}
+				node++;
+				continue;
+			}
+			F d[3] = { nd.CoM[0] - sp[0], nd.CoM[1] - sp[1], nd.CoM[2] - sp[2] };
+			nearest(c, d);
+			F r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+			F nmass = nd.Mass;
+			F nsz = node_size(c, (int) (nd.Bitfield & 0x3F));
+			if (c.p.use_bh) {
+				if ((double) (nsz * nsz) > r2 * c.p.open_bh) { node++; continue; }
+			} else {
+				if (nmass * nsz * nsz > r2 * r2 * fac) { node++; continue; }
+				F ds[3] = { nd.Pos[0] - sp[0], nd.Pos[1] - sp[1], nd.Pos[2] - sp[2] };
+				nearest(c, ds);
+				if (fabs((double) ds[0]) < 0.6 * nsz && fabs((double) ds[1]) < 0.6 * nsz
+				    && fabs((double) ds[2]) < 0.6 * nsz) { node++; continue; }
+			}
+			interact(c, nmass, d, r2, acc, cost);
+			node += dn;
+		}
+	}
+}
+
+// Ewald_Correction, Gravity/periodic.c:35-113
+template <typename F>
+__device__ __forceinline__ void ewald_corr(const PlainCtx<F> &c, const F dr[3], F f[3])
+{
+	int sg[3] = { -1, -1, -1 };
+	F dx = dr[0], dy = dr[1], dz = dr[2];
+	if (dx < 0) { dx = -dx; sg[0] = 1; }
+	if (dy < 0) { dy = -dy; sg[1] = 1; }
+	if (dz < 0) { dz = -dz; sg[2] = 1; }
+	F u = (F) (dx * c.p.box2grid), v = (F) (dy * c.p.box2grid), w = (F) (dz * c.p.box2grid);
+	int i = (int) u, j = (int) v, k = (int) w;
+	if (i >= 64) i = 63;
+	if (j >= 64) j = 63;
+	if (k >= 64) k = 63;
+	u -= i; v -= j; w -= k;
+	const F one = 1;
+	const F wt[8] = { (one - u) * (one - v) * (one - w), (one - u) * (one - v) * w,
+	                  (one - u) * v * (one - w), (one - u) * v * w,
+	                  u * (one - v) * (one - w), u * (one - v) * w,
+	                  u * v * (one - w), u * v * w };
+	const int64_t b = ((int64_t) i * 65 + j) * 65 + k;
+	const int64_t o1 = 1, o2 = 65, o3 = 66, o4 = 65 * 65, o5 = 65 * 65 + 1, o6 = 65 * 65 + 65,
+	              o7 = 65 * 65 + 66;
+	const F *tab[3] = { c.fx, c.fy, c.fz };
+#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		const F *T = tab[d];
+		f[d] = wt[0] * T[b] + wt[1] * T[b + o1] + wt[2] * T[b + o2] + wt[3] * T[b + o3]
+		     + wt[4] * T[b + o4] + wt[5] * T[b + o5] + wt[6] * T[b + o6] + wt[7] * T[b + o7];
+	}
+	f[0] *= sg[0];
+	f[1] *= sg[1];
+	f[2] *= sg[2];
+}
+
+template <typename F>
+__device__ __forceinline__ void ewald_cube(const PlainCtx<F> &c, const F dr[3], F mass, double acc[3],
+                                           F &cost)
+{
+	F r[3];
+	ewald_corr(c, dr, r);
+	acc[0] += c.p.gravity * mass * r[0];
+	acc[1] += c.p.gravity * mass * r[1];
+	acc[2] += c.p.gravity * mass * r[2];
+	cost += 1;
+}
+
+template <typename F>
+__device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double acc[3], F &cost)
+{
+	const double box = c.p.boxsize;
+	const F fac = (F) (sacc / c.p.gravity * c.p.open_rel);
+	const double bh2 = c.p.open_bh * c.p.open_bh;
+	for (int j = 0; j < c.p.ntop; j++) {
+		const tvg_topnode &t = c.top[j];
+		const F nsize = (F) (c.p.domain_size / (double) (1UL << t.level));
+		bool want = false;
+		F dr[3] = { (F) t.com[0] - sp[0], (F) t.com[1] - sp[1], (F) t.com[2] - sp[2] };
+		nearest(c, dr);
+		F r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+		if (c.p.use_bh) {
+			if ((double) (nsize * nsize) > r2 * c.p.open_bh) want = true;
+		} else {
+			F nmass = (F) t.mass;
+			if (nmass * nsize * nsize > r2 * r2 * fac) want = true;
+		}
+		double dx = fabs((double) (F) (sp[0] - (F) t.pos[0]));
+		if (dx < 0.6 * nsize) {
+			double dy = fabs((double) (F) (sp[1] - (F) t.pos[1]));
+			if (dy < 0.6 * nsize) {
+				double dz = fabs((double) (F) (sp[2] - (F) t.pos[2]));
+				if (dz < 0.6 * nsize) want = true;
+			}
+		}
+		bool open = false;
+		if (want) {
+			const double lim = 0.5 * (box - nsize);
+			if (fabs((double) dr[0]) > lim || fabs((double) dr[1]) > lim || fabs((double) dr[2]) > lim
+			    || nsize > 0.2 * box)
+				open = true;
+		}
+		if (!open) { ewald_cube(c, dr, (F) t.mass, acc, cost); continue; }
+		if (t.npart <= c.p.vsize) {
+			const int64_t f0 = c.p.fix_small ? t.first_part : t.target;
+			for (int64_t jp = f0; jp < f0 + t.npart; jp++) {
+				F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
+				nearest(c, d);
+				if (d[0] != 0 && d[1] != 0 && d[2] != 0) ewald_cube(c, d, c.m[jp], acc, cost);
+			}
+			continue;
+		}
+		const int start = t.target;
+		const int end = start + c.tree[start].DNext;
+		int node = start;
+		while (node != end) {
+			const WNode<F> &nd = c.tree[node];
+			const int32_t dn = nd.DNext;
+			if (dn < 0) {
+				const int64_t f = -(int64_t) dn - 1;
+				const int np = nd.Npart;
+				for (int64_t jp = f; jp < f + np; jp++) {
+					F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
+					nearest(c, d);
+					if (d[0] != 0 && d[1] != 0 && d[2] != 0) ewald_cube(c, d, c.m[jp], acc, cost);
+				}
+				node++;
+				continue;
+			}
+			F d[3] = { nd.CoM[0] - sp[0], nd.CoM[1] - sp[1], nd.CoM[2] - sp[2] };
+			nearest(c, d);
+			F rr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+			F nmass = nd.Mass;
+			F nsz = node_size(c, (int) (nd.Bitfield & 0x3F));
+			F ds[3] = { nd.Pos[0] - sp[0], nd.Pos[1] - sp[1], nd.Pos[2] - sp[2] };
+			bool wo = false;
+			if (c.p.use_bh) {
+				if ((double) (nsz * nsz) > rr * bh2) wo = true;
+			} else {
+				if (nmass * nsz * nsz > rr * rr * fac) wo = true;
+			}
+			if (!wo && fabs((double) ds[0]) < 0.6 * nsz && fabs((double) ds[1]) < 0.6 * nsz
+			    && fabs((double) ds[2]) < 0.6 * nsz)
+				wo = true;
+			nearest(c, ds);
+			if (wo) {
+				const double dl = 0.5 * (box - nsz);
+				if (fabs((double) ds[0]) > dl || fabs((double) ds[1]) > dl || fabs((double) ds[2]) > dl
+				    || nsz > 0.2 * box) { node++; continue; }
+			}
+			ewald_cube(c, d, nmass, acc, cost);
+			node += dn;
+		}
+	}
+}
+
+template <typename F>
+__global__ void __launch_bounds__(128)
+k_walk_plain(int64_t n, PlainCtx<F> c, int ewald, const F *__restrict__ last_acc, F *acc0, F *acc1,
+             F *acc2, F *gacc0, F *gacc1, F *gacc2, F *cost_out, double *counter)
+{
+	__shared__ tvg_topnode s_top[TVG_MAX_TOP];
+	for (int j = threadIdx.x; j < c.p.ntop; j += blockDim.x) s_top[j] = c.top[j];
+	__syncthreads();
+	PlainCtx<F> cc = c;
+	cc.top = s_top;
+	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	F cost = 0;
+	if (i < n) {
+		const F sp[3] = { c.x[i], c.y[i], c.z[i] };
+		double a[3] = { 0, 0, 0 };
+		if (ewald) walk_ewald(cc, sp, last_acc[i], a, cost);
+		else walk_gravity(cc, sp, last_acc[i], a, cost);
+		// add_recv_to (tree_accel.c:110-129, tree_periodic.c:91-110)
+		acc0[i] += a[0];
+		acc1[i] += a[1];
+		acc2[i] += a[2];
+		if (ewald) {
+			gacc0[i] += a[0];
+			gacc1[i] += a[1];
+			gacc2[i] += a[2];
+			cost_out[i] += cost;
+		} else {
+			gacc0[i] = (F) a[0];
+			gacc1[i] = (F) a[1];
+			gacc2[i] = (F) a[2];
+			cost_out[i] = cost;
+		}
+	}
+	// interaction count for the roofline accounting
+	double cw = (double) cost;
+#pragma unroll
+	for (int o = 16; o; o >>= 1) cw += __shfl_xor_sync(0xFFFFFFFFu, cw, o);
+	if ((threadIdx.x & 31) == 0 && cw != 0) atomicAdd(counter, cw);
+}
+
+template <typename F>
+static int walk_typed(tvg_context *ctx, int use_bh, uint32_t parts)
+{
+	const int64_t n = ctx->n;
+	if (n == 0) return TVG_OK;
+	PlainCtx<F> c;
+	c.x = (const F *) ctx->f[FS_POS0];
+	c.y = (const F *) ctx->f[FS_POS1];
+	c.z = (const F *) ctx->f[FS_POS2];
+	c.m = (const F *) ctx->f[FS_MASS];
+	c.top = ctx->d_top;
+	c.tree = (const WNode<F> *) ctx->tree;
+	c.fx = (const F *) ctx->ewald_f[0];
+	c.fy = (const F *) ctx->ewald_f[1];
+	c.fz = (const F *) ctx->ewald_f[2];
+	const tvg_config &cf = ctx->cfg;
+	c.p.gravity = cf.gravity;
+	c.p.domain_size = ctx->dsize;
+	c.p.boxsize = cf.periodic ? cf.boxsize : 0;
+	c.p.open_bh = cf.open_bh;
+	c.p.open_rel = cf.open_rel;
+	const double eps = -41.0 / 32.0 * cf.softening;    // tree_build.c:136-138
+	c.p.eps2 = eps * eps;
+	c.p.eps3 = eps * eps * eps;
+	c.p.box2grid = cf.periodic ? 2 * 64 / cf.boxsize : 0;
+	c.p.periodic = cf.periodic;
+	c.p.use_bh = use_bh;
+	c.p.vsize = cf.vector_size;
+	c.p.ntop = ctx->ntop;
+	c.p.fix_small = (cf.flags & TVG_CFG_FIX_SMALL_TOPNODES) ? 1 : 0;
+	c.boxhalf = (F) (c.p.boxsize / 2.0);
+	cudaStream_t s = ctx->stream;
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16, s));
+	for (int part = 0; part < 2; part++) {
+		const bool ew = part == 1;
+		if (!(parts & (ew ? TVG_WALK_EWALD : TVG_WALK_GRAVITY))) continue;
+		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+		k_walk_plain<F><<<tvg_blocks(n, 128), 128, 0, s>>>(
+		    n, c, ew ? 1 : 0, (const F *) ctx->f[FS_LAST_ACC], (F *) ctx->f[FS_ACC0],
+		    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0],
+		    (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2], (F *) ctx->f[FS_COST],
+		    ctx->counters + (ew ? 1 : 0));
+		TVG_CUDA(ctx, cudaGetLastError());
+		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+		TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+		float ms = 0;
+		TVG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+		ctx->phase_ms[ew ? 5 : 4] = ms;
+	}
+	double cnt[2];
+	TVG_CUDA(ctx, cudaMemcpy(cnt, ctx->counters, 16, cudaMemcpyDeviceToHost));
+	ctx->last_counts[0] = cnt[0];
+	ctx->last_counts[1] = cnt[1];
+	return TVG_OK;
+}
+
+int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts)
+{
+	if (ctx->cfg.float_bytes == 4) return walk_typed<float>(ctx, use_bh, parts);
+	return walk_typed<double>(ctx, use_bh, parts);
+}
+
+// accel.c:28-43: Last_Acc_Mag = |Acc|, Acc = 0
+template <typename F>
+__global__ void k_save_last(int64_t n, F *a0, F *a1, F *a2, F *last)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	last[i] = fsqrt<F>(a0[i] * a0[i] + a1[i] * a1[i] + a2[i] * a2[i]);
+	a0[i] = a1[i] = a2[i] = 0;
+}
+
+int tvg_impl_save_last_accel(tvg_context *ctx)
+{
+	const int64_t n = ctx->n;
+	if (!n) return TVG_OK;
+	if (ctx->cfg.float_bytes == 4)
+		k_save_last<float><<<tvg_blocks(n, 256), 256, 0, ctx->stream>>>(
+		    n, (float *) ctx->f[FS_ACC0], (float *) ctx->f[FS_ACC1], (float *) ctx->f[FS_ACC2],
+		    (float *) ctx->f[FS_LAST_ACC]);
+	else
+		k_save_last<double><<<tvg_blocks(n, 256), 256, 0, ctx->stream>>>(
+		    n, (double *) ctx->f[FS_ACC0], (double *) ctx->f[FS_ACC1], (double *) ctx->f[FS_ACC2],
+		    (double *) ctx->f[FS_LAST_ACC]);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
+}
+
+int tvg_impl_zero_accel(tvg_context *ctx)
+{
+	const size_t b = tvg_fsize(ctx) * ctx->n;
+	const int slots[] = { FS_ACC0, FS_ACC1, FS_ACC2, FS_GACC0, FS_GACC1, FS_GACC2, FS_COST };
+	for (int s : slots) TVG_CUDA(ctx, cudaMemsetAsync(ctx->f[s], 0, b, ctx->stream));
+	return TVG_OK;
+}

@@ -1,0 +1,251 @@
+"""Python view of the C ABI (include/tandav_gpu.h), one method per entry point.
+
+The method names follow the reference entry points they replace
+(src/peano.c, src/Gravity/tree_build.c, tree_accel.c, tree_periodic.c,
+Gravity/periodic.c, kick.c, drift.c). Arrays are numpy; the Float width is
+``float_bytes`` (4 or 8, the reference's DOUBLE_PRECISION switch).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import lib
+
+TVG_OK = 0
+ERRORS = {1: "TVG_E_CUDA", 2: "TVG_E_NOMEM", 3: "TVG_E_TREE_FULL", 4: "TVG_E_TIMEOUT",
+          5: "TVG_E_BADINPUT", 6: "TVG_E_COINCIDENT", 7: "TVG_E_STATE"}
+
+FORM_PLAIN, FORM_GROUP = 0, 1
+WALK_GRAVITY, WALK_EWALD = 1, 2
+EWALD_TABLE, EWALD_MLP = 0, 1
+BUILD_EXACT_MOMENTS = 1
+CFG_FIX_SMALL_TOPNODES = 1
+
+F_TYPE, F_TIME_BIN, F_IT_DRIFT, F_IT_KICK, F_KEY, F_ID, F_COST = (1 << k for k in range(7))
+F_POS, F_VEL, F_ACC, F_MASS, F_GRAV_ACC, F_LAST_ACC, F_TREE_PARENT = (1 << k for k in range(7, 14))
+
+# struct Tree_Node of the reference (src/Gravity/tree.h:23-32)
+TREE_DTYPE = {
+    4: np.dtype([("DNext", "<i4"), ("Bitfield", "<u4"), ("DUp", "<i4"), ("Npart", "<i4"),
+                 ("Pos", "<f4", 3), ("Mass", "<f4"), ("CoM", "<f4", 3), ("Dp", "<f4", 3)]),
+    8: np.dtype([("DNext", "<i4"), ("Bitfield", "<u4"), ("DUp", "<i4"), ("Npart", "<i4"),
+                 ("Pos", "<f8", 3), ("Mass", "<f8"), ("CoM", "<f8", 3), ("Dp", "<f8", 3)]),
+}
+TOPNODE_DTYPE = np.dtype([("Key", "<u8"), ("Target", "<i4"), ("Level", "<i4"),
+                          ("First_Part", "<i4"), ("Npart", "<i4"), ("Pos", "<f4", 3),
+                          ("Mass", "<f4"), ("CoM", "<f4", 3), ("Dp", "<f4", 3)])
+
+
+class Config(C.Structure):
+    _fields_ = [("float_bytes", C.c_int32), ("periodic", C.c_int32), ("boxsize", C.c_double),
+                ("gravity", C.c_double), ("softening", C.c_double), ("open_bh", C.c_double),
+                ("open_rel", C.c_double), ("vector_size", C.c_int32), ("flags", C.c_int32),
+                ("max_particles", C.c_int64)]
+
+
+class Particles(C.Structure):
+    _fields_ = [("type", C.c_void_p), ("time_bin", C.c_void_p), ("it_drift_pos", C.c_void_p),
+                ("it_kick_pos", C.c_void_p), ("key", C.c_void_p), ("id", C.c_void_p),
+                ("cost", C.c_void_p), ("pos", C.c_void_p * 3), ("vel", C.c_void_p * 3),
+                ("acc", C.c_void_p * 3), ("mass", C.c_void_p), ("grav_acc", C.c_void_p * 3),
+                ("last_acc_mag", C.c_void_p), ("tree_parent", C.c_void_p)]
+
+
+class TvgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class GravityContext:
+    """Device context of the gravity hot path (tvg_init ... tvg_finalize)."""
+
+    def __init__(self, max_particles, float_bytes=4, periodic=False, boxsize=0.0,
+                 gravity=43007.1, softening=0.01, open_bh=0.25, open_rel=0.005,
+                 vector_size=64, flags=0, device=0):
+        self.lib = lib()
+        self.fb = float_bytes
+        self.ft = np.float32 if float_bytes == 4 else np.float64
+        cfg = Config(float_bytes, int(periodic), boxsize, gravity, softening, open_bh, open_rel,
+                     vector_size, flags, int(max_particles))
+        self.cfg = cfg
+        self.ctx = C.c_void_p()
+        rc = self.lib.tvg_init(C.c_int(device), C.byref(cfg), C.byref(self.ctx))
+        if rc != TVG_OK:
+            msg = self.lib.tvg_last_error(self.ctx).decode() if self.ctx else ""
+            if self.ctx:
+                self.lib.tvg_finalize(self.ctx)
+            self.ctx = None
+            raise TvgError(rc, f"tvg_init failed {msg}")
+        self.n = 0
+
+    def close(self):
+        if self.ctx:
+            self.lib.tvg_finalize(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != TVG_OK:
+            raise TvgError(rc, f"{what}: {self.lib.tvg_last_error(self.ctx).decode()}")
+
+    # ------------------------------------------------------------ data
+
+    def upload(self, pos, mass, vel=None, ids=None, last_acc=None):
+        ft = self.ft
+        n = int(np.asarray(mass).shape[0])
+        self._keep = []
+        p = Particles()
+        fields = F_POS | F_MASS
+        for k in range(3):
+            a = np.ascontiguousarray(pos[k], dtype=ft)
+            self._keep.append(a)
+            p.pos[k] = a.ctypes.data
+        m = np.ascontiguousarray(mass, dtype=ft)
+        self._keep.append(m)
+        p.mass = m.ctypes.data
+        if vel is not None:
+            fields |= F_VEL
+            for k in range(3):
+                a = np.ascontiguousarray(vel[k], dtype=ft)
+                self._keep.append(a)
+                p.vel[k] = a.ctypes.data
+        ids = np.arange(n, dtype=np.uint32) if ids is None else np.ascontiguousarray(ids, np.uint32)
+        self._keep.append(ids)
+        p.id = ids.ctypes.data
+        fields |= F_ID
+        la = np.zeros(n, ft) if last_acc is None else np.ascontiguousarray(last_acc, dtype=ft)
+        self._keep.append(la)
+        p.last_acc_mag = la.ctypes.data
+        fields |= F_LAST_ACC
+        self._check(self.lib.tvg_upload(self.ctx, C.c_int64(n), C.byref(p), C.c_uint32(fields)),
+                    "upload")
+        self.n = n
+
+    def download(self, fields=F_POS | F_MASS | F_ID | F_ACC | F_GRAV_ACC | F_COST):
+        n, ft = self.n, self.ft
+        out = {}
+        p = Particles()
+        if fields & F_POS:
+            out["pos"] = np.zeros((3, n), ft)
+            for k in range(3):
+                p.pos[k] = out["pos"][k].ctypes.data
+        for name, bit in (("acc", F_ACC), ("grav_acc", F_GRAV_ACC), ("vel", F_VEL)):
+            if fields & bit:
+                out[name] = np.zeros((3, n), ft)
+                arr = getattr(p, name)
+                for k in range(3):
+                    arr[k] = out[name][k].ctypes.data
+        for name, bit, dt in (("mass", F_MASS, ft), ("cost", F_COST, ft),
+                              ("last_acc_mag", F_LAST_ACC, ft), ("id", F_ID, np.uint32),
+                              ("tree_parent", F_TREE_PARENT, np.int32),
+                              ("time_bin", F_TIME_BIN, np.int32), ("type", F_TYPE, np.int32),
+                              ("it_drift_pos", F_IT_DRIFT, np.uint32),
+                              ("it_kick_pos", F_IT_KICK, np.uint32)):
+            if fields & bit:
+                out[name] = np.zeros(n, dt)
+                setattr(p, name, out[name].ctypes.data)
+        if fields & F_KEY:
+            out["key"] = np.zeros((n, 2), np.uint64)
+            p.key = out["key"].ctypes.data
+        self._check(self.lib.tvg_download(self.ctx, C.byref(p), C.c_uint32(fields)), "download")
+        if "key" in out:   # little-endian 128-bit -> [hi, lo]
+            out["key"] = np.ascontiguousarray(out["key"][:, ::-1])
+        return out
+
+    # ------------------------------------------------- reference entry points
+
+    def set_domain(self, origin, size):
+        o = (C.c_double * 3)(*origin)
+        self._check(self.lib.tvg_set_domain(self.ctx, o, C.c_double(size)), "set_domain")
+
+    def peano_keys(self):
+        self._check(self.lib.tvg_peano_keys(self.ctx), "peano_keys")
+
+    def reverse_keys(self):
+        self._check(self.lib.tvg_reverse_keys(self.ctx), "reverse_keys")
+
+    def sort_particles(self, want_perm=True):
+        perm = np.zeros(self.n, np.uint32) if want_perm else None
+        self._check(self.lib.tvg_sort_particles(self.ctx, C.c_void_p(_ptr(perm))), "sort")
+        return perm
+
+    def top_nodes(self):
+        nt = C.c_int32()
+        self._check(self.lib.tvg_top_nodes(self.ctx, C.byref(nt)), "top_nodes")
+        return nt.value
+
+    def tree_build(self, exact_moments=True):
+        self._check(self.lib.tvg_tree_build(self.ctx, C.c_uint32(
+            BUILD_EXACT_MOMENTS if exact_moments else 0)), "tree_build")
+
+    def download_tree(self):
+        nn = C.c_int64()
+        nt = C.c_int32()
+        self._check(self.lib.tvg_download_tree(self.ctx, None, C.c_int64(0), C.byref(nn), None,
+                                               C.c_int32(0), C.byref(nt)), "download_tree")
+        tree = np.zeros(max(nn.value, 1), TREE_DTYPE[self.fb])
+        top = np.zeros(64, TOPNODE_DTYPE)
+        self._check(self.lib.tvg_download_tree(self.ctx, C.c_void_p(tree.ctypes.data),
+                                               C.c_int64(len(tree)), C.byref(nn),
+                                               C.c_void_p(top.ctypes.data), C.c_int32(64),
+                                               C.byref(nt)), "download_tree")
+        return tree[:nn.value].copy(), top[:nt.value].copy()
+
+    def ewald_init(self):
+        self._check(self.lib.tvg_ewald_init(self.ctx), "ewald_init")
+
+    def download_ewald_table(self):
+        m = 65 ** 3
+        t = [np.zeros(m, self.ft) for _ in range(4)]
+        self._check(self.lib.tvg_download_ewald_table(self.ctx, *[C.c_void_p(a.ctypes.data) for a in t]),
+                    "download_ewald_table")
+        return t
+
+    def upload_ewald_table(self, fx, fy, fz, fp):
+        """Raw box-unit tables as in the reference's ./ewald_tables.dat."""
+        t = [np.ascontiguousarray(a, dtype=self.ft) for a in (fx, fy, fz, fp)]
+        self._check(self.lib.tvg_upload_ewald_table(self.ctx, *[C.c_void_p(a.ctypes.data) for a in t]),
+                    "upload_ewald_table")
+
+    def zero_accel(self):
+        self._check(self.lib.tvg_zero_accel(self.ctx), "zero_accel")
+
+    def save_last_accel(self):
+        self._check(self.lib.tvg_save_last_accel(self.ctx), "save_last_accel")
+
+    def walk(self, form=FORM_PLAIN, use_bh=True, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE):
+        self._check(self.lib.tvg_walk(self.ctx, C.c_int32(form), C.c_int32(int(use_bh)),
+                                      C.c_uint32(parts), C.c_int32(ewald_kind)), "walk")
+
+    def force_step(self, form=FORM_GROUP, use_bh=False, parts=WALK_GRAVITY,
+                   ewald_kind=EWALD_TABLE):
+        self._check(self.lib.tvg_force_step(self.ctx, C.c_int32(form), C.c_int32(int(use_bh)),
+                                            C.c_uint32(parts), C.c_int32(ewald_kind)), "force_step")
+
+    def phase_times(self):
+        ms = (C.c_double * 8)()
+        self._check(self.lib.tvg_phase_times(self.ctx, ms, C.c_int32(8)), "phase_times")
+        return dict(zip(("keys", "sort", "top", "build", "walk", "ewald", "total"), list(ms)[:7]))
+
+    def walk_counters(self):
+        g, e = C.c_double(), C.c_double()
+        self._check(self.lib.tvg_walk_counters(self.ctx, C.byref(g), C.byref(e)), "walk_counters")
+        return g.value, e.value

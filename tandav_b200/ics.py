@@ -194,7 +194,7 @@ def zeldovich_box(n_side: int = 128, box_mpc: float = 100.0, z_start: float = 50
     disp = np.empty((3, n, n, n))
     for d, kc in enumerate((kx, ky, kzz)):
         # psi_k = i k / k^2 delta_k  (Mpc/h); displacement in kpc/h
-        disp[d] = np.fft.irfftn(1j * kc / k2 * delta_k, s=(n, n, n)) * 1000.0
+        disp[d] = np.fft.irfftn(1j * kc / k2 * delta_k, s=(n, n, n), axes=(0, 1, 2)) * 1000.0
     del delta_k
     spacing = L / n
     g = (np.arange(n) + 0.5) * spacing

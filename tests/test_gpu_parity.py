@@ -1,0 +1,215 @@
+"""CUDA path against the oracle and the reference's golden fixtures, through
+the C ABI. Keys, sort permutation, top nodes, every tree field and
+Tree_Parent must be bit-exact; so must the plain-form accelerations and
+interaction counts (the plain form replays the reference's arithmetic) where
+the Ewald table is the reference's own (FP32); the FP64 periodic walk is
+compared within 1e-12 relative, because the GPU's erfc/exp/sin differ from
+glibc's in the last bit of the FP64 table."""
+import numpy as np
+import pytest
+
+import port
+from pipeline import oracle_pipeline, oracle_ewald_tables, assert_struct_equal
+from tandav_b200 import gravity as G
+from tandav_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+TREE_FIELDS = ["DNext", "Bitfield", "DUp", "Npart", "Pos", "Mass", "CoM", "Dp"]
+TOP_FIELDS = ["Key", "Target", "Level", "First_Part", "Npart", "Pos", "Mass", "CoM"]
+FORCE_CASES = ["hernquist_iso_f64", "hernquist_iso_f32", "box_per_f32", "zeldovich_per_f64"]
+
+
+def make_ctx(n, fsize, box=0.0, softening=0.01, gravity=43007.1, **kw):
+    return G.GravityContext(max(n, 1024), float_bytes=fsize, periodic=box > 0, boxsize=box,
+                            gravity=gravity, softening=softening, **kw)
+
+
+@pytest.mark.parametrize("fsize,variant", [(4, "iso_f32"), (8, "iso_f64")])
+def test_keys_grid(golden_dir, fsize, variant):
+    g = np.load(golden_dir / "keys_grid.npz")
+    pos = g["pos"]
+    n = pos.shape[1]
+    with make_ctx(n, fsize) as ctx:
+        ctx.upload(pos, np.ones(n))
+        ctx.set_domain((0.0, 0.0, 0.0), 1.0)
+        ctx.peano_keys()
+        assert np.array_equal(ctx.download(G.F_KEY)["key"], g[f"{variant}_std"])
+        ctx.reverse_keys()
+        assert np.array_equal(ctx.download(G.F_KEY)["key"], g[f"{variant}_rev"])
+
+
+def gpu_pipeline(ctx, pos, mass, origin, size, exact=True):
+    ctx.upload(pos, mass)
+    ctx.set_domain(origin, size)
+    ctx.peano_keys()
+    perm = ctx.sort_particles()
+    keys = ctx.download(G.F_KEY)["key"]
+    ctx.top_nodes()
+    ctx.tree_build(exact_moments=exact)
+    tree, top = ctx.download_tree()
+    return perm, keys, tree, top
+
+
+_RAW_TABLE = {}
+
+
+def reference_table(fsize):
+    """The reference's raw Float tables (the oracle's FP64 sums, verified
+    bit-identical to the reference's ./ewald_tables.dat), as a drop-in host
+    would read them from that file."""
+    if fsize not in _RAW_TABLE:
+        fx, fy, fz, fp = port.ewald_table(potential=True)
+        _RAW_TABLE[fsize] = [t.astype(port.ftype(fsize)) for t in (fx, fy, fz, fp)]
+    return _RAW_TABLE[fsize]
+
+
+def walks(ctx, periodic, fsize):
+    parts = G.WALK_GRAVITY | (G.WALK_EWALD if periodic else 0)
+    if periodic:
+        ctx.upload_ewald_table(*reference_table(fsize))
+    ctx.zero_accel()
+    ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+    bh = ctx.download(G.F_GRAV_ACC | G.F_COST)
+    ctx.save_last_accel()
+    last = ctx.download(G.F_LAST_ACC)["last_acc_mag"]
+    ctx.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
+    rel = ctx.download(G.F_GRAV_ACC | G.F_COST)
+    return bh, last, rel
+
+
+@pytest.mark.parametrize("case", FORCE_CASES)
+def test_pipeline_matches_reference_golden(golden_dir, case):
+    g = np.load(golden_dir / f"{case}.npz")
+    fsize = int(g["float_size"])
+    box = float(g["box"])
+    n = len(g["mass_in"])
+    with make_ctx(n, fsize, box=box, softening=float(g["softening"]),
+                  gravity=float(g["gravity"][0])) as ctx:
+        perm, keys, tree, top = gpu_pipeline(ctx, g["pos_in"], g["mass_in"], g["domain_origin"],
+                                             float(g["domain_size"][0]))
+        assert np.array_equal(perm, g["perm"])
+        assert np.array_equal(keys, g["std_key"])
+        assert_struct_equal(top, g["topnodes"], TOP_FIELDS, "topnodes")
+        assert_struct_equal(tree, g["tree"], TREE_FIELDS, "tree")
+        assert np.array_equal(ctx.download(G.F_TREE_PARENT)["tree_parent"], g["tree_parent"])
+        bh, last, rel = walks(ctx, box > 0, fsize)
+        for name, got in (("bh", bh), ("rel", rel)):
+            assert np.array_equal(got["cost"].astype(np.float64), g[name + "_cost"]), name
+            ref = g[name + "_gacc"]
+            a = got["grav_acc"].astype(np.float64)
+            assert np.array_equal(a, ref), f"{name}: max diff {np.abs(a - ref).max()}"
+        assert np.array_equal(last.astype(np.float64), g["last_acc_mag"])
+        ctx.reverse_keys()
+        assert np.array_equal(ctx.download(G.F_KEY)["key"], g["rev_key"])
+
+
+RANDOM_CASES = [
+    ("hernquist", 8, 32768),
+    ("hernquist", 4, 65536),
+    ("clumpy_box", 4, 40000),
+    ("zeldovich", 4, 32 ** 3),
+]
+
+
+def make_case(kind, n):
+    if kind == "hernquist":
+        p = ics.hernquist(n=n, seed=21)
+        c = np.median(p.pos, axis=1)
+        size = 2.001 * np.abs(p.pos - c[:, None]).max()
+        return p, c - 0.5 * size, size
+    if kind == "clumpy_box":
+        p = ics.random_box(n, box=2000.0, seed=22, clumps=9)
+    else:
+        p = ics.zeldovich_box(n_side=round(n ** (1 / 3)), seed=23)
+    return p, np.zeros(3), p.box
+
+
+@pytest.mark.parametrize("kind,fsize,n", RANDOM_CASES)
+def test_tree_and_plain_walk_vs_oracle(kind, fsize, n):
+    p, origin, size = make_case(kind, n)
+    ew = oracle_ewald_tables(fsize, p.box) if p.box > 0 else None
+    o = oracle_pipeline(p.pos, p.mass, origin, size, fsize, box=p.box, softening=p.softening,
+                        ewald=ew, passes=("bh",))
+    with make_ctx(p.n, fsize, box=p.box, softening=p.softening) as ctx:
+        perm, keys, tree, top = gpu_pipeline(ctx, p.pos, p.mass, origin, size)
+        assert np.array_equal(perm, o["perm"])
+        assert_struct_equal(top, o["top"], TOP_FIELDS, "topnodes")
+        assert_struct_equal(tree, o["tree"], TREE_FIELDS, "tree")
+        assert np.array_equal(ctx.download(G.F_TREE_PARENT)["tree_parent"], o["tree_parent"])
+        parts = G.WALK_GRAVITY | (G.WALK_EWALD if p.box > 0 else 0)
+        if p.box > 0:
+            ctx.upload_ewald_table(*reference_table(fsize))
+        ctx.zero_accel()
+        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+        got = ctx.download(G.F_GRAV_ACC | G.F_COST)
+        assert np.array_equal(got["cost"], o["bh_cost"])
+        a, ref = got["grav_acc"].astype(np.float64), o["bh_gacc"].astype(np.float64)
+        assert np.array_equal(a, ref), f"max diff {np.abs(a - ref).max()}"
+
+
+def test_fast_moments_close_to_exact():
+    p, origin, size = make_case("zeldovich", 32 ** 3)
+    with make_ctx(p.n, 4, box=p.box, softening=p.softening) as ctx:
+        _, _, exact, top_e = gpu_pipeline(ctx, p.pos, p.mass, origin, size, exact=True)
+        _, _, fast, top_f = gpu_pipeline(ctx, p.pos, p.mass, origin, size, exact=False)
+    assert_struct_equal(exact, fast, ["DNext", "Bitfield", "DUp", "Npart", "Pos"], "topology")
+    assert np.allclose(exact["Mass"], fast["Mass"], rtol=1e-5)
+    assert np.allclose(exact["CoM"], fast["CoM"], rtol=0, atol=1e-4 * p.box)
+
+
+@pytest.mark.parametrize("fsize", [4, 8])
+def test_ewald_table_vs_oracle(fsize):
+    box = 1000.0
+    with make_ctx(1024, fsize, box=box) as ctx:
+        ctx.upload(np.full((3, 4), 1.0), np.ones(4))
+        ctx.ewald_init()
+        fx, fy, fz, fp = ctx.download_ewald_table()
+    ox, oy, oz, op = port.ewald_table(potential=True)
+    ft = port.ftype(fsize)
+    for name, got, ref in (("fx", fx, ox), ("fy", fy, oy), ("fz", fz, oz), ("fp", fp, op)):
+        # the same FP64 sums with the GPU's erfc/exp/sin/cos: the terms cancel
+        # to ~1e-3 of their size, so the last FP64 bits differ; stored in
+        # Float they agree to within one Float ulp of the table's scale
+        r = ref.astype(ft).astype(np.float64)
+        scale = np.abs(ref).max()
+        err = np.abs(got.astype(np.float64) - r)
+        tol = 1e-13 * scale if fsize == 8 else float(np.spacing(np.float32(scale)))
+        assert err.max() <= tol, f"{name}: max err {err.max()} > {tol}"
+
+
+def test_coincident_particles_reported():
+    p = ics.random_box(2000, box=100.0, seed=3)
+    p.pos[:, 1] = p.pos[:, 0]
+    with make_ctx(p.n, 4, box=p.box) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.peano_keys()
+        ctx.sort_particles()
+        ctx.top_nodes()
+        with pytest.raises(G.TvgError) as e:
+            ctx.tree_build()
+        assert e.value.code == 6
+
+
+def test_nonfinite_position_reported():
+    p = ics.random_box(1000, box=100.0, seed=4)
+    p.pos[1, 17] = np.nan
+    with make_ctx(p.n, 4, box=p.box) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        with pytest.raises(G.TvgError) as e:
+            ctx.peano_keys()
+        assert e.value.code == 5
+
+
+def test_state_errors():
+    with make_ctx(1024, 4) as ctx:
+        ctx.upload(np.random.default_rng(0).uniform(0, 1, (3, 100)), np.ones(100))
+        with pytest.raises(G.TvgError) as e:
+            ctx.peano_keys()                     # no domain
+        assert e.value.code == 7
+        ctx.set_domain((0.0, 0.0, 0.0), 1.0)
+        with pytest.raises(G.TvgError) as e:
+            ctx.walk()                           # no tree
+        assert e.value.code == 7

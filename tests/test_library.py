@@ -1,0 +1,53 @@
+"""The C ABI library: it loads, exports every entry point declared in
+include/tandav_gpu.h, and fails cleanly (no crash, an error code) where no
+GPU is present. No compute call is made here."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+import tandav_b200
+from tandav_b200 import gravity
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "tandav_gpu.h").read_text()
+    return sorted(set(re.findall(r"\b(tvg_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_and_exports_agree():
+    assert set(declared_symbols()) == set(tandav_b200.EXPORTS)
+
+
+def test_library_exports_every_symbol():
+    lib = tandav_b200.lib()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version_string():
+    assert b"sm_100a" in tandav_b200.lib().tvg_version()
+
+
+def test_init_rejects_bad_config():
+    lib = tandav_b200.lib()
+    ctx = C.c_void_p()
+    cfg = gravity.Config(3, 0, 0.0, 1.0, 0.01, 0.25, 0.005, 64, 0, 100)
+    assert lib.tvg_init(0, C.byref(cfg), C.byref(ctx)) == 5      # TVG_E_BADINPUT
+    cfg = gravity.Config(4, 1, 0.0, 1.0, 0.01, 0.25, 0.005, 64, 0, 100)
+    assert lib.tvg_init(0, C.byref(cfg), C.byref(ctx)) == 5      # periodic without box
+
+
+def test_init_without_gpu_reports_cuda_error():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = tandav_b200.lib()
+    ctx = C.c_void_p()
+    cfg = gravity.Config(4, 0, 0.0, 1.0, 0.01, 0.25, 0.005, 64, 0, 100)
+    assert lib.tvg_init(0, C.byref(cfg), C.byref(ctx)) == 1      # TVG_E_CUDA
+    with pytest.raises(gravity.TvgError):
+        gravity.GravityContext(100)
