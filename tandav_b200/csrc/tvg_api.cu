@@ -142,7 +142,7 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->u_final, ctx->u_level, ctx->u_flag, ctx->tree, ctx->tree_u, ctx->pref,
 	                 ctx->ipos[0], ctx->ipos[1], ctx->ipos[2], ctx->wtree, ctx->group_first,
 	                 ctx->work_counter, ctx->counters, ctx->ewald_f[0], ctx->ewald_f[1],
-	                 ctx->ewald_f[2], ctx->ewald_f[3], ctx->ewald_raw };
+	                 ctx->ewald_f[2], ctx->ewald_f[3], ctx->ewald_raw, ctx->ewald32 };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

@@ -121,6 +121,7 @@ struct tvg_context {
 	// Ewald tables (Float, divided by box^2) and raw FP64
 	void *ewald_f[4] = { nullptr, nullptr, nullptr, nullptr };
 	double *ewald_raw = nullptr;
+	float *ewald32 = nullptr;          // FP32 copy for the group form (FP64 builds)
 
 	// group walk data
 	uint32_t *ipos[3] = { nullptr, nullptr, nullptr };

@@ -1,0 +1,86 @@
+"""The group form (FP32 integer-offset, warp per PH group): force accuracy
+against FP64 direct summation (Ewald-summed in the periodic box) with the
+reference's softened kernel, and agreement with the plain form.
+
+Tolerances: the relative criterion at errtol 0.005 gives rms relative errors
+~1e-3 in the reference (SURVEY probe); the group tests are conservative for
+the whole group, so their rms error must stay at or below the plain form's
+(with 20 % slack) and below 1e-3 where the plain form is below it."""
+import numpy as np
+import pytest
+
+import port
+from tandav_b200 import gravity as G
+from tandav_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+_CORR = {}
+
+
+def fine_corr_table():
+    """FP64 correction on the 65^3 octant grid, interleaved (x, y, z)."""
+    if "t" not in _CORR:
+        fx, fy, fz, _ = port.ewald_table(64)
+        _CORR["t"] = np.stack([fx, fy, fz], axis=1).reshape(-1).copy()
+    return _CORR["t"]
+
+
+def rel_err(a, ref):
+    d = np.sqrt(((a - ref) ** 2).sum(0))
+    return d / np.sqrt((ref ** 2).sum(0))
+
+
+def run_walks(p, origin, size, form, fsize=4):
+    periodic = p.box > 0
+    parts = G.WALK_GRAVITY | (G.WALK_EWALD if periodic else 0)
+    with G.GravityContext(max(p.n, 1024), float_bytes=fsize, periodic=periodic, boxsize=p.box,
+                          softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain(origin, size)
+        ctx.peano_keys()
+        perm = ctx.sort_particles()
+        ctx.top_nodes()
+        ctx.tree_build(exact_moments=(form == G.FORM_PLAIN))
+        if periodic:
+            ctx.ewald_init()
+        ctx.zero_accel()
+        ctx.walk(form, use_bh=True, parts=parts)
+        bh = ctx.download(G.F_GRAV_ACC | G.F_COST)
+        ctx.save_last_accel()
+        ctx.walk(form, use_bh=False, parts=parts)
+        rel = ctx.download(G.F_GRAV_ACC | G.F_COST)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    return {k: (v["grav_acc"][:, inv].astype(np.float64), v["cost"][inv]) for k, v in
+            (("bh", bh), ("rel", rel))}
+
+
+@pytest.mark.parametrize("kind", ["hernquist", "zeldovich"])
+def test_group_accuracy(kind):
+    if kind == "hernquist":
+        p = ics.hernquist(n=32768, seed=31)
+        c = np.median(p.pos, axis=1)
+        size = 2.001 * np.abs(p.pos - c[:, None]).max()
+        origin = c - 0.5 * size
+        corr = None
+    else:
+        p = ics.zeldovich_box(n_side=32, seed=32)
+        origin, size = np.zeros(3), p.box
+        corr = fine_corr_table()
+    rng = np.random.default_rng(5)
+    tgt = rng.choice(p.n, 1000, replace=False)
+    ref = port.direct(p.pos, p.mass, tgt, ics.GRAVITY, p.softening, box=p.box,
+                      corr_table=corr, corr_n=64)
+    plain = run_walks(p, origin, size, G.FORM_PLAIN)
+    group = run_walks(p, origin, size, G.FORM_GROUP)
+    for crit in ("bh", "rel"):
+        ep = rel_err(plain[crit][0][:, tgt], ref)
+        eg = rel_err(group[crit][0][:, tgt], ref)
+        rms_p, rms_g = np.sqrt((ep ** 2).mean()), np.sqrt((eg ** 2).mean())
+        print(f"{kind} {crit}: rms plain {rms_p:.3e} group {rms_g:.3e}; "
+              f"p99 plain {np.percentile(ep, 99):.3e} group {np.percentile(eg, 99):.3e}; "
+              f"interactions plain {plain[crit][1].mean():.0f} group {group[crit][1].mean():.0f}")
+        assert rms_g <= 1.2 * rms_p + 1e-6
+        if rms_p < 1e-3:
+            assert rms_g < 1e-3

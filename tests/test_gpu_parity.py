@@ -174,12 +174,14 @@ def test_ewald_table_vs_oracle(fsize):
         r = ref.astype(ft).astype(np.float64)
         scale = np.abs(ref).max()
         err = np.abs(got.astype(np.float64) - r)
-        tol = 1e-13 * scale if fsize == 8 else float(np.spacing(np.float32(scale)))
+        # FP64: the near-origin terms are ~1e4, so one FP64 ulp of those is ~1e-12
+        tol = 1e-10 if fsize == 8 else float(np.spacing(np.float32(scale)))
         assert err.max() <= tol, f"{name}: max err {err.max()} > {tol}"
 
 
 def test_coincident_particles_reported():
-    p = ics.random_box(2000, box=100.0, seed=3)
+    # enough particles that every top node gets a subtree (> 64 particles)
+    p = ics.random_box(20000, box=100.0, seed=3)
     p.pos[:, 1] = p.pos[:, 0]
     with make_ctx(p.n, 4, box=p.box) as ctx:
         ctx.upload(p.pos, p.mass)
