@@ -310,9 +310,12 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	const float hx = ((float) ((int64_t) maxx - minx) * 0.5f + 1.f) * p.scale;
 	const float hy = ((float) ((int64_t) maxy - miny) * 0.5f + 1.f) * p.scale;
 	const float hz = ((float) ((int64_t) maxz - minz) * 0.5f + 1.f) * p.scale;
-	t.tx = (float) (int) (px - cx) * p.scale;
-	t.ty = (float) (int) (py - cy) * p.scale;
-	t.tz = (float) (int) (pz - cz) * p.scale;
+	// rounded products (no FMA contraction into the later subtraction): a
+	// particle's own list entry must sit at exactly zero separation, since the
+	// reference's inner kernel (h < 0) turns any residue into a large force
+	t.tx = __fmul_rn((float) (int) (px - cx), p.scale);
+	t.ty = __fmul_rn((float) (int) (py - cy), p.scale);
+	t.tz = __fmul_rn((float) (int) (pz - cz), p.scale);
 	t.ax = t.ay = t.az = 0.f;
 	t.cost = 0.f;
 	// group-wide relative criterion: the smallest |a_old| opens the most
@@ -344,27 +347,31 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 		int nchild = 0, child = 0;
 		if (node >= 0) {
 			const tvg_wnode nd = wt[node];
-			const float dx = (float) (int) (nd.cx - cx) * p.scale;
-			const float dy = (float) (int) (nd.cy - cy) * p.scale;
-			const float dz = (float) (int) (nd.cz - cz) * p.scale;
+			const float dx = __fmul_rn((float) (int) (nd.cx - cx), p.scale);
+			const float dy = __fmul_rn((float) (int) (nd.cy - cy), p.scale);
+			const float dz = __fmul_rn((float) (int) (nd.cz - cz), p.scale);
 			const float qx = fmaxf(fabsf(dx) - hx, 0.f), qy = fmaxf(fabsf(dy) - hy, 0.f),
 			            qz = fmaxf(fabsf(dz) - hz, 0.f);
 			const float r2 = qx * qx + qy * qy + qz * qz;
 			bool want;
 			if (p.use_bh) want = nd.size2 > r2 * p.theta2;
 			else want = nd.mass * nd.size2 > r2 * r2 * fac;
-			const float gx = (float) (int) (nd.gx - cx) * p.scale;
-			const float gy = (float) (int) (nd.gy - cy) * p.scale;
-			const float gz = (float) (int) (nd.gz - cz) * p.scale;
+			const float gx = __fmul_rn((float) (int) (nd.gx - cx), p.scale);
+			const float gy = __fmul_rn((float) (int) (nd.gy - cy), p.scale);
+			const float gz = __fmul_rn((float) (int) (nd.gz - cz), p.scale);
 			const float lim = 0.6f * nd.size;
 			if (fabsf(gx) < lim + hx && fabsf(gy) < lim + hy && fabsf(gz) < lim + hz) want = true;
-			bool open = want;
+			// a bundle below the top level is never a monopole: the reference
+			// interacts its particles whenever the walk reaches it
+			// (tree_accel.c:221-243, tree_periodic.c:228-251)
+			const bool force_open = nd.nchild < 0 && node >= p.ntop;
+			bool open = want || force_open;
 			if (EWALD && want) {
 				// open only when the node straddles the half-box plane for some
 				// target, or is larger than 0.2 L (tree_periodic.c:158-172, 278-310)
 				const float dl = 0.5f * (p.box - nd.size);
-				open = fabsf(gx) + hx > dl || fabsf(gy) + hy > dl || fabsf(gz) + hz > dl
-				    || nd.size > 0.2f * p.box;
+				open = force_open || fabsf(gx) + hx > dl || fabsf(gy) + hy > dl
+				    || fabsf(gz) + hz > dl || nd.size > 0.2f * p.box;
 			}
 			if (!open) {
 				accept = true;
@@ -424,9 +431,9 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 				bool w = false;
 				if (have) {
 					const int64_t jp = (int64_t) q.x + j;
-					e.x = (float) (int) (ix[jp] - cx) * p.scale;
-					e.y = (float) (int) (iy[jp] - cy) * p.scale;
-					e.z = (float) (int) (iz[jp] - cz) * p.scale;
+					e.x = __fmul_rn((float) (int) (ix[jp] - cx), p.scale);
+					e.y = __fmul_rn((float) (int) (iy[jp] - cy), p.scale);
+					e.z = __fmul_rn((float) (int) (iz[jp] - cz), p.scale);
 					e.w = p.gravity * mass_f[jp];
 					w = !EWALD && p.periodic
 					 && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz);
@@ -448,6 +455,7 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 				if (tw) S.wlist[nw + __popc(m2 & lt)] = e;
 				nl += __popc(m1);
 				nw += __popc(m2);
+				__syncwarp();
 			}
 		}
 		__syncwarp();

@@ -12,6 +12,7 @@ import ctypes as C
 import numpy as np
 
 from . import lib
+from .ics import GRAVITY
 
 TVG_OK = 0
 ERRORS = {1: "TVG_E_CUDA", 2: "TVG_E_NOMEM", 3: "TVG_E_TREE_FULL", 4: "TVG_E_TIMEOUT",
@@ -67,7 +68,7 @@ class GravityContext:
     """Device context of the gravity hot path (tvg_init ... tvg_finalize)."""
 
     def __init__(self, max_particles, float_bytes=4, periodic=False, boxsize=0.0,
-                 gravity=43007.1, softening=0.01, open_bh=0.25, open_rel=0.005,
+                 gravity=GRAVITY, softening=0.01, open_bh=0.25, open_rel=0.005,
                  vector_size=64, flags=0, device=0):
         self.lib = lib()
         self.fb = float_bytes
