@@ -1,0 +1,387 @@
+#!/usr/bin/env python3
+"""Tree-force throughput of the Tandav gravity hot path on B200.
+
+Workload (the reference's headline configuration, synthetic): a periodic
+cosmological box of 256^3 particles, 100 Mpc/h, Zel'dovich displacements at
+z = 50 from a seeded Gaussian field (Eisenstein & Hu 1998 P(k)), softening
+1/30 of the mean spacing. One step = one tree-force evaluation of all
+particles: Peano-Hilbert keys, sort of every particle field, top nodes, tree
+build, the gravity walk with the relative opening criterion (errtol 0.005,
+|a_old| from an untimed Barnes-Hut prepare pass, as src/accel.c:51-71 does)
+and the Ewald periodic correction walk.
+
+Our arm: the group form (FP32 integer-offset walk, warp per PH group) with
+the tabulated Ewald correction, particles resident in HBM (`value`), and the
+same step through the C ABI with host buffers (`e2e`). The plain GPU form
+(the reference algorithm, one thread per particle, exact moments) is timed on
+a strided subset of the particles and reported beside it.
+`--impl reference`: the unmodified reference C code (oracle/_ref timing
+build) on the host cores, the walk timed on a strided subset.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+       (for N > 1 launched by torch.distributed.run, one independent replica
+        per GPU: the path has no data-path collective on one GPU's box)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "tree-force particles/s at 256^3 periodic: chosen vs plain GPU form @≤1e-3 rms err"
+UNIT = "particles/s"
+FLOP_PER_GRAV = 20.0      # per monopole / particle interaction (SURVEY measurement convention)
+FLOP_PER_EWALD = 60.0     # per table-Ewald interaction
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nside", type=int, default=256)
+    ap.add_argument("--plain-stride", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    """Barrier and max over ranks (gloo on host tensors); a no-op at N = 1."""
+
+    def __init__(self, ws):
+        self.ws = ws
+        if ws > 1:
+            import datetime
+            import torch.distributed as td
+            td.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.td = td
+
+    def barrier(self):
+        if self.ws > 1:
+            self.td.barrier()
+
+    def max(self, v):
+        if self.ws == 1:
+            return v
+        import torch
+        t = torch.tensor([float(v)], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if self.ws == 1:
+            return v
+        import torch
+        t = torch.tensor([float(v)], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            self.td.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def make_ics(nside, seed):
+    from tandav_b200 import ics
+    return ics.zeldovich_box(n_side=nside, seed=seed)
+
+
+def cpu_reference(p, cores, target_s=20.0):
+    """The reference's OpenMP path (oracle/_ref/per_f32_t) on a strided sample
+    of active particles; returns the step rate extrapolated to all particles."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import refrun
+    if not refrun.available("per_f32_t"):
+        return None, "reference timing build missing (make -C oracle ref)"
+    # ~4 ms of one core per particle for the relative walk at this size
+    stride = max(8, int(p.n / (target_s * cores / 4e-3)))
+    stride = 1 << int(round(math.log2(stride)))
+    t0 = time.time()
+    r = refrun.run("per_f32_t", "force", p.pos, p.vel, p.mass, box=p.box, softening=p.softening,
+                   flags=3 | 4 | (stride << 8), threads=cores, timeout=3000)
+    wall = time.time() - t0
+    tm = r["timings"]      # ewald_init, dd, build, bh, bh_ew, rel, rel_ew, threads
+    n_sample = len(range(0, p.n, stride))
+    t_step = tm[1] + tm[2] + tm[5] * (p.n / n_sample)
+    return {
+        "value": p.n / t_step, "unit": UNIT, "cores": int(tm[7]), "kind": "reference",
+        "sample": (f"unmodified reference (per_f32 timing build, -O3 -march=x86-64-v3) on the "
+                   f"same {p.n}-particle box: domain decomposition {tm[1]:.2f} s and tree build "
+                   f"{tm[2]:.2f} s for all particles, relative-criterion walk incl. Ewald "
+                   f"{tm[5]:.2f} s for every {stride}th particle ({n_sample}), extrapolated "
+                   f"linearly to all; run wall {wall:.0f} s"),
+    }, None
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_info()
+    if rank != 0:
+        return 0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    p = make_ics(args.nside, 1234)
+    cb, err = cpu_reference(p, cores)
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    out = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": 0,
+        "steps": 1, "warmup": 0, "ms_per_step": 1e3 * p.n / cb["value"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded Zel'dovich box (see config)",
+        "config": workload_config(args, p, ws),
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "one sampled force evaluation (the CPU step is minutes long at this size)",
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def workload_config(args, p, ws):
+    return {
+        "workload": f"zeldovich_{args.nside}^3_periodic_z50",
+        "n_particles": int(p.n), "box_mpc_h": 100.0, "z_start": 50.0,
+        "softening_kpc_h": round(float(p.softening), 4),
+        "criterion": "relative, TREE_OPEN_PARAM_REL 0.005, |a_old| from a BH (theta^2 0.25) pass",
+        "ewald": "65^3 table, trilinear",
+        "form": "group: warp per 32-particle PH group, FP32 on 32-bit integer box offsets",
+        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+        "l2": "inputs larger than L2 (16.7M particles, ~2 GB of particle state)",
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    ws, rank, local = dist_info()
+    dist = Dist(ws)
+    from tandav_b200 import gravity as G
+
+    p = make_ics(args.nside, 1234 + rank)
+    n = p.n
+    ctx = G.GravityContext(n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
+                           device=local)
+    parts = G.WALK_GRAVITY | G.WALK_EWALD
+    ctx.upload(p.pos, p.mass)
+    ctx.set_domain((0.0, 0.0, 0.0), p.box)
+    ctx.ewald_init()
+    fp32_peak = ctx.fp32_peak(ms_target=1500.0)
+
+    # prepare step (accel.c:51-71): BH pass, |a| -> Last_Acc_Mag
+    ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
+    ctx.save_last_accel()
+    for _ in range(args.warmup):
+        ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
+
+    # ---- device-resident timed region
+    clocks = ClockSampler(local)
+    dist.barrier()
+    clocks.start()
+    l0 = ctx.launch_count()
+    ctx.timer_start()
+    walk_ms, ew_ms, grav_i, ew_i, phases = 0.0, 0.0, 0.0, 0.0, []
+    for _ in range(args.steps):
+        ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
+        ph = ctx.phase_times()
+        phases.append(ph)
+        walk_ms += ph["walk"]
+        ew_ms += ph["ewald"]
+        g, e = ctx.walk_counters()
+        grav_i += g
+        ew_i += e
+    total_ms = ctx.timer_stop()
+    launches = ctx.launch_count() - l0
+    clk = clocks.stop()
+    dist.barrier()
+    t_step = dist.max(total_ms / args.steps) / 1e3
+    value = dist.sum(n) / t_step
+
+    # ---- end to end through the C ABI with host buffers (pinned)
+    ids = G.PinnedArray((n,), np.uint32)
+    ctx.download_into(ids=ids.array)
+    last = ctx.download(G.F_LAST_ACC)["last_acc_mag"]
+    h_pos = G.PinnedArray((3, n), np.float32)
+    h_mass = G.PinnedArray((n,), np.float32)
+    h_last = G.PinnedArray((n,), np.float32)
+    h_acc = G.PinnedArray((3, n), np.float32)
+    h_ids = G.PinnedArray((n,), np.uint32)
+    h_oid = G.PinnedArray((n,), np.uint32)
+    h_ids.array[:] = np.arange(n, dtype=np.uint32)
+    h_pos.array[:] = p.pos.astype(np.float32)
+    h_mass.array[:] = p.mass.astype(np.float32)
+    h_last.array[ids.array] = last            # back to the host (input) order
+    dist.barrier()
+    ctx.timer_start()
+    for _ in range(args.steps):
+        ctx.upload_fields(n, pos=h_pos.array, mass=h_mass.array, last_acc=h_last.array,
+                          ids=h_ids.array)
+        ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
+        ctx.download_into(grav_acc=h_acc.array, ids=h_oid.array)
+    e2e_ms = ctx.timer_stop()
+    dist.barrier()
+    t_e2e = dist.max(e2e_ms / args.steps) / 1e3
+    e2e_value = dist.sum(n) / t_e2e
+    h2d = n * 4 * 6        # pos[3], mass, last |a|, id
+    d2h = n * 4 * 4        # grav_acc[3], id (the order of the result)
+
+    # ---- roofline of the dominant kernel (the gravity walk)
+    achieved = FLOP_PER_GRAV * grav_i / (walk_ms * 1e-3) / 1e12
+    roofline = {
+        "kernel": "k_walk_group<false> (gravity walk)", "bound": "fp32",
+        "achieved": round(achieved, 3), "peak": round(fp32_peak, 3), "unit": "TFLOP/s",
+        "frac": round(achieved / fp32_peak, 4) if fp32_peak > 0 else None,
+        "peak_source": "measured FFMA loop on this GPU (1.5 s, sustained under the power cap)",
+        "traffic": None,
+        "algorithmic": f"{FLOP_PER_GRAV:.0f} flop x {grav_i / args.steps / n:.0f} interactions/particle",
+    }
+    prof = ROOT / "profiles" / "walk_group_traffic.json"
+    if prof.exists():
+        try:
+            roofline["traffic"] = json.loads(prof.read_text()).get("bytes_per_launch_256")
+        except (OSError, ValueError):
+            pass
+
+    # ---- plain GPU form on a strided sample of active particles
+    plain = None
+    if not args.no_plain:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.timer_start()
+        ctx.peano_keys()
+        ctx.sort_particles(want_perm=False)
+        ctx.top_nodes()
+        ctx.tree_build(exact_moments=True)
+        pre_ms = ctx.timer_stop()
+        # same |a_old| as the group steps: BH plain pass on the sample first
+        act = np.arange(0, n, args.plain_stride, dtype=np.int32)
+        ctx.set_active(act)
+        ctx.zero_accel()
+        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+        ctx.save_last_accel()
+        ctx.timer_start()
+        ctx.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
+        w_ms = ctx.timer_stop()
+        g_pl, e_pl = ctx.walk_counters()
+        t_plain = pre_ms * 1e-3 + w_ms * 1e-3 * n / len(act)
+        plain = {"value": n / t_plain, "unit": UNIT, "form": "plain (reference walk, FP32 Float)",
+                 "sample": f"walk of every {args.plain_stride}th particle ({len(act)}), "
+                           f"keys/sort/build for all, extrapolated",
+                 "interactions_per_particle": round((g_pl + e_pl) / len(act), 1),
+                 "speedup_group_over_plain": round(value / ws / (n / t_plain), 2)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        cpu, err = cpu_reference(p, cores)
+        if cpu is None:
+            cpu = {"value": None, "unavailable": err}
+
+    if rank == 0:
+        ph = {k: round(statistics.mean(x[k] for x in phases), 3) for k in phases[0]}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded Zel'dovich box, EH98 P(k), sigma8 0.8, n_s 0.96, z 50",
+            "config": workload_config(args, p, ws),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": t_e2e * 1e3},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "phases_ms": ph,
+            "interactions_per_particle": {"gravity": round(grav_i / args.steps / n, 1),
+                                          "ewald": round(ew_i / args.steps / n, 1)},
+            "plain_form": plain,
+        }
+        print(json.dumps(out))
+    for a in (ids, h_pos, h_mass, h_last, h_acc, h_ids, h_oid):
+        a.free()
+    ctx.close()
+    dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

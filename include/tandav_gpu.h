@@ -202,9 +202,30 @@ int tvg_zero_accel(tvg_context *ctx);
 int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
                    int32_t ewald_kind);
 
+/* Active_Particle_List / NActive_Particles (src/timestep.c:280-299): the walks
+ * compute forces for these particles only (indices into the current, sorted
+ * order, ascending). NULL selects all particles. Sorting resets it to all. */
+int tvg_set_active(tvg_context *ctx, const int32_t *list, int64_t n_active);
+
 /* Per-phase device times (ms) of the last calls, CUDA events on the
  * context stream: [keys, sort, top, build, walk, ewald walk, total]. */
 int tvg_phase_times(tvg_context *ctx, double *ms, int32_t n);
+
+/* Device-timed region on the context stream: stop = 0 records the start
+ * event, stop = 1 records the end event, waits for it and returns the
+ * elapsed milliseconds in *ms. */
+int tvg_timer(tvg_context *ctx, int32_t stop, double *ms);
+
+/* Number of kernels this context has launched since it was created. */
+int tvg_launch_count(tvg_context *ctx, int64_t *count);
+
+/* Page-locked host memory for transfers that overlap with device work. */
+int tvg_host_alloc(size_t bytes, void **ptr);
+int tvg_host_free(void *ptr);
+
+/* Measured FP32 FFMA throughput of the device (TFLOP/s, FMA = 2 flop) over
+ * `ms_target` milliseconds: the denominator of the walk's roofline. */
+int tvg_fp32_peak(tvg_context *ctx, double ms_target, double *tflops);
 
 /* Counters of the last walk: total gravity and Ewald interactions. */
 int tvg_walk_counters(tvg_context *ctx, double *grav_interactions, double *ewald_interactions);

@@ -47,6 +47,7 @@ struct dump_topnode {
 };
 
 static FILE *Out = NULL;
+static bool Dump_Bulk = true;     /* false: timing run, no per-particle dumps */
 
 static void put(const char *name, const void *data, int64_t nbytes)
 {
@@ -167,6 +168,7 @@ static void zero_accumulators(void)
 /* Dump Acc/Grav_Acc/Cost as doubles under a name prefix. */
 static void dump_forces(const char *prefix, int64_t n)
 {
+	if (!Dump_Bulk) return;
 	double *buf = malloc(3 * n * sizeof(double));
 	char name[16];
 	for (int k = 0; k < 3; k++)
@@ -191,7 +193,7 @@ static void init_memory(int64_t n)
 	size_t tree_bytes = sizeof(struct Tree_Node);
 	/* per-thread scratch: the PH reorder needs N*8 bytes (peano.c:56-58) and
 	 * a subtree is built in the buffer when it fits (tree_build.c:65-96) */
-	double per_thread = fmax(1.05 * n * 8.0, 2.0 * n * tree_bytes) + (16 << 20);
+	double per_thread = fmax(1.05 * n * 8.0, 0.1 * n * tree_bytes) + (16 << 20);
 	Param.Buffer_Size = (int) ceil(per_thread * NThreads / (1 << 20));
 	double pool = (double) n * 1.3 * (sizeof_P + 64.0 + 16.0) + 1.2 * 0.3 * n * tree_bytes;
 	Param.Max_Mem_Size = Param.Buffer_Size + (int) ceil(pool / (1 << 20)) + 512;
@@ -273,8 +275,19 @@ static int run_force(const struct input *in)
 		t_build = now() - t0;
 	}
 
+	/* bounded CPU sample (flags bits 8..31 = stride s > 1): the walks run for
+	 * every s-th particle only, as a reduced Active_Particle_List */
+	const int stride = (flags >> 8) > 1 ? (flags >> 8) : 1;
+	if (stride > 1) {
+		int na = 0;
+		for (int64_t i = 0; i < n; i += stride) Active_Particle_List[na++] = (int) i;
+		NActive_Particles = na;
+	}
+	const bool dump_bulk = (flags & 4) == 0;
+	Dump_Bulk = dump_bulk;
+
 	/* ---- dump decomposition and tree ---- */
-	{
+	if (dump_bulk) {
 		put("domain_size", &Domain.Size, sizeof(double));
 		put("domain_origin", Domain.Origin, 3 * sizeof(double));
 		uint32_t *ids = malloc(n * sizeof(uint32_t));
@@ -331,7 +344,7 @@ static int run_force(const struct input *in)
 					for (int64_t i = 0; i < n; i++) acc_bh[k * n + i] = P.Acc[k][i];
 			}
 			#pragma omp barrier
-			if (periodic) {
+			if (periodic && dump_bulk) {
 				zero_accumulators();
 				#pragma omp master
 				t0 = now();
@@ -360,7 +373,7 @@ static int run_force(const struct input *in)
 			#pragma omp master
 			{ t_rel = now() - t0; dump_forces("rel", n); }
 			#pragma omp barrier
-			if (periodic) {
+			if (periodic && dump_bulk) {
 				zero_accumulators();
 				#pragma omp master
 				t0 = now();
@@ -372,7 +385,7 @@ static int run_force(const struct input *in)
 			}
 		}
 	}
-	{
+	if (dump_bulk) {
 		double *lam = malloc(n * sizeof(double));
 		for (int64_t i = 0; i < n; i++) lam[i] = P.Last_Acc_Mag[i];
 		put("last_acc_mag", lam, n * sizeof(double));

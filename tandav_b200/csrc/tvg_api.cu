@@ -222,9 +222,14 @@ extern "C" int tvg_upload(tvg_context *ctx, int64_t n, const tvg_particles *p, u
 		// stage the 16-byte keys in the prefix-sum buffer (32 * (cap + 1) bytes)
 		uint64_t *k16 = (uint64_t *) ctx->pref;
 		TVG_CUDA(ctx, cudaMemcpyAsync(k16, p->key, 16 * n, cudaMemcpyHostToDevice, ctx->stream));
-		k_split_keys<<<tvg_blocks(n, 256), 256, 0, ctx->stream>>>(n, k16, ctx->key_hi, ctx->key_lo);
+		k_split_keys<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(n, k16, ctx->key_hi, ctx->key_lo);
 	}
-	if (fields & TVG_F_POS) { ctx->sorted = false; ctx->have_tree = false; ctx->have_top = false; }
+	if (fields & TVG_F_POS) {
+		ctx->sorted = false;
+		ctx->have_tree = false;
+		ctx->have_top = false;
+		ctx->use_active = false;
+	}
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
 	return TVG_OK;
@@ -245,7 +250,7 @@ extern "C" int tvg_download(tvg_context *ctx, tvg_particles *p, uint32_t fields)
 	if (fields & TVG_F_KEY) {
 		if (!p->key) return tvg_fail(ctx, TVG_E_BADINPUT, "download: key is NULL");
 		uint64_t *k16 = (uint64_t *) ctx->pref;   // 32*(cap+1) bytes >= 16*n
-		k_join_keys<<<tvg_blocks(n, 256), 256, 0, ctx->stream>>>(n, ctx->key_hi, ctx->key_lo, k16);
+		k_join_keys<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(n, ctx->key_hi, ctx->key_lo, k16);
 		TVG_CUDA(ctx, cudaMemcpyAsync(p->key, k16, 16 * n, cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	TVG_CUDA(ctx, cudaGetLastError());
@@ -289,6 +294,7 @@ extern "C" int tvg_sort_particles(tvg_context *ctx, uint32_t *perm)
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	TVG_CHECK(tvg_impl_sort(ctx, perm));
 	ctx->sorted = true;
+	ctx->use_active = false;
 	ctx->have_tree = false;
 	return tvg_sync_status(ctx, "sort");
 }
@@ -397,5 +403,107 @@ extern "C" int tvg_walk_counters(tvg_context *ctx, double *g, double *e)
 	if (!ctx) return TVG_E_BADINPUT;
 	if (g) *g = ctx->last_counts[0];
 	if (e) *e = ctx->last_counts[1];
+	return TVG_OK;
+}
+
+__global__ void k_ffma_peak(float *out, int iters, float a, float b)
+{
+	// 8 independent FMA chains per thread keep every FP32 lane busy
+	float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5,
+	      x6 = x0 + 6, x7 = x0 + 7;
+	for (int i = 0; i < iters; i++) {
+#pragma unroll 16
+		for (int j = 0; j < 16; j++) {
+			x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+			x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+		}
+	}
+	const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+	if (s == 1234.5f) out[blockIdx.x] = s;     // keeps the chains alive
+}
+
+extern "C" int tvg_fp32_peak(tvg_context *ctx, double ms_target, double *tflops)
+{
+	if (!ctx || !tflops) return TVG_E_BADINPUT;
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	int nsm = 0;
+	TVG_CUDA(ctx, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+	const int blocks = nsm * 8, threads = 256;
+	float *out = (float *) ctx->scan_tmp;
+	int iters = 256;
+	double best = 0;
+	int measured = 0;
+	for (int rep = 0; rep < 40 && measured < 3; rep++) {
+		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[14], ctx->stream));
+		k_ffma_peak<<<TVG_CNT(ctx, blocks), threads, 0, ctx->stream>>>(out, iters, 0.999999f, 1e-7f);
+		TVG_CUDA(ctx, cudaGetLastError());
+		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[15], ctx->stream));
+		TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[15]));
+		float ms = 0;
+		TVG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[14], ctx->ev[15]));
+		const double flop = 2.0 * 8 * 16 * (double) iters * blocks * threads;
+		if (ms > 0.5 * ms_target) {
+			best = fmax(best, flop / (ms * 1e-3) / 1e12);
+			measured++;
+		} else {
+			iters = (int) fmin(iters * 2.0, 1 << 26);
+		}
+	}
+	*tflops = best;
+	return TVG_OK;
+}
+
+extern "C" int tvg_set_active(tvg_context *ctx, const int32_t *list, int64_t n_active)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	if (!list) {
+		ctx->use_active = false;
+		ctx->n_active = ctx->n;
+		return TVG_OK;
+	}
+	if (n_active < 0 || n_active > ctx->n) return tvg_fail(ctx, TVG_E_BADINPUT, "n_active out of range");
+	if (!ctx->active) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->active, 4 * (size_t) ctx->cap));
+	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->active, list, 4 * (size_t) n_active, cudaMemcpyHostToDevice,
+	                              ctx->stream));
+	TVG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+	ctx->use_active = true;
+	ctx->n_active = n_active;
+	return TVG_OK;
+}
+
+extern "C" int tvg_launch_count(tvg_context *ctx, int64_t *count)
+{
+	if (!ctx || !count) return TVG_E_BADINPUT;
+	*count = ctx->launches;
+	return TVG_OK;
+}
+
+extern "C" int tvg_host_alloc(size_t bytes, void **ptr)
+{
+	if (!ptr) return TVG_E_BADINPUT;
+	cudaError_t e = cudaMallocHost(ptr, bytes ? bytes : 16);
+	if (e != cudaSuccess) { cudaGetLastError(); *ptr = nullptr; return TVG_E_NOMEM; }
+	return TVG_OK;
+}
+
+extern "C" int tvg_host_free(void *ptr)
+{
+	return cudaFreeHost(ptr) == cudaSuccess ? TVG_OK : TVG_E_CUDA;
+}
+
+extern "C" int tvg_timer(tvg_context *ctx, int32_t stop, double *ms)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	if (!stop) {
+		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[6], ctx->stream));
+		return TVG_OK;
+	}
+	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[7], ctx->stream));
+	TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[7]));
+	float f = 0;
+	TVG_CUDA(ctx, cudaEventElapsedTime(&f, ctx->ev[6], ctx->ev[7]));
+	if (ms) *ms = f;
 	return TVG_OK;
 }

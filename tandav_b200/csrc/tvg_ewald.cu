@@ -84,11 +84,11 @@ int tvg_impl_ewald_init(tvg_context *ctx)
 	if (!ctx->ewald_raw) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->ewald_raw, 4 * 8 * npt));
 	const unsigned nb = tvg_blocks((int64_t) npt, 128);
 	if (ctx->cfg.float_bytes == 4)
-		k_ewald_table<float><<<nb, 128, 0, ctx->stream>>>(
+		k_ewald_table<float><<<TVG_CNT(ctx, nb), 128, 0, ctx->stream>>>(
 		    ctx->cfg.boxsize, (float *) ctx->ewald_f[0], (float *) ctx->ewald_f[1],
 		    (float *) ctx->ewald_f[2], (float *) ctx->ewald_f[3], ctx->ewald_raw);
 	else
-		k_ewald_table<double><<<nb, 128, 0, ctx->stream>>>(
+		k_ewald_table<double><<<TVG_CNT(ctx, nb), 128, 0, ctx->stream>>>(
 		    ctx->cfg.boxsize, (double *) ctx->ewald_f[0], (double *) ctx->ewald_f[1],
 		    (double *) ctx->ewald_f[2], (double *) ctx->ewald_f[3], ctx->ewald_raw);
 	TVG_CUDA(ctx, cudaGetLastError());
@@ -132,12 +132,12 @@ extern "C" int tvg_upload_ewald_table(tvg_context *ctx, const void *fx, const vo
 	const unsigned nb = tvg_blocks((int64_t) npt, 256);
 	if (ctx->cfg.float_bytes == 4) {
 		const float *r = (const float *) tmp;
-		k_ewald_from_raw<float><<<nb, 256, 0, ctx->stream>>>(
+		k_ewald_from_raw<float><<<TVG_CNT(ctx, nb), 256, 0, ctx->stream>>>(
 		    ctx->cfg.boxsize, r, r + npt, r + 2 * npt, r + 3 * npt, (float *) ctx->ewald_f[0],
 		    (float *) ctx->ewald_f[1], (float *) ctx->ewald_f[2], (float *) ctx->ewald_f[3], ctx->ewald_raw);
 	} else {
 		const double *r = (const double *) tmp;
-		k_ewald_from_raw<double><<<nb, 256, 0, ctx->stream>>>(
+		k_ewald_from_raw<double><<<TVG_CNT(ctx, nb), 256, 0, ctx->stream>>>(
 		    ctx->cfg.boxsize, r, r + npt, r + 2 * npt, r + 3 * npt, (double *) ctx->ewald_f[0],
 		    (double *) ctx->ewald_f[1], (double *) ctx->ewald_f[2], (double *) ctx->ewald_f[3],
 		    ctx->ewald_raw);
@@ -169,10 +169,10 @@ extern "C" int tvg_download_ewald_table(tvg_context *ctx, void *fx, void *fy, vo
 	for (int c = 0; c < 4; c++) {
 		if (!outs[c]) continue;
 		if (ctx->cfg.float_bytes == 4)
-			k_ewald_raw_float<float><<<tvg_blocks(npt, 256), 256, 0, ctx->stream>>>(ctx->ewald_raw,
+			k_ewald_raw_float<float><<<TVG_CNT(ctx, tvg_blocks(npt, 256)), 256, 0, ctx->stream>>>(ctx->ewald_raw,
 			                                                                          (float *) tmp, c, npt);
 		else
-			k_ewald_raw_float<double><<<tvg_blocks(npt, 256), 256, 0, ctx->stream>>>(ctx->ewald_raw,
+			k_ewald_raw_float<double><<<TVG_CNT(ctx, tvg_blocks(npt, 256)), 256, 0, ctx->stream>>>(ctx->ewald_raw,
 			                                                                           (double *) tmp, c, npt);
 		cudaError_t e = cudaMemcpyAsync(outs[c], tmp, tvg_fsize(ctx) * npt, cudaMemcpyDeviceToHost,
 		                                ctx->stream);

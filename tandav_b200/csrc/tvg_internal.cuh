@@ -30,6 +30,9 @@
 			                #call, cudaGetErrorString(e_));                         \
 	} while (0)
 
+// wraps the grid argument of every kernel launch: counts the launch
+#define TVG_CNT(ctx, grid) ((ctx)->launches++, (grid))
+
 #define TVG_CHECK(expr)                                                            \
 	do {                                                                           \
 		int rc_ = (expr);                                                          \
@@ -131,6 +134,12 @@ struct tvg_context {
 	int64_t ngroups = 0;
 	int32_t *work_counter = nullptr;
 	double *counters = nullptr;        // device interaction counters [4]
+
+	// active particles (Active_Particle_List); all particles when !use_active
+	int32_t *active = nullptr;
+	int64_t n_active = 0;
+	bool use_active = false;
+	int64_t launches = 0;              // kernels launched by this context
 
 	// timings
 	cudaEvent_t ev[16];

@@ -124,12 +124,12 @@ int tvg_impl_keys(tvg_context *ctx, bool reversed)
 	const double fac = (double) (1ULL << 63) / ctx->dsize;
 	const unsigned nb = tvg_blocks(n, 256);
 	if (ctx->cfg.float_bytes == 4)
-		k_ph_keys<float><<<nb, 256, 0, ctx->stream>>>(
+		k_ph_keys<float><<<TVG_CNT(ctx, nb), 256, 0, ctx->stream>>>(
 		    n, (const float *) ctx->f[FS_POS0], (const float *) ctx->f[FS_POS1],
 		    (const float *) ctx->f[FS_POS2], ctx->origin[0], ctx->origin[1], ctx->origin[2], fac,
 		    reversed, ctx->key_hi, ctx->key_lo, ctx->status);
 	else
-		k_ph_keys<double><<<nb, 256, 0, ctx->stream>>>(
+		k_ph_keys<double><<<TVG_CNT(ctx, nb), 256, 0, ctx->stream>>>(
 		    n, (const double *) ctx->f[FS_POS0], (const double *) ctx->f[FS_POS1],
 		    (const double *) ctx->f[FS_POS2], ctx->origin[0], ctx->origin[1], ctx->origin[2], fac,
 		    reversed, ctx->key_hi, ctx->key_lo, ctx->status);

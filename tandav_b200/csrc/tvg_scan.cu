@@ -83,17 +83,17 @@ static int scan_rec(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n
 {
 	const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
 	if (nb <= 1) {
-		k_scan_apply<<<1, SCAN_THREADS, 0, ctx->stream>>>(in, out, n, nullptr);
+		k_scan_apply<<<TVG_CNT(ctx, 1), SCAN_THREADS, 0, ctx->stream>>>(in, out, n, nullptr);
 		TVG_CUDA(ctx, cudaGetLastError());
 		return TVG_OK;
 	}
 	if ((size_t) (2 * nb) > tmp_elems)
 		return tvg_fail(ctx, TVG_E_NOMEM, "scan scratch too small (%lld blocks)", (long long) nb);
 	int32_t *sums = tmp, *offs = tmp + nb;
-	k_scan_reduce<<<(unsigned) nb, SCAN_THREADS, 0, ctx->stream>>>(in, n, sums);
+	k_scan_reduce<<<TVG_CNT(ctx, (unsigned) nb), SCAN_THREADS, 0, ctx->stream>>>(in, n, sums);
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CHECK(scan_rec(ctx, sums, offs, nb, tmp + 2 * nb, tmp_elems - 2 * nb));
-	k_scan_apply<<<(unsigned) nb, SCAN_THREADS, 0, ctx->stream>>>(in, out, n, offs);
+	k_scan_apply<<<TVG_CNT(ctx, (unsigned) nb), SCAN_THREADS, 0, ctx->stream>>>(in, out, n, offs);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }

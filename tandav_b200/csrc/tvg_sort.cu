@@ -227,9 +227,9 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 	if (n == 0) return TVG_OK;
 	cudaStream_t s = ctx->stream;
 	const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
-	k_iota<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->perm);
+	k_iota<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->perm);
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->digit_count, 0, 4 * 8 * 256, s));
-	k_digit_counts<<<296, 512, 0, s>>>(n, ctx->key_hi, ctx->digit_count);
+	k_digit_counts<<<TVG_CNT(ctx, 296), 512, 0, s>>>(n, ctx->key_hi, ctx->digit_count);
 	TVG_CUDA(ctx, cudaGetLastError());
 	uint32_t h_count[8 * 256];
 	TVG_CUDA(ctx, cudaMemcpyAsync(h_count, ctx->digit_count, sizeof(h_count), cudaMemcpyDeviceToHost, s));
@@ -249,11 +249,11 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 			if (h_count[d * 256 + b] == (uint32_t) n) constant = true;
 		if (constant) continue;
 		const int shift = 8 * d;
-		k_tile_hist<<<(unsigned) ntiles, RS_THREADS, 0, s>>>(n, shift, kin, ctx->sort_hist, ntiles);
+		k_tile_hist<<<TVG_CNT(ctx, (unsigned) ntiles), RS_THREADS, 0, s>>>(n, shift, kin, ctx->sort_hist, ntiles);
 		TVG_CUDA(ctx, cudaGetLastError());
 		TVG_CHECK(tvg_device_scan_i32(ctx, (const int32_t *) ctx->sort_hist, (int32_t *) ctx->sort_off,
 		                              256 * ntiles, nullptr));
-		k_radix_scatter<<<(unsigned) ntiles, RS_THREADS, smem, s>>>(n, shift, kin, vin, kout, vout,
+		k_radix_scatter<<<TVG_CNT(ctx, (unsigned) ntiles), RS_THREADS, smem, s>>>(n, shift, kin, vin, kout, vout,
 		                                                            ctx->sort_off, ntiles);
 		TVG_CUDA(ctx, cudaGetLastError());
 		uint64_t *kt = kin; kin = kout; kout = kt;
@@ -261,8 +261,8 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 	}
 	ctx->key_hi = kin; ctx->key_tmp = kout;
 	ctx->perm = vin; ctx->perm_tmp = vout;
-	k_fix_ties<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->perm);
-	k_gather_u64<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->perm, ctx->key_lo, ctx->key_tmp);
+	k_fix_ties<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->perm);
+	k_gather_u64<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->perm, ctx->key_lo, ctx->key_tmp);
 	{ uint64_t *t = ctx->key_lo; ctx->key_lo = ctx->key_tmp; ctx->key_tmp = t; }
 	GatherList g;
 	g.nf = 0;
@@ -272,7 +272,7 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 		g.bytes[g.nf] = (int) tvg_field_bytes(ctx, f);
 		g.nf++;
 	}
-	k_gather_fields<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->perm, g);
+	k_gather_fields<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->perm, g);
 	TVG_CUDA(ctx, cudaGetLastError());
 	for (int f = 0; f < FS_NFIELDS; f++) { void *t = ctx->f[f]; ctx->f[f] = ctx->falt[f]; ctx->falt[f] = t; }
 	if (perm_out)

@@ -16,6 +16,7 @@ extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, ui
 	TVG_CUDA(ctx, cudaEventRecord(ev[9], s));
 	TVG_CHECK(tvg_impl_sort(ctx, nullptr));
 	ctx->sorted = true;
+	ctx->use_active = false;
 	TVG_CUDA(ctx, cudaEventRecord(ev[10], s));
 	TVG_CHECK(tvg_impl_top_nodes(ctx));
 	ctx->have_top = true;

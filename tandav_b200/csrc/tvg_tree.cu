@@ -95,15 +95,15 @@ int tvg_impl_top_nodes(tvg_context *ctx)
 	const int64_t n = ctx->n;
 	cudaStream_t s = ctx->stream;
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->top_first, 0xFF, 4 * TVG_MAX_TOP, s));
-	k_top_first<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ctx->top_first);
+	k_top_first<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->top_first);
 	int32_t *d_nt = (int32_t *) ctx->work_counter;
 	if (ctx->cfg.float_bytes == 4)
-		k_make_top<float><<<1, 1, 0, s>>>(n, ctx->top_first, (const float *) ctx->f[FS_POS0],
+		k_make_top<float><<<TVG_CNT(ctx, 1), 1, 0, s>>>(n, ctx->top_first, (const float *) ctx->f[FS_POS0],
 		                                  (const float *) ctx->f[FS_POS1], (const float *) ctx->f[FS_POS2],
 		                                  ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
 		                                  ctx->d_top, ctx->top_count, d_nt);
 	else
-		k_make_top<double><<<1, 1, 0, s>>>(n, ctx->top_first, (const double *) ctx->f[FS_POS0],
+		k_make_top<double><<<TVG_CNT(ctx, 1), 1, 0, s>>>(n, ctx->top_first, (const double *) ctx->f[FS_POS0],
 		                                   (const double *) ctx->f[FS_POS1], (const double *) ctx->f[FS_POS2],
 		                                   ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
 		                                   ctx->d_top, ctx->top_count, d_nt);
@@ -547,7 +547,7 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 		ti.tidx[c] = t;
 		ti.big[c] = ctx->h_top[t].npart > vsize;
 	}
-	k_levels<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ti, ctx->lvl, ctx->ncnt,
+	k_levels<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ti, ctx->lvl, ctx->ncnt,
 	                                             ctx->lvl_min64, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CHECK(tvg_sync_status(ctx, "tree_build(levels)"));
@@ -558,20 +558,20 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 		                (long long) nu, (long long) ctx->ucap);
 	ctx->nu = nu;
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->u_diff, 0, 4 * (nu + 1), s));
-	k_nodes<<<tvg_blocks(n, 128), 128, 0, s>>>(n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, vsize,
+	k_nodes<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, s>>>(n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, vsize,
 	                                            ctx->u_start, ctx->u_level, ctx->u_count, ctx->u_endu,
 	                                            ctx->u_flag, ctx->u_diff);
 	TVG_CUDA(ctx, cudaGetLastError());
 	// removal marks -> survivor flags -> final (per top node) indices
 	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, nu + 1, nullptr));
-	k_survivors<<<tvg_blocks(nu + 1, 256), 256, 0, s>>>(nu, ctx->u_final, ctx->u_diff);
+	k_survivors<<<TVG_CNT(ctx, tvg_blocks(nu + 1, 256)), 256, 0, s>>>(nu, ctx->u_final, ctx->u_diff);
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, nu + 1, nullptr));
 	// placement of the subtrees
 	int32_t *d_toff = (int32_t *) ctx->scan_tmp;     // scan scratch is free here
 	int32_t *d_nsurv = d_toff + 64;
 	int64_t *d_total = (int64_t *) (d_toff + 128);
-	k_place_subtrees<<<1, 1, 0, s>>>(ctx->ntop, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, d_toff,
+	k_place_subtrees<<<TVG_CNT(ctx, 1), 1, 0, s>>>(ctx->ntop, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, d_toff,
 	                                  d_nsurv, d_total);
 	TVG_CUDA(ctx, cudaGetLastError());
 	int32_t h_toff[64], h_nsurv[64];
@@ -598,25 +598,25 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 		ctx->h_nsurv[t] = tp.nsurv[t];
 	}
 	TNode<F> *tree = (TNode<F> *) ctx->tree;
-	k_emit_nodes<F><<<tvg_blocks(nu, 256), 256, 0, s>>>(
+	k_emit_nodes<F><<<TVG_CNT(ctx, tvg_blocks(nu, 256)), 256, 0, s>>>(
 	    nu, n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, ctx->u_start, ctx->u_level, ctx->u_count,
 	    ctx->u_endu, ctx->u_flag, ctx->u_diff, ctx->u_final, ctx->key_hi, ctx->key_lo, tp, tree,
 	    ctx->tree_u, tree_parent, ctx->tcap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
-	k_small_parent<<<tvg_blocks(n, 256), 256, 0, s>>>(n, ctx->key_hi, ti, tree_parent);
+	k_small_parent<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ti, tree_parent);
 	TVG_CUDA(ctx, cudaGetLastError());
 	if (total > 0) {
-		k_node_pos<F><<<tvg_blocks(total, 128), 128, 0, s>>>(total, tree, ctx->tree_u, ctx->u_start,
+		k_node_pos<F><<<TVG_CNT(ctx, tvg_blocks(total, 128)), 128, 0, s>>>(total, tree, ctx->tree_u, ctx->u_start,
 		                                                       x, y, z, ctx->d_top, ctx->dsize);
 		const int exact = (flags & TVG_BUILD_EXACT_MOMENTS) ? 1 : 0;
-		k_moments_seq<F><<<tvg_blocks(total, 128), 128, 0, s>>>(total, tree, ctx->tree_u,
+		k_moments_seq<F><<<TVG_CNT(ctx, tvg_blocks(total, 128)), 128, 0, s>>>(total, tree, ctx->tree_u,
 		                                                          ctx->u_start, x, y, z, m, exact);
 		if (!exact)
-			k_moments_warp<F><<<tvg_blocks(total * 32, 256), 256, 0, s>>>(total, tree, ctx->tree_u,
+			k_moments_warp<F><<<TVG_CNT(ctx, tvg_blocks(total * 32, 256)), 256, 0, s>>>(total, tree, ctx->tree_u,
 			                                                               ctx->u_start, x, y, z, m);
 		TVG_CUDA(ctx, cudaGetLastError());
 	}
-	k_finish_top<F><<<1, 64, 0, s>>>(ctx->ntop, ctx->d_top, tree, d_nsurv, x, y, z, m, vsize);
+	k_finish_top<F><<<TVG_CNT(ctx, 1), 64, 0, s>>>(ctx->ntop, ctx->d_top, tree, d_nsurv, x, y, z, m, vsize);
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
 	                              cudaMemcpyDeviceToHost, s));

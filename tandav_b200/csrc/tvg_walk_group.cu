@@ -291,12 +291,13 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
                            const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
                            const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
                            const float *__restrict__ last_acc, const float *fx, const float *fy,
-                           const float *fz, int64_t first, int cnt, Target &t, int *status)
+                           const float *fz, int64_t first, int cnt, const int32_t *__restrict__ active,
+                           Target &t, int *status)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned lt = (1u << lane) - 1u;
 	t.valid = lane < cnt;
-	const int64_t me = first + (t.valid ? lane : 0);
+	const int64_t me = active ? (int64_t) active[first + (t.valid ? lane : 0)] : first + (t.valid ? lane : 0);
 	const uint32_t px = ix[me], py = iy[me], pz = iz[me];
 	const uint32_t rx = __shfl_sync(0xFFFFFFFFu, px, 0), ry = __shfl_sync(0xFFFFFFFFu, py, 0),
 	               rz = __shfl_sync(0xFFFFFFFFu, pz, 0);
@@ -474,7 +475,8 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 
 template <bool EWALD, typename F>
 __global__ void __launch_bounds__(GW_THREADS)
-k_walk_group(GroupParams p, const tvg_wnode *__restrict__ wt, const uint32_t *__restrict__ ix,
+k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
+             const uint32_t *__restrict__ ix,
              const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
              const float *__restrict__ mass_f, const float *__restrict__ last_acc,
              const float *fx, const float *fy, const float *fz, F *acc0, F *acc1, F *acc2,
@@ -492,9 +494,10 @@ k_walk_group(GroupParams p, const tvg_wnode *__restrict__ wt, const uint32_t *__
 		const int64_t first = g * p.gsize;
 		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
 		Target t;
-		walk_group<EWALD>(p, S, wt, ix, iy, iz, mass_f, last_acc, fx, fy, fz, first, cnt, t, status);
+		walk_group<EWALD>(p, S, wt, ix, iy, iz, mass_f, last_acc, fx, fy, fz, first, cnt, active, t,
+		                  status);
 		if (t.valid) {
-			const int64_t i = first + lane;
+			const int64_t i = active ? (int64_t) active[first + lane] : first + lane;
 			acc0[i] += (F) t.ax;
 			acc1[i] += (F) t.ay;
 			acc2[i] += (F) t.az;
@@ -530,22 +533,22 @@ static int prepare_typed(tvg_context *ctx)
 	const int64_t n = ctx->n, nn = ctx->nnodes;
 	cudaStream_t s = ctx->stream;
 	const double fac = ctx->cfg.periodic ? 4294967296.0 / ctx->dsize : 2147483648.0 / ctx->dsize;
-	k_int_pos<F><<<tvg_blocks(n, 256), 256, 0, s>>>(
+	k_int_pos<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(
 	    n, (const F *) ctx->f[FS_POS0], (const F *) ctx->f[FS_POS1], (const F *) ctx->f[FS_POS2],
 	    ctx->origin[0], ctx->origin[1], ctx->origin[2], fac, ctx->ipos[0], ctx->ipos[1], ctx->ipos[2]);
 	TVG_CUDA(ctx, cudaGetLastError());
 	int32_t *nch = ctx->u_count, *choff = ctx->u_endu;     // free after the build
 	if (nn > 0) {
 		const GNode<F> *tree = (const GNode<F> *) ctx->tree;
-		k_wt_nchild<F><<<tvg_blocks(nn, 256), 256, 0, s>>>(nn, tree, nch);
+		k_wt_nchild<F><<<TVG_CNT(ctx, tvg_blocks(nn, 256)), 256, 0, s>>>(nn, tree, nch);
 		TVG_CUDA(ctx, cudaGetLastError());
 		TVG_CHECK(tvg_device_scan_i32(ctx, nch, choff, nn, nullptr));
-		k_wt_emit<F><<<tvg_blocks(nn, 256), 256, 0, s>>>(nn, ctx->ntop, tree, nch, choff,
+		k_wt_emit<F><<<TVG_CNT(ctx, tvg_blocks(nn, 256)), 256, 0, s>>>(nn, ctx->ntop, tree, nch, choff,
 		                                                 ctx->origin[0], ctx->origin[1],
 		                                                 ctx->origin[2], fac, ctx->dsize, ctx->wtree);
 		TVG_CUDA(ctx, cudaGetLastError());
 	}
-	k_wt_small_top<<<1, 64, 0, s>>>(ctx->ntop, ctx->d_top, ctx->cfg.vector_size, ctx->origin[0],
+	k_wt_small_top<<<TVG_CNT(ctx, 1), 64, 0, s>>>(ctx->ntop, ctx->d_top, ctx->cfg.vector_size, ctx->origin[0],
 	                                 ctx->origin[1], ctx->origin[2], fac, ctx->dsize, ctx->wtree);
 	TVG_CUDA(ctx, cudaGetLastError());
 	ctx->have_walktree = true;
@@ -566,8 +569,8 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	const float *last_f = (const float *) ctx->f[FS_LAST_ACC];
 	if (sizeof(F) == 8) {
 		float *mf = (float *) ctx->falt[FS_MASS], *lf = (float *) ctx->falt[FS_LAST_ACC];
-		k_to_float<F><<<tvg_blocks(n, 256), 256, 0, s>>>(n, (const F *) ctx->f[FS_MASS], mf);
-		k_to_float<F><<<tvg_blocks(n, 256), 256, 0, s>>>(n, (const F *) ctx->f[FS_LAST_ACC], lf);
+		k_to_float<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, (const F *) ctx->f[FS_MASS], mf);
+		k_to_float<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, (const F *) ctx->f[FS_LAST_ACC], lf);
 		mass_f = mf;
 		last_f = lf;
 	}
@@ -579,7 +582,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 			if (!ctx->ewald32) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->ewald32, 3 * 4 * (size_t) npt));
 			float *tf = ctx->ewald32;
 			for (int d = 0; d < 3; d++)
-				k_to_float<F><<<tvg_blocks(npt, 256), 256, 0, s>>>(npt, (const F *) ctx->ewald_f[d],
+				k_to_float<F><<<TVG_CNT(ctx, tvg_blocks(npt, 256)), 256, 0, s>>>(npt, (const F *) ctx->ewald_f[d],
 				                                                    tf + d * npt);
 			fx = tf; fy = tf + npt; fz = tf + 2 * npt;
 		} else {
@@ -590,9 +593,10 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	}
 	const tvg_config &cf = ctx->cfg;
 	GroupParams p;
-	p.n = n;
+	const int64_t n_act = ctx->use_active ? ctx->n_active : n;
+	p.n = n_act;
 	p.gsize = 32;
-	p.ngroups = (n + p.gsize - 1) / p.gsize;
+	p.ngroups = (n_act + p.gsize - 1) / p.gsize;
 	p.ntop = ctx->ntop;
 	p.periodic = cf.periodic;
 	p.use_bh = use_bh;
@@ -628,8 +632,9 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 4, s));
 		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
 		auto kern = ew ? k_walk_group<true, F> : k_walk_group<false, F>;
-		kern<<<nblk, GW_THREADS, smem, s>>>(
-		    p, ctx->wtree, ctx->ipos[0], ctx->ipos[1], ctx->ipos[2], mass_f, last_f, fx, fy, fz,
+		kern<<<TVG_CNT(ctx, nblk), GW_THREADS, smem, s>>>(
+		    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
+		    ctx->ipos[2], mass_f, last_f, fx, fy, fz,
 		    (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2],
 		    (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2],
 		    (F *) ctx->f[FS_COST], ctx->work_counter, ctx->counters + (ew ? 1 : 0), ctx->status);

@@ -288,17 +288,19 @@ __device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double a
 
 template <typename F>
 __global__ void __launch_bounds__(128)
-k_walk_plain(int64_t n, PlainCtx<F> c, int ewald, const F *__restrict__ last_acc, F *acc0, F *acc1,
-             F *acc2, F *gacc0, F *gacc1, F *gacc2, F *cost_out, double *counter)
+k_walk_plain(int64_t n_act, const int32_t *__restrict__ active, PlainCtx<F> c, int ewald,
+             const F *__restrict__ last_acc, F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1,
+             F *gacc2, F *cost_out, double *counter)
 {
 	__shared__ tvg_topnode s_top[TVG_MAX_TOP];
 	for (int j = threadIdx.x; j < c.p.ntop; j += blockDim.x) s_top[j] = c.top[j];
 	__syncthreads();
 	PlainCtx<F> cc = c;
 	cc.top = s_top;
-	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	const int64_t t = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	F cost = 0;
-	if (i < n) {
+	if (t < n_act) {
+		const int64_t i = active ? active[t] : t;     // Active_Particle_List[t]
 		const F sp[3] = { c.x[i], c.y[i], c.z[i] };
 		double a[3] = { 0, 0, 0 };
 		if (ewald) walk_ewald(cc, sp, last_acc[i], a, cost);
@@ -363,8 +365,10 @@ static int walk_typed(tvg_context *ctx, int use_bh, uint32_t parts)
 		const bool ew = part == 1;
 		if (!(parts & (ew ? TVG_WALK_EWALD : TVG_WALK_GRAVITY))) continue;
 		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
-		k_walk_plain<F><<<tvg_blocks(n, 128), 128, 0, s>>>(
-		    n, c, ew ? 1 : 0, (const F *) ctx->f[FS_LAST_ACC], (F *) ctx->f[FS_ACC0],
+		const int64_t n_act = ctx->use_active ? ctx->n_active : n;
+		k_walk_plain<F><<<TVG_CNT(ctx, tvg_blocks(n_act, 128)), 128, 0, s>>>(
+		    n_act, ctx->use_active ? ctx->active : nullptr, c, ew ? 1 : 0,
+		    (const F *) ctx->f[FS_LAST_ACC], (F *) ctx->f[FS_ACC0],
 		    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0],
 		    (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2], (F *) ctx->f[FS_COST],
 		    ctx->counters + (ew ? 1 : 0));
@@ -403,11 +407,11 @@ int tvg_impl_save_last_accel(tvg_context *ctx)
 	const int64_t n = ctx->n;
 	if (!n) return TVG_OK;
 	if (ctx->cfg.float_bytes == 4)
-		k_save_last<float><<<tvg_blocks(n, 256), 256, 0, ctx->stream>>>(
+		k_save_last<float><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
 		    n, (float *) ctx->f[FS_ACC0], (float *) ctx->f[FS_ACC1], (float *) ctx->f[FS_ACC2],
 		    (float *) ctx->f[FS_LAST_ACC]);
 	else
-		k_save_last<double><<<tvg_blocks(n, 256), 256, 0, ctx->stream>>>(
+		k_save_last<double><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
 		    n, (double *) ctx->f[FS_ACC0], (double *) ctx->f[FS_ACC1], (double *) ctx->f[FS_ACC2],
 		    (double *) ctx->f[FS_LAST_ACC]);
 	TVG_CUDA(ctx, cudaGetLastError());

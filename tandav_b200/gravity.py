@@ -250,3 +250,86 @@ class GravityContext:
         g, e = C.c_double(), C.c_double()
         self._check(self.lib.tvg_walk_counters(self.ctx, C.byref(g), C.byref(e)), "walk_counters")
         return g.value, e.value
+
+    # ------------------------------------------------ active set, timing
+
+    def set_active(self, indices=None):
+        """Active_Particle_List (sorted-order indices); None = all particles."""
+        if indices is None:
+            self._check(self.lib.tvg_set_active(self.ctx, None, C.c_int64(0)), "set_active")
+            return
+        a = np.ascontiguousarray(indices, dtype=np.int32)
+        self._check(self.lib.tvg_set_active(self.ctx, C.c_void_p(a.ctypes.data), C.c_int64(len(a))),
+                    "set_active")
+
+    def timer_start(self):
+        self._check(self.lib.tvg_timer(self.ctx, C.c_int32(0), None), "timer")
+
+    def timer_stop(self):
+        ms = C.c_double()
+        self._check(self.lib.tvg_timer(self.ctx, C.c_int32(1), C.byref(ms)), "timer")
+        return ms.value
+
+    def launch_count(self):
+        n = C.c_int64()
+        self._check(self.lib.tvg_launch_count(self.ctx, C.byref(n)), "launch_count")
+        return n.value
+
+    def fp32_peak(self, ms_target=200.0):
+        t = C.c_double()
+        self._check(self.lib.tvg_fp32_peak(self.ctx, C.c_double(ms_target), C.byref(t)), "fp32_peak")
+        return t.value
+
+    def upload_fields(self, n, pos=None, mass=None, last_acc=None, ids=None):
+        """Upload pre-allocated (e.g. pinned) Float arrays without copies."""
+        p = Particles()
+        fields = 0
+        if ids is not None:
+            p.id = ids.ctypes.data
+            fields |= F_ID
+        if pos is not None:
+            for k in range(3):
+                p.pos[k] = pos[k].ctypes.data
+            fields |= F_POS
+        if mass is not None:
+            p.mass = mass.ctypes.data
+            fields |= F_MASS
+        if last_acc is not None:
+            p.last_acc_mag = last_acc.ctypes.data
+            fields |= F_LAST_ACC
+        self._check(self.lib.tvg_upload(self.ctx, C.c_int64(n), C.byref(p), C.c_uint32(fields)),
+                    "upload")
+        self.n = n
+
+    def download_into(self, grav_acc=None, ids=None):
+        """Download into pre-allocated (e.g. pinned) arrays."""
+        p = Particles()
+        fields = 0
+        if grav_acc is not None:
+            for k in range(3):
+                p.grav_acc[k] = grav_acc[k].ctypes.data
+            fields |= F_GRAV_ACC
+        if ids is not None:
+            p.id = ids.ctypes.data
+            fields |= F_ID
+        self._check(self.lib.tvg_download(self.ctx, C.byref(p), C.c_uint32(fields)), "download")
+
+
+class PinnedArray:
+    """numpy view of page-locked host memory (tvg_host_alloc)."""
+
+    def __init__(self, shape, dtype):
+        self.lib = lib()
+        self.nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = C.c_void_p()
+        rc = self.lib.tvg_host_alloc(C.c_size_t(self.nbytes), C.byref(self.ptr))
+        if rc != TVG_OK:
+            raise TvgError(rc, "tvg_host_alloc failed")
+        buf = (C.c_char * self.nbytes).from_address(self.ptr.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            self.lib.tvg_host_free(self.ptr)
+            self.ptr = None
