@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--plain-stride", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak loop (profiling runs)")
     return ap.parse_args()
 
 
@@ -245,7 +246,7 @@ def main():
     ctx.upload(p.pos, p.mass)
     ctx.set_domain((0.0, 0.0, 0.0), p.box)
     ctx.ewald_init()
-    fp32_peak = ctx.fp32_peak(ms_target=1500.0)
+    fp32_peak = 0.0 if args.no_peak else ctx.fp32_peak(ms_target=1500.0)
 
     # prepare step (accel.c:51-71): BH pass, |a| -> Last_Acc_Mag
     ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
@@ -322,30 +323,41 @@ def main():
             pass
 
     # ---- plain GPU form on a strided sample of active particles
+    for a in (ids, h_pos, h_mass, h_last, h_acc, h_ids, h_oid):
+        a.free()
+    ctx.close()
+
+    # ---- plain GPU form: the reference walk in FP64 (Float = double, exact
+    # moments, table Ewald) on a strided sample of active particles
     plain = None
     if not args.no_plain:
-        ctx.upload(p.pos, p.mass)
-        ctx.set_domain((0.0, 0.0, 0.0), p.box)
-        ctx.timer_start()
-        ctx.peano_keys()
-        ctx.sort_particles(want_perm=False)
-        ctx.top_nodes()
-        ctx.tree_build(exact_moments=True)
-        pre_ms = ctx.timer_stop()
-        # same |a_old| as the group steps: BH plain pass on the sample first
+        c64 = G.GravityContext(n, float_bytes=8, periodic=True, boxsize=p.box,
+                               softening=p.softening, device=local)
+        c64.upload(p.pos, p.mass)
+        c64.set_domain((0.0, 0.0, 0.0), p.box)
+        c64.ewald_init()
+        c64.timer_start()
+        c64.peano_keys()
+        c64.sort_particles(want_perm=False)
+        c64.top_nodes()
+        c64.tree_build(exact_moments=True)
+        pre_ms = c64.timer_stop()
         act = np.arange(0, n, args.plain_stride, dtype=np.int32)
-        ctx.set_active(act)
-        ctx.zero_accel()
-        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
-        ctx.save_last_accel()
-        ctx.timer_start()
-        ctx.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
-        w_ms = ctx.timer_stop()
-        g_pl, e_pl = ctx.walk_counters()
+        c64.set_active(act)
+        c64.zero_accel()
+        c64.walk(G.FORM_PLAIN, use_bh=True, parts=parts)      # prepare pass for |a_old|
+        c64.save_last_accel()
+        c64.timer_start()
+        c64.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
+        w_ms = c64.timer_stop()
+        g_pl, e_pl = c64.walk_counters()
+        c64.close()
         t_plain = pre_ms * 1e-3 + w_ms * 1e-3 * n / len(act)
-        plain = {"value": n / t_plain, "unit": UNIT, "form": "plain (reference walk, FP32 Float)",
+        plain = {"value": n / t_plain, "unit": UNIT,
+                 "form": "plain: reference walk, one thread per particle, FP64, table Ewald",
                  "sample": f"walk of every {args.plain_stride}th particle ({len(act)}), "
                            f"keys/sort/build for all, extrapolated",
+                 "ms_keys_sort_build": round(pre_ms, 2), "ms_walk_sample": round(w_ms, 2),
                  "interactions_per_particle": round((g_pl + e_pl) / len(act), 1),
                  "speedup_group_over_plain": round(value / ws / (n / t_plain), 2)}
 
@@ -376,9 +388,6 @@ def main():
             "plain_form": plain,
         }
         print(json.dumps(out))
-    for a in (ids, h_pos, h_mass, h_last, h_acc, h_ids, h_oid):
-        a.free()
-    ctx.close()
     dist.close()
     return 0
 
