@@ -227,6 +227,36 @@ int tvg_host_free(void *ptr);
  * `ms_target` milliseconds: the denominator of the walk's roofline. */
 int tvg_fp32_peak(tvg_context *ctx, double ms_target, double *tflops);
 
+/* ---------------------------------------------- sort without allocation */
+
+/* Largest n accepted by tvg_sort_keys_noalloc. */
+#define TVG_NOALLOC_MAX_KEYS (1 << 18)
+
+/* This entry point has no counterpart in the reference. It is the PH-key
+ * sort of tvg_sort_particles for callers that cannot allocate device memory:
+ * a host code whose memory pool already owns the GPU's memory, a caller that
+ * is recording a CUDA stream (where cudaMalloc is not allowed), or one that
+ * cannot afford the device-wide synchronisation of an allocation. It needs
+ * no context.
+ *
+ * key_hi, key_lo: n 128-bit keys (high and low 64-bit words), device memory;
+ * perm: n uint32, device memory, receives the permutation that orders the
+ * keys ascending (perm[i] = input index of the i-th smallest key; equal keys
+ * keep input order) -- the same permutation tvg_sort_particles returns.
+ * Runs on the calling thread's current device and its default stream, and
+ * returns when the result is in perm.
+ *
+ * Its scratch (about 6.4 MB) is one statically sized device array that every
+ * GPU loading this library holds until the process exits; nothing is
+ * allocated or freed by a call. The first call on each device looks up that
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture begins. All calls on a device share the array,
+ * which keeps the last call's contents; calls that overlap on the same GPU
+ * (from several host threads) race and give wrong results.
+ * Returns TVG_E_BADINPUT for n < 0 or n > TVG_NOALLOC_MAX_KEYS, TVG_E_CUDA
+ * on a CUDA error. */
+int tvg_sort_keys_noalloc(const uint64_t *key_hi, const uint64_t *key_lo, int64_t n, uint32_t *perm);
+
 /* Counters of the last walk: total gravity and Ewald interactions. */
 int tvg_walk_counters(tvg_context *ctx, double *grav_interactions, double *ewald_interactions);
 

@@ -279,3 +279,139 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 		TVG_CUDA(ctx, cudaMemcpyAsync(perm_out, ctx->perm, 4 * n, cudaMemcpyDeviceToHost, s));
 	return TVG_OK;
 }
+
+// ------------------------------------------------------------------------
+// Sort without any allocation (tvg_sort_keys_noalloc).
+//
+// Some callers cannot allocate device memory: a host code whose memory pool
+// already owns the GPU's memory and forbids other allocations, a caller in the
+// middle of recording a CUDA stream (cudaMalloc is not allowed there), or a
+// latency-bound caller that cannot pay the device-wide synchronisation an
+// allocation implies. For them this variant of the sort keeps its scratch (the
+// key and index ping-pong buffers and the digit histograms) in one file-scope
+// device array of fixed size, so a call allocates nothing; the caller passes
+// the keys and receives the permutation in its own device buffers.
+//
+// The array belongs to every GPU that loads this library, for the life of the
+// process (about 6.4 MB). All calls on a device share it and it keeps the
+// last call's contents: each pass rewrites every histogram entry it reads, so
+// nothing has to start at zero. Two calls that overlap on the same GPU (from
+// two host threads, or on two streams) corrupt each other's scratch.
+// ------------------------------------------------------------------------
+
+#include <mutex>
+
+#define NOALLOC_TILES (TVG_NOALLOC_MAX_KEYS / RS_TILE)
+
+struct NoallocScratch {
+	uint64_t key[2][TVG_NOALLOC_MAX_KEYS];   // sorted high words, ping-pong
+	uint32_t idx[2][TVG_NOALLOC_MAX_KEYS];   // permutation, ping-pong
+	uint32_t hist[256 * NOALLOC_TILES];      // per-tile digit counts (digit-major)
+	uint32_t off[256 * NOALLOC_TILES];       // their exclusive prefix sum
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
+
+// single-block exclusive prefix sum of up to 1024 * 16 counts
+__global__ void __launch_bounds__(1024) k_scan_small(const uint32_t *__restrict__ in, uint32_t *__restrict__ out, int n)
+{
+	__shared__ uint32_t s_warp[32];
+	const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+	uint32_t v[16], sum = 0;
+#pragma unroll
+	for (int k = 0; k < 16; k++) {
+		const int i = t * 16 + k;
+		v[k] = i < n ? in[i] : 0u;
+		sum += v[k];
+	}
+	uint32_t inc = sum;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		uint32_t u = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+		if (lane >= o) inc += u;
+	}
+	if (lane == 31) s_warp[w] = inc;
+	__syncthreads();
+	if (w == 0) {
+		uint32_t x = s_warp[lane], xi = x;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			uint32_t u = __shfl_up_sync(0xFFFFFFFFu, xi, o);
+			if (lane >= o) xi += u;
+		}
+		s_warp[lane] = xi - x;
+	}
+	__syncthreads();
+	uint32_t run = inc - sum + s_warp[w];
+#pragma unroll
+	for (int k = 0; k < 16; k++) {
+		const int i = t * 16 + k;
+		if (i < n) out[i] = run;
+		run += v[k];
+	}
+}
+
+__global__ void k_copy_u32(int64_t n, const uint32_t *__restrict__ in, uint32_t *__restrict__ out)
+{
+	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i < n) out[i] = in[i];
+}
+
+// Device address of the scratch array, looked up once per device with that
+// device current (the host-side symbol is not a device address).
+static NoallocScratch *noalloc_scratch(int device)
+{
+	static std::mutex mu;
+	static NoallocScratch *addr[64] = { nullptr };
+	if (device < 0 || device >= 64) return nullptr;
+	std::lock_guard<std::mutex> lock(mu);
+	if (!addr[device]) {
+		void *p = nullptr;
+		if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+			cudaGetLastError();
+			return nullptr;
+		}
+		addr[device] = (NoallocScratch *) p;
+	}
+	return addr[device];
+}
+
+extern "C" int tvg_sort_keys_noalloc(const uint64_t *key_hi, const uint64_t *key_lo, int64_t n,
+                                     uint32_t *perm)
+{
+	if (n < 0 || n > TVG_NOALLOC_MAX_KEYS) return TVG_E_BADINPUT;
+	if (n == 0) return TVG_OK;
+	if (!key_hi || !key_lo || !perm) return TVG_E_BADINPUT;
+	int device = 0;
+	if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TVG_E_CUDA; }
+	NoallocScratch *S = noalloc_scratch(device);
+	if (!S) return TVG_E_CUDA;
+	static std::once_flag smem_once;
+	const size_t smem = RS_TILE * 12 + (RS_WARPS * 256 + 3 * 256 + 33) * 4;
+	cudaError_t attr_err = cudaSuccess;
+	std::call_once(smem_once, [&] {
+		attr_err = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                                (int) smem);
+	});
+	if (attr_err != cudaSuccess) { cudaGetLastError(); return TVG_E_CUDA; }
+	const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
+	cudaStream_t s = 0;
+	k_iota<<<tvg_blocks(n, 256), 256, 0, s>>>(n, S->idx[0]);
+	const uint64_t *kin = key_hi;
+	int cur = 0;
+	for (int d = 0; d < 8; d++) {
+		const int shift = 8 * d;
+		uint64_t *kout = S->key[d & 1];
+		k_tile_hist<<<(unsigned) ntiles, RS_THREADS, 0, s>>>(n, shift, kin, S->hist, ntiles);
+		k_scan_small<<<1, 1024, 0, s>>>(S->hist, S->off, (int) (256 * ntiles));
+		k_radix_scatter<<<(unsigned) ntiles, RS_THREADS, smem, s>>>(n, shift, kin, S->idx[cur], kout,
+		                                                            S->idx[cur ^ 1], S->off, ntiles);
+		kin = kout;
+		cur ^= 1;
+	}
+	k_fix_ties<<<tvg_blocks(n, 256), 256, 0, s>>>(n, kin, key_lo, S->idx[cur]);
+	k_copy_u32<<<tvg_blocks(n, 256), 256, 0, s>>>(n, S->idx[cur], perm);
+	cudaError_t e = cudaGetLastError();
+	if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+	return e == cudaSuccess ? TVG_OK : TVG_E_CUDA;
+}

@@ -1,0 +1,67 @@
+"""The sort entry point that allocates nothing (tvg_sort_keys_noalloc).
+
+It exists for callers that cannot allocate device memory -- a host code whose
+memory pool owns the GPU, a caller recording a CUDA stream, a caller that
+cannot afford the synchronisation of an allocation -- and keeps its scratch
+in a fixed device array instead. Here the caller's device buffers are torch
+tensors; the permutation must equal the one the context-based sort
+(tvg_sort_particles) returns for the same keys, bit for bit, on two calls in
+a row (the second on different, smaller input, so stale scratch from the
+first call would show).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import tandav_b200
+from tandav_b200 import gravity as G
+from tandav_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+MAX_KEYS = 1 << 18        # TVG_NOALLOC_MAX_KEYS in include/tandav_gpu.h
+
+
+def context_keys_and_perm(p):
+    """Keys (input order) and the permutation of the existing entry point."""
+    with G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box,
+                          softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.peano_keys()
+        keys = ctx.download(G.F_KEY)["key"]          # (n, 2) [hi, lo]
+        perm = ctx.sort_particles()
+    return keys, perm
+
+
+def noalloc_perm(keys):
+    import torch
+    n = keys.shape[0]
+    hi = torch.from_numpy(np.ascontiguousarray(keys[:, 0]).view(np.int64)).cuda()
+    lo = torch.from_numpy(np.ascontiguousarray(keys[:, 1]).view(np.int64)).cuda()
+    out = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    rc = tandav_b200.lib().tvg_sort_keys_noalloc(C.c_void_p(hi.data_ptr()), C.c_void_p(lo.data_ptr()),
+                                                 C.c_int64(n), C.c_void_p(out.data_ptr()))
+    assert rc == 0, f"tvg_sort_keys_noalloc returned {rc}"
+    return out.cpu().numpy().view(np.uint32)
+
+
+def test_noalloc_sort_matches_context_sort_twice():
+    first = ics.random_box(200000, box=1000.0, seed=41, clumps=7)
+    second = ics.random_box(150001, box=1000.0, seed=42, clumps=3)
+    # coincident particles: equal 128-bit keys keep input order in both paths
+    second.pos[:, 100:110] = second.pos[:, 5:6]
+    for p in (first, second):
+        keys, perm_ref = context_keys_and_perm(p)
+        perm = noalloc_perm(keys)
+        assert np.array_equal(perm, perm_ref)
+
+
+def test_noalloc_rejects_oversized_input():
+    import torch
+    buf = torch.zeros(4, dtype=torch.int64, device="cuda")
+    rc = tandav_b200.lib().tvg_sort_keys_noalloc(C.c_void_p(buf.data_ptr()), C.c_void_p(buf.data_ptr()),
+                                                 C.c_int64(MAX_KEYS + 1), C.c_void_p(buf.data_ptr()))
+    assert rc == 5                                    # TVG_E_BADINPUT
