@@ -1,22 +1,28 @@
 // tvg_walk_group.cu -- the group form of the tree walk.
 //
-// One warp per PH-contiguous group of <= 32 active particles (one particle per
-// lane), persistent blocks fed by an atomic work counter. The warp walks the
-// tree once for the whole group with conservative (group-wide) opening tests:
-// Barnes-Hut (size^2 > r_min^2 theta^2) or the relative criterion of the
-// reference (M size^2 > r_min^4 |a_old|_min / G * alpha, tree_accel.c:167,
-// 257) where r_min is the distance from the node's centre of mass to the
-// group's bounding box, plus the reference's containment test against 0.6
-// node sizes (tree_accel.c:145-148, 270-281) widened by the box. Accepted
-// nodes and the particles of opened bundles go into a shared-memory
-// interaction list that all 32 lanes read by broadcast.
+// One warp per PH-contiguous group of 32 x TPL active particles (TPL targets
+// per lane, TPL = 1 or 2), persistent blocks fed by an atomic work counter.
+// The warp walks the tree once for the whole group with conservative
+// (group-wide) opening tests: Barnes-Hut (size^2 > r_min^2 theta^2) or the
+// relative criterion of the reference (M size^2 > r_min^4 |a_old|_min / G *
+// alpha, tree_accel.c:167, 257) where r_min is the distance from the node's
+// centre of mass to the group's bounding box, plus the reference's
+// containment test against 0.6 node sizes (tree_accel.c:145-148, 270-281)
+// widened by the box. Accepted nodes and the particles of opened bundles go
+// into shared-memory interaction lists that all 32 lanes read by broadcast.
+//
+// Two lists: sources whose distance to the group box exceeds the softening
+// length and that lie away from the half-box plane go to the far list, whose
+// pair kernel is the bare 1/r^2 law (one MUFU.RSQ and ~12 FP32 instructions);
+// the rest (the group's own particles, sources inside the softening length,
+// and sources within two group half-widths of the half-box plane, whose image
+// is chosen per target) go to the near list with the full softened kernel.
 //
 // Precision: positions are 32-bit integer box coordinates (2^32 per box when
 // periodic, so that integer wrap-around is the nearest image; 2^31 per
 // domain when isolated). Each list entry is converted once to an FP32 offset
 // from the group centre; the pair loop then runs in FP32 with FP32
-// accumulation. Sources within one group half-width of the half-box plane
-// are kept in a second list whose separations are wrapped per target.
+// accumulation.
 //
 // Ewald part: the reference's Ewald walk rules (tree_periodic.c:112-422): a
 // node is opened only when it wants opening and straddles the half-box plane
@@ -24,8 +30,10 @@
 // monopole's Ewald correction, evaluated per target from the FP32 65^3 table
 // (trilinear, Gravity/periodic.c:35-113).
 //
-// Roofline: FP32 pipe bound in the pair loop (~21 FP32 instructions and one
-// MUFU.RSQ per interaction; 20 flop per interaction by convention).
+// Roofline: FP32 pipe bound in the pair loop; 20 flop per interaction by
+// convention.
+#include <stdlib.h>
+
 #include "tvg_internal.cuh"
 
 #define GW_WARPS 4
@@ -34,6 +42,7 @@
 #define GW_LIST 256
 #define GW_WLIST 64
 #define GW_BQ 64
+#define GW_DEFAULT_TPL 1
 
 // -------------------------------------------------- integer coordinates
 
@@ -174,13 +183,14 @@ struct GroupParams {
 	float rel_fac;      // TREE_OPEN_PARAM_REL / G
 	float gravity;
 	float eps2, inv_eps2, c16;     // softening (h^2, 1/h^2, 1/(16 h^3))
+	float near2;        // h^2 with a rounding margin: closer sources use the softened kernel
 	float box2grid;
 };
 
 struct WarpSmem {
 	int32_t stack[GW_STACK];
-	float4 list[GW_LIST];
-	float4 wlist[GW_WLIST];
+	float4 list[GW_LIST];      // far sources (plain 1/r^2), or Ewald sources
+	float4 wlist[GW_WLIST];    // near or wrapped sources (softened kernel, per-target image)
 	int2 bq[GW_BQ];
 };
 
@@ -191,10 +201,22 @@ struct Target {
 	bool valid;
 };
 
+// a source certainly outside the softening length of every target: 1/r^2 law
+__device__ __forceinline__ void pair_far(float4 s, Target &t)
+{
+	const float dx = s.x - t.tx, dy = s.y - t.ty, dz = s.z - t.tz;
+	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+	const float ri = rsqrtf(r2);
+	const float f = (s.w * ri) * (ri * ri);
+	t.ax = fmaf(f, dx, t.ax);
+	t.ay = fmaf(f, dy, t.ay);
+	t.az = fmaf(f, dz, t.az);
+}
+
 // softened monopole, reference kernel (Dehnen K1 with h = -41/32 eps,
 // tree_accel.c:362-394) in FP32; the r2 = 0 self term selects the inner
 // branch and adds exactly zero
-__device__ __forceinline__ void pair(const GroupParams &p, float4 s, Target &t)
+__device__ __forceinline__ void pair_full(const GroupParams &p, float4 s, Target &t)
 {
 	const float dx = s.x - t.tx, dy = s.y - t.ty, dz = s.z - t.tz;
 	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -208,19 +230,28 @@ __device__ __forceinline__ void pair(const GroupParams &p, float4 s, Target &t)
 	t.az = fmaf(f, dz, t.az);
 }
 
-__device__ __forceinline__ void flush_list(const GroupParams &p, const float4 *list, int nl, Target &t)
+template <int TPL>
+__device__ __forceinline__ void flush_far(const float4 *list, int nl, Target (&t)[TPL])
 {
 	int e = 0;
 #pragma unroll 1
 	for (; e + 4 <= nl; e += 4) {
 		const float4 s0 = list[e], s1 = list[e + 1], s2 = list[e + 2], s3 = list[e + 3];
-		pair(p, s0, t);
-		pair(p, s1, t);
-		pair(p, s2, t);
-		pair(p, s3, t);
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			pair_far(s0, t[k]);
+			pair_far(s1, t[k]);
+			pair_far(s2, t[k]);
+			pair_far(s3, t[k]);
+		}
 	}
-	for (; e < nl; e++) pair(p, list[e], t);
-	t.cost += (float) nl;
+	for (; e < nl; e++) {
+		const float4 s = list[e];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) pair_far(s, t[k]);
+	}
+#pragma unroll
+	for (int k = 0; k < TPL; k++) t[k].cost += (float) nl;
 }
 
 __device__ __forceinline__ float wrap_half(float d, float box, float half)
@@ -229,16 +260,25 @@ __device__ __forceinline__ float wrap_half(float d, float box, float half)
 	return d < -half ? d + box : d;
 }
 
-__device__ __forceinline__ void flush_wlist(const GroupParams &p, const float4 *list, int nl, Target &t)
+template <int TPL>
+__device__ __forceinline__ void flush_slow(const GroupParams &p, const float4 *list, int nl,
+                                           Target (&t)[TPL])
 {
 	for (int e = 0; e < nl; e++) {
-		float4 s = list[e];
-		s.x = wrap_half(s.x - t.tx, p.box, p.half_box) + t.tx;
-		s.y = wrap_half(s.y - t.ty, p.box, p.half_box) + t.ty;
-		s.z = wrap_half(s.z - t.tz, p.box, p.half_box) + t.tz;
-		pair(p, s, t);
+		const float4 s = list[e];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			float4 q = s;
+			if (p.periodic) {
+				q.x = wrap_half(s.x - t[k].tx, p.box, p.half_box) + t[k].tx;
+				q.y = wrap_half(s.y - t[k].ty, p.box, p.half_box) + t[k].ty;
+				q.z = wrap_half(s.z - t[k].tz, p.box, p.half_box) + t[k].tz;
+			}
+			pair_full(p, q, t[k]);
+		}
 	}
-	t.cost += (float) nl;
+#pragma unroll
+	for (int k = 0; k < TPL; k++) t[k].cost += (float) nl;
 }
 
 // Ewald_Correction (Gravity/periodic.c:35-113) in FP32 for one separation
@@ -257,74 +297,95 @@ __device__ __forceinline__ void ewald_table(const GroupParams &p, const float *_
 	const float *T[3] = { fx, fy, fz };
 #pragma unroll
 	for (int d = 0; d < 3; d++) {
-		const float *t = T[d];
-		out[d] = w000 * __ldg(t + b) + w001 * __ldg(t + b + 1) + w010 * __ldg(t + b + 65)
-		       + w011 * __ldg(t + b + 66) + w100 * __ldg(t + b + 4225) + w101 * __ldg(t + b + 4226)
-		       + w110 * __ldg(t + b + 4290) + w111 * __ldg(t + b + 4291);
+		const float *tb = T[d];
+		out[d] = w000 * __ldg(tb + b) + w001 * __ldg(tb + b + 1) + w010 * __ldg(tb + b + 65)
+		       + w011 * __ldg(tb + b + 66) + w100 * __ldg(tb + b + 4225) + w101 * __ldg(tb + b + 4226)
+		       + w110 * __ldg(tb + b + 4290) + w111 * __ldg(tb + b + 4291);
 	}
 	out[0] *= sx;
 	out[1] *= sy;
 	out[2] *= sz;
 }
 
+template <int TPL>
 __device__ __forceinline__ void flush_ewald(const GroupParams &p, const float4 *list, int nl,
                                             const float *fx, const float *fy, const float *fz,
-                                            Target &t)
+                                            Target (&t)[TPL])
 {
 	for (int e = 0; e < nl; e++) {
 		const float4 s = list[e];
-		const float dx = wrap_half(s.x - t.tx, p.box, p.half_box);
-		const float dy = wrap_half(s.y - t.ty, p.box, p.half_box);
-		const float dz = wrap_half(s.z - t.tz, p.box, p.half_box);
-		if (dx == 0.f && dy == 0.f && dz == 0.f) continue;      // self
-		float c[3];
-		ewald_table(p, fx, fy, fz, dx, dy, dz, c);
-		t.ax = fmaf(s.w, c[0], t.ax);
-		t.ay = fmaf(s.w, c[1], t.ay);
-		t.az = fmaf(s.w, c[2], t.az);
-		t.cost += 1.f;
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			const float dx = wrap_half(s.x - t[k].tx, p.box, p.half_box);
+			const float dy = wrap_half(s.y - t[k].ty, p.box, p.half_box);
+			const float dz = wrap_half(s.z - t[k].tz, p.box, p.half_box);
+			if (dx == 0.f && dy == 0.f && dz == 0.f) continue;      // self
+			float c[3];
+			ewald_table(p, fx, fy, fz, dx, dy, dz, c);
+			t[k].ax = fmaf(s.w, c[0], t[k].ax);
+			t[k].ay = fmaf(s.w, c[1], t[k].ay);
+			t[k].az = fmaf(s.w, c[2], t[k].az);
+			t[k].cost += 1.f;
+		}
 	}
 }
 
-template <bool EWALD>
+// one group: 32 * TPL PH-contiguous active particles, lane l holds the
+// particles first + l + 32 k
+template <bool EWALD, int TPL>
 __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *__restrict__ wt,
                            const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
                            const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
                            const float *__restrict__ last_acc, const float *fx, const float *fy,
                            const float *fz, int64_t first, int cnt, const int32_t *__restrict__ active,
-                           Target &t, int *status)
+                           Target (&t)[TPL], int *status)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned lt = (1u << lane) - 1u;
-	t.valid = lane < cnt;
-	const int64_t me = active ? (int64_t) active[first + (t.valid ? lane : 0)] : first + (t.valid ? lane : 0);
-	const uint32_t px = ix[me], py = iy[me], pz = iz[me];
-	const uint32_t rx = __shfl_sync(0xFFFFFFFFu, px, 0), ry = __shfl_sync(0xFFFFFFFFu, py, 0),
-	               rz = __shfl_sync(0xFFFFFFFFu, pz, 0);
-	const int ox = (int) (px - rx), oy = (int) (py - ry), oz = (int) (pz - rz);
-	const int minx = __reduce_min_sync(0xFFFFFFFFu, ox), maxx = __reduce_max_sync(0xFFFFFFFFu, ox);
-	const int miny = __reduce_min_sync(0xFFFFFFFFu, oy), maxy = __reduce_max_sync(0xFFFFFFFFu, oy);
-	const int minz = __reduce_min_sync(0xFFFFFFFFu, oz), maxz = __reduce_max_sync(0xFFFFFFFFu, oz);
+	uint32_t px[TPL], py[TPL], pz[TPL];
+	int64_t me0 = active ? (int64_t) active[first] : first;
+	const uint32_t rx = ix[me0], ry = iy[me0], rz = iz[me0];
+	int minx = 0, maxx = 0, miny = 0, maxy = 0, minz = 0, maxz = 0;
+	float amin = 3.0e38f;
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		const int slot = lane + 32 * k;
+		t[k].valid = slot < cnt;
+		const int64_t me = t[k].valid ? (active ? (int64_t) active[first + slot] : first + slot) : me0;
+		px[k] = ix[me];
+		py[k] = iy[me];
+		pz[k] = iz[me];
+		const int ox = (int) (px[k] - rx), oy = (int) (py[k] - ry), oz = (int) (pz[k] - rz);
+		minx = min(minx, ox); maxx = max(maxx, ox);
+		miny = min(miny, oy); maxy = max(maxy, oy);
+		minz = min(minz, oz); maxz = max(maxz, oz);
+		if (t[k].valid) amin = fminf(amin, last_acc[me]);
+	}
+	minx = __reduce_min_sync(0xFFFFFFFFu, minx); maxx = __reduce_max_sync(0xFFFFFFFFu, maxx);
+	miny = __reduce_min_sync(0xFFFFFFFFu, miny); maxy = __reduce_max_sync(0xFFFFFFFFu, maxy);
+	minz = __reduce_min_sync(0xFFFFFFFFu, minz); maxz = __reduce_max_sync(0xFFFFFFFFu, maxz);
 	const uint32_t cx = rx + (uint32_t) (((int64_t) minx + maxx) >> 1);
 	const uint32_t cy = ry + (uint32_t) (((int64_t) miny + maxy) >> 1);
 	const uint32_t cz = rz + (uint32_t) (((int64_t) minz + maxz) >> 1);
 	const float hx = ((float) ((int64_t) maxx - minx) * 0.5f + 1.f) * p.scale;
 	const float hy = ((float) ((int64_t) maxy - miny) * 0.5f + 1.f) * p.scale;
 	const float hz = ((float) ((int64_t) maxz - minz) * 0.5f + 1.f) * p.scale;
-	// rounded products (no FMA contraction into the later subtraction): a
-	// particle's own list entry must sit at exactly zero separation, since the
-	// reference's inner kernel (h < 0) turns any residue into a large force
-	t.tx = __fmul_rn((float) (int) (px - cx), p.scale);
-	t.ty = __fmul_rn((float) (int) (py - cy), p.scale);
-	t.tz = __fmul_rn((float) (int) (pz - cz), p.scale);
-	t.ax = t.ay = t.az = 0.f;
-	t.cost = 0.f;
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		// rounded products (no FMA contraction into the later subtraction): a
+		// particle's own list entry must sit at exactly zero separation, since
+		// the reference's inner kernel (h < 0) turns any residue into a force
+		t[k].tx = __fmul_rn((float) (int) (px[k] - cx), p.scale);
+		t[k].ty = __fmul_rn((float) (int) (py[k] - cy), p.scale);
+		t[k].tz = __fmul_rn((float) (int) (pz[k] - cz), p.scale);
+		t[k].ax = t[k].ay = t[k].az = 0.f;
+		t[k].cost = 0.f;
+	}
 	// group-wide relative criterion: the smallest |a_old| opens the most
-	float amin = t.valid ? last_acc[me] : 3.0e38f;
 #pragma unroll
 	for (int o = 16; o; o >>= 1) amin = fminf(amin, __shfl_xor_sync(0xFFFFFFFFu, amin, o));
 	const float fac = amin * p.rel_fac;
-	// wrap margin: a source this close to the half-box plane needs per-target images
+	// a source this close to the half-box plane needs per-target images
 	const float wlimx = p.half_box - 2.f * hx, wlimy = p.half_box - 2.f * hy,
 	            wlimz = p.half_box - 2.f * hz;
 
@@ -343,7 +404,7 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 		if (lane < k) node = S.stack[sp - 1 - lane];
 		sp -= k;
 		__syncwarp();
-		bool accept = false, open_int = false, open_bundle = false, needs_wrap = false;
+		bool accept = false, open_int = false, open_bundle = false, slow = false;
 		float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
 		int nchild = 0, child = 0;
 		if (node >= 0) {
@@ -377,7 +438,8 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 			if (!open) {
 				accept = true;
 				entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
-				needs_wrap = p.periodic && (fabsf(dx) > wlimx || fabsf(dy) > wlimy || fabsf(dz) > wlimz);
+				slow = (p.periodic && (fabsf(dx) > wlimx || fabsf(dy) > wlimy || fabsf(dz) > wlimz))
+				    || r2 < p.near2;
 			} else if (nd.nchild > 0) {
 				open_int = true;
 				nchild = nd.nchild;
@@ -389,23 +451,23 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 			}
 		}
 		// accepted nodes -> interaction lists
-		const bool to_main = accept && (EWALD || !needs_wrap);
-		const bool to_wrap = accept && !EWALD && needs_wrap;
-		unsigned bm = __ballot_sync(0xFFFFFFFFu, to_main);
-		unsigned bw = __ballot_sync(0xFFFFFFFFu, to_wrap);
+		const bool to_main = accept && (EWALD || !slow);
+		const bool to_slow = accept && !EWALD && slow;
+		const unsigned bm = __ballot_sync(0xFFFFFFFFu, to_main);
+		const unsigned bw = __ballot_sync(0xFFFFFFFFu, to_slow);
 		if (nl + __popc(bm) > GW_LIST) {
-			if (EWALD) flush_ewald(p, S.list, nl, fx, fy, fz, t);
-			else flush_list(p, S.list, nl, t);
+			if (EWALD) flush_ewald<TPL>(p, S.list, nl, fx, fy, fz, t);
+			else flush_far<TPL>(S.list, nl, t);
 			nl = 0;
 			__syncwarp();
 		}
 		if (!EWALD && nw + __popc(bw) > GW_WLIST) {
-			flush_wlist(p, S.wlist, nw, t);
+			flush_slow<TPL>(p, S.wlist, nw, t);
 			nw = 0;
 			__syncwarp();
 		}
 		if (to_main) S.list[nl + __popc(bm & lt)] = entry;
-		if (to_wrap) S.wlist[nw + __popc(bw & lt)] = entry;
+		if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
 		nl += __popc(bm);
 		nw += __popc(bw);
 		// children -> stack (exclusive prefix sum of child counts)
@@ -419,7 +481,7 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 		for (int q = 0; q < c; q++) S.stack[sp + incl - c + q] = child + c - 1 - q;
 		sp += tot;
 		// opened bundles -> bundle queue
-		unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
+		const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
 		if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
 		__syncwarp();
 		const int nb = __popc(bb);
@@ -429,26 +491,30 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 				const int j = o + lane;
 				const bool have = j < q.y;
 				float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-				bool w = false;
+				bool sl = false;
 				if (have) {
 					const int64_t jp = (int64_t) q.x + j;
 					e.x = __fmul_rn((float) (int) (ix[jp] - cx), p.scale);
 					e.y = __fmul_rn((float) (int) (iy[jp] - cy), p.scale);
 					e.z = __fmul_rn((float) (int) (iz[jp] - cz), p.scale);
 					e.w = p.gravity * mass_f[jp];
-					w = !EWALD && p.periodic
-					 && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz);
+					if (!EWALD) {
+						const float ax = fmaxf(fabsf(e.x) - hx, 0.f), ay = fmaxf(fabsf(e.y) - hy, 0.f),
+						            az = fmaxf(fabsf(e.z) - hz, 0.f);
+						sl = ax * ax + ay * ay + az * az < p.near2
+						  || (p.periodic && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz));
+					}
 				}
-				const bool tm = have && !w, tw = have && w;
+				const bool tm = have && !sl, tw = have && sl;
 				const unsigned m1 = __ballot_sync(0xFFFFFFFFu, tm), m2 = __ballot_sync(0xFFFFFFFFu, tw);
 				if (nl + __popc(m1) > GW_LIST) {
-					if (EWALD) flush_ewald(p, S.list, nl, fx, fy, fz, t);
-					else flush_list(p, S.list, nl, t);
+					if (EWALD) flush_ewald<TPL>(p, S.list, nl, fx, fy, fz, t);
+					else flush_far<TPL>(S.list, nl, t);
 					nl = 0;
 					__syncwarp();
 				}
 				if (!EWALD && nw + __popc(m2) > GW_WLIST) {
-					flush_wlist(p, S.wlist, nw, t);
+					flush_slow<TPL>(p, S.wlist, nw, t);
 					nw = 0;
 					__syncwarp();
 				}
@@ -463,24 +529,25 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	}
 	__syncwarp();
 	if (EWALD) {
-		flush_ewald(p, S.list, nl, fx, fy, fz, t);
+		flush_ewald<TPL>(p, S.list, nl, fx, fy, fz, t);
 	} else {
-		flush_list(p, S.list, nl, t);
-		flush_wlist(p, S.wlist, nw, t);
+		flush_far<TPL>(S.list, nl, t);
+		flush_slow<TPL>(p, S.wlist, nw, t);
 		// the self pair is counted by the list but not by the reference
-		t.cost -= 1.f;
+#pragma unroll
+		for (int k = 0; k < TPL; k++) t[k].cost -= 1.f;
 	}
 	__syncwarp();
 }
 
-template <bool EWALD, typename F>
+template <bool EWALD, int TPL, typename F>
 __global__ void __launch_bounds__(GW_THREADS)
 k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
-             const uint32_t *__restrict__ ix,
-             const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
-             const float *__restrict__ mass_f, const float *__restrict__ last_acc,
-             const float *fx, const float *fy, const float *fz, F *acc0, F *acc1, F *acc2,
-             F *gacc0, F *gacc1, F *gacc2, F *cost_out, int32_t *work, double *counter, int *status)
+             const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
+             const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
+             const float *__restrict__ last_acc, const float *fx, const float *fy, const float *fz,
+             F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1, F *gacc2, F *cost_out, int32_t *work,
+             double *counter, int *status)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	WarpSmem &S = ((WarpSmem *) smem_raw)[threadIdx.x >> 5];
@@ -493,26 +560,29 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode 
 		if (g >= p.ngroups) break;
 		const int64_t first = g * p.gsize;
 		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
-		Target t;
-		walk_group<EWALD>(p, S, wt, ix, iy, iz, mass_f, last_acc, fx, fy, fz, first, cnt, active, t,
-		                  status);
-		if (t.valid) {
-			const int64_t i = active ? (int64_t) active[first + lane] : first + lane;
-			acc0[i] += (F) t.ax;
-			acc1[i] += (F) t.ay;
-			acc2[i] += (F) t.az;
+		Target t[TPL];
+		walk_group<EWALD, TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, fx, fy, fz, first, cnt, active,
+		                       t, status);
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			if (!t[k].valid) continue;
+			const int slot = lane + 32 * k;
+			const int64_t i = active ? (int64_t) active[first + slot] : first + slot;
+			acc0[i] += (F) t[k].ax;
+			acc1[i] += (F) t[k].ay;
+			acc2[i] += (F) t[k].az;
 			if (EWALD) {
-				gacc0[i] += (F) t.ax;
-				gacc1[i] += (F) t.ay;
-				gacc2[i] += (F) t.az;
-				cost_out[i] += (F) t.cost;
+				gacc0[i] += (F) t[k].ax;
+				gacc1[i] += (F) t[k].ay;
+				gacc2[i] += (F) t[k].az;
+				cost_out[i] += (F) t[k].cost;
 			} else {
-				gacc0[i] = (F) t.ax;
-				gacc1[i] = (F) t.ay;
-				gacc2[i] = (F) t.az;
-				cost_out[i] = (F) t.cost;
+				gacc0[i] = (F) t[k].ax;
+				gacc1[i] = (F) t[k].ay;
+				gacc2[i] = (F) t[k].az;
+				cost_out[i] = (F) t[k].cost;
 			}
-			cnt_acc += t.cost;
+			cnt_acc += t[k].cost;
 		}
 	}
 #pragma unroll
@@ -555,6 +625,43 @@ static int prepare_typed(tvg_context *ctx)
 	return TVG_OK;
 }
 
+// targets per lane: 1 (32-particle groups) or 2 (64); TVG_GROUP_TPL overrides
+static int group_tpl()
+{
+	static int tpl = 0;
+	if (!tpl) {
+		const char *e = getenv("TVG_GROUP_TPL");
+		tpl = (e && atoi(e) == 1) ? 1 : (e && atoi(e) == 2) ? 2 : GW_DEFAULT_TPL;
+	}
+	return tpl;
+}
+
+template <bool EWALD, int TPL, typename F>
+static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
+                       const float *fx, const float *fy, const float *fz, double *counter)
+{
+	static int nblk = 0;
+	const size_t smem = sizeof(WarpSmem) * GW_WARPS;
+	if (!nblk) {
+		TVG_CUDA(ctx, cudaFuncSetAttribute(k_walk_group<EWALD, TPL, F>,
+		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+		int per_sm = 0, nsm = 0;
+		TVG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<EWALD, TPL, F>,
+		                                                             GW_THREADS, smem));
+		TVG_CUDA(ctx, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+		nblk = (per_sm > 0 ? per_sm : 1) * nsm;
+	}
+	p.gsize = 32 * TPL;
+	p.ngroups = (p.n + p.gsize - 1) / p.gsize;
+	k_walk_group<EWALD, TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
+	    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
+	    ctx->ipos[2], mass_f, last_f, fx, fy, fz, (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1],
+	    (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2],
+	    (F *) ctx->f[FS_COST], ctx->work_counter, counter, ctx->status);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
+}
+
 template <typename F>
 static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind)
 {
@@ -593,10 +700,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	}
 	const tvg_config &cf = ctx->cfg;
 	GroupParams p;
-	const int64_t n_act = ctx->use_active ? ctx->n_active : n;
-	p.n = n_act;
-	p.gsize = 32;
-	p.ngroups = (n_act + p.gsize - 1) / p.gsize;
+	p.n = ctx->use_active ? ctx->n_active : n;
 	p.ntop = ctx->ntop;
 	p.periodic = cf.periodic;
 	p.use_bh = use_bh;
@@ -610,35 +714,20 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	p.eps2 = (float) (h * h);
 	p.inv_eps2 = (float) (1.0 / (h * h));
 	p.c16 = (float) (1.0 / (16.0 * h * h * h));
+	p.near2 = (float) (h * h * 1.001);
 	p.box2grid = (float) (cf.periodic ? 2.0 * 64.0 / cf.boxsize : 0.0);
-
-	static int nblk = 0;
-	const size_t smem = sizeof(WarpSmem) * GW_WARPS;
-	if (!nblk) {
-		TVG_CUDA(ctx, cudaFuncSetAttribute(k_walk_group<false, F>,
-		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-		TVG_CUDA(ctx, cudaFuncSetAttribute(k_walk_group<true, F>,
-		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-		int per_sm = 0, nsm = 0;
-		TVG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<false, F>,
-		                                                             GW_THREADS, smem));
-		TVG_CUDA(ctx, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
-		nblk = (per_sm > 0 ? per_sm : 1) * nsm;
-	}
+	const int tpl = group_tpl();
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16, s));
 	for (int part = 0; part < 2; part++) {
 		const bool ew = part == 1;
 		if (!(parts & (ew ? TVG_WALK_EWALD : TVG_WALK_GRAVITY))) continue;
 		TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 4, s));
 		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
-		auto kern = ew ? k_walk_group<true, F> : k_walk_group<false, F>;
-		kern<<<TVG_CNT(ctx, nblk), GW_THREADS, smem, s>>>(
-		    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
-		    ctx->ipos[2], mass_f, last_f, fx, fy, fz,
-		    (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2],
-		    (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2],
-		    (F *) ctx->f[FS_COST], ctx->work_counter, ctx->counters + (ew ? 1 : 0), ctx->status);
-		TVG_CUDA(ctx, cudaGetLastError());
+		double *cnt = ctx->counters + (ew ? 1 : 0);
+		if (ew && tpl == 1) TVG_CHECK((launch_walk<true, 1, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
+		else if (ew) TVG_CHECK((launch_walk<true, 2, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
+		else if (tpl == 1) TVG_CHECK((launch_walk<false, 1, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
+		else TVG_CHECK((launch_walk<false, 2, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
 		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
 		TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
 		float ms = 0;
