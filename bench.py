@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak loop (profiling runs)")
+    ap.add_argument("--forcetest-targets", type=int, default=10000,
+                    help="particles in the FP64 direct-sum error check (0: skip)")
     return ap.parse_args()
 
 
@@ -277,9 +279,25 @@ def main():
     t_step = dist.max(total_ms / args.steps) / 1e3
     value = dist.sum(n) / t_step
 
-    # ---- end to end through the C ABI with host buffers (pinned)
+    # ---- force error of the timed step against the FP64 direct (Ewald) sum
     ids = G.PinnedArray((n,), np.uint32)
     ctx.download_into(ids=ids.array)
+    tgt_ids = None
+    accuracy = None
+    if args.forcetest_targets > 0:
+        nt = min(args.forcetest_targets, n)
+        tgt_ids = np.sort(np.random.default_rng(777).choice(n, nt, replace=False))
+        inv = np.empty(n, np.int64)
+        inv[ids.array] = np.arange(n)
+        ctx.timer_start()
+        _, _, err = ctx.forcetest(np.sort(inv[tgt_ids]))
+        ft_ms = ctx.timer_stop()
+        accuracy = {"targets": int(nt), "group": {k: float(f"{v:.4e}") for k, v in err.items()},
+                    "oracle": "FP64 direct sum on the GPU over all particles, softened kernel, "
+                              "Ewald-summed (alpha L = 12, nearest-image real space, |h|^2 <= 576)",
+                    "forcetest_ms": round(ft_ms, 1)}
+
+    # ---- end to end through the C ABI with host buffers (pinned)
     last = ctx.download(G.F_LAST_ACC)["last_acc_mag"]
     h_pos = G.PinnedArray((3, n), np.float32)
     h_mass = G.PinnedArray((n,), np.float32)
@@ -351,6 +369,20 @@ def main():
         c64.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
         w_ms = c64.timer_stop()
         g_pl, e_pl = c64.walk_counters()
+        if tgt_ids is not None:
+            # the same particles, walked in the plain form, against the same sum
+            ids64 = c64.download(G.F_ID)["id"]
+            inv = np.empty(n, np.int64)
+            inv[ids64] = np.arange(n)
+            t64 = np.sort(inv[tgt_ids])
+            c64.set_active(t64.astype(np.int32))
+            c64.zero_accel()
+            c64.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+            c64.save_last_accel()
+            c64.zero_accel()
+            c64.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
+            _, _, err64 = c64.forcetest(t64)
+            accuracy["plain"] = {k: float(f"{v:.4e}") for k, v in err64.items()}
         c64.close()
         t_plain = pre_ms * 1e-3 + w_ms * 1e-3 * n / len(act)
         plain = {"value": n / t_plain, "unit": UNIT,
@@ -386,6 +418,7 @@ def main():
             "interactions_per_particle": {"gravity": round(grav_i / args.steps / n, 1),
                                           "ewald": round(ew_i / args.steps / n, 1)},
             "plain_form": plain,
+            "accuracy": accuracy,
         }
         print(json.dumps(out))
     dist.close()

@@ -58,7 +58,12 @@ enum {
 	 * Target (tree_accel.c:185, tree_periodic.c:188), which for top nodes with
 	 * <= VECTOR_SIZE particles holds a tree index (tree_build.c:91). Set this
 	 * flag to use First_Part instead. Default: the reference's behaviour. */
-	TVG_CFG_FIX_SMALL_TOPNODES = 1
+	TVG_CFG_FIX_SMALL_TOPNODES = 1,
+	/* Group form: interact every particle of a bundle (a tree leaf of <=
+	 * VECTOR_SIZE particles) that the walk reaches below the top level, as the
+	 * reference's walks do (tree_accel.c:221-243). Default: such a bundle is a
+	 * monopole like any other node when the opening criterion accepts it. */
+	TVG_CFG_OPEN_BUNDLES = 2
 };
 
 /* Host view of struct Particle_Data (src/Gravity/../particles.h:17-37). Any
@@ -259,6 +264,36 @@ int tvg_sort_keys_noalloc(const uint64_t *key_hi, const uint64_t *key_lo, int64_
 
 /* Counters of the last walk: total gravity and Ewald interactions. */
 int tvg_walk_counters(tvg_context *ctx, double *grav_interactions, double *ewald_interactions);
+
+/* Largest n_targets accepted by tvg_forcetest. */
+#define TVG_FORCETEST_MAX_TARGETS (1 << 20)
+
+/* Replaces Gravity_Forcetest (Gravity/forcetest.c:25-172), which checks
+ * NTEST = 10 random active particles on the host: FP64 direct summation over
+ * all resident particles for n_targets targets (indices into the current,
+ * i.e. PH-sorted, particle order), with the reference's softened kernel on
+ * the nearest image; with TVG_WALK_EWALD in parts (periodic box) the periodic
+ * images are Ewald-summed (alpha L = 12, real space on the nearest image,
+ * k space |h|^2 <= 576). parts must include TVG_WALK_GRAVITY. Outputs, each optional:
+ * acc_direct and acc_tree (3 * n_targets doubles, x block then y then z) hold
+ * the direct sum and the resident Grav_Acc; err[4] = rms, 99th percentile
+ * (nearest rank), mean and max of |a_tree - a_direct| / |a_direct|.
+ * Allocates and frees its own device scratch. */
+int tvg_forcetest(tvg_context *ctx, uint32_t parts, int64_t n_targets, const int64_t *targets,
+                  double *acc_direct, double *acc_tree, double *err);
+
+/* Sets the opening parameters (the reference's compile-time constants
+ * TREE_OPEN_PARAM_BH, used as theta^2, and TREE_OPEN_PARAM_REL) for the
+ * following walks; no reference counterpart. Values must be > 0. */
+int tvg_set_opening(tvg_context *ctx, double open_bh, double open_rel);
+
+/* Opening of the group form's Ewald walk (no reference counterpart): a node
+ * is opened for the Ewald correction when the monopole error of the
+ * correction, G M h2 s^2 / (8 L^4) (h2: bound of its second derivatives in
+ * box units), exceeds rel_alpha |a_old| (relative mode), or when
+ * h2 s^2 / L^2 exceeds bh_factor times TREE_OPEN_PARAM_BH (Barnes-Hut mode).
+ * Defaults 2.5e-4 and 0.5. */
+int tvg_set_ewald_opening(tvg_context *ctx, double rel_alpha, double bh_factor);
 
 #ifdef __cplusplus
 }

@@ -23,7 +23,8 @@ EXPORTS = (
     "tvg_download_ewald_table", "tvg_upload_ewald_table", "tvg_walk", "tvg_save_last_accel", "tvg_zero_accel",
     "tvg_force_step", "tvg_phase_times", "tvg_walk_counters", "tvg_set_active", "tvg_timer",
     "tvg_launch_count", "tvg_host_alloc", "tvg_host_free", "tvg_fp32_peak",
-    "tvg_sort_keys_noalloc",
+    "tvg_sort_keys_noalloc", "tvg_forcetest", "tvg_set_opening",
+    "tvg_set_ewald_opening",
 )
 
 

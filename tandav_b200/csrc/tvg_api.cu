@@ -142,7 +142,8 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->u_final, ctx->u_level, ctx->u_flag, ctx->tree, ctx->tree_u, ctx->pref,
 	                 ctx->ipos[0], ctx->ipos[1], ctx->ipos[2], ctx->wtree, ctx->group_first,
 	                 ctx->work_counter, ctx->counters, ctx->ewald_f[0], ctx->ewald_f[1],
-	                 ctx->ewald_f[2], ctx->ewald_f[3], ctx->ewald_raw, ctx->ewald32 };
+	                 ctx->ewald_f[2], ctx->ewald_f[3], ctx->ewald_raw, ctx->ewald32,
+	                 ctx->ewald_ext, ctx->active };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -450,6 +451,26 @@ extern "C" int tvg_fp32_peak(tvg_context *ctx, double ms_target, double *tflops)
 		}
 	}
 	*tflops = best;
+	return TVG_OK;
+}
+
+extern "C" int tvg_set_opening(tvg_context *ctx, double open_bh, double open_rel)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!(open_bh > 0) || !(open_rel > 0))
+		return tvg_fail(ctx, TVG_E_BADINPUT, "set_opening: parameters must be > 0");
+	ctx->cfg.open_bh = open_bh;
+	ctx->cfg.open_rel = open_rel;
+	return TVG_OK;
+}
+
+extern "C" int tvg_set_ewald_opening(tvg_context *ctx, double rel_alpha, double bh_factor)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!(rel_alpha > 0) || !(bh_factor > 0))
+		return tvg_fail(ctx, TVG_E_BADINPUT, "set_ewald_opening: parameters must be > 0");
+	ctx->ewald_open_rel = rel_alpha;
+	ctx->ewald_open_bh = bh_factor;
 	return TVG_OK;
 }
 

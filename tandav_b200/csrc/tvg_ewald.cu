@@ -96,6 +96,36 @@ int tvg_impl_ewald_init(tvg_context *ctx)
 	return TVG_OK;
 }
 
+// The group form's correction table: T(x) (box units, unit G m: the force of
+// the periodic lattice minus the image at the origin, the quantity of the
+// table above) at x = 0.5 i / 64 for i = -1..66 per axis, in FP64 then stored
+// FP32 as (Tx, Ty, Tz, 0). The layer at i = -1 and the layers beyond L/2 let
+// a 4-point stencil stay centred everywhere on the octant; beyond L/2 the
+// values are the analytic continuation of that correction, which a Taylor
+// expansion about a point near the half-box plane needs.
+#define N_EXT 68
+
+__global__ void k_ewald_ext(float4 *ext)
+{
+	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+	if (idx >= N_EXT * N_EXT * N_EXT) return;
+	const int i = idx / (N_EXT * N_EXT) - 1, j = (idx / N_EXT) % N_EXT - 1, k = idx % N_EXT - 1;
+	const double x[3] = { (0.5 * i) / N_EWALD, (0.5 * j) / N_EWALD, (0.5 * k) / N_EWALD };
+	double f[3], pot;
+	ewald_point(x, f, &pot);
+	ext[idx] = make_float4((float) f[0], (float) f[1], (float) f[2], 0.f);
+}
+
+int tvg_impl_ewald_ext(tvg_context *ctx)
+{
+	const size_t npt = (size_t) N_EXT * N_EXT * N_EXT;
+	if (!ctx->ewald_ext) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->ewald_ext, 16 * npt));
+	k_ewald_ext<<<TVG_CNT(ctx, tvg_blocks((int64_t) npt, 128)), 128, 0, ctx->stream>>>(
+	    (float4 *) ctx->ewald_ext);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
+}
+
 // raw Float tables (box units) -> device tables, as after
 // read_ewald_correction_table + the division at periodic.c:215-228
 template <typename F>

@@ -125,6 +125,12 @@ struct tvg_context {
 	void *ewald_f[4] = { nullptr, nullptr, nullptr, nullptr };
 	double *ewald_raw = nullptr;
 	float *ewald32 = nullptr;          // FP32 copy for the group form (FP64 builds)
+	float *ewald_ext = nullptr;        // (Tx, Ty, Tz, 0) on 68^3 points, x = 0.5 i / 64, i = -1..66
+	// Ewald-walk opening of the group form: the monopole error of the
+	// correction may reach ewald_open_rel |a_old| (relative mode); the limit of
+	// h2 s^2 / L^2 in units of TREE_OPEN_PARAM_BH (Barnes-Hut mode)
+	double ewald_open_rel = 2.5e-4;
+	double ewald_open_bh = 0.5;
 
 	// group walk data
 	uint32_t *ipos[3] = { nullptr, nullptr, nullptr };
@@ -167,6 +173,7 @@ int tvg_impl_top_nodes(tvg_context *ctx);
 int tvg_impl_tree_build(tvg_context *ctx, uint32_t flags);
 int tvg_impl_download_tree(tvg_context *ctx, void *tree, int64_t cap, int64_t *nnodes);
 int tvg_impl_ewald_init(tvg_context *ctx);
+int tvg_impl_ewald_ext(tvg_context *ctx);
 int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts);
 int tvg_impl_walk_group(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind);
 int tvg_impl_save_last_accel(tvg_context *ctx);

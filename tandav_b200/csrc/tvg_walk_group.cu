@@ -11,24 +11,43 @@
 // widened by the box. Accepted nodes and the particles of opened bundles go
 // into shared-memory interaction lists that all 32 lanes read by broadcast.
 //
-// Two lists: sources whose distance to the group box exceeds the softening
-// length and that lie away from the half-box plane go to the far list, whose
-// pair kernel is the bare 1/r^2 law (one MUFU.RSQ and ~12 FP32 instructions);
-// the rest (the group's own particles, sources inside the softening length,
-// and sources within two group half-widths of the half-box plane, whose image
-// is chosen per target) go to the near list with the full softened kernel.
+// Lists: sources whose distance to the group box exceeds the softening
+// length go to the far list, whose pair kernel is the bare 1/r^2 law (one
+// MUFU.RSQ and ~12 FP32 instructions); the group's own particles and sources
+// inside the softening length go to the near list with the full softened
+// kernel. Each list flush is summed in FP32 and carried in FP64: the net force
+// at high redshift is a small remainder of partial sums hundreds of times
+// larger, and a running FP32 sum over 1e5-1e6 interactions loses it.
 //
 // Precision: positions are 32-bit integer box coordinates (2^32 per box when
 // periodic, so that integer wrap-around is the nearest image; 2^31 per
 // domain when isolated). Each list entry is converted once to an FP32 offset
-// from the group centre; the pair loop then runs in FP32 with FP32
-// accumulation.
+// from the group centre.
 //
-// Ewald part: the reference's Ewald walk rules (tree_periodic.c:112-422): a
-// node is opened only when it wants opening and straddles the half-box plane
-// for some target or is larger than 0.2 L; everything else contributes its
-// monopole's Ewald correction, evaluated per target from the FP32 65^3 table
-// (trilinear, Gravity/periodic.c:35-113).
+// Periodic images. With the Ewald part, every source is taken at its image
+// nearest to the group centre, for all targets of the group, and the Ewald
+// correction K (the force of the periodic lattice minus that image) is added
+// for the same image: Newton + K is the lattice force, which is smooth across
+// the half-box plane, so no target needs its own image. K is evaluated by a
+// second, per-group traversal (k_ewald_group): at the centre of mass of each
+// accepted node it evaluates K, its Jacobian J and Hessian H (tricubic
+// interpolation of the lattice sum tabulated on the octant, with the
+// analytic continuation one cell beyond L/2), sums them over the group's
+// nodes, and each target adds the second-order Taylor expansion
+// K - J t + H:tt/2 about the group centre. Nodes are opened for K by their
+// own error estimate (the monopole error of K, G M h2 s^2 / (8 L^4) with h2 a
+// bound of |d2K| in box units), except that a node whose extent reaches the
+// half-box plane takes the gravity walk's decision, so that both parts always
+// use the same image for the same particles. Without the Ewald part
+// (parts = gravity only) sources within two group half-widths of the half-box
+// plane go to the near list and take per-target nearest images, as the
+// reference's gravity walk does (Periodic_Nearest, periodic.c:62-80).
+//
+// This replaces the reference's Ewald walk (tree_periodic.c:112-422), which
+// accepts every node that does not straddle the half-box plane and is at most
+// 0.2 L, even where the gravity criterion opens it, and interpolates the
+// 65^3 table trilinearly (Gravity/periodic.c:35-113): both leave a force error
+// (~3e-3 rms on the 256^3 box at z = 50) that no opening parameter removes.
 //
 // Roofline: FP32 pipe bound in the pair loop; 20 flop per interaction by
 // convention.
@@ -39,10 +58,12 @@
 #define GW_WARPS 4
 #define GW_THREADS (GW_WARPS * 32)
 #define GW_STACK 1024
+#define GW_RESERVE (7 * (TVG_MAX_LEVEL - 2) + 8)
 #define GW_LIST 256
 #define GW_WLIST 64
 #define GW_BQ 64
-#define GW_DEFAULT_TPL 1
+#define GW_ELIST 64
+#define GW_DEFAULT_TPL 2
 
 // -------------------------------------------------- integer coordinates
 
@@ -168,7 +189,14 @@ __global__ void k_wt_small_top(int ntop, const tvg_topnode *__restrict__ top, in
 	wt[t] = r;
 }
 
+
 // ------------------------------------------------------------- the walk
+
+// images the gravity walk uses
+enum {
+	GM_NEAREST = 0,     // per-target nearest image (isolated, or periodic without Ewald)
+	GM_CENTRE = 1       // the image nearest to the group centre (periodic, with k_ewald_group)
+};
 
 struct GroupParams {
 	int64_t n;
@@ -177,6 +205,7 @@ struct GroupParams {
 	int ntop;
 	int periodic;
 	int use_bh;
+	int open_bundles;   // TVG_CFG_OPEN_BUNDLES
 	float scale;        // length per integer unit
 	float box, half_box;
 	float theta2;       // TREE_OPEN_PARAM_BH
@@ -184,166 +213,51 @@ struct GroupParams {
 	float gravity;
 	float eps2, inv_eps2, c16;     // softening (h^2, 1/h^2, 1/(16 h^3))
 	float near2;        // h^2 with a rounding margin: closer sources use the softened kernel
-	float box2grid;
+	float grid;         // Ewald table cells per length (2 * 64 / L)
+	float inv_box;
+	float ew_rel;       // Ewald opening: alpha_E / TREE_OPEN_PARAM_REL (relative mode)
+	float ew_bh;        // Ewald opening: s^2 h2 limit in units of L^2 (Barnes-Hut mode)
+	float taylor_h;     // groups with a larger half extent take per-target images (with Ewald)
 };
 
 struct WarpSmem {
 	int32_t stack[GW_STACK];
-	float4 list[GW_LIST];      // far sources (plain 1/r^2), or Ewald sources
-	float4 wlist[GW_WLIST];    // near or wrapped sources (softened kernel, per-target image)
+	float4 list[GW_LIST];      // far sources: bare 1/r^2 kernel
+	float4 wlist[GW_WLIST];    // near sources (w > 0) and, per-target image, half-box-plane sources (w < 0)
+	int2 bq[GW_BQ];
+};
+
+struct EwaldSmem {
+	int32_t stack[GW_STACK];
+	float4 list[GW_ELIST];     // accepted sources: offset from the group centre, G m
 	int2 bq[GW_BQ];
 };
 
 struct Target {
 	float tx, ty, tz;       // offset from the group centre
-	float ax, ay, az;
+	double ax, ay, az;      // FP32 sums of each list flush, carried in FP64
 	float cost;
 	bool valid;
 };
 
-// a source certainly outside the softening length of every target: 1/r^2 law
-__device__ __forceinline__ void pair_far(float4 s, Target &t)
-{
-	const float dx = s.x - t.tx, dy = s.y - t.ty, dz = s.z - t.tz;
-	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-	const float ri = rsqrtf(r2);
-	const float f = (s.w * ri) * (ri * ri);
-	t.ax = fmaf(f, dx, t.ax);
-	t.ay = fmaf(f, dy, t.ay);
-	t.az = fmaf(f, dz, t.az);
-}
+struct GroupBox {
+	uint32_t cx, cy, cz;    // centre, integer coordinates
+	float hx, hy, hz;       // half extents (+ one unit)
+	float fac;              // |a_old|_min * TREE_OPEN_PARAM_REL / G
+};
 
-// softened monopole, reference kernel (Dehnen K1 with h = -41/32 eps,
-// tree_accel.c:362-394) in FP32; the r2 = 0 self term selects the inner
-// branch and adds exactly zero
-__device__ __forceinline__ void pair_full(const GroupParams &p, float4 s, Target &t)
-{
-	const float dx = s.x - t.tx, dy = s.y - t.ty, dz = s.z - t.tz;
-	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-	const float ri = rsqrtf(r2);
-	const float fout = ri * ri * ri;
-	const float u2 = r2 * p.inv_eps2;
-	const float fin = fmaf(u2, fmaf(u2, 135.0f, -294.0f), 175.0f) * p.c16;
-	const float f = s.w * (r2 < p.eps2 ? fin : fout);
-	t.ax = fmaf(f, dx, t.ax);
-	t.ay = fmaf(f, dy, t.ay);
-	t.az = fmaf(f, dz, t.az);
-}
-
+// bounding box, centre and |a_old|_min of the group; target offsets
 template <int TPL>
-__device__ __forceinline__ void flush_far(const float4 *list, int nl, Target (&t)[TPL])
-{
-	int e = 0;
-#pragma unroll 1
-	for (; e + 4 <= nl; e += 4) {
-		const float4 s0 = list[e], s1 = list[e + 1], s2 = list[e + 2], s3 = list[e + 3];
-#pragma unroll
-		for (int k = 0; k < TPL; k++) {
-			pair_far(s0, t[k]);
-			pair_far(s1, t[k]);
-			pair_far(s2, t[k]);
-			pair_far(s3, t[k]);
-		}
-	}
-	for (; e < nl; e++) {
-		const float4 s = list[e];
-#pragma unroll
-		for (int k = 0; k < TPL; k++) pair_far(s, t[k]);
-	}
-#pragma unroll
-	for (int k = 0; k < TPL; k++) t[k].cost += (float) nl;
-}
-
-__device__ __forceinline__ float wrap_half(float d, float box, float half)
-{
-	d = d > half ? d - box : d;
-	return d < -half ? d + box : d;
-}
-
-template <int TPL>
-__device__ __forceinline__ void flush_slow(const GroupParams &p, const float4 *list, int nl,
-                                           Target (&t)[TPL])
-{
-	for (int e = 0; e < nl; e++) {
-		const float4 s = list[e];
-#pragma unroll
-		for (int k = 0; k < TPL; k++) {
-			float4 q = s;
-			if (p.periodic) {
-				q.x = wrap_half(s.x - t[k].tx, p.box, p.half_box) + t[k].tx;
-				q.y = wrap_half(s.y - t[k].ty, p.box, p.half_box) + t[k].ty;
-				q.z = wrap_half(s.z - t[k].tz, p.box, p.half_box) + t[k].tz;
-			}
-			pair_full(p, q, t[k]);
-		}
-	}
-#pragma unroll
-	for (int k = 0; k < TPL; k++) t[k].cost += (float) nl;
-}
-
-// Ewald_Correction (Gravity/periodic.c:35-113) in FP32 for one separation
-__device__ __forceinline__ void ewald_table(const GroupParams &p, const float *__restrict__ fx,
-                                            const float *__restrict__ fy, const float *__restrict__ fz,
-                                            float dx, float dy, float dz, float out[3])
-{
-	const float sx = dx < 0 ? 1.f : -1.f, sy = dy < 0 ? 1.f : -1.f, sz = dz < 0 ? 1.f : -1.f;
-	float u = fabsf(dx) * p.box2grid, v = fabsf(dy) * p.box2grid, w = fabsf(dz) * p.box2grid;
-	int i = min((int) u, 63), j = min((int) v, 63), k = min((int) w, 63);
-	u -= i; v -= j; w -= k;
-	const int b = (i * 65 + j) * 65 + k;
-	const float w000 = (1 - u) * (1 - v) * (1 - w), w001 = (1 - u) * (1 - v) * w,
-	            w010 = (1 - u) * v * (1 - w), w011 = (1 - u) * v * w, w100 = u * (1 - v) * (1 - w),
-	            w101 = u * (1 - v) * w, w110 = u * v * (1 - w), w111 = u * v * w;
-	const float *T[3] = { fx, fy, fz };
-#pragma unroll
-	for (int d = 0; d < 3; d++) {
-		const float *tb = T[d];
-		out[d] = w000 * __ldg(tb + b) + w001 * __ldg(tb + b + 1) + w010 * __ldg(tb + b + 65)
-		       + w011 * __ldg(tb + b + 66) + w100 * __ldg(tb + b + 4225) + w101 * __ldg(tb + b + 4226)
-		       + w110 * __ldg(tb + b + 4290) + w111 * __ldg(tb + b + 4291);
-	}
-	out[0] *= sx;
-	out[1] *= sy;
-	out[2] *= sz;
-}
-
-template <int TPL>
-__device__ __forceinline__ void flush_ewald(const GroupParams &p, const float4 *list, int nl,
-                                            const float *fx, const float *fy, const float *fz,
-                                            Target (&t)[TPL])
-{
-	for (int e = 0; e < nl; e++) {
-		const float4 s = list[e];
-#pragma unroll
-		for (int k = 0; k < TPL; k++) {
-			const float dx = wrap_half(s.x - t[k].tx, p.box, p.half_box);
-			const float dy = wrap_half(s.y - t[k].ty, p.box, p.half_box);
-			const float dz = wrap_half(s.z - t[k].tz, p.box, p.half_box);
-			if (dx == 0.f && dy == 0.f && dz == 0.f) continue;      // self
-			float c[3];
-			ewald_table(p, fx, fy, fz, dx, dy, dz, c);
-			t[k].ax = fmaf(s.w, c[0], t[k].ax);
-			t[k].ay = fmaf(s.w, c[1], t[k].ay);
-			t[k].az = fmaf(s.w, c[2], t[k].az);
-			t[k].cost += 1.f;
-		}
-	}
-}
-
-// one group: 32 * TPL PH-contiguous active particles, lane l holds the
-// particles first + l + 32 k
-template <bool EWALD, int TPL>
-__device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *__restrict__ wt,
-                           const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
-                           const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
-                           const float *__restrict__ last_acc, const float *fx, const float *fy,
-                           const float *fz, int64_t first, int cnt, const int32_t *__restrict__ active,
-                           Target (&t)[TPL], int *status)
+__device__ __forceinline__ void group_setup(const GroupParams &p, const uint32_t *__restrict__ ix,
+                                            const uint32_t *__restrict__ iy,
+                                            const uint32_t *__restrict__ iz,
+                                            const float *__restrict__ last_acc,
+                                            const int32_t *__restrict__ active, int64_t first,
+                                            int cnt, Target (&t)[TPL], GroupBox &g)
 {
 	const int lane = threadIdx.x & 31;
-	const unsigned lt = (1u << lane) - 1u;
 	uint32_t px[TPL], py[TPL], pz[TPL];
-	int64_t me0 = active ? (int64_t) active[first] : first;
+	const int64_t me0 = active ? (int64_t) active[first] : first;
 	const uint32_t rx = ix[me0], ry = iy[me0], rz = iz[me0];
 	int minx = 0, maxx = 0, miny = 0, maxy = 0, minz = 0, maxz = 0;
 	float amin = 3.0e38f;
@@ -364,30 +278,218 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	minx = __reduce_min_sync(0xFFFFFFFFu, minx); maxx = __reduce_max_sync(0xFFFFFFFFu, maxx);
 	miny = __reduce_min_sync(0xFFFFFFFFu, miny); maxy = __reduce_max_sync(0xFFFFFFFFu, maxy);
 	minz = __reduce_min_sync(0xFFFFFFFFu, minz); maxz = __reduce_max_sync(0xFFFFFFFFu, maxz);
-	const uint32_t cx = rx + (uint32_t) (((int64_t) minx + maxx) >> 1);
-	const uint32_t cy = ry + (uint32_t) (((int64_t) miny + maxy) >> 1);
-	const uint32_t cz = rz + (uint32_t) (((int64_t) minz + maxz) >> 1);
-	const float hx = ((float) ((int64_t) maxx - minx) * 0.5f + 1.f) * p.scale;
-	const float hy = ((float) ((int64_t) maxy - miny) * 0.5f + 1.f) * p.scale;
-	const float hz = ((float) ((int64_t) maxz - minz) * 0.5f + 1.f) * p.scale;
+	g.cx = rx + (uint32_t) (((int64_t) minx + maxx) >> 1);
+	g.cy = ry + (uint32_t) (((int64_t) miny + maxy) >> 1);
+	g.cz = rz + (uint32_t) (((int64_t) minz + maxz) >> 1);
+	g.hx = ((float) ((int64_t) maxx - minx) * 0.5f + 1.f) * p.scale;
+	g.hy = ((float) ((int64_t) maxy - miny) * 0.5f + 1.f) * p.scale;
+	g.hz = ((float) ((int64_t) maxz - minz) * 0.5f + 1.f) * p.scale;
 #pragma unroll
 	for (int k = 0; k < TPL; k++) {
 		// rounded products (no FMA contraction into the later subtraction): a
 		// particle's own list entry must sit at exactly zero separation, since
 		// the reference's inner kernel (h < 0) turns any residue into a force
-		t[k].tx = __fmul_rn((float) (int) (px[k] - cx), p.scale);
-		t[k].ty = __fmul_rn((float) (int) (py[k] - cy), p.scale);
-		t[k].tz = __fmul_rn((float) (int) (pz[k] - cz), p.scale);
-		t[k].ax = t[k].ay = t[k].az = 0.f;
+		t[k].tx = __fmul_rn((float) (int) (px[k] - g.cx), p.scale);
+		t[k].ty = __fmul_rn((float) (int) (py[k] - g.cy), p.scale);
+		t[k].tz = __fmul_rn((float) (int) (pz[k] - g.cz), p.scale);
+		t[k].ax = t[k].ay = t[k].az = 0.0;
 		t[k].cost = 0.f;
 	}
 	// group-wide relative criterion: the smallest |a_old| opens the most
 #pragma unroll
 	for (int o = 16; o; o >>= 1) amin = fminf(amin, __shfl_xor_sync(0xFFFFFFFFu, amin, o));
-	const float fac = amin * p.rel_fac;
-	// a source this close to the half-box plane needs per-target images
-	const float wlimx = p.half_box - 2.f * hx, wlimy = p.half_box - 2.f * hy,
-	            wlimz = p.half_box - 2.f * hz;
+	g.fac = amin * p.rel_fac;
+}
+
+// offset of an integer coordinate from the group centre (rounded product)
+__device__ __forceinline__ float ioff(uint32_t v, uint32_t c, float scale)
+{
+	return __fmul_rn((float) (int) (v - c), scale);
+}
+
+// The gravity walk's opening decision for a node (shared by both walks, so
+// that the Ewald walk can repeat it bit for bit). d: centre of mass offset,
+// gx..: geometric centre offset. r2 receives the squared distance from the
+// centre of mass to the group box.
+__device__ __forceinline__ bool gravity_opens(const GroupParams &p, const GroupBox &g,
+                                              const tvg_wnode &nd, int node, float dx, float dy,
+                                              float dz, float gx, float gy, float gz, float &r2)
+{
+	const float qx = fmaxf(fabsf(dx) - g.hx, 0.f), qy = fmaxf(fabsf(dy) - g.hy, 0.f),
+	            qz = fmaxf(fabsf(dz) - g.hz, 0.f);
+	r2 = qx * qx + qy * qy + qz * qz;
+	bool want;
+	if (p.use_bh) want = nd.size2 > r2 * p.theta2;
+	else want = nd.mass * nd.size2 > r2 * r2 * g.fac;
+	const float lim = 0.6f * nd.size;
+	if (fabsf(gx) < lim + g.hx && fabsf(gy) < lim + g.hy && fabsf(gz) < lim + g.hz) want = true;
+	// with TVG_CFG_OPEN_BUNDLES a bundle below the top level is never a
+	// monopole: the reference interacts its particles whenever the walk
+	// reaches it (tree_accel.c:221-243, tree_periodic.c:228-251)
+	return want || (p.open_bundles && nd.nchild < 0 && node >= p.ntop);
+}
+
+// Pops k <= 32 nodes of the stack (one per lane, -1 for idle lanes).
+// Batches of up to 32 nodes may push 8 children each, so a batch of k keeps
+// sp + 7k below GW_STACK - GW_RESERVE. Above that line the warp takes one
+// node at a time: from there on the stack holds at most 7 siblings per level
+// of the current path (<= 40 levels below the top nodes), which the reserve
+// covers, so the stack cannot overflow.
+__device__ __forceinline__ int pop_nodes(const int32_t *stack, int &sp, int *status, bool &stop)
+{
+	const int lane = threadIdx.x & 31;
+	int k = min(32, sp);
+	const int room = (GW_STACK - GW_RESERVE - sp) / 7;
+	if (room < k) k = max(room, 1);
+	stop = false;
+	if (sp + 7 * k > GW_STACK) {
+		atomicOr(status, TVG_ST_LIST_OVERFLOW);
+		stop = true;
+		return -1;
+	}
+	int node = -1;
+	if (lane < k) node = stack[sp - 1 - lane];
+	sp -= k;
+	__syncwarp();
+	return node;
+}
+
+// pushes the children of the lanes' opened internal nodes
+__device__ __forceinline__ void push_children(int32_t *stack, int &sp, bool open_int, int nchild,
+                                              int child)
+{
+	const int lane = threadIdx.x & 31;
+	int c = open_int ? nchild : 0, incl = c;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		int u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+		if (lane >= o) incl += u;
+	}
+	const int tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+	for (int q = 0; q < c; q++) stack[sp + incl - c + q] = child + c - 1 - q;
+	sp += tot;
+}
+
+// a source certainly outside the softening length of every target: 1/r^2 law
+__device__ __forceinline__ void pair_far(float4 s, float tx, float ty, float tz, float &ax,
+                                         float &ay, float &az)
+{
+	const float dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
+	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+	const float ri = rsqrtf(r2);
+	const float f = (s.w * ri) * (ri * ri);
+	ax = fmaf(f, dx, ax);
+	ay = fmaf(f, dy, ay);
+	az = fmaf(f, dz, az);
+}
+
+// softened monopole, reference kernel (Dehnen K1 with h = -41/32 eps,
+// tree_accel.c:362-394) in FP32 for a separation d; the r2 = 0 self term
+// selects the inner branch and adds exactly zero
+__device__ __forceinline__ void pair_full(const GroupParams &p, float dx, float dy, float dz,
+                                          float gm, float &ax, float &ay, float &az)
+{
+	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+	const float ri = rsqrtf(r2);
+	const float fout = ri * ri * ri;
+	const float u2 = r2 * p.inv_eps2;
+	const float fin = fmaf(u2, fmaf(u2, 135.0f, -294.0f), 175.0f) * p.c16;
+	const float f = gm * (r2 < p.eps2 ? fin : fout);
+	ax = fmaf(f, dx, ax);
+	ay = fmaf(f, dy, ay);
+	az = fmaf(f, dz, az);
+}
+
+template <int TPL>
+__device__ __forceinline__ void flush_far(const float4 *list, int nl, Target (&t)[TPL])
+{
+	float ax[TPL], ay[TPL], az[TPL];
+#pragma unroll
+	for (int k = 0; k < TPL; k++) ax[k] = ay[k] = az[k] = 0.f;
+	int e = 0;
+#pragma unroll 1
+	for (; e + 4 <= nl; e += 4) {
+		const float4 s0 = list[e], s1 = list[e + 1], s2 = list[e + 2], s3 = list[e + 3];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			pair_far(s0, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
+			pair_far(s1, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
+			pair_far(s2, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
+			pair_far(s3, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
+		}
+	}
+	for (; e < nl; e++) {
+		const float4 s = list[e];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) pair_far(s, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
+	}
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		t[k].ax += (double) ax[k];
+		t[k].ay += (double) ay[k];
+		t[k].az += (double) az[k];
+		t[k].cost += (float) nl;
+	}
+}
+
+__device__ __forceinline__ float wrap_half(float d, float box, float half)
+{
+	d = d > half ? d - box : d;
+	return d < -half ? d + box : d;
+}
+
+// near list: softened kernel; entries with w < 0 take per-target images
+template <int TPL>
+__device__ __forceinline__ void flush_slow(const GroupParams &p, const float4 *list, int nl,
+                                           Target (&t)[TPL])
+{
+	float ax[TPL], ay[TPL], az[TPL];
+#pragma unroll
+	for (int k = 0; k < TPL; k++) ax[k] = ay[k] = az[k] = 0.f;
+	for (int e = 0; e < nl; e++) {
+		const float4 s = list[e];
+		const bool wrap = s.w < 0.f;
+		const float gm = fabsf(s.w);
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			float dx = s.x - t[k].tx, dy = s.y - t[k].ty, dz = s.z - t[k].tz;
+			if (wrap) {
+				dx = wrap_half(dx, p.box, p.half_box);
+				dy = wrap_half(dy, p.box, p.half_box);
+				dz = wrap_half(dz, p.box, p.half_box);
+			}
+			pair_full(p, dx, dy, dz, gm, ax[k], ay[k], az[k]);
+		}
+	}
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		t[k].ax += (double) ax[k];
+		t[k].ay += (double) ay[k];
+		t[k].az += (double) az[k];
+		t[k].cost += (float) nl;
+	}
+}
+
+// gravity walk of one group: 32 * TPL PH-contiguous active particles, lane l
+// holds the particles first + l + 32 k
+template <int MODE, int TPL>
+__device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *__restrict__ wt,
+                           const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
+                           const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
+                           const float *__restrict__ last_acc, int64_t first, int cnt,
+                           const int32_t *__restrict__ active, Target (&t)[TPL], int *status)
+{
+	const int lane = threadIdx.x & 31;
+	const unsigned lt = (1u << lane) - 1u;
+	GroupBox g;
+	group_setup<TPL>(p, ix, iy, iz, last_acc, active, first, cnt, t, g);
+	// with per-target images: a source this close to the half-box plane needs
+	// them. With the Ewald walk, only groups too large for its expansion
+	// about the centre take them (the same test there).
+	const bool per_target = p.periodic
+	    && (MODE == GM_NEAREST || fmaxf(g.hx, fmaxf(g.hy, g.hz)) >= p.taylor_h);
+	const float wlimx = p.half_box - 2.f * g.hx, wlimy = p.half_box - 2.f * g.hy,
+	            wlimz = p.half_box - 2.f * g.hz;
 
 	int sp = 0, nl = 0, nw = 0;
 	for (int r = lane; r < p.ntop; r += 32) S.stack[r] = r;
@@ -396,50 +498,24 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	int guard = 0;
 	while (sp > 0) {
 		if (++guard > (1 << 24)) { atomicOr(status, TVG_ST_TIMEOUT); break; }
-		int k = min(32, sp);
-		const int room = (GW_STACK - sp) / 7;
-		if (room < k) k = room;
-		if (k <= 0) { atomicOr(status, TVG_ST_LIST_OVERFLOW); break; }
-		int node = -1;
-		if (lane < k) node = S.stack[sp - 1 - lane];
-		sp -= k;
-		__syncwarp();
-		bool accept = false, open_int = false, open_bundle = false, slow = false;
+		bool stop;
+		const int node = pop_nodes(S.stack, sp, status, stop);
+		if (stop) break;
+		bool accept = false, open_int = false, open_bundle = false, wrap = false, near = false;
 		float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
 		int nchild = 0, child = 0;
 		if (node >= 0) {
 			const tvg_wnode nd = wt[node];
-			const float dx = __fmul_rn((float) (int) (nd.cx - cx), p.scale);
-			const float dy = __fmul_rn((float) (int) (nd.cy - cy), p.scale);
-			const float dz = __fmul_rn((float) (int) (nd.cz - cz), p.scale);
-			const float qx = fmaxf(fabsf(dx) - hx, 0.f), qy = fmaxf(fabsf(dy) - hy, 0.f),
-			            qz = fmaxf(fabsf(dz) - hz, 0.f);
-			const float r2 = qx * qx + qy * qy + qz * qz;
-			bool want;
-			if (p.use_bh) want = nd.size2 > r2 * p.theta2;
-			else want = nd.mass * nd.size2 > r2 * r2 * fac;
-			const float gx = __fmul_rn((float) (int) (nd.gx - cx), p.scale);
-			const float gy = __fmul_rn((float) (int) (nd.gy - cy), p.scale);
-			const float gz = __fmul_rn((float) (int) (nd.gz - cz), p.scale);
-			const float lim = 0.6f * nd.size;
-			if (fabsf(gx) < lim + hx && fabsf(gy) < lim + hy && fabsf(gz) < lim + hz) want = true;
-			// a bundle below the top level is never a monopole: the reference
-			// interacts its particles whenever the walk reaches it
-			// (tree_accel.c:221-243, tree_periodic.c:228-251)
-			const bool force_open = nd.nchild < 0 && node >= p.ntop;
-			bool open = want || force_open;
-			if (EWALD && want) {
-				// open only when the node straddles the half-box plane for some
-				// target, or is larger than 0.2 L (tree_periodic.c:158-172, 278-310)
-				const float dl = 0.5f * (p.box - nd.size);
-				open = force_open || fabsf(gx) + hx > dl || fabsf(gy) + hy > dl
-				    || fabsf(gz) + hz > dl || nd.size > 0.2f * p.box;
-			}
+			const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
+			            dz = ioff(nd.cz, g.cz, p.scale);
+			float r2;
+			const bool open = gravity_opens(p, g, nd, node, dx, dy, dz, ioff(nd.gx, g.cx, p.scale),
+			                                ioff(nd.gy, g.cy, p.scale), ioff(nd.gz, g.cz, p.scale), r2);
 			if (!open) {
 				accept = true;
 				entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
-				slow = (p.periodic && (fabsf(dx) > wlimx || fabsf(dy) > wlimy || fabsf(dz) > wlimz))
-				    || r2 < p.near2;
+				wrap = per_target && (fabsf(dx) > wlimx || fabsf(dy) > wlimy || fabsf(dz) > wlimz);
+				near = r2 < p.near2;
 			} else if (nd.nchild > 0) {
 				open_int = true;
 				nchild = nd.nchild;
@@ -451,35 +527,26 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 			}
 		}
 		// accepted nodes -> interaction lists
-		const bool to_main = accept && (EWALD || !slow);
-		const bool to_slow = accept && !EWALD && slow;
-		const unsigned bm = __ballot_sync(0xFFFFFFFFu, to_main);
+		const bool to_far = accept && !wrap && !near;
+		const bool to_slow = accept && (wrap || near);
+		if (wrap) entry.w = -entry.w;
+		const unsigned bm = __ballot_sync(0xFFFFFFFFu, to_far);
 		const unsigned bw = __ballot_sync(0xFFFFFFFFu, to_slow);
 		if (nl + __popc(bm) > GW_LIST) {
-			if (EWALD) flush_ewald<TPL>(p, S.list, nl, fx, fy, fz, t);
-			else flush_far<TPL>(S.list, nl, t);
+			flush_far<TPL>(S.list, nl, t);
 			nl = 0;
 			__syncwarp();
 		}
-		if (!EWALD && nw + __popc(bw) > GW_WLIST) {
+		if (nw + __popc(bw) > GW_WLIST) {
 			flush_slow<TPL>(p, S.wlist, nw, t);
 			nw = 0;
 			__syncwarp();
 		}
-		if (to_main) S.list[nl + __popc(bm & lt)] = entry;
+		if (to_far) S.list[nl + __popc(bm & lt)] = entry;
 		if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
 		nl += __popc(bm);
 		nw += __popc(bw);
-		// children -> stack (exclusive prefix sum of child counts)
-		int c = open_int ? nchild : 0, incl = c;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			int u = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-			if (lane >= o) incl += u;
-		}
-		const int tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-		for (int q = 0; q < c; q++) S.stack[sp + incl - c + q] = child + c - 1 - q;
-		sp += tot;
+		push_children(S.stack, sp, open_int, nchild, child);
 		// opened bundles -> bundle queue
 		const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
 		if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
@@ -491,29 +558,27 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 				const int j = o + lane;
 				const bool have = j < q.y;
 				float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-				bool sl = false;
+				bool wr = false, nr = false;
 				if (have) {
 					const int64_t jp = (int64_t) q.x + j;
-					e.x = __fmul_rn((float) (int) (ix[jp] - cx), p.scale);
-					e.y = __fmul_rn((float) (int) (iy[jp] - cy), p.scale);
-					e.z = __fmul_rn((float) (int) (iz[jp] - cz), p.scale);
+					e.x = ioff(ix[jp], g.cx, p.scale);
+					e.y = ioff(iy[jp], g.cy, p.scale);
+					e.z = ioff(iz[jp], g.cz, p.scale);
 					e.w = p.gravity * mass_f[jp];
-					if (!EWALD) {
-						const float ax = fmaxf(fabsf(e.x) - hx, 0.f), ay = fmaxf(fabsf(e.y) - hy, 0.f),
-						            az = fmaxf(fabsf(e.z) - hz, 0.f);
-						sl = ax * ax + ay * ay + az * az < p.near2
-						  || (p.periodic && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz));
-					}
+					const float ax = fmaxf(fabsf(e.x) - g.hx, 0.f), ay = fmaxf(fabsf(e.y) - g.hy, 0.f),
+					            az = fmaxf(fabsf(e.z) - g.hz, 0.f);
+					nr = ax * ax + ay * ay + az * az < p.near2;
+					wr = per_target && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz);
 				}
-				const bool tm = have && !sl, tw = have && sl;
+				const bool tm = have && !wr && !nr, tw = have && (wr || nr);
+				if (wr) e.w = -e.w;
 				const unsigned m1 = __ballot_sync(0xFFFFFFFFu, tm), m2 = __ballot_sync(0xFFFFFFFFu, tw);
 				if (nl + __popc(m1) > GW_LIST) {
-					if (EWALD) flush_ewald<TPL>(p, S.list, nl, fx, fy, fz, t);
-					else flush_far<TPL>(S.list, nl, t);
+					flush_far<TPL>(S.list, nl, t);
 					nl = 0;
 					__syncwarp();
 				}
-				if (!EWALD && nw + __popc(m2) > GW_WLIST) {
+				if (nw + __popc(m2) > GW_WLIST) {
 					flush_slow<TPL>(p, S.wlist, nw, t);
 					nw = 0;
 					__syncwarp();
@@ -528,26 +593,20 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 		__syncwarp();
 	}
 	__syncwarp();
-	if (EWALD) {
-		flush_ewald<TPL>(p, S.list, nl, fx, fy, fz, t);
-	} else {
-		flush_far<TPL>(S.list, nl, t);
-		flush_slow<TPL>(p, S.wlist, nw, t);
-		// the self pair is counted by the list but not by the reference
+	flush_far<TPL>(S.list, nl, t);
+	flush_slow<TPL>(p, S.wlist, nw, t);
 #pragma unroll
-		for (int k = 0; k < TPL; k++) t[k].cost -= 1.f;
-	}
+	for (int k = 0; k < TPL; k++) t[k].cost -= 1.f;     // the self pair, which the reference skips
 	__syncwarp();
 }
 
-template <bool EWALD, int TPL, typename F>
+template <int MODE, int TPL, typename F>
 __global__ void __launch_bounds__(GW_THREADS)
 k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
              const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
              const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
-             const float *__restrict__ last_acc, const float *fx, const float *fy, const float *fz,
-             F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1, F *gacc2, F *cost_out, int32_t *work,
-             double *counter, int *status)
+             const float *__restrict__ last_acc, F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1,
+             F *gacc2, F *cost_out, int32_t *work, double *counter, int *status)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	WarpSmem &S = ((WarpSmem *) smem_raw)[threadIdx.x >> 5];
@@ -561,8 +620,7 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode 
 		const int64_t first = g * p.gsize;
 		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
 		Target t[TPL];
-		walk_group<EWALD, TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, fx, fy, fz, first, cnt, active,
-		                       t, status);
+		walk_group<MODE, TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, first, cnt, active, t, status);
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
 			if (!t[k].valid) continue;
@@ -571,23 +629,397 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode 
 			acc0[i] += (F) t[k].ax;
 			acc1[i] += (F) t[k].ay;
 			acc2[i] += (F) t[k].az;
-			if (EWALD) {
-				gacc0[i] += (F) t[k].ax;
-				gacc1[i] += (F) t[k].ay;
-				gacc2[i] += (F) t[k].az;
-				cost_out[i] += (F) t[k].cost;
-			} else {
-				gacc0[i] = (F) t[k].ax;
-				gacc1[i] = (F) t[k].ay;
-				gacc2[i] = (F) t[k].az;
-				cost_out[i] = (F) t[k].cost;
-			}
+			gacc0[i] = (F) t[k].ax;
+			gacc1[i] = (F) t[k].ay;
+			gacc2[i] = (F) t[k].az;
+			cost_out[i] = (F) t[k].cost;
 			cnt_acc += t[k].cost;
 		}
 	}
 #pragma unroll
 	for (int o = 16; o; o >>= 1) cnt_acc += __shfl_xor_sync(0xFFFFFFFFu, cnt_acc, o);
 	if (lane == 0 && cnt_acc != 0) atomicAdd(counter, cnt_acc);
+}
+
+// ------------------------------------------------------ the Ewald walk
+
+// 4-point Lagrange basis on the nodes -1, 0, 1, 2 at t in [0, 1]: weights,
+// first and second derivatives
+__device__ __forceinline__ void lagrange4(float t, float w[4], float d[4], float dd[4])
+{
+	const float t2 = t * t, t3 = t2 * t;
+	w[0] = (-t3 + 3.f * t2 - 2.f * t) * (1.f / 6.f);
+	w[1] = (t3 - 2.f * t2 - t + 2.f) * 0.5f;
+	w[2] = (-t3 + t2 + 2.f * t) * 0.5f;
+	w[3] = (t3 - t) * (1.f / 6.f);
+	d[0] = (-3.f * t2 + 6.f * t - 2.f) * (1.f / 6.f);
+	d[1] = (3.f * t2 - 4.f * t - 1.f) * 0.5f;
+	d[2] = (-3.f * t2 + 2.f * t + 2.f) * 0.5f;
+	d[3] = (3.f * t2 - 1.f) * (1.f / 6.f);
+	dd[0] = 1.f - t;
+	dd[1] = 3.f * t - 2.f;
+	dd[2] = 1.f - 3.f * t;
+	dd[3] = t;
+}
+
+// per-lane sums over accepted sources of m K, m J and m H (about the group
+// centre), FP32 (at most a few hundred terms per lane)
+struct CorrSum {
+	float k[3];
+	float j[9];     // J[a][b] = dK_a / dd_b
+	float h[18];    // H[a][xx, yy, zz, xy, xz, yz]
+};
+
+// The lattice-minus-image force T(x) (box units, unit G m, target at x from
+// the source) is tabulated on x = 0.5 i / 64, i = -1..66 per axis (one ghost
+// layer below 0 and the analytic continuation beyond 1/2), interleaved
+// (Tx, Ty, Tz, 0). The correction for a source at d from the target is
+// K(d) = -G m T(d / L) / L^2 (the reference's sign rule, periodic.c:100-112),
+// looked up at |d| with the symmetries T_a(.., -x_b, ..) = -T_a if a = b,
+// +T_a otherwise.
+__device__ __forceinline__ void ewald_kjh(const GroupParams &p, const float4 *__restrict__ tab,
+                                          float4 e, CorrSum &c)
+{
+	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
+	const float u = fabsf(e.x) * p.grid, v = fabsf(e.y) * p.grid, w = fabsf(e.z) * p.grid;
+	const int i = min((int) u, 64), j = min((int) v, 64), l = min((int) w, 64);
+	float wx[4], dx[4], ddx[4], wy[4], dy[4], ddy[4], wz[4], dz[4], ddz[4];
+	lagrange4(u - (float) i, wx, dx, ddx);
+	lagrange4(v - (float) j, wy, dy, ddy);
+	lagrange4(w - (float) l, wz, dz, ddz);
+	// y-z contraction for each x plane, then x
+	float val[3] = { 0, 0, 0 }, gx[3] = { 0, 0, 0 }, gy[3] = { 0, 0, 0 }, gz[3] = { 0, 0, 0 };
+	float hxx[3] = { 0, 0, 0 }, hyy[3] = { 0, 0, 0 }, hzz[3] = { 0, 0, 0 };
+	float hxy[3] = { 0, 0, 0 }, hxz[3] = { 0, 0, 0 }, hyz[3] = { 0, 0, 0 };
+	const int base = (i * 68 + j) * 68 + l;       // grid (i-1, j-1, l-1) at offset +1
+#pragma unroll 1
+	for (int a = 0; a < 4; a++) {
+		float y00[3] = { 0, 0, 0 }, y10[3] = { 0, 0, 0 }, y20[3] = { 0, 0, 0 };
+		float y01[3] = { 0, 0, 0 }, y11[3] = { 0, 0, 0 }, y02[3] = { 0, 0, 0 };
+#pragma unroll
+		for (int b = 0; b < 4; b++) {
+			const float4 *row = tab + base + (a * 68 + b) * 68;
+			const float4 t0 = __ldg(row), t1 = __ldg(row + 1), t2 = __ldg(row + 2), t3 = __ldg(row + 3);
+			const float T[4][3] = { { t0.x, t0.y, t0.z }, { t1.x, t1.y, t1.z },
+			                        { t2.x, t2.y, t2.z }, { t3.x, t3.y, t3.z } };
+#pragma unroll
+			for (int q = 0; q < 3; q++) {
+				const float z0 = wz[0] * T[0][q] + wz[1] * T[1][q] + wz[2] * T[2][q] + wz[3] * T[3][q];
+				const float z1 = dz[0] * T[0][q] + dz[1] * T[1][q] + dz[2] * T[2][q] + dz[3] * T[3][q];
+				const float z2 = ddz[0] * T[0][q] + ddz[1] * T[1][q] + ddz[2] * T[2][q] + ddz[3] * T[3][q];
+				y00[q] = fmaf(wy[b], z0, y00[q]);
+				y10[q] = fmaf(dy[b], z0, y10[q]);
+				y20[q] = fmaf(ddy[b], z0, y20[q]);
+				y01[q] = fmaf(wy[b], z1, y01[q]);
+				y11[q] = fmaf(dy[b], z1, y11[q]);
+				y02[q] = fmaf(wy[b], z2, y02[q]);
+			}
+		}
+#pragma unroll
+		for (int q = 0; q < 3; q++) {
+			val[q] = fmaf(wx[a], y00[q], val[q]);
+			gx[q] = fmaf(dx[a], y00[q], gx[q]);
+			hxx[q] = fmaf(ddx[a], y00[q], hxx[q]);
+			gy[q] = fmaf(wx[a], y10[q], gy[q]);
+			hxy[q] = fmaf(dx[a], y10[q], hxy[q]);
+			hyy[q] = fmaf(wx[a], y20[q], hyy[q]);
+			gz[q] = fmaf(wx[a], y01[q], gz[q]);
+			hxz[q] = fmaf(dx[a], y01[q], hxz[q]);
+			hyz[q] = fmaf(wx[a], y11[q], hyz[q]);
+			hzz[q] = fmaf(wx[a], y02[q], hzz[q]);
+		}
+	}
+	// unfold the symmetry and scale: K_a = -s_a T_a, J_ab = -s_a s_b g dT_a/du_b,
+	// H_abc = -s_a s_b s_c g^2 d2T_a/du_b du_c, all times G m / L^2
+	const float m0 = -e.w * p.inv_box * p.inv_box, m1 = m0 * p.grid, m2 = m1 * p.grid;
+#pragma unroll
+	for (int q = 0; q < 3; q++) {
+		const float sq = sg[q];
+		c.k[q] = fmaf(m0 * sq, val[q], c.k[q]);
+		c.j[3 * q + 0] = fmaf(m1 * sq * sg[0], gx[q], c.j[3 * q + 0]);
+		c.j[3 * q + 1] = fmaf(m1 * sq * sg[1], gy[q], c.j[3 * q + 1]);
+		c.j[3 * q + 2] = fmaf(m1 * sq * sg[2], gz[q], c.j[3 * q + 2]);
+		c.h[6 * q + 0] = fmaf(m2 * sq, hxx[q], c.h[6 * q + 0]);
+		c.h[6 * q + 1] = fmaf(m2 * sq, hyy[q], c.h[6 * q + 1]);
+		c.h[6 * q + 2] = fmaf(m2 * sq, hzz[q], c.h[6 * q + 2]);
+		c.h[6 * q + 3] = fmaf(m2 * sq * sg[0] * sg[1], hxy[q], c.h[6 * q + 3]);
+		c.h[6 * q + 4] = fmaf(m2 * sq * sg[0] * sg[2], hxz[q], c.h[6 * q + 4]);
+		c.h[6 * q + 5] = fmaf(m2 * sq * sg[1] * sg[2], hyz[q], c.h[6 * q + 5]);
+	}
+}
+
+// K(d) alone (tricubic value), for per-target evaluation, added to a
+__device__ __forceinline__ void ewald_k(const GroupParams &p, const float4 *__restrict__ tab,
+                                        float ex, float ey, float ez, float gm, float &ax,
+                                        float &ay, float &az)
+{
+	const float sx = ex < 0.f ? -1.f : 1.f, sy = ey < 0.f ? -1.f : 1.f, sz = ez < 0.f ? -1.f : 1.f;
+	const float u = fabsf(ex) * p.grid, v = fabsf(ey) * p.grid, w = fabsf(ez) * p.grid;
+	const int i = min((int) u, 64), j = min((int) v, 64), l = min((int) w, 64);
+	float wx[4], wy[4], wz[4], d_[4], dd_[4];
+	lagrange4(u - (float) i, wx, d_, dd_);
+	lagrange4(v - (float) j, wy, d_, dd_);
+	lagrange4(w - (float) l, wz, d_, dd_);
+	float vx = 0.f, vy = 0.f, vz = 0.f;
+	const int base = (i * 68 + j) * 68 + l;
+#pragma unroll 1
+	for (int a = 0; a < 4; a++) {
+		float yx = 0.f, yy = 0.f, yz = 0.f;
+#pragma unroll
+		for (int b = 0; b < 4; b++) {
+			const float4 *row = tab + base + (a * 68 + b) * 68;
+			const float4 t0 = __ldg(row), t1 = __ldg(row + 1), t2 = __ldg(row + 2), t3 = __ldg(row + 3);
+			yx = fmaf(wy[b], wz[0] * t0.x + wz[1] * t1.x + wz[2] * t2.x + wz[3] * t3.x, yx);
+			yy = fmaf(wy[b], wz[0] * t0.y + wz[1] * t1.y + wz[2] * t2.y + wz[3] * t3.y, yy);
+			yz = fmaf(wy[b], wz[0] * t0.z + wz[1] * t1.z + wz[2] * t2.z + wz[3] * t3.z, yz);
+		}
+		vx = fmaf(wx[a], yx, vx);
+		vy = fmaf(wx[a], yy, vy);
+		vz = fmaf(wx[a], yz, vz);
+	}
+	const float m0 = -gm * p.inv_box * p.inv_box;
+	ax = fmaf(m0 * sx, vx, ax);
+	ay = fmaf(m0 * sy, vy, ay);
+	az = fmaf(m0 * sz, vz, az);
+}
+
+// bound of |d2 T| (box units) within distance r (box units) of the source:
+// 92 at the face centres, growing as (2 r)^1.5 from 7 at r = 0.1
+__device__ __forceinline__ float ewald_h2(float r)
+{
+	const float x = fminf(2.f * r, 1.f);
+	return 92.f * x * sqrtf(x);
+}
+
+// Evaluates list entries [from, from + cnt), cnt <= 32: about the group
+// centre one entry per lane (K, J, H), or, for a group that takes per-target
+// images, every entry for every target of the lane (K at the target's
+// nearest image; FP32 per batch, carried in FP64).
+template <int TPL>
+__device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab,
+                                            const float4 *list, int from, int cnt, bool per_target,
+                                            CorrSum &c, Target (&t)[TPL], float &nev)
+{
+	const int lane = threadIdx.x & 31;
+	if (!per_target) {
+		if (lane < cnt) {
+			ewald_kjh(p, tab, list[from + lane], c);
+			nev += 1.f;
+		}
+	} else {
+		float ax[TPL], ay[TPL], az[TPL];
+#pragma unroll
+		for (int k = 0; k < TPL; k++) ax[k] = ay[k] = az[k] = 0.f;
+		for (int e = 0; e < cnt; e++) {
+			const float4 s = list[from + e];
+#pragma unroll
+			for (int k = 0; k < TPL; k++) {
+				const float dx = wrap_half(s.x - t[k].tx, p.box, p.half_box);
+				const float dy = wrap_half(s.y - t[k].ty, p.box, p.half_box);
+				const float dz = wrap_half(s.z - t[k].tz, p.box, p.half_box);
+				ewald_k(p, tab, dx, dy, dz, s.w, ax[k], ay[k], az[k]);
+				if (t[k].valid) nev += 1.f;
+			}
+		}
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			t[k].ax += (double) ax[k];
+			t[k].ay += (double) ay[k];
+			t[k].az += (double) az[k];
+		}
+	}
+	__syncwarp();
+}
+
+template <int TPL>
+__device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode *__restrict__ wt,
+                            const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
+                            const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
+                            const float *__restrict__ last_acc, const float4 *__restrict__ tab,
+                            int64_t first, int cnt, const int32_t *__restrict__ active,
+                            Target (&t)[TPL], float &nev, int *status)
+{
+	const int lane = threadIdx.x & 31;
+	const unsigned lt = (1u << lane) - 1u;
+	GroupBox g;
+	group_setup<TPL>(p, ix, iy, iz, last_acc, active, first, cnt, t, g);
+	const float hmax = fmaxf(g.hx, fmaxf(g.hy, g.hz));
+	// the gravity walk makes the same choice (walk_group)
+	const bool per_target = hmax >= p.taylor_h;
+	// straddling: the node (and, with per-target images, the group box) reaches
+	// the half-box plane; then the gravity walk's decision is repeated
+	const float margin = 8.f * p.scale;
+	const float ex = per_target ? g.hx : 0.f, ey = per_target ? g.hy : 0.f,
+	            ez = per_target ? g.hz : 0.f;
+	CorrSum c;
+#pragma unroll
+	for (int a = 0; a < 3; a++) c.k[a] = 0.f;
+#pragma unroll
+	for (int a = 0; a < 9; a++) c.j[a] = 0.f;
+#pragma unroll
+	for (int a = 0; a < 18; a++) c.h[a] = 0.f;
+
+	int sp = 0, nl = 0;
+	for (int r = lane; r < p.ntop; r += 32) S.stack[r] = r;
+	sp = p.ntop;
+	__syncwarp();
+	int guard = 0;
+	while (sp > 0) {
+		if (++guard > (1 << 24)) { atomicOr(status, TVG_ST_TIMEOUT); break; }
+		bool stop;
+		const int node = pop_nodes(S.stack, sp, status, stop);
+		if (stop) break;
+		bool accept = false, open_int = false, open_bundle = false;
+		float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
+		int nchild = 0, child = 0;
+		if (node >= 0) {
+			const tvg_wnode nd = wt[node];
+			const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
+			            dz = ioff(nd.cz, g.cz, p.scale);
+			const float gx = ioff(nd.gx, g.cx, p.scale), gy = ioff(nd.gy, g.cy, p.scale),
+			            gz = ioff(nd.gz, g.cz, p.scale);
+			const float hs = 0.5f * nd.size + margin;
+			const bool straddle = fabsf(gx) + hs + ex > p.half_box || fabsf(gy) + hs + ey > p.half_box
+			                   || fabsf(gz) + hs + ez > p.half_box;
+			bool open;
+			if (straddle) {
+				float r2;
+				open = gravity_opens(p, g, nd, node, dx, dy, dz, gx, gy, gz, r2);
+			} else {
+				// monopole error of K: G M h2 s^2 / (8 L^4) (s^2 / 4: the mean square
+				// offset of a uniform cube's mass from its centre)
+				const float rfar = (sqrtf(gx * gx + gy * gy + gz * gz) + nd.size + hmax) * p.inv_box;
+				const float l2 = p.inv_box * p.inv_box;
+				const float hs2 = ewald_h2(rfar) * nd.size2 * l2;     // h2 s^2 / L^2
+				if (p.use_bh) open = hs2 > p.ew_bh;
+				else open = nd.mass * hs2 * 0.125f * l2 > p.ew_rel * g.fac;
+			}
+			if (!open) {
+				accept = true;
+				entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
+			} else if (nd.nchild > 0) {
+				open_int = true;
+				nchild = nd.nchild;
+				child = nd.child;
+			} else {
+				open_bundle = true;
+				nchild = -nd.nchild;
+				child = nd.child;
+			}
+		}
+		const unsigned bm = __ballot_sync(0xFFFFFFFFu, accept);
+		if (accept) S.list[nl + __popc(bm & lt)] = entry;
+		nl += __popc(bm);
+		__syncwarp();
+		if (nl >= 32) {
+			ewald_batch<TPL>(p, tab, S.list, nl - 32, 32, per_target, c, t, nev);
+			nl -= 32;
+		}
+		push_children(S.stack, sp, open_int, nchild, child);
+		const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
+		if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
+		__syncwarp();
+		const int nb = __popc(bb);
+		for (int b = 0; b < nb; b++) {
+			const int2 q = S.bq[b];
+			for (int o = 0; o < q.y; o += 32) {
+				const int jj = o + lane;
+				const bool have = jj < q.y;
+				float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+				if (have) {
+					const int64_t jp = (int64_t) q.x + jj;
+					e = make_float4(ioff(ix[jp], g.cx, p.scale), ioff(iy[jp], g.cy, p.scale),
+					                ioff(iz[jp], g.cz, p.scale), p.gravity * mass_f[jp]);
+				}
+				const unsigned mb = __ballot_sync(0xFFFFFFFFu, have);
+				if (have) S.list[nl + __popc(mb & lt)] = e;
+				nl += __popc(mb);
+				__syncwarp();
+				if (nl >= 32) {
+					ewald_batch<TPL>(p, tab, S.list, nl - 32, 32, per_target, c, t, nev);
+					nl -= 32;
+				}
+			}
+		}
+		__syncwarp();
+	}
+	__syncwarp();
+	if (nl > 0) ewald_batch<TPL>(p, tab, S.list, 0, nl, per_target, c, t, nev);
+	if (per_target) return;
+	// sum over lanes (FP64), then K(d_c - t) ~ K - J t + H:tt / 2 per target
+	double K[3], J[9], H[18];
+#pragma unroll
+	for (int a = 0; a < 3; a++) K[a] = c.k[a];
+#pragma unroll
+	for (int a = 0; a < 9; a++) J[a] = c.j[a];
+#pragma unroll
+	for (int a = 0; a < 18; a++) H[a] = c.h[a];
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+#pragma unroll
+		for (int a = 0; a < 3; a++) K[a] += __shfl_xor_sync(0xFFFFFFFFu, K[a], o);
+#pragma unroll
+		for (int a = 0; a < 9; a++) J[a] += __shfl_xor_sync(0xFFFFFFFFu, J[a], o);
+#pragma unroll
+		for (int a = 0; a < 18; a++) H[a] += __shfl_xor_sync(0xFFFFFFFFu, H[a], o);
+	}
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		const double x = t[k].tx, y = t[k].ty, z = t[k].tz;
+		double out[3];
+#pragma unroll
+		for (int a = 0; a < 3; a++) {
+			const double *h = H + 6 * a;
+			out[a] = K[a] - (J[3 * a] * x + J[3 * a + 1] * y + J[3 * a + 2] * z)
+			       + 0.5 * (h[0] * x * x + h[1] * y * y + h[2] * z * z)
+			       + h[3] * x * y + h[4] * x * z + h[5] * y * z;
+		}
+		t[k].ax = out[0];
+		t[k].ay = out[1];
+		t[k].az = out[2];
+	}
+}
+
+template <int TPL, typename F>
+__global__ void __launch_bounds__(GW_THREADS)
+k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
+              const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
+              const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
+              const float *__restrict__ last_acc, const float4 *__restrict__ tab, F *acc0, F *acc1,
+              F *acc2, F *gacc0, F *gacc1, F *gacc2, int32_t *work, double *counter, int *status)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	EwaldSmem &S = ((EwaldSmem *) smem_raw)[threadIdx.x >> 5];
+	const int lane = threadIdx.x & 31;
+	double ev_acc = 0;
+	for (;;) {
+		int64_t g = 0;
+		if (lane == 0) g = atomicAdd(work, 1);
+		g = __shfl_sync(0xFFFFFFFFu, g, 0);
+		if (g >= p.ngroups) break;
+		const int64_t first = g * p.gsize;
+		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
+		Target t[TPL];
+		float nev = 0.f;
+		ewald_group<TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, first, cnt, active, t, nev,
+		                 status);
+		ev_acc += nev;
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			if (!t[k].valid) continue;
+			const int slot = lane + 32 * k;
+			const int64_t i = active ? (int64_t) active[first + slot] : first + slot;
+			acc0[i] += (F) t[k].ax;
+			acc1[i] += (F) t[k].ay;
+			acc2[i] += (F) t[k].az;
+			gacc0[i] += (F) t[k].ax;
+			gacc1[i] += (F) t[k].ay;
+			gacc2[i] += (F) t[k].az;
+		}
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) ev_acc += __shfl_xor_sync(0xFFFFFFFFu, ev_acc, o);
+	if (lane == 0 && ev_acc != 0) atomicAdd(counter, ev_acc);
 }
 
 template <typename F>
@@ -636,28 +1068,47 @@ static int group_tpl()
 	return tpl;
 }
 
-template <bool EWALD, int TPL, typename F>
+template <typename K>
+static int blocks_for(tvg_context *ctx, K kernel, size_t smem, int *cache)
+{
+	if (!*cache) {
+		TVG_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+		int per_sm = 0, nsm = 0;
+		TVG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, GW_THREADS, smem));
+		TVG_CUDA(ctx, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+		*cache = (per_sm > 0 ? per_sm : 1) * nsm;
+	}
+	return TVG_OK;
+}
+
+template <int MODE, int TPL, typename F>
 static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
-                       const float *fx, const float *fy, const float *fz, double *counter)
+                       double *counter)
 {
 	static int nblk = 0;
 	const size_t smem = sizeof(WarpSmem) * GW_WARPS;
-	if (!nblk) {
-		TVG_CUDA(ctx, cudaFuncSetAttribute(k_walk_group<EWALD, TPL, F>,
-		                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-		int per_sm = 0, nsm = 0;
-		TVG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk_group<EWALD, TPL, F>,
-		                                                             GW_THREADS, smem));
-		TVG_CUDA(ctx, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
-		nblk = (per_sm > 0 ? per_sm : 1) * nsm;
-	}
-	p.gsize = 32 * TPL;
-	p.ngroups = (p.n + p.gsize - 1) / p.gsize;
-	k_walk_group<EWALD, TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
+	TVG_CHECK(blocks_for(ctx, k_walk_group<MODE, TPL, F>, smem, &nblk));
+	k_walk_group<MODE, TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
-	    ctx->ipos[2], mass_f, last_f, fx, fy, fz, (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1],
+	    ctx->ipos[2], mass_f, last_f, (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1],
 	    (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2],
 	    (F *) ctx->f[FS_COST], ctx->work_counter, counter, ctx->status);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
+}
+
+template <int TPL, typename F>
+static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
+                        double *counter)
+{
+	static int nblk = 0;
+	const size_t smem = sizeof(EwaldSmem) * GW_WARPS;
+	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, F>, smem, &nblk));
+	k_ewald_group<TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
+	    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
+	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext, (F *) ctx->f[FS_ACC0],
+	    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1],
+	    (F *) ctx->f[FS_GACC2], ctx->work_counter + 1, counter, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }
@@ -667,10 +1118,16 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 {
 	const int64_t n = ctx->n;
 	if (n == 0) return TVG_OK;
-	if (ewald_kind != TVG_EWALD_TABLE && (parts & TVG_WALK_EWALD))
+	const bool ewald = (parts & TVG_WALK_EWALD) != 0;
+	if (!(parts & TVG_WALK_GRAVITY))
+		return tvg_fail(ctx, TVG_E_BADINPUT,
+		                "group form: the gravity and Ewald parts share the particle images; "
+		                "pass TVG_WALK_GRAVITY | TVG_WALK_EWALD");
+	if (ewald && ewald_kind != TVG_EWALD_TABLE)
 		return tvg_fail(ctx, TVG_E_STATE, "learned Ewald correction not loaded");
 	cudaStream_t s = ctx->stream;
 	if (!ctx->have_walktree) TVG_CHECK(prepare_typed<F>(ctx));
+	if (ewald && !ctx->ewald_ext) TVG_CHECK(tvg_impl_ewald_ext(ctx));
 	// FP32 copies of mass / last |a| (views when Float is float)
 	const float *mass_f = (const float *) ctx->f[FS_MASS];
 	const float *last_f = (const float *) ctx->f[FS_LAST_ACC];
@@ -681,29 +1138,16 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		mass_f = mf;
 		last_f = lf;
 	}
-	const float *fx = nullptr, *fy = nullptr, *fz = nullptr;
-	if (parts & TVG_WALK_EWALD) {
-		if (sizeof(F) == 8) {
-			// FP32 tables for the group form
-			const int npt = 65 * 65 * 65;
-			if (!ctx->ewald32) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->ewald32, 3 * 4 * (size_t) npt));
-			float *tf = ctx->ewald32;
-			for (int d = 0; d < 3; d++)
-				k_to_float<F><<<TVG_CNT(ctx, tvg_blocks(npt, 256)), 256, 0, s>>>(npt, (const F *) ctx->ewald_f[d],
-				                                                    tf + d * npt);
-			fx = tf; fy = tf + npt; fz = tf + 2 * npt;
-		} else {
-			fx = (const float *) ctx->ewald_f[0];
-			fy = (const float *) ctx->ewald_f[1];
-			fz = (const float *) ctx->ewald_f[2];
-		}
-	}
 	const tvg_config &cf = ctx->cfg;
+	const int tpl = group_tpl();
 	GroupParams p;
 	p.n = ctx->use_active ? ctx->n_active : n;
+	p.gsize = 32 * tpl;
+	p.ngroups = (p.n + p.gsize - 1) / p.gsize;
 	p.ntop = ctx->ntop;
 	p.periodic = cf.periodic;
 	p.use_bh = use_bh;
+	p.open_bundles = (cf.flags & TVG_CFG_OPEN_BUNDLES) ? 1 : 0;
 	p.scale = (float) (cf.periodic ? ctx->dsize / 4294967296.0 : ctx->dsize / 2147483648.0);
 	p.box = (float) (cf.periodic ? cf.boxsize : 0.0);
 	p.half_box = (float) (cf.periodic ? 0.5 * cf.boxsize : 3.0e38);
@@ -715,29 +1159,38 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	p.inv_eps2 = (float) (1.0 / (h * h));
 	p.c16 = (float) (1.0 / (16.0 * h * h * h));
 	p.near2 = (float) (h * h * 1.001);
-	p.box2grid = (float) (cf.periodic ? 2.0 * 64.0 / cf.boxsize : 0.0);
-	const int tpl = group_tpl();
+	p.grid = (float) (cf.periodic ? 2.0 * 64.0 / cf.boxsize : 0.0);
+	p.inv_box = (float) (cf.periodic ? 1.0 / cf.boxsize : 0.0);
+	p.ew_rel = (float) (ctx->ewald_open_rel / cf.open_rel);   // times g.fac: alpha_E |a_old| / G
+	p.ew_bh = (float) (ctx->ewald_open_bh * cf.open_bh);
+	// half extent beyond which a group takes per-target images with the Ewald
+	// part: the third-order remainder of the expansion about the centre grows
+	// as (h / L)^3 (2e-4 of the force at h = L / 100 on the 256^3 box at z = 50)
+	p.taylor_h = (float) (cf.periodic ? cf.boxsize / 64.0 : 3.0e38);
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16, s));
-	for (int part = 0; part < 2; part++) {
-		const bool ew = part == 1;
-		if (!(parts & (ew ? TVG_WALK_EWALD : TVG_WALK_GRAVITY))) continue;
-		TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 4, s));
-		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
-		double *cnt = ctx->counters + (ew ? 1 : 0);
-		if (ew && tpl == 1) TVG_CHECK((launch_walk<true, 1, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
-		else if (ew) TVG_CHECK((launch_walk<true, 2, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
-		else if (tpl == 1) TVG_CHECK((launch_walk<false, 1, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
-		else TVG_CHECK((launch_walk<false, 2, F>(ctx, p, mass_f, last_f, fx, fy, fz, cnt)));
-		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
-		TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
-		float ms = 0;
-		TVG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-		ctx->phase_ms[ew ? 5 : 4] = ms;
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 8, s));
+	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+	double *cnt = ctx->counters;
+	if (ewald && tpl == 1) TVG_CHECK((launch_walk<GM_CENTRE, 1, F>(ctx, p, mass_f, last_f, cnt)));
+	else if (ewald) TVG_CHECK((launch_walk<GM_CENTRE, 2, F>(ctx, p, mass_f, last_f, cnt)));
+	else if (tpl == 1) TVG_CHECK((launch_walk<GM_NEAREST, 1, F>(ctx, p, mass_f, last_f, cnt)));
+	else TVG_CHECK((launch_walk<GM_NEAREST, 2, F>(ctx, p, mass_f, last_f, cnt)));
+	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
+	if (ewald) {
+		if (tpl == 1) TVG_CHECK((launch_ewald<1, F>(ctx, p, mass_f, last_f, cnt + 1)));
+		else TVG_CHECK((launch_ewald<2, F>(ctx, p, mass_f, last_f, cnt + 1)));
 	}
-	double cnt[2];
-	TVG_CUDA(ctx, cudaMemcpy(cnt, ctx->counters, 16, cudaMemcpyDeviceToHost));
-	ctx->last_counts[0] = cnt[0];
-	ctx->last_counts[1] = cnt[1];
+	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+	TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[2]));
+	float ms = 0, ms_e = 0;
+	TVG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+	TVG_CUDA(ctx, cudaEventElapsedTime(&ms_e, ctx->ev[1], ctx->ev[2]));
+	ctx->phase_ms[4] = ms;
+	ctx->phase_ms[5] = ms_e;
+	double c[2];
+	TVG_CUDA(ctx, cudaMemcpy(c, ctx->counters, 16, cudaMemcpyDeviceToHost));
+	ctx->last_counts[0] = c[0];
+	ctx->last_counts[1] = c[1];
 	return TVG_OK;
 }
 

@@ -23,6 +23,7 @@ WALK_GRAVITY, WALK_EWALD = 1, 2
 EWALD_TABLE, EWALD_MLP = 0, 1
 BUILD_EXACT_MOMENTS = 1
 CFG_FIX_SMALL_TOPNODES = 1
+CFG_OPEN_BUNDLES = 2
 
 F_TYPE, F_TIME_BIN, F_IT_DRIFT, F_IT_KICK, F_KEY, F_ID, F_COST = (1 << k for k in range(7))
 F_POS, F_VEL, F_ACC, F_MASS, F_GRAV_ACC, F_LAST_ACC, F_TREE_PARENT = (1 << k for k in range(7, 14))
@@ -250,6 +251,34 @@ class GravityContext:
         g, e = C.c_double(), C.c_double()
         self._check(self.lib.tvg_walk_counters(self.ctx, C.byref(g), C.byref(e)), "walk_counters")
         return g.value, e.value
+
+    def set_opening(self, open_bh, open_rel):
+        """TREE_OPEN_PARAM_BH (theta^2) and TREE_OPEN_PARAM_REL for later walks."""
+        self._check(self.lib.tvg_set_opening(self.ctx, C.c_double(open_bh), C.c_double(open_rel)),
+                    "set_opening")
+
+    def set_ewald_opening(self, rel_alpha=2.5e-4, bh_factor=0.5):
+        """Opening of the group form's Ewald walk (see tvg_set_ewald_opening)."""
+        self._check(self.lib.tvg_set_ewald_opening(self.ctx, C.c_double(rel_alpha),
+                                                   C.c_double(bh_factor)), "set_ewald_opening")
+
+    def forcetest(self, targets, parts=None):
+        """Gravity_Forcetest: FP64 direct force on the targets (sorted-order
+        indices), Ewald-summed when ``parts`` has WALK_EWALD (default: when
+        periodic). Returns (a_direct (3, nt), a_tree (3, nt), {"rms", "p99",
+        "mean", "max"} of the relative error)."""
+        if parts is None:
+            parts = WALK_GRAVITY | (WALK_EWALD if self.cfg.periodic else 0)
+        t = np.ascontiguousarray(targets, dtype=np.int64)
+        nt = len(t)
+        ad = np.empty((3, nt), np.float64)
+        at = np.empty((3, nt), np.float64)
+        err = np.empty(4, np.float64)
+        self._check(self.lib.tvg_forcetest(self.ctx, C.c_uint32(parts), C.c_int64(nt),
+                                           C.c_void_p(_ptr(t)),
+                                           C.c_void_p(_ptr(ad)), C.c_void_p(_ptr(at)),
+                                           C.c_void_p(_ptr(err))), "forcetest")
+        return ad, at, dict(zip(("rms", "p99", "mean", "max"), map(float, err)))
 
     # ------------------------------------------------ active set, timing
 
