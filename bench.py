@@ -6,15 +6,19 @@ cosmological box of 256^3 particles, 100 Mpc/h, Zel'dovich displacements at
 z = 50 from a seeded Gaussian field (Eisenstein & Hu 1998 P(k)), softening
 1/30 of the mean spacing. One step = one tree-force evaluation of all
 particles: Peano-Hilbert keys, sort of every particle field, top nodes, tree
-build, the gravity walk with the relative opening criterion (errtol 0.005,
-|a_old| from an untimed Barnes-Hut prepare pass, as src/accel.c:51-71 does)
-and the Ewald periodic correction walk.
+build, the gravity walk with the relative opening criterion (|a_old| from an
+untimed Barnes-Hut prepare pass, as src/accel.c:51-71 does) and the Ewald
+periodic correction.
 
-Our arm: the group form (FP32 integer-offset walk, warp per PH group) with
-the tabulated Ewald correction, particles resident in HBM (`value`), and the
-same step through the C ABI with host buffers (`e2e`). The plain GPU form
-(the reference algorithm, one thread per particle, exact moments) is timed on
-a strided subset of the particles and reported beside it.
+Our arm: the group form (FP32 integer-offset walk, warp per PH group, a
+per-group Ewald walk) at the opening parameter that brings the rms force
+error below 1e-3 (TREE_OPEN_PARAM_REL 6e-5 on this box; the error is measured
+in every run against an FP64 Ewald-summed direct sum over all particles for
+10^4 random particles), particles resident in HBM (`value`), and the same
+step through the C ABI with host buffers (`e2e`). The plain GPU form (the
+reference algorithm, one thread per particle, FP64, exact moments, the
+reference's TREE_OPEN_PARAM_REL 0.005) is timed on a strided subset of the
+particles and reported beside it with its own measured error.
 `--impl reference`: the unmodified reference C code (oracle/_ref timing
 build) on the host cores, the walk timed on a strided subset.
 
@@ -57,6 +61,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak loop (profiling runs)")
+    ap.add_argument("--open-rel", type=float, default=6e-5,
+                    help="TREE_OPEN_PARAM_REL of the group form")
+    ap.add_argument("--ewald-alpha", type=float, default=4e-4,
+                    help="opening of the group form's Ewald walk (relative to |a_old|)")
+    ap.add_argument("--plain-open-rel", type=float, default=0.005,
+                    help="TREE_OPEN_PARAM_REL of the plain form (the reference's value)")
     ap.add_argument("--forcetest-targets", type=int, default=10000,
                     help="particles in the FP64 direct-sum error check (0: skip)")
     return ap.parse_args()
@@ -224,9 +234,13 @@ def workload_config(args, p, ws):
         "workload": f"zeldovich_{args.nside}^3_periodic_z50",
         "n_particles": int(p.n), "box_mpc_h": 100.0, "z_start": 50.0,
         "softening_kpc_h": round(float(p.softening), 4),
-        "criterion": "relative, TREE_OPEN_PARAM_REL 0.005, |a_old| from a BH (theta^2 0.25) pass",
-        "ewald": "65^3 table, trilinear",
-        "form": "group: warp per 32-particle PH group, FP32 on 32-bit integer box offsets",
+        "criterion": (f"relative, TREE_OPEN_PARAM_REL {args.open_rel:g} (group form), "
+                      f"{args.plain_open_rel:g} (plain form); |a_old| from a BH (theta^2 0.25) pass"),
+        "ewald": (f"group form: per-group Ewald walk, tricubic lattice-sum table (K, dK, d2K at node "
+                  f"centres of mass, second-order expansion about the group centre), opening "
+                  f"alpha_E {args.ewald_alpha:g}; plain form: the reference's Ewald walk, 65^3 "
+                  f"table, trilinear"),
+        "form": "group: warp per 64-particle PH group (2 per lane), FP32 on 32-bit integer box offsets",
         "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
         "l2": "inputs larger than L2 (16.7M particles, ~2 GB of particle state)",
     }
@@ -248,11 +262,13 @@ def main():
     ctx.upload(p.pos, p.mass)
     ctx.set_domain((0.0, 0.0, 0.0), p.box)
     ctx.ewald_init()
+    ctx.set_ewald_opening(args.ewald_alpha)
     fp32_peak = 0.0 if args.no_peak else ctx.fp32_peak(ms_target=1500.0)
 
     # prepare step (accel.c:51-71): BH pass, |a| -> Last_Acc_Mag
     ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
     ctx.save_last_accel()
+    ctx.set_opening(0.25, args.open_rel)
     for _ in range(args.warmup):
         ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
 
@@ -326,7 +342,7 @@ def main():
     # ---- roofline of the dominant kernel (the gravity walk)
     achieved = FLOP_PER_GRAV * grav_i / (walk_ms * 1e-3) / 1e12
     roofline = {
-        "kernel": "k_walk_group<false> (gravity walk)", "bound": "fp32",
+        "kernel": "k_walk_group<GM_CENTRE, 2, float> (gravity walk)", "bound": "fp32",
         "achieved": round(achieved, 3), "peak": round(fp32_peak, 3), "unit": "TFLOP/s",
         "frac": round(achieved / fp32_peak, 4) if fp32_peak > 0 else None,
         "peak_source": "measured FFMA loop on this GPU (1.5 s, sustained under the power cap)",
@@ -354,6 +370,7 @@ def main():
         c64.upload(p.pos, p.mass)
         c64.set_domain((0.0, 0.0, 0.0), p.box)
         c64.ewald_init()
+        c64.set_opening(0.25, args.plain_open_rel)
         c64.timer_start()
         c64.peano_keys()
         c64.sort_particles(want_perm=False)
@@ -416,7 +433,11 @@ def main():
             "clocks": clk,
             "phases_ms": ph,
             "interactions_per_particle": {"gravity": round(grav_i / args.steps / n, 1),
-                                          "ewald": round(ew_i / args.steps / n, 1)},
+                                          "ewald_evaluations": round(ew_i / args.steps / n, 1)},
+            "ewald_walk": {"kernel": "k_ewald_group<2, float>",
+                           "ms_per_step": round(ew_ms / args.steps, 2),
+                           "evaluations_per_group_of_64": round(ew_i / args.steps / (n / 64), 1),
+                           "evaluation": "tricubic K, dK, d2K: 64 float4 loads, ~1100 FP32 ops"},
             "plain_form": plain,
             "accuracy": accuracy,
         }

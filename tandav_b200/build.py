@@ -25,6 +25,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
           "-I", str(ROOT / "include")]
 # translation units that replay the reference's rounding order
 NO_FMA = {"tvg_walk_plain.cu", "tvg_tree.cu", "tvg_ewald.cu", "tvg_keys.cu"}
+# FP32 walks with no parity constraint: denormals flushed (rsqrtf and the
+# divisions then need no range fix-up around MUFU)
+FTZ = {"tvg_walk_group.cu"}
 
 
 def nvcc() -> str:
@@ -42,6 +45,8 @@ def _compile(src: Path) -> Path:
     flags = list(COMMON)
     if src.name in NO_FMA:
         flags.append("-fmad=false")
+    if src.name in FTZ:
+        flags.append("-ftz=true")
     cmd = [nvcc(), *ARCH, *flags, "-c", str(src), "-o", str(obj)]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:

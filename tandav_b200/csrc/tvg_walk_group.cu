@@ -233,6 +233,14 @@ struct EwaldSmem {
 	int2 bq[GW_BQ];
 };
 
+// per-lane sums over accepted sources of m K, m J and m H (about the group
+// centre), FP32 (a few hundred terms per lane)
+struct CorrSum {
+	float k[3];
+	float j[9];     // J[a][b] = dK_a / dd_b
+	float h[18];    // H[a][xx, yy, zz, xy, xz, yz]
+};
+
 struct Target {
 	float tx, ty, tz;       // offset from the group centre
 	double ax, ay, az;      // FP32 sums of each list flush, carried in FP64
@@ -661,14 +669,6 @@ __device__ __forceinline__ void lagrange4(float t, float w[4], float d[4], float
 	dd[2] = 1.f - 3.f * t;
 	dd[3] = t;
 }
-
-// per-lane sums over accepted sources of m K, m J and m H (about the group
-// centre), FP32 (at most a few hundred terms per lane)
-struct CorrSum {
-	float k[3];
-	float j[9];     // J[a][b] = dK_a / dd_b
-	float h[18];    // H[a][xx, yy, zz, xy, xz, yz]
-};
 
 // The lattice-minus-image force T(x) (box units, unit G m, target at x from
 // the source) is tabulated on x = 0.5 i / 64, i = -1..66 per axis (one ghost
