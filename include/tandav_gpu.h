@@ -295,6 +295,81 @@ int tvg_set_opening(tvg_context *ctx, double open_bh, double open_rel);
  * Defaults 2.5e-4 and 0.5. */
 int tvg_set_ewald_opening(tvg_context *ctx, double rel_alpha, double bh_factor);
 
+/* ------------------------------------------- hierarchical time stepping */
+
+/* Parameters of the timeline and background cosmology that the kick, drift
+ * and time-step code reads (Time.Begin/End, Cosmo, Param; src/timestep.c,
+ * src/cosmology.c, src/comoving.c). */
+typedef struct {
+	int32_t comoving;          /* COMOVING: time is the expansion factor a */
+	double time_begin;         /* Time.Begin */
+	double time_end;           /* Time.End */
+	double hubble_constant;    /* Cosmo.Hubble_Constant (code units: 0.1 for km/s/kpc) */
+	double omega_matter;       /* Cosmo.Omega_Matter */
+	double omega_lambda;       /* Cosmo.Omega_Lambda */
+	double omega_rad;          /* Cosmo.Omega_Rad */
+	double omega_0;            /* Cosmo.Omega_0 = Omega_Matter + Omega_Lambda + OMEGA_RAD */
+	double omega_baryon;       /* Cosmo.Omega_Baryon */
+	double rho_crit0;          /* Cosmo.Rho_Crit0 (code units) */
+	double time_int_accuracy;  /* Param.Time_Int_Accuracy */
+	double max_timestep;       /* Param.Max_Timestep */
+	double displ_constraint;   /* TIME_DISPL_CONSTRAINT (Config) */
+} tvg_timeline_config;
+
+/* struct IntegerTimeLine Int_Time, the parts of struct TimeData Time and of
+ * Cosmo that change, and the step signals (src/timestep.h:24-32,
+ * src/signal.h). */
+typedef struct {
+	uint32_t beg, current, next, end, step, next_sync_point;   /* Int_Time */
+	double time_current, time_next, time_step;                 /* Time.Current/Next/Step */
+	double step_max, step_min;                                 /* Time.Step_Max/Min */
+	double expansion_factor, hubble_parameter;                 /* Cosmo (Set_Current_Cosmology) */
+	float dt_max_global;                                       /* Dt_Max_Global */
+	int32_t max_active_bin;                                    /* Time.Max_Active_Bin */
+	int32_t time_bin_min, time_bin_max;
+	int32_t sync_point, first_step, prepare_step;              /* Sig */
+	int64_t n_active;                                          /* NActive_Particles */
+	int64_t step_counter;                                      /* Time.Step_Counter */
+} tvg_timeline_state;
+
+/* Setup_Time_Integration (timestep.c:108-178) and setup_kick_drift_factors
+ * (comoving.c:109-153): the integer timeline, and with COMOVING the 512-knot
+ * kick/drift factor tables (FP64 quadrature on the device, natural cubic
+ * spline; knot 0 at a = 0 as in the reference). All particles start active. */
+int tvg_timeline_init(tvg_context *ctx, const tvg_timeline_config *cfg);
+/* The 512 knots a_i and the tabulated kick and drift integrals (comoving). */
+int tvg_download_kick_drift_table(tvg_context *ctx, double *a, double *kick, double *drift);
+/* Particle_Kick_Step / Particle_Drift_Step (comoving.c:30-50, kick.c:78-84,
+ * drift.c:115-121) for two points of the integer timeline. */
+int tvg_kick_drift_factors(tvg_context *ctx, uint32_t it_curr, uint32_t it_next, double *kick,
+                           double *drift);
+/* Set_New_Timesteps (timestep.c:35-89): new time bins of all particles from
+ * |Grav_Acc| (set_new_particle_timebins, timestep.c:200-236), the system step
+ * and the Active_Particle_List of the next step, kept on the device. */
+int tvg_set_new_timesteps(tvg_context *ctx);
+/* Kick_First_Halfstep / Kick_Second_Halfstep (kick.c:9-70) over the active
+ * particles; the second also ends the step (Sig.First_Step = false, as
+ * Update(AFTER_STEP) does). The GPU path rebuilds the tree every force
+ * computation, so the node kicks of the reference have no counterpart. */
+int tvg_kick_first_halfstep(tvg_context *ctx);
+int tvg_kick_second_halfstep(tvg_context *ctx);
+/* Drift_To_Sync_Point (drift.c:12-62): drifts the active particles to
+ * Int_Time.Next, wraps all particles into the box, advances the clock. */
+int tvg_drift_to_sync_point(tvg_context *ctx);
+/* Reads / replaces the timeline state (e.g. to restart). */
+int tvg_timeline_get(tvg_context *ctx, tvg_timeline_state *st);
+int tvg_timeline_set(tvg_context *ctx, const tvg_timeline_state *st);
+/* Number of particles in each of the 32 time bins. */
+int tvg_rung_histogram(tvg_context *ctx, int32_t *hist);
+/* Compute_Acceleration (accel.c:15-71) with the domain decomposition of the
+ * single-rank reference: keys, sort (Sort_Particles_By_Peano_Key rebuilds
+ * the Active_Particle_List, peano.c:42), top nodes, tree build, then for the
+ * active particles safe_last_accel (Last_Acc_Mag = |Acc|, Acc = 0), with
+ * prepare (Sig.Prepare_Step) a Barnes-Hut walk and safe_last_accel again, and
+ * the relative-criterion walk. Without a timeline every particle is active. */
+int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts, int32_t ewald_kind,
+                             int32_t prepare);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,10 @@ EXPORTS = (
     "tvg_force_step", "tvg_phase_times", "tvg_walk_counters", "tvg_set_active", "tvg_timer",
     "tvg_launch_count", "tvg_host_alloc", "tvg_host_free", "tvg_fp32_peak",
     "tvg_sort_keys_noalloc", "tvg_forcetest", "tvg_set_opening",
-    "tvg_set_ewald_opening",
+    "tvg_set_ewald_opening", "tvg_timeline_init", "tvg_download_kick_drift_table",
+    "tvg_kick_drift_factors", "tvg_set_new_timesteps", "tvg_kick_first_halfstep",
+    "tvg_kick_second_halfstep", "tvg_drift_to_sync_point", "tvg_timeline_get", "tvg_timeline_set",
+    "tvg_rung_histogram", "tvg_compute_acceleration",
 )
 
 

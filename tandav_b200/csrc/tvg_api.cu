@@ -37,6 +37,9 @@ int tvg_sync_status(tvg_context *ctx, const char *phase)
 		return tvg_fail(ctx, TVG_E_TIMEOUT, "%s: bounded device wait expired", phase);
 	if (st & TVG_ST_LIST_OVERFLOW)
 		return tvg_fail(ctx, TVG_E_TREE_FULL, "%s: interaction list overflow", phase);
+	if (st & TVG_ST_TIMESTEP)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "%s: time step below the integer timeline's resolution "
+		                "or not finite (timestep.c:219-222)", phase);
 	return tvg_fail(ctx, TVG_E_CUDA, "%s: device status 0x%x", phase, st);
 }
 
@@ -143,7 +146,9 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->ipos[0], ctx->ipos[1], ctx->ipos[2], ctx->wtree, ctx->group_first,
 	                 ctx->work_counter, ctx->counters, ctx->ewald_f[0], ctx->ewald_f[1],
 	                 ctx->ewald_f[2], ctx->ewald_f[3], ctx->ewald_raw, ctx->ewald32,
-	                 ctx->ewald_ext, ctx->active };
+	                 ctx->ewald_ext, ctx->active, ctx->kd_x, ctx->kd_kick, ctx->kd_drift,
+	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
+	                 ctx->act_off };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

@@ -45,7 +45,8 @@ enum {
 	TVG_ST_BADPOS = 2,
 	TVG_ST_TREE_FULL = 4,
 	TVG_ST_TIMEOUT = 8,
-	TVG_ST_LIST_OVERFLOW = 16
+	TVG_ST_LIST_OVERFLOW = 16,
+	TVG_ST_TIMESTEP = 32
 };
 
 struct tvg_buf {
@@ -147,6 +148,17 @@ struct tvg_context {
 	bool use_active = false;
 	int64_t launches = 0;              // kernels launched by this context
 
+	// hierarchical time integration (tvg_integrate.cu)
+	bool have_timeline = false;
+	struct {
+		tvg_timeline_config cfg;
+		tvg_timeline_state state;
+	} tl{};
+	double *kd_x = nullptr, *kd_kick = nullptr, *kd_drift = nullptr;   // 512 knots
+	double *kd_m2k = nullptr, *kd_m2d = nullptr, *kd_work = nullptr;   // spline second derivatives
+	void *tl_scratch = nullptr;        // reductions (256 B)
+	int32_t *act_flag = nullptr, *act_off = nullptr;
+
 	// timings
 	cudaEvent_t ev[16];
 	double phase_ms[8] = { 0 };
@@ -178,6 +190,7 @@ int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts);
 int tvg_impl_walk_group(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind);
 int tvg_impl_save_last_accel(tvg_context *ctx);
 int tvg_impl_zero_accel(tvg_context *ctx);
+int tvg_impl_active_from_bins(tvg_context *ctx);
 
 static inline size_t tvg_fsize(const tvg_context *ctx) { return (size_t) ctx->cfg.float_bytes; }
 

@@ -392,34 +392,66 @@ int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts)
 	return walk_typed<double>(ctx, use_bh, parts);
 }
 
-// accel.c:28-43: Last_Acc_Mag = |Acc|, Acc = 0
+// accel.c:28-43: Last_Acc_Mag = |Acc|, Acc = 0 (the active particles)
 template <typename F>
-__global__ void k_save_last(int64_t n, F *a0, F *a1, F *a2, F *last)
+__global__ void k_save_last(int64_t n, const int32_t *__restrict__ active, F *a0, F *a1, F *a2,
+                            F *last)
 {
-	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (i >= n) return;
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k >= n) return;
+	const int64_t i = active ? active[k] : k;
 	last[i] = fsqrt<F>(a0[i] * a0[i] + a1[i] * a1[i] + a2[i] * a2[i]);
 	a0[i] = a1[i] = a2[i] = 0;
 }
 
 int tvg_impl_save_last_accel(tvg_context *ctx)
 {
-	const int64_t n = ctx->n;
+	const int64_t n = ctx->use_active ? ctx->n_active : ctx->n;
+	const int32_t *act = ctx->use_active ? ctx->active : nullptr;
 	if (!n) return TVG_OK;
 	if (ctx->cfg.float_bytes == 4)
 		k_save_last<float><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
-		    n, (float *) ctx->f[FS_ACC0], (float *) ctx->f[FS_ACC1], (float *) ctx->f[FS_ACC2],
+		    n, act, (float *) ctx->f[FS_ACC0], (float *) ctx->f[FS_ACC1], (float *) ctx->f[FS_ACC2],
 		    (float *) ctx->f[FS_LAST_ACC]);
 	else
 		k_save_last<double><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
-		    n, (double *) ctx->f[FS_ACC0], (double *) ctx->f[FS_ACC1], (double *) ctx->f[FS_ACC2],
+		    n, act, (double *) ctx->f[FS_ACC0], (double *) ctx->f[FS_ACC1], (double *) ctx->f[FS_ACC2],
 		    (double *) ctx->f[FS_LAST_ACC]);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }
 
+template <typename F>
+__global__ void k_zero_active(int64_t n, const int32_t *__restrict__ active, F *a0, F *a1, F *a2,
+                              F *g0, F *g1, F *g2, F *cost)
+{
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k >= n) return;
+	const int64_t i = active[k];
+	a0[i] = a1[i] = a2[i] = 0;
+	g0[i] = g1[i] = g2[i] = 0;
+	cost[i] = 0;
+}
+
+// Acc, Grav_Acc and Cost of the active particles (all when no list is set)
 int tvg_impl_zero_accel(tvg_context *ctx)
 {
+	if (ctx->use_active) {
+		const int64_t n = ctx->n_active;
+		if (!n) return TVG_OK;
+		void **f = ctx->f;
+		if (ctx->cfg.float_bytes == 4)
+			k_zero_active<float><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
+			    n, ctx->active, (float *) f[FS_ACC0], (float *) f[FS_ACC1], (float *) f[FS_ACC2],
+			    (float *) f[FS_GACC0], (float *) f[FS_GACC1], (float *) f[FS_GACC2], (float *) f[FS_COST]);
+		else
+			k_zero_active<double><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
+			    n, ctx->active, (double *) f[FS_ACC0], (double *) f[FS_ACC1], (double *) f[FS_ACC2],
+			    (double *) f[FS_GACC0], (double *) f[FS_GACC1], (double *) f[FS_GACC2],
+			    (double *) f[FS_COST]);
+		TVG_CUDA(ctx, cudaGetLastError());
+		return TVG_OK;
+	}
 	const size_t b = tvg_fsize(ctx) * ctx->n;
 	const int slots[] = { FS_ACC0, FS_ACC1, FS_ACC2, FS_GACC0, FS_GACC1, FS_GACC2, FS_COST };
 	for (int s : slots) TVG_CUDA(ctx, cudaMemsetAsync(ctx->f[s], 0, b, ctx->stream));

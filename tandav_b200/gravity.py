@@ -55,6 +55,30 @@ class Particles(C.Structure):
                 ("last_acc_mag", C.c_void_p), ("tree_parent", C.c_void_p)]
 
 
+class TimelineConfig(C.Structure):
+    _fields_ = [("comoving", C.c_int32), ("time_begin", C.c_double), ("time_end", C.c_double),
+                ("hubble_constant", C.c_double), ("omega_matter", C.c_double),
+                ("omega_lambda", C.c_double), ("omega_rad", C.c_double), ("omega_0", C.c_double),
+                ("omega_baryon", C.c_double), ("rho_crit0", C.c_double),
+                ("time_int_accuracy", C.c_double), ("max_timestep", C.c_double),
+                ("displ_constraint", C.c_double)]
+
+
+class TimelineState(C.Structure):
+    _fields_ = [("beg", C.c_uint32), ("current", C.c_uint32), ("next", C.c_uint32),
+                ("end", C.c_uint32), ("step", C.c_uint32), ("next_sync_point", C.c_uint32),
+                ("time_current", C.c_double), ("time_next", C.c_double), ("time_step", C.c_double),
+                ("step_max", C.c_double), ("step_min", C.c_double),
+                ("expansion_factor", C.c_double), ("hubble_parameter", C.c_double),
+                ("dt_max_global", C.c_float), ("max_active_bin", C.c_int32),
+                ("time_bin_min", C.c_int32), ("time_bin_max", C.c_int32),
+                ("sync_point", C.c_int32), ("first_step", C.c_int32), ("prepare_step", C.c_int32),
+                ("n_active", C.c_int64), ("step_counter", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class TvgError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -110,12 +134,30 @@ class GravityContext:
 
     # ------------------------------------------------------------ data
 
-    def upload(self, pos, mass, vel=None, ids=None, last_acc=None):
+    def upload(self, pos, mass, vel=None, ids=None, last_acc=None, types=None, time_bin=None,
+               it_drift=None, it_kick=None, acc=None, grav_acc=None):
         ft = self.ft
         n = int(np.asarray(mass).shape[0])
         self._keep = []
         p = Particles()
         fields = F_POS | F_MASS
+        for name, bit, arr, dt in (("type", F_TYPE, types, np.int32),
+                                   ("time_bin", F_TIME_BIN, time_bin, np.int32),
+                                   ("it_drift_pos", F_IT_DRIFT, it_drift, np.uint32),
+                                   ("it_kick_pos", F_IT_KICK, it_kick, np.uint32)):
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=dt)
+                self._keep.append(a)
+                setattr(p, name, a.ctypes.data)
+                fields |= bit
+        for name, bit, arr in (("acc", F_ACC, acc), ("grav_acc", F_GRAV_ACC, grav_acc)):
+            if arr is not None:
+                fields |= bit
+                dst = getattr(p, name)
+                for k in range(3):
+                    a = np.ascontiguousarray(arr[k], dtype=ft)
+                    self._keep.append(a)
+                    dst[k] = a.ctypes.data
         for k in range(3):
             a = np.ascontiguousarray(pos[k], dtype=ft)
             self._keep.append(a)
@@ -256,6 +298,57 @@ class GravityContext:
         """TREE_OPEN_PARAM_BH (theta^2) and TREE_OPEN_PARAM_REL for later walks."""
         self._check(self.lib.tvg_set_opening(self.ctx, C.c_double(open_bh), C.c_double(open_rel)),
                     "set_opening")
+
+    # ------------------------------------------- hierarchical time stepping
+
+    def timeline_init(self, **kw):
+        """Setup_Time_Integration (+ comoving kick/drift tables); keyword
+        arguments are the TimelineConfig fields."""
+        cfg = TimelineConfig(**kw)
+        self._check(self.lib.tvg_timeline_init(self.ctx, C.byref(cfg)), "timeline_init")
+
+    def kick_drift_table(self):
+        a, k, d = (np.zeros(512) for _ in range(3))
+        self._check(self.lib.tvg_download_kick_drift_table(
+            self.ctx, C.c_void_p(_ptr(a)), C.c_void_p(_ptr(k)), C.c_void_p(_ptr(d))), "kd_table")
+        return a, k, d
+
+    def kick_drift_factors(self, it_curr, it_next):
+        k, d = C.c_double(), C.c_double()
+        self._check(self.lib.tvg_kick_drift_factors(self.ctx, C.c_uint32(it_curr), C.c_uint32(it_next),
+                                                    C.byref(k), C.byref(d)), "kd_factors")
+        return k.value, d.value
+
+    def set_new_timesteps(self):
+        self._check(self.lib.tvg_set_new_timesteps(self.ctx), "set_new_timesteps")
+
+    def kick_first_halfstep(self):
+        self._check(self.lib.tvg_kick_first_halfstep(self.ctx), "kick_first_halfstep")
+
+    def kick_second_halfstep(self):
+        self._check(self.lib.tvg_kick_second_halfstep(self.ctx), "kick_second_halfstep")
+
+    def drift_to_sync_point(self):
+        self._check(self.lib.tvg_drift_to_sync_point(self.ctx), "drift_to_sync_point")
+
+    def timeline(self):
+        st = TimelineState()
+        self._check(self.lib.tvg_timeline_get(self.ctx, C.byref(st)), "timeline_get")
+        return st
+
+    def set_timeline(self, st):
+        self._check(self.lib.tvg_timeline_set(self.ctx, C.byref(st)), "timeline_set")
+
+    def rung_histogram(self):
+        h = np.zeros(32, np.int32)
+        self._check(self.lib.tvg_rung_histogram(self.ctx, C.c_void_p(_ptr(h))), "rung_histogram")
+        return h
+
+    def compute_acceleration(self, form=FORM_GROUP, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE,
+                             prepare=False):
+        self._check(self.lib.tvg_compute_acceleration(self.ctx, C.c_int32(form), C.c_uint32(parts),
+                                                      C.c_int32(ewald_kind), C.c_int32(int(prepare))),
+                    "compute_acceleration")
 
     def set_ewald_opening(self, rel_alpha=2.5e-4, bh_factor=0.5):
         """Opening of the group form's Ewald walk (see tvg_set_ewald_opening)."""
