@@ -370,6 +370,42 @@ int tvg_rung_histogram(tvg_context *ctx, int32_t *hist);
 int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts, int32_t ewald_kind,
                              int32_t prepare);
 
+/* ---------------------------------------------- learned Ewald correction */
+
+/* Training of the 3 -> 64 -> 64 -> 3 network (tanh) that stands in for the
+ * Ewald table interpolation (no reference counterpart): n_samples points
+ * uniform on the folded octant with FP64 Ewald-sum targets, Adam over
+ * minibatches of `batch`, cosine learning-rate decay from lr to lr_final.
+ * resume != 0 continues from the current weights. */
+typedef struct {
+	int32_t steps;
+	int32_t batch;
+	int64_t n_samples;
+	float lr, lr_final;
+	uint64_t seed;
+	int32_t resume;
+} tvg_mlp_train_config;
+
+/* Number of network parameters (float). */
+#define TVG_MLP_NPARAM 4611
+
+/* Trains on the device; final_loss = mean square residual per component
+ * (box units) of the FP32 weights over all samples. Leaves the weights
+ * unjudged (see tvg_ewald_mlp_judge). */
+int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config *cfg, float *final_loss);
+/* Copies the FP32 parameters out (set = 0) or in (set != 0). */
+int tvg_ewald_mlp_weights(tvg_context *ctx, float *params, int32_t set);
+/* Gradient of the mean-square loss over n samples x[3n] (octant, box units)
+ * with residual targets y[3n] (T(x) - 4 pi x / 3), from the training kernels. */
+int tvg_ewald_mlp_grad(tvg_context *ctx, int64_t n, const float *x, const float *y, float *grad,
+                       float *loss);
+/* T(x) at n octant points x[3n] (box units) from the BF16 weights. */
+int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, double *t);
+/* The exact FP64 table (tvg_ewald_init) judges the BF16 network at its 65^3
+ * nodes: max and rms |T_mlp - T|; the walk accepts TVG_EWALD_MLP only while
+ * the max error is at most max_allowed. */
+int tvg_ewald_mlp_judge(tvg_context *ctx, double max_allowed, double *max_err, double *rms_err);
+
 #ifdef __cplusplus
 }
 #endif

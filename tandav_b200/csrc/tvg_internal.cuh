@@ -148,6 +148,12 @@ struct tvg_context {
 	bool use_active = false;
 	int64_t launches = 0;              // kernels launched by this context
 
+	// learned Ewald correction (tvg_ewald_mlp.cu)
+	float *mlp_prm = nullptr;          // FP32 parameters (4611)
+	void *mlp_bf16 = nullptr;          // BF16 copy used for inference
+	bool have_mlp = false, mlp_ok = false;
+	double mlp_max_err = 0;
+
 	// hierarchical time integration (tvg_integrate.cu)
 	bool have_timeline = false;
 	struct {

@@ -54,6 +54,7 @@
 #include <stdlib.h>
 
 #include "tvg_internal.cuh"
+#include "tvg_ewald_mlp.cuh"
 
 #define GW_WARPS 4
 #define GW_THREADS (GW_WARPS * 32)
@@ -677,8 +678,9 @@ __device__ __forceinline__ void lagrange4(float t, float w[4], float d[4], float
 // K(d) = -G m T(d / L) / L^2 (the reference's sign rule, periodic.c:100-112),
 // looked up at |d| with the symmetries T_a(.., -x_b, ..) = -T_a if a = b,
 // +T_a otherwise.
+template <bool MLP>
 __device__ __forceinline__ void ewald_kjh(const GroupParams &p, const float4 *__restrict__ tab,
-                                          float4 e, CorrSum &c)
+                                          const float *mlp, float4 e, CorrSum &c)
 {
 	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
 	const float u = fabsf(e.x) * p.grid, v = fabsf(e.y) * p.grid, w = fabsf(e.z) * p.grid;
@@ -729,6 +731,12 @@ __device__ __forceinline__ void ewald_kjh(const GroupParams &p, const float4 *__
 			hzz[q] = fmaf(wx[a], y02[q], hzz[q]);
 		}
 	}
+	if (MLP) {
+		// the learned correction stands in for the table value; the table
+		// still gives the derivatives of the expansion
+		const float xs[3] = { u * (1.f / 128.f), v * (1.f / 128.f), w * (1.f / 128.f) };
+		mlp_forward(mlp, xs, val);
+	}
 	// unfold the symmetry and scale: K_a = -s_a T_a, J_ab = -s_a s_b g dT_a/du_b,
 	// H_abc = -s_a s_b s_c g^2 d2T_a/du_b du_c, all times G m / L^2
 	const float m0 = -e.w * p.inv_box * p.inv_box, m1 = m0 * p.grid, m2 = m1 * p.grid;
@@ -749,12 +757,23 @@ __device__ __forceinline__ void ewald_kjh(const GroupParams &p, const float4 *__
 }
 
 // K(d) alone (tricubic value), for per-target evaluation, added to a
+template <bool MLP>
 __device__ __forceinline__ void ewald_k(const GroupParams &p, const float4 *__restrict__ tab,
-                                        float ex, float ey, float ez, float gm, float &ax,
-                                        float &ay, float &az)
+                                        const float *mlp, float ex, float ey, float ez, float gm,
+                                        float &ax, float &ay, float &az)
 {
 	const float sx = ex < 0.f ? -1.f : 1.f, sy = ey < 0.f ? -1.f : 1.f, sz = ez < 0.f ? -1.f : 1.f;
 	const float u = fabsf(ex) * p.grid, v = fabsf(ey) * p.grid, w = fabsf(ez) * p.grid;
+	if (MLP) {
+		const float xs[3] = { u * (1.f / 128.f), v * (1.f / 128.f), w * (1.f / 128.f) };
+		float t[3];
+		mlp_forward(mlp, xs, t);
+		const float m0 = -gm * p.inv_box * p.inv_box;
+		ax = fmaf(m0 * sx, t[0], ax);
+		ay = fmaf(m0 * sy, t[1], ay);
+		az = fmaf(m0 * sz, t[2], az);
+		return;
+	}
 	const int i = min((int) u, 64), j = min((int) v, 64), l = min((int) w, 64);
 	float wx[4], wy[4], wz[4], d_[4], dd_[4];
 	lagrange4(u - (float) i, wx, d_, dd_);
@@ -795,15 +814,15 @@ __device__ __forceinline__ float ewald_h2(float r)
 // centre one entry per lane (K, J, H), or, for a group that takes per-target
 // images, every entry for every target of the lane (K at the target's
 // nearest image; FP32 per batch, carried in FP64).
-template <int TPL>
-__device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab,
+template <int TPL, bool MLP>
+__device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab, const float *mlp,
                                             const float4 *list, int from, int cnt, bool per_target,
                                             CorrSum &c, Target (&t)[TPL], float &nev)
 {
 	const int lane = threadIdx.x & 31;
 	if (!per_target) {
 		if (lane < cnt) {
-			ewald_kjh(p, tab, list[from + lane], c);
+			ewald_kjh<MLP>(p, tab, mlp, list[from + lane], c);
 			nev += 1.f;
 		}
 	} else {
@@ -817,7 +836,7 @@ __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *
 				const float dx = wrap_half(s.x - t[k].tx, p.box, p.half_box);
 				const float dy = wrap_half(s.y - t[k].ty, p.box, p.half_box);
 				const float dz = wrap_half(s.z - t[k].tz, p.box, p.half_box);
-				ewald_k(p, tab, dx, dy, dz, s.w, ax[k], ay[k], az[k]);
+				ewald_k<MLP>(p, tab, mlp, dx, dy, dz, s.w, ax[k], ay[k], az[k]);
 				if (t[k].valid) nev += 1.f;
 			}
 		}
@@ -831,11 +850,12 @@ __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *
 	__syncwarp();
 }
 
-template <int TPL>
+template <int TPL, bool MLP>
 __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode *__restrict__ wt,
                             const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
                             const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
                             const float *__restrict__ last_acc, const float4 *__restrict__ tab,
+                            const float *mlp,
                             int64_t first, int cnt, const int32_t *__restrict__ active,
                             Target (&t)[TPL], float &nev, int *status)
 {
@@ -912,7 +932,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		nl += __popc(bm);
 		__syncwarp();
 		if (nl >= 32) {
-			ewald_batch<TPL>(p, tab, S.list, nl - 32, 32, per_target, c, t, nev);
+			ewald_batch<TPL, MLP>(p, tab, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
 			nl -= 32;
 		}
 		push_children(S.stack, sp, open_int, nchild, child);
@@ -936,7 +956,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 				nl += __popc(mb);
 				__syncwarp();
 				if (nl >= 32) {
-					ewald_batch<TPL>(p, tab, S.list, nl - 32, 32, per_target, c, t, nev);
+					ewald_batch<TPL, MLP>(p, tab, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
 					nl -= 32;
 				}
 			}
@@ -944,7 +964,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		__syncwarp();
 	}
 	__syncwarp();
-	if (nl > 0) ewald_batch<TPL>(p, tab, S.list, 0, nl, per_target, c, t, nev);
+	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, mlp, S.list, 0, nl, per_target, c, t, nev);
 	if (per_target) return;
 	// sum over lanes (FP64), then K(d_c - t) ~ K - J t + H:tt / 2 per target
 	double K[3], J[9], H[18];
@@ -980,16 +1000,23 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 	}
 }
 
-template <int TPL, typename F>
+template <int TPL, bool MLP, typename F>
 __global__ void __launch_bounds__(GW_THREADS)
 k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
               const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
-              const float *__restrict__ last_acc, const float4 *__restrict__ tab, F *acc0, F *acc1,
+              const float *__restrict__ last_acc, const float4 *__restrict__ tab,
+              const __nv_bfloat16 *__restrict__ mlp_w, F *acc0, F *acc1,
               F *acc2, F *gacc0, F *gacc1, F *gacc2, int32_t *work, double *counter, int *status)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EwaldSmem &S = ((EwaldSmem *) smem_raw)[threadIdx.x >> 5];
+	// the learned correction's weights, BF16 -> FP32 once per block
+	float *mlp = (float *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS);
+	if (MLP) {
+		for (int e = threadIdx.x; e < MLP_NPARAM; e += GW_THREADS) mlp[e] = __bfloat162float(mlp_w[e]);
+		__syncthreads();
+	}
 	const int lane = threadIdx.x & 31;
 	double ev_acc = 0;
 	for (;;) {
@@ -1001,7 +1028,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode
 		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
 		Target t[TPL];
 		float nev = 0.f;
-		ewald_group<TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, first, cnt, active, t, nev,
+		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, mlp, first, cnt, active, t, nev,
 		                 status);
 		ev_acc += nev;
 #pragma unroll
@@ -1097,16 +1124,17 @@ static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, con
 	return TVG_OK;
 }
 
-template <int TPL, typename F>
+template <int TPL, bool MLP, typename F>
 static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
                         double *counter)
 {
 	static int nblk = 0;
-	const size_t smem = sizeof(EwaldSmem) * GW_WARPS;
-	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, F>, smem, &nblk));
-	k_ewald_group<TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
+	const size_t smem = sizeof(EwaldSmem) * GW_WARPS + (MLP ? 4 * MLP_NPARAM : 0);
+	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
+	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
-	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext, (F *) ctx->f[FS_ACC0],
+	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext,
+	    (const __nv_bfloat16 *) ctx->mlp_bf16, (F *) ctx->f[FS_ACC0],
 	    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1],
 	    (F *) ctx->f[FS_GACC2], ctx->work_counter + 1, counter, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
@@ -1123,8 +1151,12 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		return tvg_fail(ctx, TVG_E_BADINPUT,
 		                "group form: the gravity and Ewald parts share the particle images; "
 		                "pass TVG_WALK_GRAVITY | TVG_WALK_EWALD");
-	if (ewald && ewald_kind != TVG_EWALD_TABLE)
-		return tvg_fail(ctx, TVG_E_STATE, "learned Ewald correction not loaded");
+	const bool mlp = ewald && ewald_kind == TVG_EWALD_MLP;
+	if (ewald && ewald_kind != TVG_EWALD_TABLE && ewald_kind != TVG_EWALD_MLP)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "unknown Ewald kind %d", ewald_kind);
+	if (mlp && !(ctx->have_mlp && ctx->mlp_ok))
+		return tvg_fail(ctx, TVG_E_STATE, "learned Ewald correction not trained or not accepted by "
+		                "the table (tvg_ewald_mlp_judge)");
 	cudaStream_t s = ctx->stream;
 	if (!ctx->have_walktree) TVG_CHECK(prepare_typed<F>(ctx));
 	if (ewald && !ctx->ewald_ext) TVG_CHECK(tvg_impl_ewald_ext(ctx));
@@ -1177,8 +1209,10 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	else TVG_CHECK((launch_walk<GM_NEAREST, 2, F>(ctx, p, mass_f, last_f, cnt)));
 	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
 	if (ewald) {
-		if (tpl == 1) TVG_CHECK((launch_ewald<1, F>(ctx, p, mass_f, last_f, cnt + 1)));
-		else TVG_CHECK((launch_ewald<2, F>(ctx, p, mass_f, last_f, cnt + 1)));
+		if (mlp && tpl == 1) TVG_CHECK((launch_ewald<1, true, F>(ctx, p, mass_f, last_f, cnt + 1)));
+		else if (mlp) TVG_CHECK((launch_ewald<2, true, F>(ctx, p, mass_f, last_f, cnt + 1)));
+		else if (tpl == 1) TVG_CHECK((launch_ewald<1, false, F>(ctx, p, mass_f, last_f, cnt + 1)));
+		else TVG_CHECK((launch_ewald<2, false, F>(ctx, p, mass_f, last_f, cnt + 1)));
 	}
 	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
 	TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[2]));

@@ -79,6 +79,15 @@ class TimelineState(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class MlpTrainConfig(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("n_samples", C.c_int64),
+                ("lr", C.c_float), ("lr_final", C.c_float), ("seed", C.c_uint64),
+                ("resume", C.c_int32)]
+
+
+MLP_NPARAM = 4611
+
+
 class TvgError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -349,6 +358,48 @@ class GravityContext:
         self._check(self.lib.tvg_compute_acceleration(self.ctx, C.c_int32(form), C.c_uint32(parts),
                                                       C.c_int32(ewald_kind), C.c_int32(int(prepare))),
                     "compute_acceleration")
+
+    # ------------------------------------------ learned Ewald correction
+
+    def mlp_train(self, steps=4000, batch=16384, n_samples=1 << 20, lr=3e-3, lr_final=1e-5,
+                  seed=1, resume=False):
+        cfg = MlpTrainConfig(steps, batch, n_samples, lr, lr_final, seed, int(resume))
+        loss = C.c_float()
+        self._check(self.lib.tvg_ewald_mlp_train(self.ctx, C.byref(cfg), C.byref(loss)), "mlp_train")
+        return loss.value
+
+    def mlp_weights(self, params=None):
+        if params is None:
+            out = np.zeros(MLP_NPARAM, np.float32)
+            self._check(self.lib.tvg_ewald_mlp_weights(self.ctx, C.c_void_p(_ptr(out)), C.c_int32(0)),
+                        "mlp_weights")
+            return out
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(self.lib.tvg_ewald_mlp_weights(self.ctx, C.c_void_p(_ptr(p)), C.c_int32(1)),
+                    "mlp_weights")
+
+    def mlp_grad(self, x, y):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        loss = C.c_float()
+        self._check(self.lib.tvg_ewald_mlp_grad(self.ctx, C.c_int64(len(x)), C.c_void_p(_ptr(x)),
+                                                C.c_void_p(_ptr(y)), C.c_void_p(_ptr(g)),
+                                                C.byref(loss)), "mlp_grad")
+        return g, loss.value
+
+    def mlp_eval(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        t = np.zeros_like(x)
+        self._check(self.lib.tvg_ewald_mlp_eval(self.ctx, C.c_int64(len(x)), C.c_void_p(_ptr(x)),
+                                                C.c_void_p(_ptr(t))), "mlp_eval")
+        return t
+
+    def mlp_judge(self, max_allowed=1e-2):
+        mx, rms = C.c_double(), C.c_double()
+        self._check(self.lib.tvg_ewald_mlp_judge(self.ctx, C.c_double(max_allowed), C.byref(mx),
+                                                 C.byref(rms)), "mlp_judge")
+        return mx.value, rms.value
 
     def set_ewald_opening(self, rel_alpha=2.5e-4, bh_factor=0.5):
         """Opening of the group form's Ewald walk (see tvg_set_ewald_opening)."""

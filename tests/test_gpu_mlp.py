@@ -1,0 +1,95 @@
+"""The learned Ewald correction (tvg_ewald_mlp.cu): the training kernels'
+gradient against the FP64 oracle (oracle/mlp.py); a network trained on the
+GPU, judged by the exact table and compared with the reference's trilinear
+interpolation of that table (Gravity/periodic.c:35-113); and the walk with
+the learned correction against the same walk without a correction and with
+the table, by the FP64 Ewald-summed direct force."""
+import numpy as np
+import pytest
+
+import mlp as O
+import port
+from tandav_b200 import gravity as G
+from tandav_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+TRAIN = dict(steps=20000, batch=16384, n_samples=1 << 20, lr=2e-3, lr_final=1e-6, seed=3)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    with G.GravityContext(1024, periodic=True, boxsize=1.0) as ctx:
+        ctx.set_domain((0, 0, 0), 1.0)
+        ctx.ewald_init()
+        loss = ctx.mlp_train(**TRAIN)
+        mx, rms = ctx.mlp_judge(max_allowed=1.0)
+        return ctx.mlp_weights(), loss, mx, rms
+
+
+def test_mlp_gradient_matches_oracle():
+    rng = np.random.default_rng(5)
+    p = (rng.standard_normal(O.NPARAM) * 0.3).astype(np.float32)
+    x = (rng.random((777, 3)) * 0.5).astype(np.float32)
+    y = (rng.standard_normal((777, 3)) * 0.5).astype(np.float32)
+    with G.GravityContext(1024, periodic=True, boxsize=1.0) as ctx:
+        ctx.mlp_weights(p)
+        g, loss = ctx.mlp_grad(x, y)
+        np.testing.assert_array_equal(ctx.mlp_weights(), p)
+    go, lo = O.grad(p.astype(np.float64), x.astype(np.float64), y.astype(np.float64))
+    assert loss == pytest.approx(lo, rel=1e-4)
+    scale = np.abs(go).max()
+    assert np.abs(g - go).max() < 2e-4 * scale
+    for name, lo_, hi_ in (("W1", 0, 192), ("W2", 256, 4352), ("W3", 4416, 4608)):
+        assert np.abs(go[lo_:hi_]).max() > 0, name
+
+
+def test_mlp_training_judged_by_table(trained):
+    w, loss, mx, rms = trained
+    rng = np.random.default_rng(8)
+    xs = rng.random((2000, 3)) * 0.5
+    with G.GravityContext(1024, periodic=True, boxsize=1.0) as ctx:
+        ctx.mlp_weights(w)
+        t_mlp = ctx.mlp_eval(xs)
+    t_ref = port.ewald_force(xs)                 # FP64 Ewald sum (alpha 2, |n|, |h| <= 4)
+    fx, fy, fz, _ = port.ewald_table(64)
+    t_tri = O.trilinear((fx, fy, fz), xs)
+    t_fp32 = O.forward(w.astype(np.float64), xs)
+    e = {k: np.sqrt(((v - t_ref) ** 2).sum(1)) for k, v in
+         (("mlp_bf16", t_mlp), ("mlp_fp32", t_fp32), ("trilinear", t_tri))}
+    print(f"train loss {loss:.3e}; judge (65^3 nodes): max {mx:.3e} rms {rms:.3e}; "
+          + "; ".join(f"{k}: max {v.max():.3e} rms {np.sqrt((v ** 2).mean()):.3e}" for k, v in e.items())
+          + f"; max |T| {np.abs(t_ref).max():.2f}")
+    assert loss < 1e-4
+    assert np.sqrt((e["mlp_bf16"] ** 2).mean()) < 2e-2
+    # the BF16 evaluation follows the FP32 network
+    assert np.abs(t_mlp - t_fp32).max() < 0.1
+
+
+def test_walk_with_learned_correction(trained):
+    w, *_ = trained
+    p = ics.zeldovich_box(n_side=32, seed=32)
+    parts = G.WALK_GRAVITY | G.WALK_EWALD
+    res = {}
+    with G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box,
+                          softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0, 0, 0), p.box)
+        ctx.ewald_init()
+        ctx.mlp_weights(w)
+        with pytest.raises(G.TvgError):         # not judged yet
+            ctx.force_step(form=G.FORM_GROUP, parts=parts, ewald_kind=G.EWALD_MLP)
+        ctx.mlp_judge(max_allowed=1.0)
+        ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
+        ctx.save_last_accel()
+        tgt = np.sort(np.random.default_rng(1).choice(p.n, 2000, replace=False))
+        ad, _, _ = ctx.forcetest(tgt)
+        for name, kind, pr in (("none", G.EWALD_TABLE, G.WALK_GRAVITY),
+                               ("learned", G.EWALD_MLP, parts), ("table", G.EWALD_TABLE, parts)):
+            ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=pr, ewald_kind=kind)
+            at = ctx.download(G.F_GRAV_ACC)["grav_acc"][:, tgt].astype(np.float64)
+            err = np.sqrt(((at - ad) ** 2).sum(0) / (ad ** 2).sum(0))
+            res[name] = float(np.sqrt((err ** 2).mean()))
+    print("rms force error vs FP64 Ewald direct sum:", res)
+    assert res["learned"] < res["none"] / 5
+    assert res["table"] <= res["learned"]
