@@ -67,6 +67,9 @@ def parse():
                     help="opening of the group form's Ewald walk (relative to |a_old|)")
     ap.add_argument("--plain-open-rel", type=float, default=0.005,
                     help="TREE_OPEN_PARAM_REL of the plain form (the reference's value)")
+    ap.add_argument("--rung-steps", type=int, default=0,
+                    help="also run this many hierarchical time steps from z = 50 (rung workload)")
+    ap.add_argument("--time-int-accuracy", type=float, default=0.025)
     ap.add_argument("--forcetest-targets", type=int, default=10000,
                     help="particles in the FP64 direct-sum error check (0: skip)")
     return ap.parse_args()
@@ -229,6 +232,68 @@ def run_reference_arm(args):
     return 0
 
 
+def rung_run(args, p, G, device):
+    """Hierarchical time stepping from z = 50 (src/main.c:43-70): per step
+    Set_New_Timesteps, first kick, drift, Compute_Acceleration of the active
+    particles, second kick; per-step active particles, time and rung counts."""
+    ctx = G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
+                           device=device)
+    try:
+        n = p.n
+        ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32),
+                   time_bin=np.zeros(n, np.int32), it_drift=np.zeros(n, np.uint32),
+                   it_kick=np.zeros(n, np.uint32))
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.ewald_init()
+        ctx.set_opening(0.25, args.open_rel)
+        ctx.set_ewald_opening(args.ewald_alpha)
+        h0 = 0.1
+        ctx.timeline_init(comoving=1, time_begin=p.a_start, time_end=1.0, hubble_constant=h0,
+                          omega_matter=0.3, omega_lambda=0.7, omega_rad=0.0, omega_0=1.0,
+                          omega_baryon=0.0, rho_crit0=3 * h0 * h0 / (8 * math.pi * 43020.0),
+                          time_int_accuracy=args.time_int_accuracy, max_timestep=0.05,
+                          displ_constraint=0.25)
+        parts = G.WALK_GRAVITY | G.WALK_EWALD
+        ctx.timer_start()
+        ctx.compute_acceleration(form=G.FORM_GROUP, parts=parts, prepare=True)
+        prep_ms = ctx.timer_stop()
+        tpl, _ = ctx.autotune(use_bh=False, parts=parts)
+        steps = []
+        for _ in range(args.rung_steps):
+            st = ctx.timeline()
+            if st.current >= st.end:
+                break
+            ctx.timer_start()
+            ctx.set_new_timesteps()
+            st = ctx.timeline()
+            ctx.kick_first_halfstep()
+            ctx.drift_to_sync_point()
+            ctx.compute_acceleration(form=G.FORM_GROUP, parts=parts)
+            ctx.kick_second_halfstep()
+            ms = ctx.timer_stop()
+            h = ctx.rung_histogram()
+            ph = ctx.phase_times()
+            g_i, e_i = ctx.walk_counters()
+            steps.append({"a": round(st.time_current, 6), "n_active": int(st.n_active),
+                          "max_active_bin": int(st.max_active_bin), "ms": round(ms, 2),
+                          "walk_ms": round(ph["walk"], 1), "ewald_ms": round(ph["ewald"], 1),
+                          "interactions_per_active": round(g_i / max(st.n_active, 1)),
+                          "ewald_evals_per_active": round(e_i / max(st.n_active, 1), 1),
+                          "particles_per_s": round(st.n_active / (ms * 1e-3)),
+                          "rungs": {int(b): int(c) for b, c in enumerate(h) if c}})
+        tot_ms = sum(s["ms"] for s in steps)
+        tot_act = sum(s["n_active"] for s in steps)
+        return {"workload": f"zeldovich_{args.nside}^3 from z = 50, hierarchical steps, "
+                            f"TimeIntAccuracy {args.time_int_accuracy}",
+                "prepare_ms": round(prep_ms, 1), "targets_per_lane": tpl,
+                "steps": len(steps), "total_ms": round(tot_ms, 1),
+                "active_particles_per_s": round(tot_act / (tot_ms * 1e-3)) if tot_ms else None,
+                "rungs_populated_max": max(len(s["rungs"]) for s in steps) if steps else 0,
+                "per_step": steps}
+    finally:
+        ctx.close()
+
+
 def workload_config(args, p, ws):
     return {
         "workload": f"zeldovich_{args.nside}^3_periodic_z50",
@@ -269,6 +334,8 @@ def main():
     ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
     ctx.save_last_accel()
     ctx.set_opening(0.25, args.open_rel)
+    ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
+    tune_choice, tune_ms = ctx.autotune(use_bh=False, parts=parts)
     for _ in range(args.warmup):
         ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
 
@@ -410,6 +477,8 @@ def main():
                  "interactions_per_particle": round((g_pl + e_pl) / len(act), 1),
                  "speedup_group_over_plain": round(value / ws / (n / t_plain), 2)}
 
+    rungs = rung_run(args, p, G, local) if args.rung_steps > 0 else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
@@ -440,6 +509,9 @@ def main():
                            "evaluation": "tricubic K, dK, d2K: 64 float4 loads, ~1100 FP32 ops"},
             "plain_form": plain,
             "accuracy": accuracy,
+            "autotune": {"targets_per_lane": tune_choice,
+                         "walk_ms_1_and_2_targets_per_lane": [round(x, 1) for x in tune_ms]},
+            "rung_run": rungs,
         }
         print(json.dumps(out))
     dist.close()

@@ -370,6 +370,14 @@ int tvg_rung_histogram(tvg_context *ctx, int32_t *hist);
 int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts, int32_t ewald_kind,
                              int32_t prepare);
 
+/* Autotuner of the group form (no reference counterpart): on the current tree
+ * and active set, times the gravity + Ewald walks with 32- and 64-particle
+ * groups (one or two targets per lane) and keeps the faster for the later
+ * walks of this context. choice receives 1 or 2, ms[2] the two times. The
+ * chosen walk runs last: the accelerations left are its result. */
+int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
+                 int32_t *choice, double *ms);
+
 /* ---------------------------------------------- learned Ewald correction */
 
 /* Training of the 3 -> 64 -> 64 -> 3 network (tanh) that stands in for the

@@ -147,6 +147,7 @@ struct tvg_context {
 	int64_t n_active = 0;
 	bool use_active = false;
 	int64_t launches = 0;              // kernels launched by this context
+	int group_tpl = 0;                 // group form targets per lane (0: default)
 
 	// learned Ewald correction (tvg_ewald_mlp.cu)
 	float *mlp_prm = nullptr;          // FP32 parameters (4611)

@@ -611,7 +611,8 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 
 template <int MODE, int TPL, typename F>
 __global__ void __launch_bounds__(GW_THREADS)
-k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
+k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
+             const tvg_wnode *__restrict__ wt,
              const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
              const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
              const float *__restrict__ last_acc, F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1,
@@ -626,8 +627,15 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode 
 		if (lane == 0) g = atomicAdd(work, 1);
 		g = __shfl_sync(0xFFFFFFFFu, g, 0);
 		if (g >= p.ngroups) break;
-		const int64_t first = g * p.gsize;
-		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
+		int64_t first;
+		int cnt;
+		if (gfirst) {
+			first = gfirst[g];
+			cnt = (int) (gfirst[g + 1] - first);
+		} else {
+			first = g * p.gsize;
+			cnt = (int) min((int64_t) p.gsize, p.n - first);
+		}
 		Target t[TPL];
 		walk_group<MODE, TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, first, cnt, active, t, status);
 #pragma unroll
@@ -1002,7 +1010,8 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 
 template <int TPL, bool MLP, typename F>
 __global__ void __launch_bounds__(GW_THREADS)
-k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode *__restrict__ wt,
+k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
+              const tvg_wnode *__restrict__ wt,
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
               const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
               const float *__restrict__ last_acc, const float4 *__restrict__ tab,
@@ -1024,8 +1033,15 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const tvg_wnode
 		if (lane == 0) g = atomicAdd(work, 1);
 		g = __shfl_sync(0xFFFFFFFFu, g, 0);
 		if (g >= p.ngroups) break;
-		const int64_t first = g * p.gsize;
-		const int cnt = (int) min((int64_t) p.gsize, p.n - first);
+		int64_t first;
+		int cnt;
+		if (gfirst) {
+			first = gfirst[g];
+			cnt = (int) (gfirst[g + 1] - first);
+		} else {
+			first = g * p.gsize;
+			cnt = (int) min((int64_t) p.gsize, p.n - first);
+		}
 		Target t[TPL];
 		float nev = 0.f;
 		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, mlp, first, cnt, active, t, nev,
@@ -1084,15 +1100,51 @@ static int prepare_typed(tvg_context *ctx)
 	return TVG_OK;
 }
 
-// targets per lane: 1 (32-particle groups) or 2 (64); TVG_GROUP_TPL overrides
-static int group_tpl()
+// targets per lane: 1 (32-particle groups) or 2 (64): the context's choice
+// (tvg_autotune), else TVG_GROUP_TPL from the environment, else the default
+static int group_tpl(const tvg_context *ctx)
 {
+	if (ctx->group_tpl == 1 || ctx->group_tpl == 2) return ctx->group_tpl;
 	static int tpl = 0;
 	if (!tpl) {
 		const char *e = getenv("TVG_GROUP_TPL");
 		tpl = (e && atoi(e) == 1) ? 1 : (e && atoi(e) == 2) ? 2 : GW_DEFAULT_TPL;
 	}
 	return tpl;
+}
+
+// Groups of an active list: the active particles of each window of gsize
+// consecutive (PH-ordered) particles form one group, so that a group is as
+// compact as a full one however few of its particles are active.
+__global__ void k_window_flags(int64_t n_act, const int32_t *__restrict__ active, int gsize,
+                               int32_t *flag)
+{
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k >= n_act) return;
+	flag[k] = k == 0 || active[k] / gsize != active[k - 1] / gsize;
+}
+
+__global__ void k_window_scatter(int64_t n_act, const int32_t *__restrict__ flag,
+                                 const int32_t *__restrict__ off, int32_t *gfirst)
+{
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k < n_act && flag[k]) gfirst[off[k]] = (int32_t) k;
+	if (k == 0) gfirst[off[n_act - 1] + flag[n_act - 1]] = (int32_t) n_act;
+}
+
+static int build_groups(tvg_context *ctx, int gsize, int64_t *ngroups)
+{
+	const int64_t na = ctx->n_active;
+	cudaStream_t s = ctx->stream;
+	if (!ctx->act_flag) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_flag, 4 * (size_t) ctx->cap));
+	if (!ctx->act_off) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_off, 4 * (size_t) ctx->cap));
+	k_window_flags<<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, s>>>(na, ctx->active, gsize, ctx->act_flag);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->act_flag, ctx->act_off, na, ngroups));
+	k_window_scatter<<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, s>>>(na, ctx->act_flag, ctx->act_off,
+	                                                                   ctx->group_first);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
 }
 
 template <typename K>
@@ -1116,7 +1168,8 @@ static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, con
 	const size_t smem = sizeof(WarpSmem) * GW_WARPS;
 	TVG_CHECK(blocks_for(ctx, k_walk_group<MODE, TPL, F>, smem, &nblk));
 	k_walk_group<MODE, TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
-	    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
+	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
+	    ctx->wtree, ctx->ipos[0], ctx->ipos[1],
 	    ctx->ipos[2], mass_f, last_f, (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1],
 	    (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2],
 	    (F *) ctx->f[FS_COST], ctx->work_counter, counter, ctx->status);
@@ -1132,7 +1185,8 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	const size_t smem = sizeof(EwaldSmem) * GW_WARPS + (MLP ? 4 * MLP_NPARAM : 0);
 	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
 	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
-	    p, ctx->use_active ? ctx->active : nullptr, ctx->wtree, ctx->ipos[0], ctx->ipos[1],
+	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
+	    ctx->wtree, ctx->ipos[0], ctx->ipos[1],
 	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext,
 	    (const __nv_bfloat16 *) ctx->mlp_bf16, (F *) ctx->f[FS_ACC0],
 	    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1],
@@ -1171,11 +1225,15 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		last_f = lf;
 	}
 	const tvg_config &cf = ctx->cfg;
-	const int tpl = group_tpl();
+	const int tpl = group_tpl(ctx);
 	GroupParams p;
 	p.n = ctx->use_active ? ctx->n_active : n;
 	p.gsize = 32 * tpl;
 	p.ngroups = (p.n + p.gsize - 1) / p.gsize;
+	if (ctx->use_active) {
+		if (p.n == 0) return TVG_OK;
+		TVG_CHECK(build_groups(ctx, p.gsize, &p.ngroups));
+	}
 	p.ntop = ctx->ntop;
 	p.periodic = cf.periodic;
 	p.use_bh = use_bh;
@@ -1226,6 +1284,29 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	ctx->last_counts[0] = c[0];
 	ctx->last_counts[1] = c[1];
 	return TVG_OK;
+}
+
+// Autotuner of the group form: times the walks of the current tree and active
+// set with each group size (targets per lane) and keeps the fastest; the walk
+// of the chosen size runs last, so its accelerations are the ones left.
+extern "C" int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
+                            int32_t *choice, double *ms)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!ctx->have_tree) return tvg_fail(ctx, TVG_E_STATE, "autotune: no tree");
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	double t[2] = { 0, 0 };
+	for (int tpl = 1; tpl <= 2; tpl++) {
+		ctx->group_tpl = tpl;
+		TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
+		t[tpl - 1] = ctx->phase_ms[4] + ctx->phase_ms[5];
+	}
+	const int best = t[0] < t[1] ? 1 : 2;
+	ctx->group_tpl = best;
+	if (best == 1) TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
+	if (choice) *choice = best;
+	if (ms) { ms[0] = t[0]; ms[1] = t[1]; }
+	return tvg_sync_status(ctx, "autotune");
 }
 
 int tvg_impl_walk_group(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind)

@@ -359,6 +359,15 @@ class GravityContext:
                                                       C.c_int32(ewald_kind), C.c_int32(int(prepare))),
                     "compute_acceleration")
 
+    def autotune(self, use_bh=False, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE):
+        """Chooses the group size of the group form (1 or 2 targets per lane)
+        by timing the walks on the current tree; returns (choice, [ms1, ms2])."""
+        ch = C.c_int32()
+        ms = (C.c_double * 2)()
+        self._check(self.lib.tvg_autotune(self.ctx, C.c_int32(int(use_bh)), C.c_uint32(parts),
+                                          C.c_int32(ewald_kind), C.byref(ch), ms), "autotune")
+        return ch.value, [ms[0], ms[1]]
+
     # ------------------------------------------ learned Ewald correction
 
     def mlp_train(self, steps=4000, batch=16384, n_samples=1 << 20, lr=3e-3, lr_final=1e-5,
