@@ -219,6 +219,7 @@ struct GroupParams {
 	float ew_rel;       // Ewald opening: alpha_E / TREE_OPEN_PARAM_REL (relative mode)
 	float ew_bh;        // Ewald opening: s^2 h2 limit in units of L^2 (Barnes-Hut mode)
 	float taylor_h;     // groups with a larger half extent take per-target images (with Ewald)
+	double uniform;     // G M_total / L^2: scale of the uniform-background remainder
 };
 
 struct WarpSmem {
@@ -818,6 +819,41 @@ __device__ __forceinline__ float ewald_h2(float r)
 	return 92.f * x * sqrtf(x);
 }
 
+// Field of the uniform unit-density cube [-1/2, 1/2]^3 at tau (G = 1): the
+// closed form of the rectangular prism (the double antiderivative of 1/r,
+// F = Y ln(Z + r) + Z ln(Y + r) - X atan(Y Z / (X r)), over the corners;
+// Nagy 1966), in FP64.
+__device__ __forceinline__ double prism_f(double X, double Y, double Z)
+{
+	const double r = sqrt(X * X + Y * Y + Z * Z);
+	return Y * log(Z + r) + Z * log(Y + r) - X * atan(Y * Z / (X * r));
+}
+
+__device__ __forceinline__ double cube_field(double a1, double a2, double b1, double b2, double c1,
+                                             double c2)
+{
+	return (prism_f(a1, b2, c2) - prism_f(a2, b2, c2)) - (prism_f(a1, b1, c2) - prism_f(a2, b1, c2))
+	     - (prism_f(a1, b2, c1) - prism_f(a2, b2, c1)) + (prism_f(a1, b1, c1) - prism_f(a2, b1, c1));
+}
+
+// The expansion about the group centre misses the third and higher orders of
+// the correction's sum. Over the uniform part of the sources -- the cube of
+// side L about the centre, where every source sits at its image nearest to
+// the centre -- that sum is -G rho g_cube(t) (the lattice force has zero
+// mean over a period), whose part beyond the linear term is added exactly:
+// R(t) = -(G M / L^2) [g(t / L) + 4 pi t / (3 L)] (g of the unit cube).
+__device__ __forceinline__ void uniform_remainder(const GroupParams &p, double tx, double ty,
+                                                  double tz, double out[3])
+{
+	const double x = tx * p.inv_box, y = ty * p.inv_box, z = tz * p.inv_box;
+	const double x1 = -0.5 - x, x2 = 0.5 - x, y1 = -0.5 - y, y2 = 0.5 - y, z1 = -0.5 - z,
+	             z2 = 0.5 - z;
+	const double lin = 4.18879020478639098;      // 4 pi / 3
+	out[0] = -p.uniform * (cube_field(x1, x2, y1, y2, z1, z2) + lin * x);
+	out[1] = -p.uniform * (cube_field(y1, y2, x1, x2, z1, z2) + lin * y);
+	out[2] = -p.uniform * (cube_field(z1, z2, x1, x2, y1, y2) + lin * z);
+}
+
 // Evaluates list entries [from, from + cnt), cnt <= 32: about the group
 // centre one entry per lane (K, J, H), or, for a group that takes per-target
 // images, every entry for every target of the lane (K at the target's
@@ -1002,6 +1038,11 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 			       + 0.5 * (h[0] * x * x + h[1] * y * y + h[2] * z * z)
 			       + h[3] * x * y + h[4] * x * z + h[5] * y * z;
 		}
+		double rem[3];
+		uniform_remainder(p, x, y, z, rem);
+		out[0] += rem[0];
+		out[1] += rem[1];
+		out[2] += rem[2];
 		t[k].ax = out[0];
 		t[k].ay = out[1];
 		t[k].az = out[2];
@@ -1195,6 +1236,17 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	return TVG_OK;
 }
 
+__global__ void k_mass_total(int64_t n, const float *__restrict__ m, double *out)
+{
+	double s = 0;
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+	     i += (int64_t) gridDim.x * blockDim.x)
+		s += (double) m[i];
+#pragma unroll
+	for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+	if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
 template <typename F>
 static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind)
 {
@@ -1254,9 +1306,21 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	p.ew_rel = (float) (ctx->ewald_open_rel / cf.open_rel);   // times g.fac: alpha_E |a_old| / G
 	p.ew_bh = (float) (ctx->ewald_open_bh * cf.open_bh);
 	// half extent beyond which a group takes per-target images with the Ewald
-	// part: the third-order remainder of the expansion about the centre grows
-	// as (h / L)^3 (2e-4 of the force at h = L / 100 on the 256^3 box at z = 50)
-	p.taylor_h = (float) (cf.periodic ? cf.boxsize / 64.0 : 3.0e38);
+	// part. The expansion's third-order remainder is dominated by the uniform
+	// background, which uniform_remainder adds exactly; what is left (the
+	// density fluctuations' share) kept the expansion within 1.2x of the
+	// per-target force error at h ~ L / 32 (64^3 box, z = 50).
+	p.taylor_h = (float) (cf.periodic ? cf.boxsize / 20.0 : 3.0e38);
+	p.uniform = 0;
+	if (ewald) {
+		double *dm = ctx->counters + 2, mt = 0;
+		TVG_CUDA(ctx, cudaMemsetAsync(dm, 0, 8, s));
+		k_mass_total<<<TVG_CNT(ctx, 148 * 4), 256, 0, s>>>(n, mass_f, dm);
+		TVG_CUDA(ctx, cudaGetLastError());
+		TVG_CUDA(ctx, cudaMemcpyAsync(&mt, dm, 8, cudaMemcpyDeviceToHost, s));
+		TVG_CUDA(ctx, cudaStreamSynchronize(s));
+		p.uniform = cf.gravity * mt / (cf.boxsize * cf.boxsize);
+	}
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16, s));
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 8, s));
 	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
