@@ -510,7 +510,7 @@ def main():
             "plain_form": plain,
             "accuracy": accuracy,
             "autotune": {"targets_per_lane": tune_choice,
-                         "walk_ms_1_and_2_targets_per_lane": [round(x, 1) for x in tune_ms]},
+                         "walk_ms_1_2_4_targets_per_lane": [round(x, 1) for x in tune_ms]},
             "rung_run": rungs,
         }
         print(json.dumps(out))

@@ -371,10 +371,11 @@ int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts, int
                              int32_t prepare);
 
 /* Autotuner of the group form (no reference counterpart): on the current tree
- * and active set, times the gravity + Ewald walks with 32- and 64-particle
- * groups (one or two targets per lane) and keeps the faster for the later
- * walks of this context. choice receives 1 or 2, ms[2] the two times. The
- * chosen walk runs last: the accelerations left are its result. */
+ * and active set, times the gravity + Ewald walks with 32-, 64- and
+ * 128-particle groups (one, two or four targets per lane) and keeps the
+ * fastest for the later walks of this context. choice receives 1, 2 or 4,
+ * ms[3] the three times. The chosen walk runs last: the accelerations left
+ * are its result. */
 int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
                  int32_t *choice, double *ms);
 

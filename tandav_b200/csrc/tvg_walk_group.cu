@@ -65,6 +65,13 @@
 #define GW_BQ 64
 #define GW_ELIST 64
 #define GW_DEFAULT_TPL 2
+// resident blocks per SM the Ewald walk is compiled for; capping its
+// registers for 3 or 4 blocks made it slower (1340, 1442 ms against 1252 ms
+// per step at 256^3): the table gathers need the registers more than the SM
+// needs the warps
+#ifndef GW_EWALD_MINB
+#define GW_EWALD_MINB 1
+#endif
 
 // -------------------------------------------------- integer coordinates
 
@@ -1050,7 +1057,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 }
 
 template <int TPL, bool MLP, typename F>
-__global__ void __launch_bounds__(GW_THREADS)
+__global__ void __launch_bounds__(GW_THREADS, GW_EWALD_MINB)
 k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
               const tvg_wnode *__restrict__ wt,
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
@@ -1145,11 +1152,12 @@ static int prepare_typed(tvg_context *ctx)
 // (tvg_autotune), else TVG_GROUP_TPL from the environment, else the default
 static int group_tpl(const tvg_context *ctx)
 {
-	if (ctx->group_tpl == 1 || ctx->group_tpl == 2) return ctx->group_tpl;
+	if (ctx->group_tpl == 1 || ctx->group_tpl == 2 || ctx->group_tpl == 4) return ctx->group_tpl;
 	static int tpl = 0;
 	if (!tpl) {
 		const char *e = getenv("TVG_GROUP_TPL");
-		tpl = (e && atoi(e) == 1) ? 1 : (e && atoi(e) == 2) ? 2 : GW_DEFAULT_TPL;
+		const int v = e ? atoi(e) : 0;
+		tpl = (v == 1 || v == 2 || v == 4) ? v : GW_DEFAULT_TPL;
 	}
 	return tpl;
 }
@@ -1247,6 +1255,20 @@ __global__ void k_mass_total(int64_t n, const float *__restrict__ m, double *out
 	if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
 
+// the gravity walk, then (with Ewald) the Ewald walk, for one group size;
+// events ev[0], ev[1] bracket the gravity walk, ev[1], ev[2] the Ewald walk
+template <int TPL, typename F>
+static int launch_pair(tvg_context *ctx, const GroupParams &p, bool ewald, bool mlp,
+                       const float *mass_f, const float *last_f, double *cnt)
+{
+	if (ewald) TVG_CHECK((launch_walk<GM_CENTRE, TPL, F>(ctx, p, mass_f, last_f, cnt)));
+	else TVG_CHECK((launch_walk<GM_NEAREST, TPL, F>(ctx, p, mass_f, last_f, cnt)));
+	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+	if (ewald && mlp) TVG_CHECK((launch_ewald<TPL, true, F>(ctx, p, mass_f, last_f, cnt + 1)));
+	else if (ewald) TVG_CHECK((launch_ewald<TPL, false, F>(ctx, p, mass_f, last_f, cnt + 1)));
+	return TVG_OK;
+}
+
 template <typename F>
 static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind)
 {
@@ -1325,17 +1347,9 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 8, s));
 	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
 	double *cnt = ctx->counters;
-	if (ewald && tpl == 1) TVG_CHECK((launch_walk<GM_CENTRE, 1, F>(ctx, p, mass_f, last_f, cnt)));
-	else if (ewald) TVG_CHECK((launch_walk<GM_CENTRE, 2, F>(ctx, p, mass_f, last_f, cnt)));
-	else if (tpl == 1) TVG_CHECK((launch_walk<GM_NEAREST, 1, F>(ctx, p, mass_f, last_f, cnt)));
-	else TVG_CHECK((launch_walk<GM_NEAREST, 2, F>(ctx, p, mass_f, last_f, cnt)));
-	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
-	if (ewald) {
-		if (mlp && tpl == 1) TVG_CHECK((launch_ewald<1, true, F>(ctx, p, mass_f, last_f, cnt + 1)));
-		else if (mlp) TVG_CHECK((launch_ewald<2, true, F>(ctx, p, mass_f, last_f, cnt + 1)));
-		else if (tpl == 1) TVG_CHECK((launch_ewald<1, false, F>(ctx, p, mass_f, last_f, cnt + 1)));
-		else TVG_CHECK((launch_ewald<2, false, F>(ctx, p, mass_f, last_f, cnt + 1)));
-	}
+	if (tpl == 1) TVG_CHECK((launch_pair<1, F>(ctx, p, ewald, mlp, mass_f, last_f, cnt)));
+	else if (tpl == 2) TVG_CHECK((launch_pair<2, F>(ctx, p, ewald, mlp, mass_f, last_f, cnt)));
+	else TVG_CHECK((launch_pair<4, F>(ctx, p, ewald, mlp, mass_f, last_f, cnt)));
 	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
 	TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[2]));
 	float ms = 0, ms_e = 0;
@@ -1359,17 +1373,19 @@ extern "C" int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, in
 	if (!ctx) return TVG_E_BADINPUT;
 	if (!ctx->have_tree) return tvg_fail(ctx, TVG_E_STATE, "autotune: no tree");
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
-	double t[2] = { 0, 0 };
-	for (int tpl = 1; tpl <= 2; tpl++) {
-		ctx->group_tpl = tpl;
+	const int sizes[3] = { 1, 2, 4 };
+	double t[3] = { 0, 0, 0 };
+	int best = 0;
+	for (int c = 0; c < 3; c++) {
+		ctx->group_tpl = sizes[c];
 		TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
-		t[tpl - 1] = ctx->phase_ms[4] + ctx->phase_ms[5];
+		t[c] = ctx->phase_ms[4] + ctx->phase_ms[5];
+		if (t[c] < t[best]) best = c;
 	}
-	const int best = t[0] < t[1] ? 1 : 2;
-	ctx->group_tpl = best;
-	if (best == 1) TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
-	if (choice) *choice = best;
-	if (ms) { ms[0] = t[0]; ms[1] = t[1]; }
+	ctx->group_tpl = sizes[best];
+	if (best != 2) TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
+	if (choice) *choice = sizes[best];
+	if (ms) for (int c = 0; c < 3; c++) ms[c] = t[c];
 	return tvg_sync_status(ctx, "autotune");
 }
 

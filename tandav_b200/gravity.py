@@ -360,13 +360,13 @@ class GravityContext:
                     "compute_acceleration")
 
     def autotune(self, use_bh=False, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE):
-        """Chooses the group size of the group form (1 or 2 targets per lane)
-        by timing the walks on the current tree; returns (choice, [ms1, ms2])."""
+        """Chooses the group size of the group form (1, 2 or 4 targets per lane)
+        by timing the walks on the current tree; returns (choice, [ms1, ms2, ms4])."""
         ch = C.c_int32()
-        ms = (C.c_double * 2)()
+        ms = (C.c_double * 3)()
         self._check(self.lib.tvg_autotune(self.ctx, C.c_int32(int(use_bh)), C.c_uint32(parts),
                                           C.c_int32(ewald_kind), C.byref(ch), ms), "autotune")
-        return ch.value, [ms[0], ms[1]]
+        return ch.value, [ms[0], ms[1], ms[2]]
 
     # ------------------------------------------ learned Ewald correction
 
