@@ -301,11 +301,13 @@ def workload_config(args, p, ws):
         "softening_kpc_h": round(float(p.softening), 4),
         "criterion": (f"relative, TREE_OPEN_PARAM_REL {args.open_rel:g} (group form), "
                       f"{args.plain_open_rel:g} (plain form); |a_old| from a BH (theta^2 0.25) pass"),
-        "ewald": (f"group form: per-group Ewald walk, tricubic lattice-sum table (K, dK, d2K at node "
-                  f"centres of mass, second-order expansion about the group centre), opening "
+        "ewald": (f"group form: per-group Ewald walk, Taylor table of the lattice sum (33^3 nodes, "
+                  f"third order; K, dK, d2K at node centres of mass, second-order expansion about "
+                  f"the group centre plus the exact uniform-cube remainder), opening "
                   f"alpha_E {args.ewald_alpha:g}; plain form: the reference's Ewald walk, 65^3 "
                   f"table, trilinear"),
-        "form": "group: warp per 64-particle PH group (2 per lane), FP32 on 32-bit integer box offsets",
+        "form": ("group: warp per PH group of 32 x (targets per lane, autotuned) particles, FP32 on "
+                 "32-bit integer box offsets"),
         "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
         "l2": "inputs larger than L2 (16.7M particles, ~2 GB of particle state)",
     }
@@ -503,10 +505,10 @@ def main():
             "phases_ms": ph,
             "interactions_per_particle": {"gravity": round(grav_i / args.steps / n, 1),
                                           "ewald_evaluations": round(ew_i / args.steps / n, 1)},
-            "ewald_walk": {"kernel": "k_ewald_group<2, float>",
+            "ewald_walk": {"kernel": f"k_ewald_group<{tune_choice}, false, float>",
                            "ms_per_step": round(ew_ms / args.steps, 2),
-                           "evaluations_per_group_of_64": round(ew_i / args.steps / (n / 64), 1),
-                           "evaluation": "tricubic K, dK, d2K: 64 float4 loads, ~1100 FP32 ops"},
+                           "evaluations_per_group": round(ew_i / args.steps / (n / (32 * tune_choice)), 1),
+                           "evaluation": "Taylor-table K, dK, d2K: 15 float4 loads, ~200 FP32 ops"},
             "plain_form": plain,
             "accuracy": accuracy,
             "autotune": {"targets_per_lane": tune_choice,

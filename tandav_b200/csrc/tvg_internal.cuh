@@ -127,6 +127,7 @@ struct tvg_context {
 	double *ewald_raw = nullptr;
 	float *ewald32 = nullptr;          // FP32 copy for the group form (FP64 builds)
 	float *ewald_ext = nullptr;        // (Tx, Ty, Tz, 0) on 68^3 points, x = 0.5 i / 64, i = -1..66
+	float *ewald_taylor = nullptr;     // T and 3 derivatives at TVG_TAYLOR_NODES^3 nodes, 64 floats each
 	// Ewald-walk opening of the group form: the monopole error of the
 	// correction may reach ewald_open_rel |a_old| (relative mode); the limit of
 	// h2 s^2 / L^2 in units of TREE_OPEN_PARAM_BH (Barnes-Hut mode)
@@ -193,6 +194,11 @@ int tvg_impl_tree_build(tvg_context *ctx, uint32_t flags);
 int tvg_impl_download_tree(tvg_context *ctx, void *tree, int64_t cap, int64_t *nnodes);
 int tvg_impl_ewald_init(tvg_context *ctx);
 int tvg_impl_ewald_ext(tvg_context *ctx);
+int tvg_impl_ewald_taylor(tvg_context *ctx);
+// nodes per axis of the group form's Taylor table of the Ewald correction
+#ifndef TVG_TAYLOR_NODES
+#define TVG_TAYLOR_NODES 33
+#endif
 int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts);
 int tvg_impl_walk_group(tvg_context *ctx, int use_bh, uint32_t parts, int ewald_kind);
 int tvg_impl_save_last_accel(tvg_context *ctx);

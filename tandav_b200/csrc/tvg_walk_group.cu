@@ -226,6 +226,7 @@ struct GroupParams {
 	float ew_rel;       // Ewald opening: alpha_E / TREE_OPEN_PARAM_REL (relative mode)
 	float ew_bh;        // Ewald opening: s^2 h2 limit in units of L^2 (Barnes-Hut mode)
 	float taylor_h;     // groups with a larger half extent take per-target images (with Ewald)
+	float tay_grid;     // Taylor-table node spacings per length (2 (TVG_TAYLOR_NODES - 1) / L)
 	double uniform;     // G M_total / L^2: scale of the uniform-background remainder
 };
 
@@ -772,6 +773,63 @@ __device__ __forceinline__ void ewald_kjh(const GroupParams &p, const float4 *__
 	}
 }
 
+// K, J, H as ewald_kjh, from the Taylor table (tvg_ewald.cu, k_ewald_taylor):
+// the record of the node nearest to |d| holds T and its first three
+// derivatives in node units; with D = d3T . du, the value is
+// T + du . (dT + 1/2 (d2T + D/3) du), the gradient dT + (d2T + D/2) du and the
+// second derivatives d2T + D (exact for a cubic).
+__device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const float4 *__restrict__ tay,
+                                                 float4 e, CorrSum &c)
+{
+	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
+	const float u = fabsf(e.x) * p.tay_grid, v = fabsf(e.y) * p.tay_grid, w = fabsf(e.z) * p.tay_grid;
+	const int i = min(__float2int_rn(u), TVG_TAYLOR_NODES - 1);
+	const int j = min(__float2int_rn(v), TVG_TAYLOR_NODES - 1);
+	const int l = min(__float2int_rn(w), TVG_TAYLOR_NODES - 1);
+	const float du = u - (float) i, dv = v - (float) j, dw = w - (float) l;
+	const float4 *rec = tay + 16 * ((i * TVG_TAYLOR_NODES + j) * TVG_TAYLOR_NODES + l);
+	const float m0 = -e.w * p.inv_box * p.inv_box, m1 = m0 * p.tay_grid, m2 = m1 * p.tay_grid;
+#pragma unroll
+	for (int q = 0; q < 3; q++) {
+		const float4 r0 = __ldg(rec + 5 * q), r1 = __ldg(rec + 5 * q + 1), r2 = __ldg(rec + 5 * q + 2),
+		             r3 = __ldg(rec + 5 * q + 3), r4 = __ldg(rec + 5 * q + 4);
+		// D_bc = sum_d d3T_bcd du_d
+		const float dxx = fmaf(r2.z, du, fmaf(r3.y, dv, r3.z * dw));
+		const float dyy = fmaf(r3.w, du, fmaf(r2.w, dv, r4.x * dw));
+		const float dzz = fmaf(r4.y, du, fmaf(r4.z, dv, r3.x * dw));
+		const float dxy = fmaf(r3.y, du, fmaf(r3.w, dv, r4.w * dw));
+		const float dxz = fmaf(r3.z, du, fmaf(r4.w, dv, r4.y * dw));
+		const float dyz = fmaf(r4.w, du, fmaf(r4.x, dv, r4.z * dw));
+		const float hxx = r1.x + dxx, hyy = r1.y + dyy, hzz = r1.z + dzz;
+		const float hxy = r1.w + dxy, hxz = r2.x + dxz, hyz = r2.y + dyz;
+		// gradient: dT + (d2T + D/2) du
+		const float gx = r0.y + fmaf(fmaf(0.5f, dxx, r1.x), du, fmaf(fmaf(0.5f, dxy, r1.w), dv,
+		                              fmaf(0.5f, dxz, r2.x) * dw));
+		const float gy = r0.z + fmaf(fmaf(0.5f, dxy, r1.w), du, fmaf(fmaf(0.5f, dyy, r1.y), dv,
+		                              fmaf(0.5f, dyz, r2.y) * dw));
+		const float gz = r0.w + fmaf(fmaf(0.5f, dxz, r2.x), du, fmaf(fmaf(0.5f, dyz, r2.y), dv,
+		                              fmaf(0.5f, dzz, r1.z) * dw));
+		// value: T + du . (dT + 1/2 (d2T + D/3) du)
+		const float t3 = 1.f / 3.f;
+		const float bx = fmaf(fmaf(t3, dxx, r1.x), du, fmaf(fmaf(t3, dxy, r1.w), dv, fmaf(t3, dxz, r2.x) * dw));
+		const float by = fmaf(fmaf(t3, dxy, r1.w), du, fmaf(fmaf(t3, dyy, r1.y), dv, fmaf(t3, dyz, r2.y) * dw));
+		const float bz = fmaf(fmaf(t3, dxz, r2.x), du, fmaf(fmaf(t3, dyz, r2.y), dv, fmaf(t3, dzz, r1.z) * dw));
+		const float val = r0.x + fmaf(fmaf(0.5f, bx, r0.y), du, fmaf(fmaf(0.5f, by, r0.z), dv,
+		                               fmaf(0.5f, bz, r0.w) * dw));
+		const float sq = sg[q];
+		c.k[q] = fmaf(m0 * sq, val, c.k[q]);
+		c.j[3 * q + 0] = fmaf(m1 * sq * sg[0], gx, c.j[3 * q + 0]);
+		c.j[3 * q + 1] = fmaf(m1 * sq * sg[1], gy, c.j[3 * q + 1]);
+		c.j[3 * q + 2] = fmaf(m1 * sq * sg[2], gz, c.j[3 * q + 2]);
+		c.h[6 * q + 0] = fmaf(m2 * sq, hxx, c.h[6 * q + 0]);
+		c.h[6 * q + 1] = fmaf(m2 * sq, hyy, c.h[6 * q + 1]);
+		c.h[6 * q + 2] = fmaf(m2 * sq, hzz, c.h[6 * q + 2]);
+		c.h[6 * q + 3] = fmaf(m2 * sq * sg[0] * sg[1], hxy, c.h[6 * q + 3]);
+		c.h[6 * q + 4] = fmaf(m2 * sq * sg[0] * sg[2], hxz, c.h[6 * q + 4]);
+		c.h[6 * q + 5] = fmaf(m2 * sq * sg[1] * sg[2], hyz, c.h[6 * q + 5]);
+	}
+}
+
 // K(d) alone (tricubic value), for per-target evaluation, added to a
 template <bool MLP>
 __device__ __forceinline__ void ewald_k(const GroupParams &p, const float4 *__restrict__ tab,
@@ -866,14 +924,16 @@ __device__ __forceinline__ void uniform_remainder(const GroupParams &p, double t
 // images, every entry for every target of the lane (K at the target's
 // nearest image; FP32 per batch, carried in FP64).
 template <int TPL, bool MLP>
-__device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab, const float *mlp,
-                                            const float4 *list, int from, int cnt, bool per_target,
+__device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab, const float4 *tay,
+                                            const float *mlp, const float4 *list, int from, int cnt,
+                                            bool per_target,
                                             CorrSum &c, Target (&t)[TPL], float &nev)
 {
 	const int lane = threadIdx.x & 31;
 	if (!per_target) {
 		if (lane < cnt) {
-			ewald_kjh<MLP>(p, tab, mlp, list[from + lane], c);
+			if (MLP) ewald_kjh<MLP>(p, tab, mlp, list[from + lane], c);
+			else ewald_kjh_taylor(p, tay, list[from + lane], c);
 			nev += 1.f;
 		}
 	} else {
@@ -906,7 +966,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
                             const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
                             const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
                             const float *__restrict__ last_acc, const float4 *__restrict__ tab,
-                            const float *mlp,
+                            const float4 *__restrict__ tay, const float *mlp,
                             int64_t first, int cnt, const int32_t *__restrict__ active,
                             Target (&t)[TPL], float &nev, int *status)
 {
@@ -983,7 +1043,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		nl += __popc(bm);
 		__syncwarp();
 		if (nl >= 32) {
-			ewald_batch<TPL, MLP>(p, tab, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
+			ewald_batch<TPL, MLP>(p, tab, tay, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
 			nl -= 32;
 		}
 		push_children(S.stack, sp, open_int, nchild, child);
@@ -1007,7 +1067,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 				nl += __popc(mb);
 				__syncwarp();
 				if (nl >= 32) {
-					ewald_batch<TPL, MLP>(p, tab, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
+					ewald_batch<TPL, MLP>(p, tab, tay, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
 					nl -= 32;
 				}
 			}
@@ -1015,7 +1075,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		__syncwarp();
 	}
 	__syncwarp();
-	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, mlp, S.list, 0, nl, per_target, c, t, nev);
+	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, tay, mlp, S.list, 0, nl, per_target, c, t, nev);
 	if (per_target) return;
 	// sum over lanes (FP64), then K(d_c - t) ~ K - J t + H:tt / 2 per target
 	double K[3], J[9], H[18];
@@ -1063,7 +1123,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
               const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
               const float *__restrict__ last_acc, const float4 *__restrict__ tab,
-              const __nv_bfloat16 *__restrict__ mlp_w, F *acc0, F *acc1,
+              const float4 *__restrict__ tay, const __nv_bfloat16 *__restrict__ mlp_w, F *acc0, F *acc1,
               F *acc2, F *gacc0, F *gacc1, F *gacc2, int32_t *work, double *counter, int *status)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1092,7 +1152,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 		}
 		Target t[TPL];
 		float nev = 0.f;
-		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, mlp, first, cnt, active, t, nev,
+		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, tay, mlp, first, cnt, active, t, nev,
 		                 status);
 		ev_acc += nev;
 #pragma unroll
@@ -1237,7 +1297,7 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
 	    ctx->wtree, ctx->ipos[0], ctx->ipos[1],
 	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext,
-	    (const __nv_bfloat16 *) ctx->mlp_bf16, (F *) ctx->f[FS_ACC0],
+	    (const float4 *) ctx->ewald_taylor, (const __nv_bfloat16 *) ctx->mlp_bf16, (F *) ctx->f[FS_ACC0],
 	    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1],
 	    (F *) ctx->f[FS_GACC2], ctx->work_counter + 1, counter, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
@@ -1288,6 +1348,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	cudaStream_t s = ctx->stream;
 	if (!ctx->have_walktree) TVG_CHECK(prepare_typed<F>(ctx));
 	if (ewald && !ctx->ewald_ext) TVG_CHECK(tvg_impl_ewald_ext(ctx));
+	if (ewald && !ctx->ewald_taylor) TVG_CHECK(tvg_impl_ewald_taylor(ctx));
 	// FP32 copies of mass / last |a| (views when Float is float)
 	const float *mass_f = (const float *) ctx->f[FS_MASS];
 	const float *last_f = (const float *) ctx->f[FS_LAST_ACC];
@@ -1325,6 +1386,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	p.near2 = (float) (h * h * 1.001);
 	p.grid = (float) (cf.periodic ? 2.0 * 64.0 / cf.boxsize : 0.0);
 	p.inv_box = (float) (cf.periodic ? 1.0 / cf.boxsize : 0.0);
+	p.tay_grid = (float) (cf.periodic ? 2.0 * (TVG_TAYLOR_NODES - 1) / cf.boxsize : 0.0);
 	p.ew_rel = (float) (ctx->ewald_open_rel / cf.open_rel);   // times g.fac: alpha_E |a_old| / G
 	p.ew_bh = (float) (ctx->ewald_open_bh * cf.open_bh);
 	// half extent beyond which a group takes per-target images with the Ewald
