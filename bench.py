@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--plain-stride", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-mlp", action="store_true", help="skip the learned-Ewald step")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak loop (profiling runs)")
     ap.add_argument("--open-rel", type=float, default=6e-5,
                     help="TREE_OPEN_PARAM_REL of the group form")
@@ -425,6 +426,38 @@ def main():
         except (OSError, ValueError):
             pass
 
+    # ---- the same step with the learned Ewald correction: trained here by the
+    # library's own kernels, judged by the exact table, then run in the walk
+    learned = None
+    if not args.no_mlp:
+        ctx.timer_start()
+        loss = ctx.mlp_train(steps=20000, batch=16384, n_samples=1 << 20, lr=2e-3, lr_final=1e-6,
+                             seed=3)
+        train_ms = ctx.timer_stop()
+        mx, rms = ctx.mlp_judge(max_allowed=1.0)
+        ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts, ewald_kind=G.EWALD_MLP)
+        ml_ms = ml_ew = 0.0
+        for _ in range(args.steps):
+            ctx.timer_start()
+            ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts, ewald_kind=G.EWALD_MLP)
+            ml_ms += ctx.timer_stop()
+            ml_ew += ctx.phase_times()["ewald"]
+        t_ml = dist.max(ml_ms / args.steps) / 1e3
+        learned = {"particles_per_s": dist.sum(n) / t_ml, "ms_per_step": round(t_ml * 1e3, 2),
+                   "ewald_walk_ms": round(ml_ew / args.steps, 2),
+                   "train": {"steps": 20000, "batch": 16384, "samples": 1 << 20, "loss": loss,
+                             "ms": round(train_ms, 1)},
+                   "correction_error_vs_fp64_table": {"max": mx, "rms": rms},
+                   "model": ("T = 4 pi x / 3 + seven nearest images + fitted cubic + s N(x); N "
+                             "3-64-64-3 tanh, BF16 weights, FP32 arithmetic; J and H from the "
+                             "tricubic table")}
+        if tgt_ids is not None:
+            ids_m = ctx.download(G.F_ID)["id"]
+            inv = np.empty(n, np.int64)
+            inv[ids_m] = np.arange(n)
+            _, _, err_m = ctx.forcetest(np.sort(inv[tgt_ids]))
+            learned["force_error"] = {k: float(f"{v:.4e}") for k, v in err_m.items()}
+
     # ---- plain GPU form on a strided sample of active particles
     for a in (ids, h_pos, h_mass, h_last, h_acc, h_ids, h_oid):
         a.free()
@@ -510,6 +543,7 @@ def main():
                            "evaluations_per_group": round(ew_i / args.steps / (n / (32 * tune_choice)), 1),
                            "evaluation": "Taylor-table K, dK, d2K: 15 float4 loads, ~200 FP32 ops"},
             "plain_form": plain,
+            "learned_ewald": learned,
             "accuracy": accuracy,
             "autotune": {"targets_per_lane": tune_choice,
                          "walk_ms_1_2_4_targets_per_lane": [round(x, 1) for x in tune_ms]},

@@ -395,17 +395,22 @@ typedef struct {
 	int32_t resume;
 } tvg_mlp_train_config;
 
-/* Number of network parameters (float). */
-#define TVG_MLP_NPARAM 4611
+/* Number of parameters (float): the 3-64-64-3 network (4611, trained), then
+ * the cubic fit of the correction's smooth part (3 x 20) and the network's
+ * output scale (fitted). The model is T(x) = 4 pi x / 3 + S(x) + C . m(4x-1)
+ * + s N(4x-1), S the seven lattice images nearest to the octant. */
+#define TVG_MLP_NPARAM 4672
 
-/* Trains on the device; final_loss = mean square residual per component
- * (box units) of the FP32 weights over all samples. Leaves the weights
- * unjudged (see tvg_ewald_mlp_judge). */
+/* Trains on the device (fits C and s first unless resume != 0);
+ * final_loss = mean square error per component of T (box units) with the
+ * FP32 weights over all samples. Leaves the weights unjudged (see
+ * tvg_ewald_mlp_judge). */
 int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config *cfg, float *final_loss);
 /* Copies the FP32 parameters out (set = 0) or in (set != 0). */
 int tvg_ewald_mlp_weights(tvg_context *ctx, float *params, int32_t set);
-/* Gradient of the mean-square loss over n samples x[3n] (octant, box units)
- * with residual targets y[3n] (T(x) - 4 pi x / 3), from the training kernels. */
+/* Gradient of the network's mean-square loss over n samples x[3n] (octant,
+ * box units) with targets y[3n] for N (what the rest of the model leaves,
+ * divided by s), from the training kernels; the fitted entries get 0. */
 int tvg_ewald_mlp_grad(tvg_context *ctx, int64_t n, const float *x, const float *y, float *grad,
                        float *loss);
 /* T(x) at n octant points x[3n] (box units) from the BF16 weights. */

@@ -6,18 +6,24 @@
 // Model: x in [0, 1/2]^3 (box units, the folded octant; the other octants
 // follow from the symmetries T_a(.., -x_b, ..) = -T_a if a = b, +T_a
 // otherwise), v = 4 x - 1, and
-//     T(x) = (4 pi / 3) x + W3 tanh(W2 tanh(W1 v + b1) + b2) + b3,
-// i.e. the network learns what is left after the exact linear term of T at
-// the origin (the uniform background). Parameters, 4611 floats:
+//     T(x) = 4 pi x / 3 + S(x) + C . m(v) + s N(v)
+// (tvg_ewald_mlp.cuh): the linear background term, the seven nearest lattice
+// images, a cubic least-squares fit, and the network N on what is left,
+// scaled by that rest's rms s. Without S and the fit the same network reached
+// 5.6e-3 rms in T; with them, 1.4e-4 (FP64 fits of 2^15 points, 6000 Adam
+// steps). Parameters, 4672 floats:
 //     W1[64][3] @0, b1[64] @192, W2[64][64] @256, b2[64] @4352,
-//     W3[3][64] @4416, b3[3] @4608.
+//     W3[3][64] @4416, b3[3] @4608 (the network, 4611, trained);
+//     C[3][20] @4611, s @4671 (fitted).
 //
-// Training (own kernels, FP32): 2^20 seeded points uniform on the octant,
-// targets T(x) by the FP64 Ewald sum of the table generator
-// (tvg_ewald_sum.cuh); minibatch mean-square loss over the three components;
-// one thread per sample runs forward and backward, gradients are summed over
-// the warp by shuffles into one slot per warp, then over the slots in fixed
-// order (deterministic), then Adam.
+// Training (own kernels): 2^20 seeded points uniform on the octant, FP64
+// targets T(x) by the Ewald sum of the table generator (tvg_ewald_sum.cuh)
+// minus the analytic part; the normal equations of the cubic fit summed in
+// FP64 (fixed-order block sums) and solved on the host (Cholesky); then the
+// network's FP32 minibatch mean-square loss on the normalised rest: one
+// thread per sample runs forward and backward, gradients are summed over the
+// warp by shuffles into one slot per warp, then over the slots in fixed order
+// (deterministic), then Adam.
 //
 // Inference: BF16 weights (rounded once after training), FP32 arithmetic and
 // accumulation. The exact FP64 table (the reference's 65^3 nodes) is the
@@ -25,6 +31,8 @@
 // walk refuses the learned correction when the max error is above the limit
 // the caller gives.
 #include <math.h>
+
+#include <cmath>
 #include <stdlib.h>
 
 #include <vector>
@@ -45,17 +53,79 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t z)
 
 __device__ __forceinline__ double u01(uint64_t r) { return (double) (r >> 11) * (1.0 / 9007199254740992.0); }
 
-// points uniform on [0, 1/2]^3 and their residual targets T(x) - 4 pi x / 3
-__global__ void k_mlp_data(int64_t n, uint64_t seed, float *x, float *y)
+// points uniform on [0, 1/2]^3 (FP32-representable) and, in FP64, what the
+// analytic part leaves of T there
+__global__ void k_mlp_data(int64_t n, uint64_t seed, float *x, double *yraw)
 {
 	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	double p[3], f[3], pot;
-	for (int d = 0; d < 3; d++) p[d] = 0.5 * u01(splitmix64(seed ^ (uint64_t) (3 * i + d) * 0x2545F4914F6CDD1Dull));
+	double p[3], f[3], a[3], pot;
+	for (int d = 0; d < 3; d++)
+		p[d] = (double) (float) (0.5 * u01(splitmix64(seed ^ (uint64_t) (3 * i + d) * 0x2545F4914F6CDD1Dull)));
 	ewald_point(p, f, &pot);
+	mlp_analytic(p, a);
 	for (int d = 0; d < 3; d++) {
 		x[3 * i + d] = (float) p[d];
-		y[3 * i + d] = (float) (f[d] - MLP_LIN * p[d]);
+		yraw[3 * i + d] = f[d] - a[d];
+	}
+}
+
+// normal equations of the cubic fit: entry e < 210 is G_ij = sum m_i m_j
+// (i <= j, row by row), e < 270 is b_ai = sum y_a m_i, e < 273 is sum y_a^2;
+// block (e, c) sums the samples of chunk c in a fixed order
+#define LSQ_NE 273
+#define LSQ_CHUNKS 64
+__global__ void __launch_bounds__(128)
+k_mlp_lsq(int64_t n, const float *__restrict__ x, const double *__restrict__ yraw, double *part)
+{
+	const int e = blockIdx.x, c = blockIdx.y;
+	int kind, i = 0, j = 0, a = 0;
+	if (e < 210) {
+		kind = 0;
+		int r = e;
+		while (r >= MLP_NMONO - i) { r -= MLP_NMONO - i; i++; }
+		j = i + r;
+	} else if (e < 270) {
+		kind = 1;
+		a = (e - 210) / MLP_NMONO;
+		i = (e - 210) % MLP_NMONO;
+	} else {
+		kind = 2;
+		a = e - 270;
+	}
+	const int64_t lo = n * c / LSQ_CHUNKS, hi = n * (c + 1) / LSQ_CHUNKS;
+	double acc = 0;
+	for (int64_t q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+		const double v[3] = { 4.0 * x[3 * q] - 1.0, 4.0 * x[3 * q + 1] - 1.0, 4.0 * x[3 * q + 2] - 1.0 };
+		double m[MLP_NMONO];
+		mlp_monomials<double>(v, m);
+		if (kind == 0) acc += m[i] * m[j];
+		else if (kind == 1) acc += yraw[3 * q + a] * m[i];
+		else acc += yraw[3 * q + a] * yraw[3 * q + a];
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+	__shared__ double ws[4];
+	if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x == 0) part[(int64_t) e * LSQ_CHUNKS + c] = ((ws[0] + ws[1]) + ws[2]) + ws[3];
+}
+
+// network targets: (what the analytic part and the fit leave) / s, with the
+// FP32 coefficients inference uses
+__global__ void k_mlp_target(int64_t n, const float *__restrict__ x, const double *__restrict__ yraw,
+                             const float *__restrict__ prm, float *y)
+{
+	const int64_t q = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (q >= n) return;
+	const double v[3] = { 4.0 * x[3 * q] - 1.0, 4.0 * x[3 * q + 1] - 1.0, 4.0 * x[3 * q + 2] - 1.0 };
+	double m[MLP_NMONO];
+	mlp_monomials<double>(v, m);
+	const double inv_s = 1.0 / (double) prm[MLP_SCALE];
+	for (int a = 0; a < 3; a++) {
+		double r = yraw[3 * q + a];
+		for (int k = 0; k < MLP_NMONO; k++) r -= (double) prm[MLP_POLY + MLP_NMONO * a + k] * m[k];
+		y[3 * q + a] = (float) (r * inv_s);
 	}
 }
 
@@ -89,7 +159,7 @@ k_mlp_grad(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
 	const int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	const bool have = s < n;
 	const int64_t gw = s >> 5;
-	float *slot = slots + gw * MLP_NPARAM;
+	float *slot = slots + gw * MLP_NNET;
 	float v[3] = { 0.f, 0.f, 0.f }, t[3] = { 0.f, 0.f, 0.f };
 	if (have) {
 		for (int d = 0; d < 3; d++) {
@@ -157,12 +227,12 @@ __global__ void k_mlp_sum(int nslots, const float *__restrict__ slots, const flo
                           float *grad, float *loss)
 {
 	const int e = blockIdx.x * blockDim.x + threadIdx.x;
-	if (e < MLP_NPARAM) {
+	if (e < MLP_NNET) {
 		float g = 0.f;
-		for (int w = 0; w < nslots; w++) g += slots[(int64_t) w * MLP_NPARAM + e];
+		for (int w = 0; w < nslots; w++) g += slots[(int64_t) w * MLP_NNET + e];
 		grad[e] = g;
 	}
-	if (e == MLP_NPARAM) {
+	if (e == MLP_NNET) {
 		double l = 0;
 		for (int w = 0; w < nslots; w++) l += lslots[w];
 		*loss = (float) l;
@@ -174,7 +244,7 @@ __global__ void k_mlp_adam(float *prm, const float *__restrict__ grad, float *m,
                            float c1, float c2)
 {
 	const int e = blockIdx.x * blockDim.x + threadIdx.x;
-	if (e >= MLP_NPARAM) return;
+	if (e >= MLP_NNET) return;
 	const float g = grad[e];
 	m[e] = 0.9f * m[e] + 0.1f * g;
 	v[e] = 0.999f * v[e] + 0.001f * g * g;
@@ -187,7 +257,8 @@ __global__ void k_mlp_to_bf16(const float *__restrict__ prm, __nv_bfloat16 *out)
 	if (e < MLP_NPARAM) out[e] = __float2bfloat16_rn(prm[e]);
 }
 
-// forward only: per-warp sums of the squared residual
+// forward only: per-warp sums of the network's squared residual (in units
+// of s^2)
 __global__ void __launch_bounds__(128)
 k_mlp_loss(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
            const float *__restrict__ prm, float *loss_slots)
@@ -198,11 +269,11 @@ k_mlp_loss(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
 	const int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	float l = 0.f;
 	if (s < n) {
-		float xs[3], out[3];
-		for (int d = 0; d < 3; d++) xs[d] = x[3 * s + d];
-		mlp_forward(P, xs, out);
+		float v[3], out[3];
+		for (int d = 0; d < 3; d++) v[d] = 4.f * x[3 * s + d] - 1.f;
+		mlp_net(P, v, out);
 		for (int d = 0; d < 3; d++) {
-			const float r = out[d] - MLP_LIN * xs[d] - y[3 * s + d];
+			const float r = out[d] - y[3 * s + d];
 			l += r * r;
 		}
 	}
@@ -212,12 +283,13 @@ k_mlp_loss(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
 
 // ------------------------------------------------------------ inference
 
-// T(x) for points of the octant, BF16 weights, FP32 arithmetic
+// T(x) for points of the octant, BF16 network weights, FP32 arithmetic
 __global__ void __launch_bounds__(128)
-k_mlp_eval(int64_t n, const double *__restrict__ x, const __nv_bfloat16 *__restrict__ w, double *t)
+k_mlp_eval(int64_t n, const double *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
+           const float *__restrict__ f32, double *t)
 {
 	__shared__ float P[MLP_NPARAM];
-	for (int e = threadIdx.x; e < MLP_NPARAM; e += blockDim.x) P[e] = __bfloat162float(w[e]);
+	for (int e = threadIdx.x; e < MLP_NPARAM; e += blockDim.x) P[e] = mlp_param(w, f32, e);
 	__syncthreads();
 	const int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (s >= n) return;
@@ -255,6 +327,64 @@ static void init_params(std::vector<float> &p, uint64_t seed)
 	for (int e = 0; e < 3 * MLP_H; e++) p[MLP_W3 + e] = (float) ((2 * next() - 1) * l3);
 }
 
+// the cubic fit from the summed normal equations (k_mlp_lsq): Cholesky in
+// FP64 for the three components; the coefficients are stored as FP32 and s is
+// the rms of what they leave (evaluated with the FP32 coefficients)
+static int fit_cubic(tvg_context *ctx, const std::vector<double> &part, int64_t ns,
+                     std::vector<float> &p0)
+{
+	const int M = MLP_NMONO;
+	double sum[LSQ_NE];
+	for (int e = 0; e < LSQ_NE; e++) {
+		double t = 0;
+		for (int c = 0; c < LSQ_CHUNKS; c++) t += part[(size_t) e * LSQ_CHUNKS + c];
+		sum[e] = t;
+	}
+	double G[M][M], L[M][M] = {};
+	int e = 0;
+	for (int i = 0; i < M; i++)
+		for (int j = i; j < M; j++, e++) G[i][j] = G[j][i] = sum[e];
+	for (int i = 0; i < M; i++) {
+		for (int j = 0; j <= i; j++) {
+			double t = G[i][j];
+			for (int k = 0; k < j; k++) t -= L[i][k] * L[j][k];
+			if (i == j) {
+				if (!(t > 0)) return tvg_fail(ctx, TVG_E_CUDA, "mlp fit: normal equations not positive definite");
+				L[i][i] = sqrt(t);
+			} else {
+				L[i][j] = t / L[j][j];
+			}
+		}
+	}
+	double r2 = 0;
+	for (int a = 0; a < 3; a++) {
+		double z[M], c[M];
+		for (int i = 0; i < M; i++) {
+			double t = sum[210 + M * a + i];
+			for (int k = 0; k < i; k++) t -= L[i][k] * z[k];
+			z[i] = t / L[i][i];
+		}
+		for (int i = M - 1; i >= 0; i--) {
+			double t = z[i];
+			for (int k = i + 1; k < M; k++) t -= L[k][i] * c[k];
+			c[i] = t / L[i][i];
+		}
+		double cf[M], gc = 0, bc = 0;
+		for (int i = 0; i < M; i++) {
+			p0[MLP_POLY + M * a + i] = (float) c[i];
+			cf[i] = (double) (float) c[i];
+		}
+		for (int i = 0; i < M; i++) {
+			bc += cf[i] * sum[210 + M * a + i];
+			for (int j = 0; j < M; j++) gc += cf[i] * G[i][j] * cf[j];
+		}
+		r2 += sum[270 + a] - 2 * bc + gc;
+	}
+	const double sc = sqrt(r2 / (3.0 * (double) ns));
+	p0[MLP_SCALE] = (sc > 1e-30 && std::isfinite(sc)) ? (float) sc : 1.f;
+	return TVG_OK;
+}
+
 static int ensure_mlp(tvg_context *ctx)
 {
 	TVG_CHECK(dmalloc(ctx, (void **) &ctx->mlp_prm, 4 * MLP_NPARAM));
@@ -279,8 +409,8 @@ static int grad_batch(tvg_context *ctx, int64_t n, const float *x, const float *
 	k_mlp_grad<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, ctx->stream>>>(
 	    n, x, y, ctx->mlp_prm, 1.f / (3.f * (float) n), slots, lslots);
 	TVG_CUDA(ctx, cudaGetLastError());
-	k_mlp_sum<<<TVG_CNT(ctx, (MLP_NPARAM + 1 + 255) / 256), 256, 0, ctx->stream>>>(nslots, slots, lslots,
-	                                                                               grad, loss);
+	k_mlp_sum<<<TVG_CNT(ctx, (MLP_NNET + 1 + 255) / 256), 256, 0, ctx->stream>>>(nslots, slots, lslots,
+	                                                                             grad, loss);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }
@@ -296,7 +426,7 @@ extern "C" int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config 
 	TVG_CHECK(ensure_mlp(ctx));
 	const int64_t ns = cfg->n_samples, nb = cfg->batch;
 	float *x = nullptr, *y = nullptr, *slots = nullptr, *lslots = nullptr, *grad = nullptr,
-	      *m = nullptr, *v = nullptr, *loss = nullptr;
+	      *m = nullptr, *v = nullptr, *loss = nullptr, *yraw_f = nullptr, *part_f = nullptr;
 	std::vector<void *> bufs;
 	auto alloc = [&](float **p, size_t b) -> int {
 		cudaError_t e = cudaMalloc((void **) p, b);
@@ -312,24 +442,36 @@ extern "C" int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config 
 	if ((rc = alloc(&x, 12 * (size_t) ns)) || (rc = alloc(&y, 12 * (size_t) ns))
 	    || (rc = alloc(&slots, 4 * (size_t) nslots * MLP_NPARAM)) || (rc = alloc(&lslots, 4 * (size_t) nslots))
 	    || (rc = alloc(&grad, 4 * MLP_NPARAM)) || (rc = alloc(&m, 4 * MLP_NPARAM))
-	    || (rc = alloc(&v, 4 * MLP_NPARAM)) || (rc = alloc(&loss, 4))) {
+	    || (rc = alloc(&v, 4 * MLP_NPARAM)) || (rc = alloc(&loss, 4))
+	    || (rc = alloc(&yraw_f, 24 * (size_t) ns)) || (rc = alloc(&part_f, 8 * LSQ_NE * LSQ_CHUNKS))) {
 		for (void *b : bufs) cudaFree(b);
 		return rc;
 	}
+	double *yraw = (double *) yraw_f, *part = (double *) part_f;
 	auto done = [&](int r) {
 		cudaStreamSynchronize(s);
 		for (void *b : bufs) cudaFree(b);
 		return r;
 	};
+	k_mlp_data<<<TVG_CNT(ctx, tvg_blocks(ns, 128)), 128, 0, s>>>(ns, cfg->seed, x, yraw);
+	if (cudaGetLastError() != cudaSuccess) return done(tvg_fail(ctx, TVG_E_CUDA, "mlp data launch"));
 	if (!cfg->resume) {
+		// the cubic fit of what the analytic part leaves, then the network's
+		// initial weights (a resumed training keeps both)
 		std::vector<float> p0;
 		init_params(p0, cfg->seed);
+		k_mlp_lsq<<<TVG_CNT(ctx, dim3(LSQ_NE, LSQ_CHUNKS)), 128, 0, s>>>(ns, x, yraw, part);
+		if (cudaGetLastError() != cudaSuccess) return done(tvg_fail(ctx, TVG_E_CUDA, "mlp lsq launch"));
+		std::vector<double> hp((size_t) LSQ_NE * LSQ_CHUNKS);
+		if (cudaMemcpyAsync(hp.data(), part, 8 * hp.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess
+		    || cudaStreamSynchronize(s) != cudaSuccess)
+			return done(tvg_fail(ctx, TVG_E_CUDA, "mlp lsq copy"));
+		if ((rc = fit_cubic(ctx, hp, ns, p0))) return done(rc);
 		if (cudaMemcpyAsync(ctx->mlp_prm, p0.data(), 4 * MLP_NPARAM, cudaMemcpyHostToDevice, s) != cudaSuccess)
 			return done(tvg_fail(ctx, TVG_E_CUDA, "mlp train: upload failed"));
-		cudaStreamSynchronize(s);
 	}
-	k_mlp_data<<<TVG_CNT(ctx, tvg_blocks(ns, 128)), 128, 0, s>>>(ns, cfg->seed, x, y);
-	if (cudaGetLastError() != cudaSuccess) return done(tvg_fail(ctx, TVG_E_CUDA, "mlp data launch"));
+	k_mlp_target<<<TVG_CNT(ctx, tvg_blocks(ns, 128)), 128, 0, s>>>(ns, x, yraw, ctx->mlp_prm, y);
+	if (cudaGetLastError() != cudaSuccess) return done(tvg_fail(ctx, TVG_E_CUDA, "mlp target launch"));
 	cudaMemsetAsync(m, 0, 4 * MLP_NPARAM, s);
 	cudaMemsetAsync(v, 0, 4 * MLP_NPARAM, s);
 	const int64_t nbatches = ns / nb;
@@ -341,7 +483,7 @@ extern "C" int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config 
 		rc = grad_batch(ctx, nb, x + 3 * off, y + 3 * off, grad, loss, slots, lslots);
 		if (rc) return done(rc);
 		const float c1 = (float) (1.0 / (1.0 - pow(0.9, st + 1))), c2 = (float) (1.0 / (1.0 - pow(0.999, st + 1)));
-		k_mlp_adam<<<TVG_CNT(ctx, (MLP_NPARAM + 255) / 256), 256, 0, s>>>(ctx->mlp_prm, grad, m, v, lr, c1, c2);
+		k_mlp_adam<<<TVG_CNT(ctx, (MLP_NNET + 255) / 256), 256, 0, s>>>(ctx->mlp_prm, grad, m, v, lr, c1, c2);
 		if (cudaGetLastError() != cudaSuccess) return done(tvg_fail(ctx, TVG_E_CUDA, "mlp adam launch"));
 	}
 	// mean-square residual of the trained FP32 weights over all samples
@@ -350,12 +492,15 @@ extern "C" int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config 
 	k_mlp_loss<<<TVG_CNT(ctx, tvg_blocks(ns, 128)), 128, 0, s>>>(ns, x, y, ctx->mlp_prm, lall);
 	if (cudaGetLastError() != cudaSuccess) return done(tvg_fail(ctx, TVG_E_CUDA, "mlp loss launch"));
 	std::vector<float> lw((size_t) mlp_slots(ns));
-	if (cudaMemcpyAsync(lw.data(), lall, 4 * lw.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+	float sc = 1.f;
+	if (cudaMemcpyAsync(lw.data(), lall, 4 * lw.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess
+	    || cudaMemcpyAsync(&sc, ctx->mlp_prm + MLP_SCALE, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
 		return done(tvg_fail(ctx, TVG_E_CUDA, "mlp loss copy"));
 	cudaStreamSynchronize(s);
 	double tot = 0;
 	for (float q : lw) tot += q;
-	if (final_loss) *final_loss = (float) (tot / (3.0 * (double) ns));
+	// in units of T^2
+	if (final_loss) *final_loss = (float) (tot / (3.0 * (double) ns) * (double) sc * (double) sc);
 	rc = refresh_bf16(ctx);
 	return done(rc);
 }
@@ -391,6 +536,7 @@ extern "C" int tvg_ewald_mlp_grad(tvg_context *ctx, int64_t n, const float *x, c
 	TVG_CUDA(ctx, cudaMalloc((void **) &ll, 4 * (size_t) nslots));
 	TVG_CUDA(ctx, cudaMalloc((void **) &g, 4 * MLP_NPARAM + 4));
 	l = g + MLP_NPARAM;
+	cudaMemsetAsync(g, 0, 4 * MLP_NPARAM + 4, s);      // the fitted entries have no gradient
 	cudaMemcpyAsync(dx, x, 12 * (size_t) n, cudaMemcpyHostToDevice, s);
 	cudaMemcpyAsync(dy, y, 12 * (size_t) n, cudaMemcpyHostToDevice, s);
 	int rc = grad_batch(ctx, n, dx, dy, g, l, sl, ll);
@@ -412,7 +558,8 @@ extern "C" int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, 
 	TVG_CUDA(ctx, cudaMalloc((void **) &dx, 24 * (size_t) n));
 	TVG_CUDA(ctx, cudaMalloc((void **) &dt, 24 * (size_t) n));
 	cudaMemcpyAsync(dx, x, 24 * (size_t) n, cudaMemcpyHostToDevice, ctx->stream);
-	k_mlp_eval<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, ctx->stream>>>(n, dx, (const __nv_bfloat16 *) ctx->mlp_bf16, dt);
+	k_mlp_eval<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, ctx->stream>>>(n, dx, (const __nv_bfloat16 *) ctx->mlp_bf16,
+	                                                                      ctx->mlp_prm, dt);
 	cudaError_t e = cudaGetLastError();
 	if (e == cudaSuccess) e = cudaMemcpyAsync(t, dt, 24 * (size_t) n, cudaMemcpyDeviceToHost, ctx->stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -424,10 +571,10 @@ extern "C" int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, 
 
 // errors of the BF16 network at the 65^3 nodes of the exact FP64 table
 __global__ void k_mlp_judge(const double *__restrict__ raw, const __nv_bfloat16 *__restrict__ w,
-                            double *err)
+                            const float *__restrict__ f32, double *err)
 {
 	__shared__ float P[MLP_NPARAM];
-	for (int e = threadIdx.x; e < MLP_NPARAM; e += blockDim.x) P[e] = __bfloat162float(w[e]);
+	for (int e = threadIdx.x; e < MLP_NPARAM; e += blockDim.x) P[e] = mlp_param(w, f32, e);
 	__syncthreads();
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
 	if (idx >= 65 * 65 * 65) return;
@@ -454,7 +601,8 @@ extern "C" int tvg_ewald_mlp_judge(tvg_context *ctx, double max_allowed, double 
 	const int npt = 65 * 65 * 65;
 	double *d;
 	TVG_CUDA(ctx, cudaMalloc((void **) &d, 8 * (size_t) npt));
-	k_mlp_judge<<<TVG_CNT(ctx, (npt + 127) / 128), 128, 0, ctx->stream>>>(ctx->ewald_raw, (const __nv_bfloat16 *) ctx->mlp_bf16, d);
+	k_mlp_judge<<<TVG_CNT(ctx, (npt + 127) / 128), 128, 0, ctx->stream>>>(ctx->ewald_raw, (const __nv_bfloat16 *) ctx->mlp_bf16,
+	                                                                       ctx->mlp_prm, d);
 	std::vector<double> h(npt);
 	cudaError_t e = cudaGetLastError();
 	if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, 8 * (size_t) npt, cudaMemcpyDeviceToHost, ctx->stream);

@@ -1123,15 +1123,17 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
               const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
               const float *__restrict__ last_acc, const float4 *__restrict__ tab,
-              const float4 *__restrict__ tay, const __nv_bfloat16 *__restrict__ mlp_w, F *acc0, F *acc1,
+              const float4 *__restrict__ tay, const __nv_bfloat16 *__restrict__ mlp_w,
+              const float *__restrict__ mlp_f32, F *acc0, F *acc1,
               F *acc2, F *gacc0, F *gacc1, F *gacc2, int32_t *work, double *counter, int *status)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EwaldSmem &S = ((EwaldSmem *) smem_raw)[threadIdx.x >> 5];
-	// the learned correction's weights, BF16 -> FP32 once per block
+	// the learned correction's parameters, once per block: the network BF16 ->
+	// FP32, the fitted cubic and scale FP32
 	float *mlp = (float *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS);
 	if (MLP) {
-		for (int e = threadIdx.x; e < MLP_NPARAM; e += GW_THREADS) mlp[e] = __bfloat162float(mlp_w[e]);
+		for (int e = threadIdx.x; e < MLP_NPARAM; e += GW_THREADS) mlp[e] = mlp_param(mlp_w, mlp_f32, e);
 		__syncthreads();
 	}
 	const int lane = threadIdx.x & 31;
@@ -1297,7 +1299,8 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
 	    ctx->wtree, ctx->ipos[0], ctx->ipos[1],
 	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext,
-	    (const float4 *) ctx->ewald_taylor, (const __nv_bfloat16 *) ctx->mlp_bf16, (F *) ctx->f[FS_ACC0],
+	    (const float4 *) ctx->ewald_taylor, (const __nv_bfloat16 *) ctx->mlp_bf16, ctx->mlp_prm,
+	    (F *) ctx->f[FS_ACC0],
 	    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1],
 	    (F *) ctx->f[FS_GACC2], ctx->work_counter + 1, counter, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());

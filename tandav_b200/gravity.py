@@ -85,7 +85,7 @@ class MlpTrainConfig(C.Structure):
                 ("resume", C.c_int32)]
 
 
-MLP_NPARAM = 4611
+MLP_NPARAM = 4672
 
 
 class TvgError(RuntimeError):

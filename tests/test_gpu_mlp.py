@@ -60,10 +60,14 @@ def test_mlp_training_judged_by_table(trained):
     print(f"train loss {loss:.3e}; judge (65^3 nodes): max {mx:.3e} rms {rms:.3e}; "
           + "; ".join(f"{k}: max {v.max():.3e} rms {np.sqrt((v ** 2).mean()):.3e}" for k, v in e.items())
           + f"; max |T| {np.abs(t_ref).max():.2f}")
-    assert loss < 1e-4
-    assert np.sqrt((e["mlp_bf16"] ** 2).mean()) < 2e-2
+    assert loss < 1e-7
+    # measured: rms 6.8e-5 (BF16 network) vs 7.9e-5 (the reference's trilinear
+    # lookup of its 65^3 table), max 7.4e-4
+    assert np.sqrt((e["mlp_bf16"] ** 2).mean()) < 2e-4
+    assert e["mlp_bf16"].max() < 5e-3
+    assert rms < 3e-4 and mx < 1e-2
     # the BF16 evaluation follows the FP32 network
-    assert np.abs(t_mlp - t_fp32).max() < 0.1
+    assert np.abs(t_mlp - t_fp32).max() < 2e-3
 
 
 def test_walk_with_learned_correction(trained):
@@ -91,5 +95,7 @@ def test_walk_with_learned_correction(trained):
             err = np.sqrt(((at - ad) ** 2).sum(0) / (ad ** 2).sum(0))
             res[name] = float(np.sqrt((err ** 2).mean()))
     print("rms force error vs FP64 Ewald direct sum:", res)
-    assert res["learned"] < res["none"] / 5
-    assert res["table"] <= res["learned"]
+    # measured at 32^3: none 3.7, learned 5.69e-4, table 5.75e-4 (the gravity
+    # walk's own error dominates both)
+    assert res["learned"] < res["none"] / 1000
+    assert res["learned"] <= 1.1 * res["table"]
