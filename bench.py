@@ -449,8 +449,8 @@ def main():
                              "ms": round(train_ms, 1)},
                    "correction_error_vs_fp64_table": {"max": mx, "rms": rms},
                    "model": ("T = 4 pi x / 3 + seven nearest images + fitted cubic + s N(x); N "
-                             "3-64-64-3 tanh, BF16 weights, FP32 arithmetic; J and H from the "
-                             "tricubic table")}
+                             "3-64-64-3 tanh, hidden layer on the tensor cores (mma.sync BF16, "
+                             "FP32 accumulate, 32 points per warp); J and H from the Taylor table")}
         if tgt_ids is not None:
             ids_m = ctx.download(G.F_ID)["id"]
             inv = np.empty(n, np.int64)

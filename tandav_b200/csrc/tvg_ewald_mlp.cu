@@ -283,20 +283,24 @@ k_mlp_loss(int64_t n, const float *__restrict__ x, const float *__restrict__ y,
 
 // ------------------------------------------------------------ inference
 
-// T(x) for points of the octant, BF16 network weights, FP32 arithmetic
+// T(x) for points of the octant by the walk's evaluation (mlp_forward_warp:
+// BF16 network on the tensor cores, FP32 elsewhere)
 __global__ void __launch_bounds__(128)
 k_mlp_eval(int64_t n, const double *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
            const float *__restrict__ f32, double *t)
 {
 	__shared__ float P[MLP_NPARAM];
-	for (int e = threadIdx.x; e < MLP_NPARAM; e += blockDim.x) P[e] = mlp_param(w, f32, e);
+	__shared__ uint32_t W2b[MLP_H * MLP_H / 2];
+	mlp_load_shared(w, f32, P, W2b);
 	__syncthreads();
 	const int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (s >= n) return;
-	float xs[3], out[3];
-	for (int d = 0; d < 3; d++) xs[d] = (float) x[3 * s + d];
-	mlp_forward(P, xs, out);
-	for (int d = 0; d < 3; d++) t[3 * s + d] = (double) out[d];
+	const bool have = s < n;          // every lane of a warp takes part
+	float xs[3] = { 0.f, 0.f, 0.f }, out[3];
+	if (have)
+		for (int d = 0; d < 3; d++) xs[d] = (float) x[3 * s + d];
+	mlp_forward_warp(P, W2b, xs, out);
+	if (have)
+		for (int d = 0; d < 3; d++) t[3 * s + d] = (double) out[d];
 }
 
 // ------------------------------------------------------------ host
@@ -569,19 +573,24 @@ extern "C" int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, 
 	return TVG_OK;
 }
 
-// errors of the BF16 network at the 65^3 nodes of the exact FP64 table
-__global__ void k_mlp_judge(const double *__restrict__ raw, const __nv_bfloat16 *__restrict__ w,
-                            const float *__restrict__ f32, double *err)
+// errors of the walk's evaluation of the model at the 65^3 nodes of the
+// exact FP64 table
+__global__ void __launch_bounds__(128)
+k_mlp_judge(const double *__restrict__ raw, const __nv_bfloat16 *__restrict__ w,
+            const float *__restrict__ f32, double *err)
 {
 	__shared__ float P[MLP_NPARAM];
-	for (int e = threadIdx.x; e < MLP_NPARAM; e += blockDim.x) P[e] = mlp_param(w, f32, e);
+	__shared__ uint32_t W2b[MLP_H * MLP_H / 2];
+	mlp_load_shared(w, f32, P, W2b);
 	__syncthreads();
 	const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-	if (idx >= 65 * 65 * 65) return;
-	const int i = idx / (65 * 65), j = (idx / 65) % 65, k = idx % 65;
+	const bool have = idx < 65 * 65 * 65;      // every lane of a warp takes part
+	const int id = have ? idx : 0;
+	const int i = id / (65 * 65), j = (id / 65) % 65, k = id % 65;
 	const float xs[3] = { 0.5f * i / 64.f, 0.5f * j / 64.f, 0.5f * k / 64.f };
 	float out[3];
-	mlp_forward(P, xs, out);
+	mlp_forward_warp(P, W2b, xs, out);
+	if (!have) return;
 	double e2 = 0;
 	for (int d = 0; d < 3; d++) {
 		const double r = (double) out[d] - raw[4 * idx + d];

@@ -695,91 +695,19 @@ __device__ __forceinline__ void lagrange4(float t, float w[4], float d[4], float
 // K(d) = -G m T(d / L) / L^2 (the reference's sign rule, periodic.c:100-112),
 // looked up at |d| with the symmetries T_a(.., -x_b, ..) = -T_a if a = b,
 // +T_a otherwise.
-template <bool MLP>
-__device__ __forceinline__ void ewald_kjh(const GroupParams &p, const float4 *__restrict__ tab,
-                                          const float *mlp, float4 e, CorrSum &c)
-{
-	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
-	const float u = fabsf(e.x) * p.grid, v = fabsf(e.y) * p.grid, w = fabsf(e.z) * p.grid;
-	const int i = min((int) u, 64), j = min((int) v, 64), l = min((int) w, 64);
-	float wx[4], dx[4], ddx[4], wy[4], dy[4], ddy[4], wz[4], dz[4], ddz[4];
-	lagrange4(u - (float) i, wx, dx, ddx);
-	lagrange4(v - (float) j, wy, dy, ddy);
-	lagrange4(w - (float) l, wz, dz, ddz);
-	// y-z contraction for each x plane, then x
-	float val[3] = { 0, 0, 0 }, gx[3] = { 0, 0, 0 }, gy[3] = { 0, 0, 0 }, gz[3] = { 0, 0, 0 };
-	float hxx[3] = { 0, 0, 0 }, hyy[3] = { 0, 0, 0 }, hzz[3] = { 0, 0, 0 };
-	float hxy[3] = { 0, 0, 0 }, hxz[3] = { 0, 0, 0 }, hyz[3] = { 0, 0, 0 };
-	const int base = (i * 68 + j) * 68 + l;       // grid (i-1, j-1, l-1) at offset +1
-#pragma unroll 1
-	for (int a = 0; a < 4; a++) {
-		float y00[3] = { 0, 0, 0 }, y10[3] = { 0, 0, 0 }, y20[3] = { 0, 0, 0 };
-		float y01[3] = { 0, 0, 0 }, y11[3] = { 0, 0, 0 }, y02[3] = { 0, 0, 0 };
-#pragma unroll
-		for (int b = 0; b < 4; b++) {
-			const float4 *row = tab + base + (a * 68 + b) * 68;
-			const float4 t0 = __ldg(row), t1 = __ldg(row + 1), t2 = __ldg(row + 2), t3 = __ldg(row + 3);
-			const float T[4][3] = { { t0.x, t0.y, t0.z }, { t1.x, t1.y, t1.z },
-			                        { t2.x, t2.y, t2.z }, { t3.x, t3.y, t3.z } };
-#pragma unroll
-			for (int q = 0; q < 3; q++) {
-				const float z0 = wz[0] * T[0][q] + wz[1] * T[1][q] + wz[2] * T[2][q] + wz[3] * T[3][q];
-				const float z1 = dz[0] * T[0][q] + dz[1] * T[1][q] + dz[2] * T[2][q] + dz[3] * T[3][q];
-				const float z2 = ddz[0] * T[0][q] + ddz[1] * T[1][q] + ddz[2] * T[2][q] + ddz[3] * T[3][q];
-				y00[q] = fmaf(wy[b], z0, y00[q]);
-				y10[q] = fmaf(dy[b], z0, y10[q]);
-				y20[q] = fmaf(ddy[b], z0, y20[q]);
-				y01[q] = fmaf(wy[b], z1, y01[q]);
-				y11[q] = fmaf(dy[b], z1, y11[q]);
-				y02[q] = fmaf(wy[b], z2, y02[q]);
-			}
-		}
-#pragma unroll
-		for (int q = 0; q < 3; q++) {
-			val[q] = fmaf(wx[a], y00[q], val[q]);
-			gx[q] = fmaf(dx[a], y00[q], gx[q]);
-			hxx[q] = fmaf(ddx[a], y00[q], hxx[q]);
-			gy[q] = fmaf(wx[a], y10[q], gy[q]);
-			hxy[q] = fmaf(dx[a], y10[q], hxy[q]);
-			hyy[q] = fmaf(wx[a], y20[q], hyy[q]);
-			gz[q] = fmaf(wx[a], y01[q], gz[q]);
-			hxz[q] = fmaf(dx[a], y01[q], hxz[q]);
-			hyz[q] = fmaf(wx[a], y11[q], hyz[q]);
-			hzz[q] = fmaf(wx[a], y02[q], hzz[q]);
-		}
-	}
-	if (MLP) {
-		// the learned correction stands in for the table value; the table
-		// still gives the derivatives of the expansion
-		const float xs[3] = { u * (1.f / 128.f), v * (1.f / 128.f), w * (1.f / 128.f) };
-		mlp_forward(mlp, xs, val);
-	}
-	// unfold the symmetry and scale: K_a = -s_a T_a, J_ab = -s_a s_b g dT_a/du_b,
-	// H_abc = -s_a s_b s_c g^2 d2T_a/du_b du_c, all times G m / L^2
-	const float m0 = -e.w * p.inv_box * p.inv_box, m1 = m0 * p.grid, m2 = m1 * p.grid;
-#pragma unroll
-	for (int q = 0; q < 3; q++) {
-		const float sq = sg[q];
-		c.k[q] = fmaf(m0 * sq, val[q], c.k[q]);
-		c.j[3 * q + 0] = fmaf(m1 * sq * sg[0], gx[q], c.j[3 * q + 0]);
-		c.j[3 * q + 1] = fmaf(m1 * sq * sg[1], gy[q], c.j[3 * q + 1]);
-		c.j[3 * q + 2] = fmaf(m1 * sq * sg[2], gz[q], c.j[3 * q + 2]);
-		c.h[6 * q + 0] = fmaf(m2 * sq, hxx[q], c.h[6 * q + 0]);
-		c.h[6 * q + 1] = fmaf(m2 * sq, hyy[q], c.h[6 * q + 1]);
-		c.h[6 * q + 2] = fmaf(m2 * sq, hzz[q], c.h[6 * q + 2]);
-		c.h[6 * q + 3] = fmaf(m2 * sq * sg[0] * sg[1], hxy[q], c.h[6 * q + 3]);
-		c.h[6 * q + 4] = fmaf(m2 * sq * sg[0] * sg[2], hxz[q], c.h[6 * q + 4]);
-		c.h[6 * q + 5] = fmaf(m2 * sq * sg[1] * sg[2], hyz[q], c.h[6 * q + 5]);
-	}
-}
 
-// K, J, H as ewald_kjh, from the Taylor table (tvg_ewald.cu, k_ewald_taylor):
-// the record of the node nearest to |d| holds T and its first three
-// derivatives in node units; with D = d3T . du, the value is
-// T + du . (dT + 1/2 (d2T + D/3) du), the gradient dT + (d2T + D/2) du and the
-// second derivatives d2T + D (exact for a cubic).
+// K(d), its Jacobian J and Hessian H, summed into c, from the Taylor table
+// (tvg_ewald.cu, k_ewald_taylor): the record of the node nearest to |d| holds
+// T and its first three derivatives in node units; with D = d3T . du, the
+// value is T + du . (dT + 1/2 (d2T + D/3) du), the gradient dT + (d2T + D/2)
+// du and the second derivatives d2T + D (exact for a cubic). With OVR the
+// value is ovr (T at |d| from the learned correction) instead.
+// K_a = -s_a T_a, J_ab = -s_a s_b g dT_a/du_b, H_abc = -s_a s_b s_c g^2
+// d2T_a/du_b du_c, all times G m / L^2 (s the signs of d, g node spacings per
+// length).
+template <bool OVR>
 __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const float4 *__restrict__ tay,
-                                                 float4 e, CorrSum &c)
+                                                 float4 e, CorrSum &c, const float *ovr)
 {
 	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
 	const float u = fabsf(e.x) * p.tay_grid, v = fabsf(e.y) * p.tay_grid, w = fabsf(e.z) * p.tay_grid;
@@ -814,8 +742,9 @@ __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const flo
 		const float bx = fmaf(fmaf(t3, dxx, r1.x), du, fmaf(fmaf(t3, dxy, r1.w), dv, fmaf(t3, dxz, r2.x) * dw));
 		const float by = fmaf(fmaf(t3, dxy, r1.w), du, fmaf(fmaf(t3, dyy, r1.y), dv, fmaf(t3, dyz, r2.y) * dw));
 		const float bz = fmaf(fmaf(t3, dxz, r2.x), du, fmaf(fmaf(t3, dyz, r2.y), dv, fmaf(t3, dzz, r1.z) * dw));
-		const float val = r0.x + fmaf(fmaf(0.5f, bx, r0.y), du, fmaf(fmaf(0.5f, by, r0.z), dv,
-		                               fmaf(0.5f, bz, r0.w) * dw));
+		const float val = OVR ? ovr[q]
+		                      : r0.x + fmaf(fmaf(0.5f, bx, r0.y), du, fmaf(fmaf(0.5f, by, r0.z), dv,
+		                                                                    fmaf(0.5f, bz, r0.w) * dw));
 		const float sq = sg[q];
 		c.k[q] = fmaf(m0 * sq, val, c.k[q]);
 		c.j[3 * q + 0] = fmaf(m1 * sq * sg[0], gx, c.j[3 * q + 0]);
@@ -830,24 +759,13 @@ __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const flo
 	}
 }
 
-// K(d) alone (tricubic value), for per-target evaluation, added to a
-template <bool MLP>
-__device__ __forceinline__ void ewald_k(const GroupParams &p, const float4 *__restrict__ tab,
-                                        const float *mlp, float ex, float ey, float ez, float gm,
-                                        float &ax, float &ay, float &az)
+// K(d) alone (tricubic value of the extended table), for per-target
+// evaluation, added to a
+__device__ __forceinline__ void ewald_k(const GroupParams &p, const float4 *__restrict__ tab, float ex,
+                                        float ey, float ez, float gm, float &ax, float &ay, float &az)
 {
 	const float sx = ex < 0.f ? -1.f : 1.f, sy = ey < 0.f ? -1.f : 1.f, sz = ez < 0.f ? -1.f : 1.f;
 	const float u = fabsf(ex) * p.grid, v = fabsf(ey) * p.grid, w = fabsf(ez) * p.grid;
-	if (MLP) {
-		const float xs[3] = { u * (1.f / 128.f), v * (1.f / 128.f), w * (1.f / 128.f) };
-		float t[3];
-		mlp_forward(mlp, xs, t);
-		const float m0 = -gm * p.inv_box * p.inv_box;
-		ax = fmaf(m0 * sx, t[0], ax);
-		ay = fmaf(m0 * sy, t[1], ay);
-		az = fmaf(m0 * sz, t[2], az);
-		return;
-	}
 	const int i = min((int) u, 64), j = min((int) v, 64), l = min((int) w, 64);
 	float wx[4], wy[4], wz[4], d_[4], dd_[4];
 	lagrange4(u - (float) i, wx, d_, dd_);
@@ -919,21 +837,40 @@ __device__ __forceinline__ void uniform_remainder(const GroupParams &p, double t
 	out[2] = -p.uniform * (cube_field(z1, z2, x1, x2, y1, y2) + lin * z);
 }
 
-// Evaluates list entries [from, from + cnt), cnt <= 32: about the group
-// centre one entry per lane (K, J, H), or, for a group that takes per-target
-// images, every entry for every target of the lane (K at the target's
-// nearest image; FP32 per batch, carried in FP64).
+// the learned correction for per-target images (groups wider than L/20,
+// rare): out of line, so that its registers do not add to the walk's
+__device__ __noinline__ void mlp_forward_warp_call(const float *mlp, const uint32_t *w2b, const float x[3],
+                                                   float out[3])
+{
+	mlp_forward_warp(mlp, w2b, x, out);
+}
+
+// Evaluates list entries [from, from + cnt), 1 <= cnt <= 32 (every lane of
+// the warp calls): about the group centre one entry per lane (K, J, H), or,
+// for a group that takes per-target images, every entry for every target of
+// the lane (K at the target's nearest image; FP32 per batch, carried in
+// FP64). With the learned correction the value of K comes from the warp's
+// tensor-core evaluation of the network (one point per lane).
 template <int TPL, bool MLP>
 __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab, const float4 *tay,
-                                            const float *mlp, const float4 *list, int from, int cnt,
-                                            bool per_target,
-                                            CorrSum &c, Target (&t)[TPL], float &nev)
+                                            const float *mlp, const uint32_t *w2b, const float4 *list,
+                                            int from, int cnt, bool per_target, CorrSum &c,
+                                            Target (&t)[TPL], float &nev)
 {
 	const int lane = threadIdx.x & 31;
 	if (!per_target) {
-		if (lane < cnt) {
-			if (MLP) ewald_kjh<MLP>(p, tab, mlp, list[from + lane], c);
-			else ewald_kjh_taylor(p, tay, list[from + lane], c);
+		if (MLP) {
+			// lanes past cnt repeat the last entry and drop the result
+			const float4 e = list[from + min(lane, cnt - 1)];
+			const float xs[3] = { fabsf(e.x) * p.inv_box, fabsf(e.y) * p.inv_box, fabsf(e.z) * p.inv_box };
+			float tv[3];
+			mlp_forward_warp(mlp, w2b, xs, tv);
+			if (lane < cnt) {
+				ewald_kjh_taylor<true>(p, tay, e, c, tv);
+				nev += 1.f;
+			}
+		} else if (lane < cnt) {
+			ewald_kjh_taylor<false>(p, tay, list[from + lane], c, nullptr);
 			nev += 1.f;
 		}
 	} else {
@@ -947,7 +884,17 @@ __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *
 				const float dx = wrap_half(s.x - t[k].tx, p.box, p.half_box);
 				const float dy = wrap_half(s.y - t[k].ty, p.box, p.half_box);
 				const float dz = wrap_half(s.z - t[k].tz, p.box, p.half_box);
-				ewald_k<MLP>(p, tab, mlp, dx, dy, dz, s.w, ax[k], ay[k], az[k]);
+				if (MLP) {
+					const float xs[3] = { fabsf(dx) * p.inv_box, fabsf(dy) * p.inv_box, fabsf(dz) * p.inv_box };
+					float tv[3];
+					mlp_forward_warp_call(mlp, w2b, xs, tv);
+					const float m0 = -s.w * p.inv_box * p.inv_box;
+					ax[k] = fmaf(dx < 0.f ? -m0 : m0, tv[0], ax[k]);
+					ay[k] = fmaf(dy < 0.f ? -m0 : m0, tv[1], ay[k]);
+					az[k] = fmaf(dz < 0.f ? -m0 : m0, tv[2], az[k]);
+				} else {
+					ewald_k(p, tab, dx, dy, dz, s.w, ax[k], ay[k], az[k]);
+				}
 				if (t[k].valid) nev += 1.f;
 			}
 		}
@@ -958,7 +905,6 @@ __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *
 			t[k].az += (double) az[k];
 		}
 	}
-	__syncwarp();
 }
 
 template <int TPL, bool MLP>
@@ -966,7 +912,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
                             const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
                             const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
                             const float *__restrict__ last_acc, const float4 *__restrict__ tab,
-                            const float4 *__restrict__ tay, const float *mlp,
+                            const float4 *__restrict__ tay, const float *mlp, const uint32_t *w2b,
                             int64_t first, int cnt, const int32_t *__restrict__ active,
                             Target (&t)[TPL], float &nev, int *status)
 {
@@ -1043,7 +989,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		nl += __popc(bm);
 		__syncwarp();
 		if (nl >= 32) {
-			ewald_batch<TPL, MLP>(p, tab, tay, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
+			ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
 			nl -= 32;
 		}
 		push_children(S.stack, sp, open_int, nchild, child);
@@ -1067,7 +1013,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 				nl += __popc(mb);
 				__syncwarp();
 				if (nl >= 32) {
-					ewald_batch<TPL, MLP>(p, tab, tay, mlp, S.list, nl - 32, 32, per_target, c, t, nev);
+					ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
 					nl -= 32;
 				}
 			}
@@ -1075,7 +1021,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		__syncwarp();
 	}
 	__syncwarp();
-	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, tay, mlp, S.list, 0, nl, per_target, c, t, nev);
+	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, 0, nl, per_target, c, t, nev);
 	if (per_target) return;
 	// sum over lanes (FP64), then K(d_c - t) ~ K - J t + H:tt / 2 per target
 	double K[3], J[9], H[18];
@@ -1130,10 +1076,11 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EwaldSmem &S = ((EwaldSmem *) smem_raw)[threadIdx.x >> 5];
 	// the learned correction's parameters, once per block: the network BF16 ->
-	// FP32, the fitted cubic and scale FP32
+	// FP32, the fitted cubic and scale FP32, and W2 as BF16 pairs for the MMAs
 	float *mlp = (float *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS);
+	uint32_t *w2b = (uint32_t *) (mlp + MLP_NPARAM);
 	if (MLP) {
-		for (int e = threadIdx.x; e < MLP_NPARAM; e += GW_THREADS) mlp[e] = mlp_param(mlp_w, mlp_f32, e);
+		mlp_load_shared(mlp_w, mlp_f32, mlp, w2b);
 		__syncthreads();
 	}
 	const int lane = threadIdx.x & 31;
@@ -1154,7 +1101,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 		}
 		Target t[TPL];
 		float nev = 0.f;
-		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, tay, mlp, first, cnt, active, t, nev,
+		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, tay, mlp, w2b, first, cnt, active, t, nev,
 		                 status);
 		ev_acc += nev;
 #pragma unroll
@@ -1293,7 +1240,7 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
                         double *counter)
 {
 	static int nblk = 0;
-	const size_t smem = sizeof(EwaldSmem) * GW_WARPS + (MLP ? 4 * MLP_NPARAM : 0);
+	const size_t smem = sizeof(EwaldSmem) * GW_WARPS + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : 0);
 	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
 	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
