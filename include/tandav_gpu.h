@@ -369,6 +369,17 @@ int tvg_rung_histogram(tvg_context *ctx, int32_t *hist);
  * the relative-criterion walk. Without a timeline every particle is active. */
 int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts, int32_t ewald_kind,
                              int32_t prepare);
+/* tvg_compute_acceleration of the group form (prepare = 0) with the step's
+ * whole launch sequence as one CUDA graph (no host round trip inside: the
+ * counts of the step stay on the device). The first call with a given
+ * configuration (parts, ewald_kind, group size, timeline, particle count)
+ * runs the step directly; later calls capture it once for each of the two
+ * buffer states the sort alternates between, then launch the captured graph.
+ * The timeline's active-bin limit is passed to the device before each launch.
+ * Results, phase times and counters as tvg_compute_acceleration. */
+int tvg_step_graph(tvg_context *ctx, uint32_t parts, int32_t ewald_kind);
+/* Releases the captured step graphs (tvg_finalize does too). */
+int tvg_step_graph_reset(tvg_context *ctx);
 
 /* Autotuner of the group form (no reference counterpart): on the current tree
  * and active set, times the gravity + Ewald walks with 32-, 64- and

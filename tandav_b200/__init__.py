@@ -27,7 +27,8 @@ EXPORTS = (
     "tvg_set_ewald_opening", "tvg_timeline_init", "tvg_download_kick_drift_table",
     "tvg_kick_drift_factors", "tvg_set_new_timesteps", "tvg_kick_first_halfstep",
     "tvg_kick_second_halfstep", "tvg_drift_to_sync_point", "tvg_timeline_get", "tvg_timeline_set",
-    "tvg_rung_histogram", "tvg_compute_acceleration", "tvg_ewald_mlp_train",
+    "tvg_rung_histogram", "tvg_compute_acceleration", "tvg_step_graph", "tvg_step_graph_reset",
+    "tvg_ewald_mlp_train",
     "tvg_ewald_mlp_weights", "tvg_ewald_mlp_grad", "tvg_ewald_mlp_eval", "tvg_ewald_mlp_judge",
     "tvg_autotune",
 )

@@ -129,6 +129,34 @@ extern "C" int tvg_init(int device, const tvg_config *cfg, tvg_context **out)
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->group_first, 4 * (cap / 8 + 1024)));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->work_counter, 64));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->counters, 8 * 8));
+	TVG_CHECK(dalloc(ctx, (void **) &ctx->dc, sizeof(tvg_devcount)));
+	TVG_CHECK(dalloc(ctx, (void **) &ctx->d_topinfo, sizeof(TopInfo)));
+	TVG_CHECK(dalloc(ctx, (void **) &ctx->d_topplace, sizeof(TopPlace)));
+	TVG_CUDA(ctx, cudaMemset(ctx->dc, 0, sizeof(tvg_devcount)));
+	return TVG_OK;
+}
+
+// the device counts of the last step into the host mirrors
+int tvg_read_counts(tvg_context *ctx)
+{
+	tvg_devcount h;
+	TopPlace tp;
+	cudaStream_t s = ctx->stream;
+	TVG_CUDA(ctx, cudaMemcpyAsync(&h, ctx->dc, sizeof(h), cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaMemcpyAsync(&tp, ctx->d_topplace, sizeof(tp), cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	ctx->ntop = h.ntop;
+	ctx->nu = h.nu;
+	ctx->nnodes = h.nnodes;
+	if (ctx->ntop > 0)
+		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
+		                              cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	for (int t = 0; t < TVG_MAX_TOP; t++) {
+		const bool ok = t < ctx->ntop;
+		ctx->h_target[t] = ok ? tp.target[t] : 0;
+		ctx->h_nsurv[t] = ok ? tp.nsurv[t] : 0;
+	}
 	return TVG_OK;
 }
 
@@ -137,6 +165,7 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	if (!ctx) return;
 	cudaSetDevice(ctx->device);
 	if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+	tvg_graph_release(ctx);
 	for (int s = 0; s < FS_NFIELDS; s++) { cudaFree(ctx->f[s]); cudaFree(ctx->falt[s]); }
 	void *bufs[] = { ctx->key_hi, ctx->key_lo, ctx->key_tmp, ctx->perm, ctx->perm_tmp,
 	                 ctx->sort_hist, ctx->sort_off, ctx->digit_count, ctx->scan_tmp, ctx->status,
@@ -148,7 +177,8 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->ewald_f[2], ctx->ewald_f[3], ctx->ewald_raw, ctx->ewald32,
 	                 ctx->ewald_ext, ctx->active, ctx->kd_x, ctx->kd_kick, ctx->kd_drift,
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
-	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor };
+	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
+	                 ctx->d_topinfo, ctx->d_topplace };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -490,8 +520,12 @@ extern "C" int tvg_set_active(tvg_context *ctx, const int32_t *list, int64_t n_a
 	}
 	if (n_active < 0 || n_active > ctx->n) return tvg_fail(ctx, TVG_E_BADINPUT, "n_active out of range");
 	if (!ctx->active) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->active, 4 * (size_t) ctx->cap));
+	if (!ctx->act_flag) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_flag, 4 * (size_t) ctx->cap));
+	if (!ctx->act_off) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_off, 4 * (size_t) ctx->cap));
 	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->active, list, 4 * (size_t) n_active, cudaMemcpyHostToDevice,
 	                              ctx->stream));
+	// the walks read the list's length on the device
+	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->dc->n_active, &n_active, 8, cudaMemcpyHostToDevice, ctx->stream));
 	TVG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
 	ctx->use_active = true;
 	ctx->n_active = n_active;

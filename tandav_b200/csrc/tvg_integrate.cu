@@ -320,11 +320,22 @@ __global__ void k_veldisp(int64_t n, const int32_t *__restrict__ type, const F *
 }
 
 // Make_Active_Particle_List (timestep.c:280-299): flags, scan, scatter
-__global__ void k_active_flags(int64_t n, const int32_t *__restrict__ bin, int max_active_bin,
-                               int32_t *flag)
+// the bin limit from the device counts (set before the step, so that a
+// captured step reads the current one)
+__global__ void k_active_flags(int64_t n, const int32_t *__restrict__ bin,
+                               const tvg_devcount *__restrict__ dc, int32_t *flag)
 {
 	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (i < n) flag[i] = bin[i] <= max_active_bin;
+	if (i < n) flag[i] = bin[i] <= dc->max_active_bin;
+}
+
+__global__ void k_set_max_bin(tvg_devcount *dc, int32_t b) { dc->max_active_bin = b; }
+
+int tvg_set_device_max_bin(tvg_context *ctx)
+{
+	k_set_max_bin<<<TVG_CNT(ctx, 1), 1, 0, ctx->stream>>>(ctx->dc, ctx->tl.state.max_active_bin);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
 }
 
 __global__ void k_active_scatter(int64_t n, const int32_t *__restrict__ flag,
@@ -479,15 +490,20 @@ int tvg_impl_active_from_bins(tvg_context *ctx)
 	TVG_CHECK(ensure(ctx, (void **) &ctx->act_flag, 4 * (size_t) ctx->cap));
 	TVG_CHECK(ensure(ctx, (void **) &ctx->act_off, 4 * (size_t) ctx->cap));
 	int32_t *flag = ctx->act_flag, *off = ctx->act_off;
+	// a captured step is given the limit before its launch (tvg_step_graph)
+	if (!ctx->capturing) TVG_CHECK(tvg_set_device_max_bin(ctx));
 	k_active_flags<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(
-	    n, (const int32_t *) ctx->f[FS_TIME_BIN], ctx->tl.state.max_active_bin, flag);
+	    n, (const int32_t *) ctx->f[FS_TIME_BIN], ctx->dc, flag);
 	TVG_CUDA(ctx, cudaGetLastError());
-	int64_t total = 0;
-	TVG_CHECK(tvg_device_scan_i32(ctx, flag, off, n, &total));
+	TVG_CHECK(tvg_device_scan_i32_dev(ctx, flag, off, n, &ctx->dc->n_active));
 	k_active_scatter<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, flag, off, ctx->active);
 	TVG_CUDA(ctx, cudaGetLastError());
-	ctx->n_active = total;
 	ctx->use_active = true;
+	if (ctx->capturing) return TVG_OK;
+	int64_t total = 0;
+	TVG_CUDA(ctx, cudaMemcpyAsync(&total, &ctx->dc->n_active, 8, cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	ctx->n_active = total;
 	ctx->tl.state.n_active = total;
 	if (total == 0)
 		return tvg_fail(ctx, TVG_E_STATE, "no active particles (max active bin %d)",

@@ -66,6 +66,39 @@ struct __align__(16) tvg_wnode {
 	int32_t level;
 };
 
+// Counts of the current step kept on the device: the kernels of a step read
+// them, so a step needs no host round trip between its phases and can be
+// captured as one CUDA graph (tvg_step_graph). The host reads them back once,
+// after the step.
+struct tvg_devcount {
+	int64_t nu;              // uncollapsed nodes of the build
+	int64_t nnodes;          // tree nodes, terminators included
+	int64_t n_active;        // active particles
+	int64_t ngroups;         // groups of the group walk
+	double mass_total;       // sum of the masses (Ewald uniform remainder)
+	int32_t ntop;            // top nodes
+	int32_t max_active_bin;  // bins <= this are active
+	int32_t sort_skip[8];    // radix digit d is the same for all keys
+};
+
+// level-2 cells and their top nodes (tree build), on the device
+struct TopInfo {            // per level-2 cell c (0..63)
+	int32_t first[64];      // first particle, -1 if empty
+	int32_t count[64];
+	int32_t tidx[64];       // index in the top node list (descending key order)
+	int32_t big[64];        // count > VECTOR_SIZE: has a subtree
+};
+
+struct TopPlace {
+	int32_t tidx[64];       // by level-2 cell
+	int32_t toff[64];       // by top index: G = toff + F[u]
+	int32_t target[64];
+	int32_t nsurv[64];
+	int32_t end[64];        // by top index: first particle after the node
+};
+
+struct tvg_graph_entry;
+
 struct tvg_context {
 	int device = 0;
 	tvg_config cfg{};
@@ -167,6 +200,17 @@ struct tvg_context {
 	void *tl_scratch = nullptr;        // reductions (256 B)
 	int32_t *act_flag = nullptr, *act_off = nullptr;
 
+	// device-resident counts and top-node tables of the step
+	tvg_devcount *dc = nullptr;
+	TopInfo *d_topinfo = nullptr;
+	TopPlace *d_topplace = nullptr;
+	// stream capture in progress: the step's functions skip every host read
+	// and synchronisation
+	bool capturing = false;
+	// CUDA graphs of the step (tvg_step.cu): one per buffer parity
+	tvg_graph_entry *graphs[2] = { nullptr, nullptr };
+	uint64_t graph_warm_key = 0;
+
 	// timings
 	cudaEvent_t ev[16];
 	double phase_ms[8] = { 0 };
@@ -185,6 +229,17 @@ int tvg_fail(tvg_context *ctx, int code, const char *fmt, ...);
 int tvg_sync_status(tvg_context *ctx, const char *phase);
 int tvg_device_scan_i32(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n,
                         int64_t *total);
+// as tvg_device_scan_i32, the total written to device memory (no host read)
+int tvg_device_scan_i32_dev(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n,
+                            int64_t *total_dev);
+// reads the device counts back into the host mirrors (top nodes, node
+// counts); synchronises the stream
+int tvg_read_counts(tvg_context *ctx);
+// times and interaction counts of the last group walk (synchronises)
+int tvg_walk_group_results(tvg_context *ctx);
+// the active-bin limit of the timeline into the device counts
+int tvg_set_device_max_bin(tvg_context *ctx);
+void tvg_graph_release(tvg_context *ctx);
 
 // phase implementations (one translation unit each)
 int tvg_impl_keys(tvg_context *ctx, bool reversed);
@@ -206,6 +261,15 @@ int tvg_impl_zero_accel(tvg_context *ctx);
 int tvg_impl_active_from_bins(tvg_context *ctx);
 
 static inline size_t tvg_fsize(const tvg_context *ctx) { return (size_t) ctx->cfg.float_bytes; }
+
+// records a timing event on the context stream; while a capture is in
+// progress as an event-record node of the graph (a plain record would only
+// mark a dependency inside the capture)
+static inline cudaError_t tvg_record(tvg_context *ctx, cudaEvent_t e)
+{
+	return ctx->capturing ? cudaEventRecordWithFlags(e, ctx->stream, cudaEventRecordExternal)
+	                      : cudaEventRecord(e, ctx->stream);
+}
 
 // element size of field slot
 static inline size_t tvg_field_bytes(const tvg_context *ctx, int slot)

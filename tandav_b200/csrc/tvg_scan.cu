@@ -54,7 +54,7 @@ __global__ void k_scan_reduce(const int32_t *__restrict__ in, int64_t n, int32_t
 }
 
 __global__ void k_scan_apply(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n,
-                             const int32_t *__restrict__ offs)
+                             const int32_t *__restrict__ offs, int64_t *total_out)
 {
 	__shared__ int32_t s_warp[33];
 	const int64_t base = (int64_t) blockIdx.x * SCAN_TILE + (int64_t) threadIdx.x * SCAN_IPT;
@@ -75,15 +75,17 @@ __global__ void k_scan_apply(const int32_t *__restrict__ in, int32_t *__restrict
 		if (i < n) out[i] = run;
 		run += v[k];
 	}
+	// the thread holding the last element: the inclusive sum of everything
+	if (total_out && base <= n - 1 && n - 1 < base + SCAN_IPT) *total_out = run;
 }
 
 // Recursive exclusive scan; `tmp` must hold the block sums of every level.
 static int scan_rec(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n, int32_t *tmp,
-                    size_t tmp_elems)
+                    size_t tmp_elems, int64_t *total_dev)
 {
 	const int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
 	if (nb <= 1) {
-		k_scan_apply<<<TVG_CNT(ctx, 1), SCAN_THREADS, 0, ctx->stream>>>(in, out, n, nullptr);
+		k_scan_apply<<<TVG_CNT(ctx, 1), SCAN_THREADS, 0, ctx->stream>>>(in, out, n, nullptr, total_dev);
 		TVG_CUDA(ctx, cudaGetLastError());
 		return TVG_OK;
 	}
@@ -92,8 +94,8 @@ static int scan_rec(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n
 	int32_t *sums = tmp, *offs = tmp + nb;
 	k_scan_reduce<<<TVG_CNT(ctx, (unsigned) nb), SCAN_THREADS, 0, ctx->stream>>>(in, n, sums);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CHECK(scan_rec(ctx, sums, offs, nb, tmp + 2 * nb, tmp_elems - 2 * nb));
-	k_scan_apply<<<TVG_CNT(ctx, (unsigned) nb), SCAN_THREADS, 0, ctx->stream>>>(in, out, n, offs);
+	TVG_CHECK(scan_rec(ctx, sums, offs, nb, tmp + 2 * nb, tmp_elems - 2 * nb, nullptr));
+	k_scan_apply<<<TVG_CNT(ctx, (unsigned) nb), SCAN_THREADS, 0, ctx->stream>>>(in, out, n, offs, total_dev);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }
@@ -110,7 +112,7 @@ int tvg_device_scan_i32(tvg_context *ctx, const int32_t *in, int32_t *out, int64
 	int32_t last_in = 0;
 	if (total)
 		TVG_CUDA(ctx, cudaMemcpyAsync(&last_in, in + n - 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
-	TVG_CHECK(scan_rec(ctx, in, out, n, (int32_t *) ctx->scan_tmp, ctx->scan_tmp_bytes / 4));
+	TVG_CHECK(scan_rec(ctx, in, out, n, (int32_t *) ctx->scan_tmp, ctx->scan_tmp_bytes / 4, nullptr));
 	if (total) {
 		int32_t last_out = 0;
 		TVG_CUDA(ctx, cudaMemcpyAsync(&last_out, out + n - 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -118,4 +120,15 @@ int tvg_device_scan_i32(tvg_context *ctx, const int32_t *in, int32_t *out, int64
 		*total = (int64_t) last_out + last_in;
 	}
 	return TVG_OK;
+}
+
+// the total stays on the device (int64 at total_dev); no synchronisation
+int tvg_device_scan_i32_dev(tvg_context *ctx, const int32_t *in, int32_t *out, int64_t n,
+                            int64_t *total_dev)
+{
+	if (n <= 0) {
+		TVG_CUDA(ctx, cudaMemsetAsync(total_dev, 0, 8, ctx->stream));
+		return TVG_OK;
+	}
+	return scan_rec(ctx, in, out, n, (int32_t *) ctx->scan_tmp, ctx->scan_tmp_bytes / 4, total_dev);
 }

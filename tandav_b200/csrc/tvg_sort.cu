@@ -3,7 +3,10 @@
 // Replaces Qsort_Index on the 128-bit keys (sort.c:90-341, cmp_peanoKeys at
 // peano.c:6-12) and reorder_collisionless_particles (peano.c:50-82).
 //  1. LSD radix sort of (key_hi, index) on the 64-bit high key word: 8-bit
-//     digits, digits that are equal for every key are skipped. Each pass is
+//     digits; a digit that is equal for every key (decided on the device) is
+//     not ranked: its pass copies the keys through, so the number of passes,
+//     and with it the buffer a step ends in, never depends on the data. Each
+//     pass is
 //     reduce-then-scan: per-tile (4096 keys) digit histograms, one device
 //     scan of the digit-major histogram, then a scatter in which every tile
 //     ranks its keys stably with warp __match_any_sync and writes them through
@@ -47,10 +50,27 @@ __global__ void k_digit_counts(int64_t n, const uint64_t *__restrict__ key, uint
 		if (h[i]) atomicAdd(&count[i], h[i]);
 }
 
-// per-tile digit histogram, stored digit-major: hist[d * ntiles + tile]
-__global__ void k_tile_hist(int64_t n, int shift, const uint64_t *__restrict__ key,
-                            uint32_t *__restrict__ hist, int64_t ntiles)
+// skip[d] = 1 when digit d has the same value in all n keys
+__global__ void k_digit_skip(int64_t n, const uint32_t *__restrict__ count, int32_t *skip)
 {
+	const int d = threadIdx.x;
+	if (d >= 8) return;
+	int sk = 0;
+	for (int b = 0; b < 256; b++)
+		if (count[d * 256 + b] == (uint32_t) n) sk = 1;
+	skip[d] = sk;
+}
+
+// per-tile digit histogram, stored digit-major: hist[d * ntiles + tile]
+// (zeros for a digit that skip marks)
+__global__ void k_tile_hist(int64_t n, int shift, const uint64_t *__restrict__ key,
+                            uint32_t *__restrict__ hist, int64_t ntiles,
+                            const int32_t *__restrict__ skip = nullptr)
+{
+	if (skip && skip[shift >> 3]) {
+		hist[(int64_t) threadIdx.x * ntiles + blockIdx.x] = 0;
+		return;
+	}
 	__shared__ uint32_t h[256];
 	h[threadIdx.x] = 0;
 	__syncthreads();
@@ -72,8 +92,18 @@ __global__ void k_tile_hist(int64_t n, int shift, const uint64_t *__restrict__ k
 __global__ void __launch_bounds__(RS_THREADS)
 k_radix_scatter(int64_t n, int shift, const uint64_t *__restrict__ kin,
                 const uint32_t *__restrict__ vin, uint64_t *__restrict__ kout,
-                uint32_t *__restrict__ vout, const uint32_t *__restrict__ off, int64_t ntiles)
+                uint32_t *__restrict__ vout, const uint32_t *__restrict__ off, int64_t ntiles,
+                const int32_t *__restrict__ skip = nullptr)
 {
+	if (skip && skip[shift >> 3]) {     // constant digit: the order stays
+		const int64_t b0 = (int64_t) blockIdx.x * RS_TILE;
+		const int c0 = (int) min((int64_t) RS_TILE, n - b0);
+		for (int p = threadIdx.x; p < c0; p += RS_THREADS) {
+			kout[b0 + p] = kin[b0 + p];
+			vout[b0 + p] = vin[b0 + p];
+		}
+		return;
+	}
 	extern __shared__ __align__(16) unsigned char smem[];
 	uint64_t *skey = (uint64_t *) smem;                          // RS_TILE
 	uint32_t *sval = (uint32_t *) (skey + RS_TILE);              // RS_TILE
@@ -230,10 +260,9 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 	k_iota<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->perm);
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->digit_count, 0, 4 * 8 * 256, s));
 	k_digit_counts<<<TVG_CNT(ctx, 296), 512, 0, s>>>(n, ctx->key_hi, ctx->digit_count);
+	int32_t *skip = ctx->dc->sort_skip;
+	k_digit_skip<<<TVG_CNT(ctx, 1), 32, 0, s>>>(n, ctx->digit_count, skip);
 	TVG_CUDA(ctx, cudaGetLastError());
-	uint32_t h_count[8 * 256];
-	TVG_CUDA(ctx, cudaMemcpyAsync(h_count, ctx->digit_count, sizeof(h_count), cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaStreamSynchronize(s));
 	static bool attr_set = false;
 	const size_t smem = RS_TILE * 12 + (RS_WARPS * 256 + 3 * 256 + 33) * 4;
 	if (!attr_set) {
@@ -244,17 +273,14 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 	uint64_t *kin = ctx->key_hi, *kout = ctx->key_tmp;
 	uint32_t *vin = ctx->perm, *vout = ctx->perm_tmp;
 	for (int d = 0; d < 8; d++) {
-		bool constant = false;
-		for (int b = 0; b < 256; b++)
-			if (h_count[d * 256 + b] == (uint32_t) n) constant = true;
-		if (constant) continue;
 		const int shift = 8 * d;
-		k_tile_hist<<<TVG_CNT(ctx, (unsigned) ntiles), RS_THREADS, 0, s>>>(n, shift, kin, ctx->sort_hist, ntiles);
+		k_tile_hist<<<TVG_CNT(ctx, (unsigned) ntiles), RS_THREADS, 0, s>>>(n, shift, kin, ctx->sort_hist, ntiles,
+		                                                                   skip);
 		TVG_CUDA(ctx, cudaGetLastError());
 		TVG_CHECK(tvg_device_scan_i32(ctx, (const int32_t *) ctx->sort_hist, (int32_t *) ctx->sort_off,
 		                              256 * ntiles, nullptr));
 		k_radix_scatter<<<TVG_CNT(ctx, (unsigned) ntiles), RS_THREADS, smem, s>>>(n, shift, kin, vin, kout, vout,
-		                                                            ctx->sort_off, ntiles);
+		                                                            ctx->sort_off, ntiles, skip);
 		TVG_CUDA(ctx, cudaGetLastError());
 		uint64_t *kt = kin; kin = kout; kout = kt;
 		uint32_t *vt = vin; vin = vout; vout = vt;

@@ -1,5 +1,6 @@
 // tvg_step.cu -- one tree-force evaluation on device-resident particles, with
-// per-phase CUDA-event timing on the context stream.
+// per-phase CUDA-event timing on the context stream; and the same evaluation
+// captured as a CUDA graph (tvg_step_graph).
 #include "tvg_internal.cuh"
 
 extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
@@ -51,22 +52,18 @@ extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, ui
 	return tvg_sync_status(ctx, "force_step");
 }
 
-// Compute_Acceleration (accel.c:15-71) after the single-rank domain
-// decomposition: keys, sort, active list, top nodes, build, walks.
-extern "C" int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts,
-                                        int32_t ewald_kind, int32_t prepare)
+// The launches of Compute_Acceleration (accel.c:15-71) after the single-rank
+// domain decomposition: keys, sort, active list, top nodes, build, walks,
+// bracketed by the phase events ev[8..13]. No host synchronisation while a
+// capture is in progress.
+static int accel_phases(tvg_context *ctx, int32_t form, uint32_t parts, int32_t ewald_kind,
+                        int32_t prepare)
 {
-	if (!ctx) return TVG_E_BADINPUT;
-	if (!ctx->have_domain) return tvg_fail(ctx, TVG_E_STATE, "compute_acceleration: domain not set");
-	if (form != TVG_FORM_PLAIN && form != TVG_FORM_GROUP)
-		return tvg_fail(ctx, TVG_E_BADINPUT, "unknown form %d", form);
-	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
-	cudaStream_t s = ctx->stream;
 	cudaEvent_t *ev = ctx->ev;
-	TVG_CUDA(ctx, cudaEventRecord(ev[8], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ev[8]));
 	TVG_CHECK(tvg_impl_keys(ctx, false));
 	ctx->keys_std = true;
-	TVG_CUDA(ctx, cudaEventRecord(ev[9], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ev[9]));
 	TVG_CHECK(tvg_impl_sort(ctx, nullptr));
 	ctx->sorted = true;
 	// Sort_Particles_By_Peano_Key ends with Make_Active_Particle_List (peano.c:42)
@@ -75,18 +72,14 @@ extern "C" int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t
 	} else {
 		ctx->use_active = false;
 	}
-	TVG_CUDA(ctx, cudaEventRecord(ev[10], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ev[10]));
 	TVG_CHECK(tvg_impl_top_nodes(ctx));
 	ctx->have_top = true;
-	TVG_CUDA(ctx, cudaEventRecord(ev[11], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ev[11]));
 	TVG_CHECK(tvg_impl_tree_build(ctx, form == TVG_FORM_PLAIN ? TVG_BUILD_EXACT_MOMENTS : 0));
 	ctx->have_tree = true;
 	ctx->have_walktree = false;
-	TVG_CUDA(ctx, cudaEventRecord(ev[12], s));
-	if ((parts & TVG_WALK_EWALD) && !ctx->have_ewald) {
-		TVG_CHECK(tvg_impl_ewald_init(ctx));
-		ctx->have_ewald = true;
-	}
+	TVG_CUDA(ctx, tvg_record(ctx, ev[12]));
 	// safe_last_accel, accel.c:28-43 (the active particles)
 	TVG_CHECK(tvg_impl_save_last_accel(ctx));
 	if (prepare) {
@@ -99,7 +92,14 @@ extern "C" int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t
 	if (form == TVG_FORM_PLAIN) TVG_CHECK(tvg_impl_walk_plain(ctx, 0, parts));
 	else TVG_CHECK(tvg_impl_walk_group(ctx, 0, parts, ewald_kind));
 	if (ctx->have_timeline) ctx->tl.state.prepare_step = 0;
-	TVG_CUDA(ctx, cudaEventRecord(ev[13], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ev[13]));
+	return TVG_OK;
+}
+
+// phase times from the events of the last step (synchronises)
+static int accel_times(tvg_context *ctx)
+{
+	cudaEvent_t *ev = ctx->ev;
 	TVG_CUDA(ctx, cudaEventSynchronize(ev[13]));
 	float ms[5];
 	TVG_CUDA(ctx, cudaEventElapsedTime(&ms[0], ev[8], ev[9]));
@@ -109,5 +109,208 @@ extern "C" int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t
 	TVG_CUDA(ctx, cudaEventElapsedTime(&ms[4], ev[8], ev[13]));
 	for (int i = 0; i < 4; i++) ctx->phase_ms[i] = ms[i];
 	ctx->phase_ms[6] = ms[4];
+	return TVG_OK;
+}
+
+static int accel_check(tvg_context *ctx, int32_t form)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!ctx->have_domain) return tvg_fail(ctx, TVG_E_STATE, "compute_acceleration: domain not set");
+	if (form != TVG_FORM_PLAIN && form != TVG_FORM_GROUP)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "unknown form %d", form);
+	return TVG_OK;
+}
+
+extern "C" int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts,
+                                        int32_t ewald_kind, int32_t prepare)
+{
+	TVG_CHECK(accel_check(ctx, form));
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	if ((parts & TVG_WALK_EWALD) && !ctx->have_ewald) {
+		TVG_CHECK(tvg_impl_ewald_init(ctx));
+		ctx->have_ewald = true;
+	}
+	TVG_CHECK(accel_phases(ctx, form, parts, ewald_kind, prepare));
+	TVG_CHECK(accel_times(ctx));
 	return tvg_sync_status(ctx, "compute_acceleration");
+}
+
+// ------------------------------------------------------------- CUDA graph
+//
+// The step's launch sequence has no host round trip (every count stays on the
+// device), so it is captured once and replayed. Captured kernels keep the
+// buffer pointers they were given; the sort leaves the particle fields and
+// the low key words in the other buffer of their pair (and the radix passes,
+// always eight, leave the high words and the permutation where they were), so
+// the buffers alternate between two states from step to step. One graph is
+// kept per state, with the pointer set it starts from and the one it leaves.
+
+enum { GP_KEY_HI, GP_KEY_LO, GP_KEY_TMP, GP_PERM, GP_PERM_TMP, GP_FIELDS };
+#define GP_N (GP_FIELDS + 2 * FS_NFIELDS)
+
+struct tvg_graph_entry {
+	cudaGraphExec_t exec = nullptr;
+	uint64_t key = 0;
+	void *start[GP_N];
+	void *end[GP_N];
+	int64_t launches = 0;
+};
+
+static void snap_ptrs(const tvg_context *ctx, void **p)
+{
+	p[GP_KEY_HI] = ctx->key_hi;
+	p[GP_KEY_LO] = ctx->key_lo;
+	p[GP_KEY_TMP] = ctx->key_tmp;
+	p[GP_PERM] = ctx->perm;
+	p[GP_PERM_TMP] = ctx->perm_tmp;
+	for (int f = 0; f < FS_NFIELDS; f++) {
+		p[GP_FIELDS + f] = ctx->f[f];
+		p[GP_FIELDS + FS_NFIELDS + f] = ctx->falt[f];
+	}
+}
+
+static void set_ptrs(tvg_context *ctx, void *const *p)
+{
+	ctx->key_hi = (uint64_t *) p[GP_KEY_HI];
+	ctx->key_lo = (uint64_t *) p[GP_KEY_LO];
+	ctx->key_tmp = (uint64_t *) p[GP_KEY_TMP];
+	ctx->perm = (uint32_t *) p[GP_PERM];
+	ctx->perm_tmp = (uint32_t *) p[GP_PERM_TMP];
+	for (int f = 0; f < FS_NFIELDS; f++) {
+		ctx->f[f] = p[GP_FIELDS + f];
+		ctx->falt[f] = p[GP_FIELDS + FS_NFIELDS + f];
+	}
+}
+
+static bool same_ptrs(void *const *a, void *const *b)
+{
+	for (int i = 0; i < GP_N; i++)
+		if (a[i] != b[i]) return false;
+	return true;
+}
+
+void tvg_graph_release(tvg_context *ctx)
+{
+	for (int i = 0; i < 2; i++) {
+		if (!ctx->graphs[i]) continue;
+		if (ctx->graphs[i]->exec) cudaGraphExecDestroy(ctx->graphs[i]->exec);
+		delete ctx->graphs[i];
+		ctx->graphs[i] = nullptr;
+	}
+	ctx->graph_warm_key = 0;
+}
+
+// the configuration a graph is valid for
+static uint64_t graph_key(const tvg_context *ctx, uint32_t parts, int32_t ewald_kind)
+{
+	uint64_t k = 1;
+	k = k * 1000003u + parts;
+	k = k * 1000003u + (uint32_t) ewald_kind;
+	k = k * 1000003u + (uint32_t) ctx->group_tpl;
+	k = k * 1000003u + (ctx->have_timeline ? 1u : 0u);
+	k = k * 1000003u + (uint64_t) ctx->n;
+	k = k * 1000003u + (ctx->mlp_ok ? 1u : 0u);
+	return k;
+}
+
+static int capture(tvg_context *ctx, uint32_t parts, int32_t ewald_kind, uint64_t key,
+                   tvg_graph_entry **out)
+{
+	cudaStream_t s = ctx->stream;
+	tvg_graph_entry *e = new tvg_graph_entry;
+	e->key = key;
+	snap_ptrs(ctx, e->start);
+	const int64_t l0 = ctx->launches;
+	cudaError_t ce = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+	if (ce != cudaSuccess) {
+		delete e;
+		return tvg_fail(ctx, TVG_E_CUDA, "step graph: begin capture: %s", cudaGetErrorString(ce));
+	}
+	ctx->capturing = true;
+	int rc = accel_phases(ctx, TVG_FORM_GROUP, parts, ewald_kind, 0);
+	ctx->capturing = false;
+	cudaGraph_t g = nullptr;
+	ce = cudaStreamEndCapture(s, &g);
+	snap_ptrs(ctx, e->end);
+	e->launches = ctx->launches - l0;
+	// nothing ran yet: the buffers are where the capture started
+	set_ptrs(ctx, e->start);
+	ctx->launches = l0;
+	if (rc == TVG_OK && ce != cudaSuccess)
+		rc = tvg_fail(ctx, TVG_E_CUDA, "step graph: capture failed: %s", cudaGetErrorString(ce));
+	if (rc == TVG_OK) {
+		ce = cudaGraphInstantiate(&e->exec, g, 0);
+		if (ce != cudaSuccess)
+			rc = tvg_fail(ctx, TVG_E_CUDA, "step graph: instantiation failed: %s", cudaGetErrorString(ce));
+	}
+	if (g) cudaGraphDestroy(g);
+	if (rc != TVG_OK) {
+		cudaGetLastError();
+		if (e->exec) cudaGraphExecDestroy(e->exec);
+		delete e;
+		return rc;
+	}
+	*out = e;
+	return TVG_OK;
+}
+
+extern "C" int tvg_step_graph(tvg_context *ctx, uint32_t parts, int32_t ewald_kind)
+{
+	TVG_CHECK(accel_check(ctx, TVG_FORM_GROUP));
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	const uint64_t key = graph_key(ctx, parts, ewald_kind);
+	if (key != ctx->graph_warm_key) {
+		// a new configuration: one direct step, which also makes every
+		// allocation, table and kernel attribute the captured step relies on
+		tvg_graph_release(ctx);
+		TVG_CHECK(tvg_compute_acceleration(ctx, TVG_FORM_GROUP, parts, ewald_kind, 0));
+		ctx->graph_warm_key = key;
+		return TVG_OK;
+	}
+	void *cur[GP_N];
+	snap_ptrs(ctx, cur);
+	tvg_graph_entry *e = nullptr;
+	int slot = -1;
+	for (int i = 0; i < 2; i++) {
+		if (ctx->graphs[i] && ctx->graphs[i]->key == key && same_ptrs(ctx->graphs[i]->start, cur)) {
+			e = ctx->graphs[i];
+			break;
+		}
+		if (slot < 0 && !ctx->graphs[i]) slot = i;
+	}
+	if (!e) {
+		if (slot < 0) {             // buffers moved: start over
+			tvg_graph_release(ctx);
+			ctx->graph_warm_key = key;
+			slot = 0;
+		}
+		TVG_CHECK(capture(ctx, parts, ewald_kind, key, &e));
+		ctx->graphs[slot] = e;
+	}
+	if (ctx->have_timeline) TVG_CHECK(tvg_set_device_max_bin(ctx));
+	TVG_CUDA(ctx, cudaGraphLaunch(e->exec, ctx->stream));
+	ctx->launches += e->launches;
+	set_ptrs(ctx, e->end);
+	ctx->keys_std = ctx->sorted = ctx->have_top = ctx->have_tree = ctx->have_walktree = true;
+	ctx->use_active = ctx->have_timeline;
+	// host mirrors of the step's counts and times (one synchronisation)
+	TVG_CHECK(accel_times(ctx));
+	TVG_CHECK(tvg_walk_group_results(ctx));
+	TVG_CHECK(tvg_read_counts(ctx));
+	if (ctx->have_timeline) {
+		int64_t na = 0;
+		TVG_CUDA(ctx, cudaMemcpy(&na, &ctx->dc->n_active, 8, cudaMemcpyDeviceToHost));
+		ctx->n_active = na;
+		ctx->tl.state.n_active = na;
+	}
+	return tvg_sync_status(ctx, "step_graph");
+}
+
+extern "C" int tvg_step_graph_reset(tvg_context *ctx)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	TVG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+	tvg_graph_release(ctx);
+	return TVG_OK;
 }

@@ -60,11 +60,12 @@ __global__ void k_top_first(int64_t n, const uint64_t *__restrict__ key_hi, int3
 // domain.c:678-684), centre from the first particle (domain.c:237-246)
 template <typename F>
 __global__ void k_make_top(int64_t n, const int32_t *first, const F *x, const F *y, const F *z,
-                           double ox, double oy, double oz, double size, tvg_topnode *top,
-                           int32_t *count, int32_t *ntop_out)
+                           double ox, double oy, double oz, double size, int vsize, tvg_topnode *top,
+                           int32_t *count, TopInfo *ti, tvg_devcount *dc)
 {
 	if (threadIdx.x || blockIdx.x) return;
 	int nt = 0;
+	for (int c = 0; c < 64; c++) { ti->first[c] = -1; ti->count[c] = 0; ti->tidx[c] = -1; ti->big[c] = 0; }
 	for (int c = 63; c >= 0; c--) {
 		if (first[c] < 0) { count[c] = 0; continue; }
 		int64_t e = n;
@@ -85,9 +86,13 @@ __global__ void k_make_top(int64_t n, const int32_t *first, const F *x, const F 
 		t.pos[2] = (float) __dadd_rn(__dmul_rn(floor(pz / sz) + 0.5, sz), oz);
 		t.mass = 0;
 		for (int k = 0; k < 3; k++) { t.com[k] = 0; t.dp[k] = 0; }
+		ti->first[c] = t.first_part;
+		ti->count[c] = t.npart;
+		ti->tidx[c] = nt;
+		ti->big[c] = t.npart > vsize;
 		top[nt++] = t;
 	}
-	*ntop_out = nt;
+	dc->ntop = nt;
 }
 
 int tvg_impl_top_nodes(tvg_context *ctx)
@@ -96,34 +101,24 @@ int tvg_impl_top_nodes(tvg_context *ctx)
 	cudaStream_t s = ctx->stream;
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->top_first, 0xFF, 4 * TVG_MAX_TOP, s));
 	k_top_first<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->top_first);
-	int32_t *d_nt = (int32_t *) ctx->work_counter;
+	const int vsize = ctx->cfg.vector_size;
 	if (ctx->cfg.float_bytes == 4)
 		k_make_top<float><<<TVG_CNT(ctx, 1), 1, 0, s>>>(n, ctx->top_first, (const float *) ctx->f[FS_POS0],
 		                                  (const float *) ctx->f[FS_POS1], (const float *) ctx->f[FS_POS2],
-		                                  ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
-		                                  ctx->d_top, ctx->top_count, d_nt);
+		                                  ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize, vsize,
+		                                  ctx->d_top, ctx->top_count, ctx->d_topinfo, ctx->dc);
 	else
 		k_make_top<double><<<TVG_CNT(ctx, 1), 1, 0, s>>>(n, ctx->top_first, (const double *) ctx->f[FS_POS0],
 		                                   (const double *) ctx->f[FS_POS1], (const double *) ctx->f[FS_POS2],
-		                                   ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
-		                                   ctx->d_top, ctx->top_count, d_nt);
+		                                   ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize, vsize,
+		                                   ctx->d_top, ctx->top_count, ctx->d_topinfo, ctx->dc);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->ntop, d_nt, 4, cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaStreamSynchronize(s));
-	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
-	                              cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaStreamSynchronize(s));
-	return TVG_OK;
+	if (ctx->capturing) return TVG_OK;
+	return tvg_read_counts(ctx);
 }
 
 // ----------------------------------------------------- build: levels
 
-struct TopInfo {            // per level-2 cell c (0..63)
-	int32_t first[64];      // first particle, -1 if empty
-	int32_t count[64];
-	int32_t tidx[64];       // index in the top node list (D order)
-	int32_t big[64];        // count > VECTOR_SIZE: has a subtree
-};
 
 __device__ __forceinline__ int lca_level(const uint64_t *hi, const uint64_t *lo, int64_t a, int64_t b)
 {
@@ -132,10 +127,14 @@ __device__ __forceinline__ int lca_level(const uint64_t *hi, const uint64_t *lo,
 }
 
 __global__ void k_levels(int64_t n, const uint64_t *__restrict__ hi, const uint64_t *__restrict__ lo,
-                         TopInfo ti, uint8_t *__restrict__ lvl, int32_t *__restrict__ ncnt,
-                         uint8_t *__restrict__ lvl_min64, int *status)
+                         const TopInfo *__restrict__ tip, uint8_t *__restrict__ lvl,
+                         int32_t *__restrict__ ncnt, uint8_t *__restrict__ lvl_min64, int *status)
 {
 	__shared__ uint8_t s_min[256 / 32];
+	__shared__ TopInfo ti;
+	for (int e = threadIdx.x; e < 256; e += blockDim.x)
+		((int32_t *) &ti)[e] = ((const int32_t *) tip)[e];
+	__syncthreads();
 	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	unsigned my = 0xFF;
 	if (i < n) {
@@ -219,7 +218,7 @@ __global__ void k_nodes(int64_t n, const uint8_t *__restrict__ lvl, const uint8_
                         const int32_t *__restrict__ base, int vsize, int32_t *__restrict__ u_start,
                         uint8_t *__restrict__ u_level, int32_t *__restrict__ u_count,
                         int32_t *__restrict__ u_endu, uint8_t *__restrict__ u_flag,
-                        int32_t *__restrict__ u_diff)
+                        int32_t *__restrict__ u_diff, int64_t ucap, int *status)
 {
 	const int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (s >= n) return;
@@ -253,6 +252,10 @@ __global__ void k_nodes(int64_t n, const uint8_t *__restrict__ lvl, const uint8_
 			}
 		}
 		const int32_t endu = base[e];
+		if (u >= ucap || endu > ucap) {      // u_diff holds ucap + 1 entries
+			atomicOr(status, TVG_ST_TREE_FULL);
+			return;
+		}
 		u_start[u] = (int32_t) s;
 		u_level[u] = (uint8_t) l;
 		u_count[u] = cnt;
@@ -265,44 +268,47 @@ __global__ void k_nodes(int64_t n, const uint8_t *__restrict__ lvl, const uint8_
 	}
 }
 
-// survivor flag from the scanned removal marks: surv[u] = (marks(u) == 0)
-__global__ void k_survivors(int64_t nu, const int32_t *__restrict__ excl, int32_t *__restrict__ surv)
+// survivor flag from the scanned removal marks: surv[u] = (marks(u) == 0),
+// for u <= nu (nu from the device, at most ucap)
+__global__ void k_survivors(const tvg_devcount *__restrict__ dc, int64_t ucap,
+                            const int32_t *__restrict__ excl, int32_t *__restrict__ surv)
 {
+	const int64_t nu = min(dc->nu, ucap);
 	int64_t u = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (u > nu) return;
 	surv[u] = (u < nu && excl[u + 1] == 0) ? 1 : 0;
 }
 
-// one thread: subtree placement in top-node order (tree_build.c:59-96)
-__global__ void k_place_subtrees(int ntop, tvg_topnode *top, const int32_t *__restrict__ base,
-                                 const int32_t *__restrict__ F, int vsize, int32_t *toff,
-                                 int32_t *nsurv, int64_t *total)
+// one thread: subtree placement in top-node order (tree_build.c:59-96); the
+// placement table for the emission and the node count, on the device
+__global__ void k_place_subtrees(tvg_devcount *dc, tvg_topnode *top, const int32_t *__restrict__ base,
+                                 const int32_t *__restrict__ F, int vsize, const TopInfo *__restrict__ ti,
+                                 TopPlace *tp, int64_t ucap, int64_t tcap, int *status)
 {
 	if (threadIdx.x || blockIdx.x) return;
+	const int ntop = dc->ntop;
 	int64_t run = 0;
+	for (int t = 0; t < 64; t++) {
+		tp->tidx[t] = ti->tidx[t];
+		tp->toff[t] = tp->target[t] = tp->nsurv[t] = tp->end[t] = 0;
+	}
 	for (int t = 0; t < ntop; t++) {
 		top[t].target = (int32_t) run;       // also for small top nodes (quirk Q3)
+		tp->target[t] = (int32_t) run;
+		tp->end[t] = top[t].first_part + top[t].npart;
 		if (top[t].npart > vsize) {
 			int64_t f = top[t].first_part, e = f + top[t].npart;
-			int32_t fs = F[base[f]], fe = F[base[e]];
-			nsurv[t] = fe - fs;
-			toff[t] = (int32_t) (run - fs);
+			// base <= nu; past the capacity the build has failed (status set)
+			int32_t fs = F[min((int64_t) base[f], ucap)], fe = F[min((int64_t) base[e], ucap)];
+			tp->nsurv[t] = fe - fs;
+			tp->toff[t] = (int32_t) (run - fs);
 			run += (fe - fs) + 1;             // + terminator
-		} else {
-			nsurv[t] = 0;
-			toff[t] = 0;
 		}
 	}
-	*total = run;
+	if (run > tcap) atomicOr(status, TVG_ST_TREE_FULL);
+	dc->nnodes = run;
 }
 
-struct TopPlace {
-	int32_t tidx[64];       // by level-2 cell
-	int32_t toff[64];       // by top index: G = toff + F[u]
-	int32_t target[64];
-	int32_t nsurv[64];
-	int32_t end[64];        // by top index: first particle after the node
-};
 
 __device__ __forceinline__ int32_t triplet_at(const uint64_t *hi, const uint64_t *lo, int64_t i, int l)
 {
@@ -310,16 +316,22 @@ __device__ __forceinline__ int32_t triplet_at(const uint64_t *hi, const uint64_t
 }
 
 template <typename F>
-__global__ void k_emit_nodes(int64_t nu, int64_t n, const uint8_t *__restrict__ lvl,
+__global__ void k_emit_nodes(const tvg_devcount *__restrict__ dc, int64_t ucap, int64_t n,
+                             const uint8_t *__restrict__ lvl,
                              const uint8_t *__restrict__ m64, const int32_t *__restrict__ base,
                              const int32_t *__restrict__ u_start, const uint8_t *__restrict__ u_level,
                              const int32_t *__restrict__ u_count, const int32_t *__restrict__ u_endu,
                              const uint8_t *__restrict__ u_flag, const int32_t *__restrict__ surv,
                              const int32_t *__restrict__ Fidx, const uint64_t *__restrict__ hi,
-                             const uint64_t *__restrict__ lo, TopPlace tp, TNode<F> *tree,
-                             int32_t *__restrict__ tree_u, int32_t *__restrict__ tree_parent,
-                             int64_t tcap, int *status)
+                             const uint64_t *__restrict__ lo, const TopPlace *__restrict__ tpp,
+                             TNode<F> *tree, int32_t *__restrict__ tree_u,
+                             int32_t *__restrict__ tree_parent, int64_t tcap, int *status)
 {
+	__shared__ TopPlace tp;
+	for (int e = threadIdx.x; e < 5 * 64; e += blockDim.x)
+		((int32_t *) &tp)[e] = ((const int32_t *) tpp)[e];
+	__syncthreads();
+	const int64_t nu = min(dc->nu, ucap);
 	const int64_t u = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (u >= nu || !surv[u]) return;
 	const int32_t s = u_start[u];
@@ -365,13 +377,13 @@ __global__ void k_emit_nodes(int64_t nu, int64_t n, const uint8_t *__restrict__ 
 
 // particles of top nodes without subtree point to their top node (-t-1),
 // set_tree_parent_pointers, tree_build.c:226-242
-__global__ void k_small_parent(int64_t n, const uint64_t *__restrict__ hi, TopInfo ti,
+__global__ void k_small_parent(int64_t n, const uint64_t *__restrict__ hi, const TopInfo *__restrict__ ti,
                                int32_t *__restrict__ tree_parent)
 {
 	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	int c = (int) (hi[i] >> 58);
-	if (!ti.big[c]) tree_parent[i] = -ti.tidx[c] - 1;
+	if (!ti->big[c]) tree_parent[i] = -ti->tidx[c] - 1;
 }
 
 // reference arithmetic for a child centre (tree_build.c:542-550)
@@ -385,14 +397,13 @@ __device__ __forceinline__ F child_pos(F ppos, F ppart, double dsize, int l)
 	return (F) __dadd_rn((double) ppos, __dmul_rn((double) ss, 0.5));
 }
 
+// centre of node G down its chain of ancestors
 template <typename F>
-__global__ void k_node_pos(int64_t nnodes, TNode<F> *tree, const int32_t *__restrict__ tree_u,
-                           const int32_t *__restrict__ u_start, const F *__restrict__ x,
-                           const F *__restrict__ y, const F *__restrict__ z,
-                           const tvg_topnode *__restrict__ top, double dsize)
+__device__ void node_pos_one(int64_t G, TNode<F> *tree, const int32_t *__restrict__ tree_u,
+                             const int32_t *__restrict__ u_start, const F *__restrict__ x,
+                             const F *__restrict__ y, const F *__restrict__ z,
+                             const tvg_topnode *__restrict__ top, double dsize)
 {
-	const int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (G >= nnodes) return;
 	const uint32_t bf = tree[G].Bitfield;
 	if (!(bf & (1u << 9))) return;              // terminator
 	int64_t chain[TVG_MAX_LEVEL + 1];
@@ -416,6 +427,19 @@ __global__ void k_node_pos(int64_t nnodes, TNode<F> *tree, const int32_t *__rest
 	tree[G].Pos[0] = p[0];
 	tree[G].Pos[1] = p[1];
 	tree[G].Pos[2] = p[2];
+}
+
+// all nodes (count from the device), grid-stride
+template <typename F>
+__global__ void k_node_pos(const tvg_devcount *__restrict__ dc, int64_t tcap, TNode<F> *tree,
+                           const int32_t *__restrict__ tree_u, const int32_t *__restrict__ u_start,
+                           const F *__restrict__ x, const F *__restrict__ y, const F *__restrict__ z,
+                           const tvg_topnode *__restrict__ top, double dsize)
+{
+	const int64_t nnodes = min(dc->nnodes, tcap);
+	for (int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; G < nnodes;
+	     G += (int64_t) gridDim.x * blockDim.x)
+		node_pos_one<F>(G, tree, tree_u, u_start, x, y, z, top, dsize);
 }
 
 // Float sums in particle order (add_particle_to_node), then CoM /= Mass
@@ -446,34 +470,33 @@ __device__ __forceinline__ void seq_moments(int64_t s, int64_t cnt, const F *__r
 }
 
 template <typename F>
-__global__ void k_moments_seq(int64_t nnodes, TNode<F> *tree, const int32_t *__restrict__ tree_u,
-                              const int32_t *__restrict__ u_start, const F *__restrict__ x,
-                              const F *__restrict__ y, const F *__restrict__ z,
+__global__ void k_moments_seq(const tvg_devcount *__restrict__ dc, int64_t tcap, TNode<F> *tree,
+                              const int32_t *__restrict__ tree_u, const int32_t *__restrict__ u_start,
+                              const F *__restrict__ x, const F *__restrict__ y, const F *__restrict__ z,
                               const F *__restrict__ m, int exact)
 {
-	const int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (G >= nnodes) return;
-	const TNode<F> &nd = tree[G];
-	if (!(nd.Bitfield & (1u << 9))) return;
-	if (!exact && nd.DNext > 0) return;         // internal node: fast path
-	F o[4];
-	seq_moments<F>(u_start[tree_u[G]], nd.Npart, x, y, z, m, o);
-	tree[G].Mass = o[0];
-	tree[G].CoM[0] = o[1];
-	tree[G].CoM[1] = o[2];
-	tree[G].CoM[2] = o[3];
+	const int64_t nnodes = min(dc->nnodes, tcap);
+	for (int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; G < nnodes;
+	     G += (int64_t) gridDim.x * blockDim.x) {
+		const TNode<F> &nd = tree[G];
+		if (!(nd.Bitfield & (1u << 9))) continue;
+		if (!exact && nd.DNext > 0) continue;       // internal node: fast path
+		F o[4];
+		seq_moments<F>(u_start[tree_u[G]], nd.Npart, x, y, z, m, o);
+		tree[G].Mass = o[0];
+		tree[G].CoM[0] = o[1];
+		tree[G].CoM[1] = o[2];
+		tree[G].CoM[2] = o[3];
+	}
 }
 
 // fast mode: one warp per internal node, FP64 sums relative to the node centre
 template <typename F>
-__global__ void k_moments_warp(int64_t nnodes, TNode<F> *tree, const int32_t *__restrict__ tree_u,
-                               const int32_t *__restrict__ u_start, const F *__restrict__ x,
-                               const F *__restrict__ y, const F *__restrict__ z,
-                               const F *__restrict__ m)
+__device__ void moments_warp_one(int64_t G, int lane, TNode<F> *tree, const int32_t *__restrict__ tree_u,
+                                 const int32_t *__restrict__ u_start, const F *__restrict__ x,
+                                 const F *__restrict__ y, const F *__restrict__ z,
+                                 const F *__restrict__ m)
 {
-	const int64_t G = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5;
-	const int lane = threadIdx.x & 31;
-	if (G >= nnodes) return;
 	const TNode<F> &nd = tree[G];
 	if (!(nd.Bitfield & (1u << 9)) || nd.DNext <= 0) return;
 	const int64_t s = u_start[tree_u[G]], cnt = nd.Npart;
@@ -501,15 +524,31 @@ __global__ void k_moments_warp(int64_t nnodes, TNode<F> *tree, const int32_t *__
 	}
 }
 
+// a warp per node, grid-stride over the device node count
+template <typename F>
+__global__ void k_moments_warp(const tvg_devcount *__restrict__ dc, int64_t tcap, TNode<F> *tree,
+                               const int32_t *__restrict__ tree_u, const int32_t *__restrict__ u_start,
+                               const F *__restrict__ x, const F *__restrict__ y, const F *__restrict__ z,
+                               const F *__restrict__ m)
+{
+	const int64_t nnodes = min(dc->nnodes, tcap);
+	const int lane = threadIdx.x & 31;
+	for (int64_t G = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5; G < nnodes;
+	     G += ((int64_t) gridDim.x * blockDim.x) >> 5)
+		moments_warp_one<F>(G, lane, tree, tree_u, u_start, x, y, z, m);
+}
+
 // top node Mass/CoM (finalise_subtree copies the subtree root, as float),
 // terminators (tree_build.c:468-474); small top nodes sum their particles
 template <typename F>
-__global__ void k_finish_top(int ntop, tvg_topnode *top, TNode<F> *tree, const int32_t *nsurv,
-                             const F *__restrict__ x, const F *__restrict__ y,
-                             const F *__restrict__ z, const F *__restrict__ m, int vsize)
+__global__ void k_finish_top(const tvg_devcount *__restrict__ dc, tvg_topnode *top, TNode<F> *tree,
+                             const TopPlace *__restrict__ tp, int64_t tcap, const F *__restrict__ x,
+                             const F *__restrict__ y, const F *__restrict__ z, const F *__restrict__ m,
+                             int vsize)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= ntop) return;
+	if (t >= dc->ntop) return;
+	const int32_t *nsurv = tp->nsurv;
 	F o[4];
 	if (top[t].npart > vsize) {
 		const TNode<F> &r = tree[top[t].target];
@@ -518,7 +557,7 @@ __global__ void k_finish_top(int ntop, tvg_topnode *top, TNode<F> *tree, const i
 		term.DNext = 0; term.Bitfield = 1u << 10; term.DUp = 0; term.Npart = 0;
 		for (int k = 0; k < 3; k++) { term.Pos[k] = 0; term.CoM[k] = 0; term.Dp[k] = 0; }
 		term.Mass = 1;
-		tree[(int64_t) top[t].target + nsurv[t]] = term;
+		if ((int64_t) top[t].target + nsurv[t] < tcap) tree[(int64_t) top[t].target + nsurv[t]] = term;
 	} else {
 		seq_moments<F>(top[t].first_part, top[t].npart, x, y, z, m, o);
 	}
@@ -528,6 +567,10 @@ __global__ void k_finish_top(int ntop, tvg_topnode *top, TNode<F> *tree, const i
 	top[t].com[2] = (float) o[3];
 }
 
+// Every count (uncollapsed nodes, nodes, top nodes) stays on the device and
+// the kernels read it, so the build needs no host round trip (and can be
+// captured in a graph); launches are sized by the capacities. The host
+// mirrors are read back at the end unless a capture is in progress.
 template <typename F>
 static int build_typed(tvg_context *ctx, uint32_t flags)
 {
@@ -537,89 +580,57 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 	const F *x = (const F *) ctx->f[FS_POS0], *y = (const F *) ctx->f[FS_POS1],
 	        *z = (const F *) ctx->f[FS_POS2], *m = (const F *) ctx->f[FS_MASS];
 	int32_t *tree_parent = (int32_t *) ctx->f[FS_TREE_PARENT];
+	const int64_t ucap = ctx->ucap, tcap = ctx->tcap;
+	tvg_devcount *dc = ctx->dc;
 
-	TopInfo ti;
-	for (int c = 0; c < 64; c++) { ti.first[c] = -1; ti.count[c] = 0; ti.tidx[c] = -1; ti.big[c] = 0; }
-	for (int t = 0; t < ctx->ntop; t++) {
-		int c = (int) (ctx->h_top[t].key >> 58);
-		ti.first[c] = ctx->h_top[t].first_part;
-		ti.count[c] = ctx->h_top[t].npart;
-		ti.tidx[c] = t;
-		ti.big[c] = ctx->h_top[t].npart > vsize;
-	}
-	k_levels<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ti, ctx->lvl, ctx->ncnt,
-	                                             ctx->lvl_min64, ctx->status);
+	k_levels<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->d_topinfo,
+	                                                          ctx->lvl, ctx->ncnt, ctx->lvl_min64, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CHECK(tvg_sync_status(ctx, "tree_build(levels)"));
-	int64_t nu = 0;
-	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->ncnt, ctx->ncnt, n + 1, &nu));
-	if (nu + 1 > ctx->ucap)
-		return tvg_fail(ctx, TVG_E_TREE_FULL, "tree_build: %lld uncollapsed nodes > capacity %lld",
-		                (long long) nu, (long long) ctx->ucap);
-	ctx->nu = nu;
-	TVG_CUDA(ctx, cudaMemsetAsync(ctx->u_diff, 0, 4 * (nu + 1), s));
+	if (!ctx->capturing) TVG_CHECK(tvg_sync_status(ctx, "tree_build(levels)"));
+	TVG_CHECK(tvg_device_scan_i32_dev(ctx, ctx->ncnt, ctx->ncnt, n + 1, &dc->nu));
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->u_diff, 0, 4 * (ucap + 1), s));
 	k_nodes<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, s>>>(n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, vsize,
 	                                            ctx->u_start, ctx->u_level, ctx->u_count, ctx->u_endu,
-	                                            ctx->u_flag, ctx->u_diff);
+	                                            ctx->u_flag, ctx->u_diff, ucap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
-	// removal marks -> survivor flags -> final (per top node) indices
-	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, nu + 1, nullptr));
-	k_survivors<<<TVG_CNT(ctx, tvg_blocks(nu + 1, 256)), 256, 0, s>>>(nu, ctx->u_final, ctx->u_diff);
+	// removal marks -> survivor flags -> final (per top node) indices; entries
+	// past nu are zero and do not change the prefix sums below them
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, ucap + 1, nullptr));
+	k_survivors<<<TVG_CNT(ctx, tvg_blocks(ucap + 1, 256)), 256, 0, s>>>(dc, ucap, ctx->u_final, ctx->u_diff);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, nu + 1, nullptr));
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, ucap + 1, nullptr));
 	// placement of the subtrees
-	int32_t *d_toff = (int32_t *) ctx->scan_tmp;     // scan scratch is free here
-	int32_t *d_nsurv = d_toff + 64;
-	int64_t *d_total = (int64_t *) (d_toff + 128);
-	k_place_subtrees<<<TVG_CNT(ctx, 1), 1, 0, s>>>(ctx->ntop, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, d_toff,
-	                                  d_nsurv, d_total);
+	k_place_subtrees<<<TVG_CNT(ctx, 1), 1, 0, s>>>(dc, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, ctx->d_topinfo,
+	                                               ctx->d_topplace, ucap, tcap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
-	int32_t h_toff[64], h_nsurv[64];
-	int64_t total = 0;
-	TVG_CUDA(ctx, cudaMemcpyAsync(h_toff, d_toff, 4 * 64, cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaMemcpyAsync(h_nsurv, d_nsurv, 4 * 64, cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
-	                              cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaStreamSynchronize(s));
-	if (total > ctx->tcap)
-		return tvg_fail(ctx, TVG_E_TREE_FULL, "tree_build: %lld nodes > capacity %lld",
-		                (long long) total, (long long) ctx->tcap);
-	ctx->nnodes = total;
-	TopPlace tp;
-	for (int c = 0; c < 64; c++) tp.tidx[c] = ti.tidx[c];
-	for (int t = 0; t < 64; t++) {
-		bool ok = t < ctx->ntop;
-		tp.toff[t] = ok ? h_toff[t] : 0;
-		tp.target[t] = ok ? ctx->h_top[t].target : 0;
-		tp.nsurv[t] = ok ? h_nsurv[t] : 0;
-		tp.end[t] = ok ? ctx->h_top[t].first_part + ctx->h_top[t].npart : 0;
-		ctx->h_target[t] = tp.target[t];
-		ctx->h_nsurv[t] = tp.nsurv[t];
-	}
 	TNode<F> *tree = (TNode<F> *) ctx->tree;
-	k_emit_nodes<F><<<TVG_CNT(ctx, tvg_blocks(nu, 256)), 256, 0, s>>>(
-	    nu, n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, ctx->u_start, ctx->u_level, ctx->u_count,
-	    ctx->u_endu, ctx->u_flag, ctx->u_diff, ctx->u_final, ctx->key_hi, ctx->key_lo, tp, tree,
-	    ctx->tree_u, tree_parent, ctx->tcap, ctx->status);
+	k_emit_nodes<F><<<TVG_CNT(ctx, tvg_blocks(ucap, 256)), 256, 0, s>>>(
+	    dc, ucap, n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, ctx->u_start, ctx->u_level, ctx->u_count,
+	    ctx->u_endu, ctx->u_flag, ctx->u_diff, ctx->u_final, ctx->key_hi, ctx->key_lo, ctx->d_topplace, tree,
+	    ctx->tree_u, tree_parent, tcap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
-	k_small_parent<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ti, tree_parent);
+	k_small_parent<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->d_topinfo, tree_parent);
 	TVG_CUDA(ctx, cudaGetLastError());
-	if (total > 0) {
-		k_node_pos<F><<<TVG_CNT(ctx, tvg_blocks(total, 128)), 128, 0, s>>>(total, tree, ctx->tree_u, ctx->u_start,
-		                                                       x, y, z, ctx->d_top, ctx->dsize);
-		const int exact = (flags & TVG_BUILD_EXACT_MOMENTS) ? 1 : 0;
-		k_moments_seq<F><<<TVG_CNT(ctx, tvg_blocks(total, 128)), 128, 0, s>>>(total, tree, ctx->tree_u,
-		                                                          ctx->u_start, x, y, z, m, exact);
-		if (!exact)
-			k_moments_warp<F><<<TVG_CNT(ctx, tvg_blocks(total * 32, 256)), 256, 0, s>>>(total, tree, ctx->tree_u,
-			                                                               ctx->u_start, x, y, z, m);
-		TVG_CUDA(ctx, cudaGetLastError());
-	}
-	k_finish_top<F><<<TVG_CNT(ctx, 1), 64, 0, s>>>(ctx->ntop, ctx->d_top, tree, d_nsurv, x, y, z, m, vsize);
+	const unsigned gs = 148 * 16;      // grid-stride launches over the node count
+	k_node_pos<F><<<TVG_CNT(ctx, gs), 128, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z,
+	                                              ctx->d_top, ctx->dsize);
+	const int exact = (flags & TVG_BUILD_EXACT_MOMENTS) ? 1 : 0;
+	k_moments_seq<F><<<TVG_CNT(ctx, gs), 128, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z, m,
+	                                                 exact);
+	if (!exact)
+		k_moments_warp<F><<<TVG_CNT(ctx, gs), 256, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z, m);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
-	                              cudaMemcpyDeviceToHost, s));
+	k_finish_top<F><<<TVG_CNT(ctx, 1), 64, 0, s>>>(dc, ctx->d_top, tree, ctx->d_topplace, tcap, x, y, z, m,
+	                                                vsize);
+	TVG_CUDA(ctx, cudaGetLastError());
+	if (ctx->capturing) return TVG_OK;
+	TVG_CHECK(tvg_read_counts(ctx));
+	if (ctx->nu + 1 > ucap)
+		return tvg_fail(ctx, TVG_E_TREE_FULL, "tree_build: %lld uncollapsed nodes > capacity %lld",
+		                (long long) ctx->nu, (long long) ucap);
+	if (ctx->nnodes > tcap)
+		return tvg_fail(ctx, TVG_E_TREE_FULL, "tree_build: %lld nodes > capacity %lld",
+		                (long long) ctx->nnodes, (long long) tcap);
 	return tvg_sync_status(ctx, "tree_build");
 }
 

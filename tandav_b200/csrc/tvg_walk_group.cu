@@ -104,10 +104,8 @@ __device__ __forceinline__ bool is_local(uint32_t bf) { return bf & (1u << 9); }
 __device__ __forceinline__ bool is_top(uint32_t bf) { return bf & (1u << 10); }
 
 template <typename F>
-__global__ void k_wt_nchild(int64_t nn, const GNode<F> *__restrict__ tree, int32_t *__restrict__ nch)
+__device__ __forceinline__ int wt_nchild_one(int64_t g, const GNode<F> *__restrict__ tree)
 {
-	const int64_t g = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (g >= nn) return;
 	const GNode<F> &nd = tree[g];
 	int cnt = 0;
 	if (is_local(nd.Bitfield) && nd.DNext > 0) {
@@ -119,7 +117,19 @@ __global__ void k_wt_nchild(int64_t nn, const GNode<F> *__restrict__ tree, int32
 			c += dn > 0 ? dn : 1;
 		}
 	}
-	nch[g] = cnt;
+	return cnt;
+}
+
+// children per node for the first min(nnodes, tcap) nodes, zeros up to
+// lscan (the length of the scan that follows)
+template <typename F>
+__global__ void k_wt_nchild(const tvg_devcount *__restrict__ dc, int64_t tcap, int64_t lscan,
+                            const GNode<F> *__restrict__ tree, int32_t *__restrict__ nch)
+{
+	const int64_t nn = min(dc->nnodes, tcap);
+	for (int64_t g = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; g < lscan;
+	     g += (int64_t) gridDim.x * blockDim.x)
+		nch[g] = g < nn ? wt_nchild_one<F>(g, tree) : 0;
 }
 
 __device__ __forceinline__ uint32_t to_int(double v, double o, double fac)
@@ -128,13 +138,12 @@ __device__ __forceinline__ uint32_t to_int(double v, double o, double fac)
 }
 
 template <typename F>
-__global__ void k_wt_emit(int64_t nn, int ntop, const GNode<F> *__restrict__ tree,
-                          const int32_t *__restrict__ nch, const int32_t *__restrict__ choff,
-                          double ox, double oy, double oz, double fac, double dsize,
-                          tvg_wnode *__restrict__ wt)
+__device__ __forceinline__ void wt_emit_one(int64_t g, int ntop, const GNode<F> *__restrict__ tree,
+                                            const int32_t *__restrict__ nch,
+                                            const int32_t *__restrict__ choff, double ox, double oy,
+                                            double oz, double fac, double dsize,
+                                            tvg_wnode *__restrict__ wt)
 {
-	const int64_t g = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (g >= nn) return;
 	const GNode<F> &nd = tree[g];
 	if (!is_local(nd.Bitfield)) return;
 	int64_t w;
@@ -173,14 +182,28 @@ __global__ void k_wt_emit(int64_t nn, int ntop, const GNode<F> *__restrict__ tre
 	wt[w] = r;
 }
 
+template <typename F>
+__global__ void k_wt_emit(const tvg_devcount *__restrict__ dc, int64_t tcap,
+                          const GNode<F> *__restrict__ tree, const int32_t *__restrict__ nch,
+                          const int32_t *__restrict__ choff, double ox, double oy, double oz, double fac,
+                          double dsize, tvg_wnode *__restrict__ wt)
+{
+	const int64_t nn = min(dc->nnodes, tcap);
+	const int ntop = dc->ntop;
+	for (int64_t g = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; g < nn;
+	     g += (int64_t) gridDim.x * blockDim.x)
+		wt_emit_one<F>(g, ntop, tree, nch, choff, ox, oy, oz, fac, dsize, wt);
+}
+
 // top nodes without subtree: one bundle record each (their First_Part; the
 // reference's interact_with_topnode_particles reads from Target instead,
 // quirk Q3, which the group form does not repeat)
-__global__ void k_wt_small_top(int ntop, const tvg_topnode *__restrict__ top, int vsize, double ox,
-                               double oy, double oz, double fac, double dsize, tvg_wnode *__restrict__ wt)
+__global__ void k_wt_small_top(const tvg_devcount *__restrict__ dc, const tvg_topnode *__restrict__ top,
+                               int vsize, double ox, double oy, double oz, double fac, double dsize,
+                               tvg_wnode *__restrict__ wt)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= ntop || top[t].npart > vsize) return;
+	if (t >= dc->ntop || top[t].npart > vsize) return;
 	tvg_wnode r;
 	r.cx = to_int((double) top[t].com[0], ox, fac);
 	r.cy = to_int((double) top[t].com[1], oy, fac);
@@ -207,10 +230,9 @@ enum {
 };
 
 struct GroupParams {
-	int64_t n;
-	int64_t ngroups;
+	int64_t n;                 // particles (groups of consecutive particles without an active list)
+	const tvg_devcount *dc;    // device counts: top nodes, groups, total mass
 	int gsize;
-	int ntop;
 	int periodic;
 	int use_bh;
 	int open_bundles;   // TVG_CFG_OPEN_BUNDLES
@@ -227,7 +249,7 @@ struct GroupParams {
 	float ew_bh;        // Ewald opening: s^2 h2 limit in units of L^2 (Barnes-Hut mode)
 	float taylor_h;     // groups with a larger half extent take per-target images (with Ewald)
 	float tay_grid;     // Taylor-table node spacings per length (2 (TVG_TAYLOR_NODES - 1) / L)
-	double uniform;     // G M_total / L^2: scale of the uniform-background remainder
+	double uniform_g;   // G / L^2: times the total mass, the scale of the uniform-background remainder
 };
 
 struct WarpSmem {
@@ -344,7 +366,7 @@ __device__ __forceinline__ bool gravity_opens(const GroupParams &p, const GroupB
 	// with TVG_CFG_OPEN_BUNDLES a bundle below the top level is never a
 	// monopole: the reference interacts its particles whenever the walk
 	// reaches it (tree_accel.c:221-243, tree_periodic.c:228-251)
-	return want || (p.open_bundles && nd.nchild < 0 && node >= p.ntop);
+	return want || (p.open_bundles && nd.nchild < 0 && node >= p.dc->ntop);
 }
 
 // Pops k <= 32 nodes of the stack (one per lane, -1 for idle lanes).
@@ -510,8 +532,9 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	            wlimz = p.half_box - 2.f * g.hz;
 
 	int sp = 0, nl = 0, nw = 0;
-	for (int r = lane; r < p.ntop; r += 32) S.stack[r] = r;
-	sp = p.ntop;
+	const int ntop = p.dc->ntop;
+	for (int r = lane; r < ntop; r += 32) S.stack[r] = r;
+	sp = ntop;
 	__syncwarp();
 	int guard = 0;
 	while (sp > 0) {
@@ -631,11 +654,12 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *_
 	WarpSmem &S = ((WarpSmem *) smem_raw)[threadIdx.x >> 5];
 	const int lane = threadIdx.x & 31;
 	double cnt_acc = 0;
+	const int64_t ngroups = p.dc->ngroups;
 	for (;;) {
 		int64_t g = 0;
 		if (lane == 0) g = atomicAdd(work, 1);
 		g = __shfl_sync(0xFFFFFFFFu, g, 0);
-		if (g >= p.ngroups) break;
+		if (g >= ngroups) break;
 		int64_t first;
 		int cnt;
 		if (gfirst) {
@@ -832,9 +856,10 @@ __device__ __forceinline__ void uniform_remainder(const GroupParams &p, double t
 	const double x1 = -0.5 - x, x2 = 0.5 - x, y1 = -0.5 - y, y2 = 0.5 - y, z1 = -0.5 - z,
 	             z2 = 0.5 - z;
 	const double lin = 4.18879020478639098;      // 4 pi / 3
-	out[0] = -p.uniform * (cube_field(x1, x2, y1, y2, z1, z2) + lin * x);
-	out[1] = -p.uniform * (cube_field(y1, y2, x1, x2, z1, z2) + lin * y);
-	out[2] = -p.uniform * (cube_field(z1, z2, x1, x2, y1, y2) + lin * z);
+	const double u = p.uniform_g * p.dc->mass_total;
+	out[0] = -u * (cube_field(x1, x2, y1, y2, z1, z2) + lin * x);
+	out[1] = -u * (cube_field(y1, y2, x1, x2, z1, z2) + lin * y);
+	out[2] = -u * (cube_field(z1, z2, x1, x2, y1, y2) + lin * z);
 }
 
 // the learned correction for per-target images (groups wider than L/20,
@@ -937,8 +962,9 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 	for (int a = 0; a < 18; a++) c.h[a] = 0.f;
 
 	int sp = 0, nl = 0;
-	for (int r = lane; r < p.ntop; r += 32) S.stack[r] = r;
-	sp = p.ntop;
+	const int ntop = p.dc->ntop;
+	for (int r = lane; r < ntop; r += 32) S.stack[r] = r;
+	sp = ntop;
 	__syncwarp();
 	int guard = 0;
 	while (sp > 0) {
@@ -1085,11 +1111,12 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 	}
 	const int lane = threadIdx.x & 31;
 	double ev_acc = 0;
+	const int64_t ngroups = p.dc->ngroups;
 	for (;;) {
 		int64_t g = 0;
 		if (lane == 0) g = atomicAdd(work, 1);
 		g = __shfl_sync(0xFFFFFFFFu, g, 0);
-		if (g >= p.ngroups) break;
+		if (g >= ngroups) break;
 		int64_t first;
 		int cnt;
 		if (gfirst) {
@@ -1132,25 +1159,26 @@ __global__ void k_to_float(int64_t n, const F *__restrict__ a, float *__restrict
 template <typename F>
 static int prepare_typed(tvg_context *ctx)
 {
-	const int64_t n = ctx->n, nn = ctx->nnodes;
+	const int64_t n = ctx->n;
 	cudaStream_t s = ctx->stream;
 	const double fac = ctx->cfg.periodic ? 4294967296.0 / ctx->dsize : 2147483648.0 / ctx->dsize;
 	k_int_pos<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(
 	    n, (const F *) ctx->f[FS_POS0], (const F *) ctx->f[FS_POS1], (const F *) ctx->f[FS_POS2],
 	    ctx->origin[0], ctx->origin[1], ctx->origin[2], fac, ctx->ipos[0], ctx->ipos[1], ctx->ipos[2]);
 	TVG_CUDA(ctx, cudaGetLastError());
+	// node count from the device: grid-stride launches, and a scan over the
+	// capacity (zeros past the count)
 	int32_t *nch = ctx->u_count, *choff = ctx->u_endu;     // free after the build
-	if (nn > 0) {
-		const GNode<F> *tree = (const GNode<F> *) ctx->tree;
-		k_wt_nchild<F><<<TVG_CNT(ctx, tvg_blocks(nn, 256)), 256, 0, s>>>(nn, tree, nch);
-		TVG_CUDA(ctx, cudaGetLastError());
-		TVG_CHECK(tvg_device_scan_i32(ctx, nch, choff, nn, nullptr));
-		k_wt_emit<F><<<TVG_CNT(ctx, tvg_blocks(nn, 256)), 256, 0, s>>>(nn, ctx->ntop, tree, nch, choff,
-		                                                 ctx->origin[0], ctx->origin[1],
-		                                                 ctx->origin[2], fac, ctx->dsize, ctx->wtree);
-		TVG_CUDA(ctx, cudaGetLastError());
-	}
-	k_wt_small_top<<<TVG_CNT(ctx, 1), 64, 0, s>>>(ctx->ntop, ctx->d_top, ctx->cfg.vector_size, ctx->origin[0],
+	const int64_t tcap = ctx->tcap, lscan = ctx->tcap < ctx->ucap ? ctx->tcap : ctx->ucap;
+	const GNode<F> *tree = (const GNode<F> *) ctx->tree;
+	k_wt_nchild<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, lscan, tree, nch);
+	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CHECK(tvg_device_scan_i32(ctx, nch, choff, lscan, nullptr));
+	k_wt_emit<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, tree, nch, choff, ctx->origin[0],
+	                                                   ctx->origin[1], ctx->origin[2], fac, ctx->dsize,
+	                                                   ctx->wtree);
+	TVG_CUDA(ctx, cudaGetLastError());
+	k_wt_small_top<<<TVG_CNT(ctx, 1), 64, 0, s>>>(ctx->dc, ctx->d_top, ctx->cfg.vector_size, ctx->origin[0],
 	                                 ctx->origin[1], ctx->origin[2], fac, ctx->dsize, ctx->wtree);
 	TVG_CUDA(ctx, cudaGetLastError());
 	ctx->have_walktree = true;
@@ -1174,33 +1202,37 @@ static int group_tpl(const tvg_context *ctx)
 // Groups of an active list: the active particles of each window of gsize
 // consecutive (PH-ordered) particles form one group, so that a group is as
 // compact as a full one however few of its particles are active.
-__global__ void k_window_flags(int64_t n_act, const int32_t *__restrict__ active, int gsize,
-                               int32_t *flag)
+// (the active count from the device; flags past it are zero, n entries)
+__global__ void k_window_flags(int64_t n, const tvg_devcount *__restrict__ dc,
+                               const int32_t *__restrict__ active, int gsize, int32_t *flag)
 {
 	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (k >= n_act) return;
-	flag[k] = k == 0 || active[k] / gsize != active[k - 1] / gsize;
+	if (k >= n) return;
+	flag[k] = k < dc->n_active && (k == 0 || active[k] / gsize != active[k - 1] / gsize);
 }
 
-__global__ void k_window_scatter(int64_t n_act, const int32_t *__restrict__ flag,
-                                 const int32_t *__restrict__ off, int32_t *gfirst)
+__global__ void k_window_scatter(int64_t n, const tvg_devcount *__restrict__ dc,
+                                 const int32_t *__restrict__ flag, const int32_t *__restrict__ off,
+                                 int32_t *gfirst)
 {
+	const int64_t n_act = dc->n_active;
 	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (k < n_act && flag[k]) gfirst[off[k]] = (int32_t) k;
-	if (k == 0) gfirst[off[n_act - 1] + flag[n_act - 1]] = (int32_t) n_act;
+	if (k == 0 && n_act > 0) gfirst[off[n_act - 1] + flag[n_act - 1]] = (int32_t) n_act;
 }
 
-static int build_groups(tvg_context *ctx, int gsize, int64_t *ngroups)
+// groups of consecutive particles: their number into the device counts
+__global__ void k_set_groups(tvg_devcount *dc, int64_t ngroups) { dc->ngroups = ngroups; }
+
+static int build_groups(tvg_context *ctx, int gsize)
 {
-	const int64_t na = ctx->n_active;
+	const int64_t n = ctx->n;
 	cudaStream_t s = ctx->stream;
-	if (!ctx->act_flag) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_flag, 4 * (size_t) ctx->cap));
-	if (!ctx->act_off) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_off, 4 * (size_t) ctx->cap));
-	k_window_flags<<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, s>>>(na, ctx->active, gsize, ctx->act_flag);
+	k_window_flags<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->dc, ctx->active, gsize, ctx->act_flag);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->act_flag, ctx->act_off, na, ngroups));
-	k_window_scatter<<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, s>>>(na, ctx->act_flag, ctx->act_off,
-	                                                                   ctx->group_first);
+	TVG_CHECK(tvg_device_scan_i32_dev(ctx, ctx->act_flag, ctx->act_off, n, &ctx->dc->ngroups));
+	k_window_scatter<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->dc, ctx->act_flag, ctx->act_off,
+	                                                                  ctx->group_first);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }
@@ -1273,7 +1305,7 @@ static int launch_pair(tvg_context *ctx, const GroupParams &p, bool ewald, bool 
 {
 	if (ewald) TVG_CHECK((launch_walk<GM_CENTRE, TPL, F>(ctx, p, mass_f, last_f, cnt)));
 	else TVG_CHECK((launch_walk<GM_NEAREST, TPL, F>(ctx, p, mass_f, last_f, cnt)));
-	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+	TVG_CUDA(ctx, tvg_record(ctx, ctx->ev[1]));
 	if (ewald && mlp) TVG_CHECK((launch_ewald<TPL, true, F>(ctx, p, mass_f, last_f, cnt + 1)));
 	else if (ewald) TVG_CHECK((launch_ewald<TPL, false, F>(ctx, p, mass_f, last_f, cnt + 1)));
 	return TVG_OK;
@@ -1312,14 +1344,15 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	const tvg_config &cf = ctx->cfg;
 	const int tpl = group_tpl(ctx);
 	GroupParams p;
-	p.n = ctx->use_active ? ctx->n_active : n;
+	p.n = n;
+	p.dc = ctx->dc;
 	p.gsize = 32 * tpl;
-	p.ngroups = (p.n + p.gsize - 1) / p.gsize;
 	if (ctx->use_active) {
-		if (p.n == 0) return TVG_OK;
-		TVG_CHECK(build_groups(ctx, p.gsize, &p.ngroups));
+		TVG_CHECK(build_groups(ctx, p.gsize));
+	} else {
+		k_set_groups<<<TVG_CNT(ctx, 1), 1, 0, s>>>(ctx->dc, (n + p.gsize - 1) / p.gsize);
+		TVG_CUDA(ctx, cudaGetLastError());
 	}
-	p.ntop = ctx->ntop;
 	p.periodic = cf.periodic;
 	p.use_bh = use_bh;
 	p.open_bundles = (cf.flags & TVG_CFG_OPEN_BUNDLES) ? 1 : 0;
@@ -1345,24 +1378,29 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	// density fluctuations' share) kept the expansion within 1.2x of the
 	// per-target force error at h ~ L / 32 (64^3 box, z = 50).
 	p.taylor_h = (float) (cf.periodic ? cf.boxsize / 20.0 : 3.0e38);
-	p.uniform = 0;
+	p.uniform_g = cf.periodic ? cf.gravity / (cf.boxsize * cf.boxsize) : 0.0;
 	if (ewald) {
-		double *dm = ctx->counters + 2, mt = 0;
+		double *dm = &ctx->dc->mass_total;
 		TVG_CUDA(ctx, cudaMemsetAsync(dm, 0, 8, s));
 		k_mass_total<<<TVG_CNT(ctx, 148 * 4), 256, 0, s>>>(n, mass_f, dm);
 		TVG_CUDA(ctx, cudaGetLastError());
-		TVG_CUDA(ctx, cudaMemcpyAsync(&mt, dm, 8, cudaMemcpyDeviceToHost, s));
-		TVG_CUDA(ctx, cudaStreamSynchronize(s));
-		p.uniform = cf.gravity * mt / (cf.boxsize * cf.boxsize);
 	}
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16, s));
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 8, s));
-	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ctx->ev[0]));
 	double *cnt = ctx->counters;
 	if (tpl == 1) TVG_CHECK((launch_pair<1, F>(ctx, p, ewald, mlp, mass_f, last_f, cnt)));
 	else if (tpl == 2) TVG_CHECK((launch_pair<2, F>(ctx, p, ewald, mlp, mass_f, last_f, cnt)));
 	else TVG_CHECK((launch_pair<4, F>(ctx, p, ewald, mlp, mass_f, last_f, cnt)));
-	TVG_CUDA(ctx, cudaEventRecord(ctx->ev[2], s));
+	TVG_CUDA(ctx, tvg_record(ctx, ctx->ev[2]));
+	if (ctx->capturing) return TVG_OK;
+	return tvg_walk_group_results(ctx);
+}
+
+// walk and Ewald-walk times and interaction counts of the last group walk
+// (synchronises)
+int tvg_walk_group_results(tvg_context *ctx)
+{
 	TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[2]));
 	float ms = 0, ms_e = 0;
 	TVG_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));

@@ -392,13 +392,14 @@ int tvg_impl_walk_plain(tvg_context *ctx, int use_bh, uint32_t parts)
 	return walk_typed<double>(ctx, use_bh, parts);
 }
 
-// accel.c:28-43: Last_Acc_Mag = |Acc|, Acc = 0 (the active particles)
+// accel.c:28-43: Last_Acc_Mag = |Acc|, Acc = 0 (the active particles; their
+// number from the device when n_dev is given, n bounds it)
 template <typename F>
-__global__ void k_save_last(int64_t n, const int32_t *__restrict__ active, F *a0, F *a1, F *a2,
-                            F *last)
+__global__ void k_save_last(int64_t n, const int64_t *__restrict__ n_dev, const int32_t *__restrict__ active,
+                            F *a0, F *a1, F *a2, F *last)
 {
 	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (k >= n) return;
+	if (k >= n || (n_dev && k >= *n_dev)) return;
 	const int64_t i = active ? active[k] : k;
 	last[i] = fsqrt<F>(a0[i] * a0[i] + a1[i] * a1[i] + a2[i] * a2[i]);
 	a0[i] = a1[i] = a2[i] = 0;
@@ -406,16 +407,19 @@ __global__ void k_save_last(int64_t n, const int32_t *__restrict__ active, F *a0
 
 int tvg_impl_save_last_accel(tvg_context *ctx)
 {
-	const int64_t n = ctx->use_active ? ctx->n_active : ctx->n;
+	// with an active list its length is read on the device (the list may be
+	// built in the same captured step)
+	const int64_t n = ctx->n;
 	const int32_t *act = ctx->use_active ? ctx->active : nullptr;
+	const int64_t *nd = ctx->use_active ? &ctx->dc->n_active : nullptr;
 	if (!n) return TVG_OK;
 	if (ctx->cfg.float_bytes == 4)
 		k_save_last<float><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
-		    n, act, (float *) ctx->f[FS_ACC0], (float *) ctx->f[FS_ACC1], (float *) ctx->f[FS_ACC2],
+		    n, nd, act, (float *) ctx->f[FS_ACC0], (float *) ctx->f[FS_ACC1], (float *) ctx->f[FS_ACC2],
 		    (float *) ctx->f[FS_LAST_ACC]);
 	else
 		k_save_last<double><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, ctx->stream>>>(
-		    n, act, (double *) ctx->f[FS_ACC0], (double *) ctx->f[FS_ACC1], (double *) ctx->f[FS_ACC2],
+		    n, nd, act, (double *) ctx->f[FS_ACC0], (double *) ctx->f[FS_ACC1], (double *) ctx->f[FS_ACC2],
 		    (double *) ctx->f[FS_LAST_ACC]);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;

@@ -359,6 +359,15 @@ class GravityContext:
                                                       C.c_int32(ewald_kind), C.c_int32(int(prepare))),
                     "compute_acceleration")
 
+    def step_graph(self, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE):
+        """compute_acceleration (group form, no prepare pass) as one CUDA
+        graph launch; the first call of a configuration runs directly."""
+        self._check(self.lib.tvg_step_graph(self.ctx, C.c_uint32(parts), C.c_int32(ewald_kind)),
+                    "step_graph")
+
+    def step_graph_reset(self):
+        self._check(self.lib.tvg_step_graph_reset(self.ctx), "step_graph_reset")
+
     def autotune(self, use_bh=False, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE):
         """Chooses the group size of the group form (1, 2 or 4 targets per lane)
         by timing the walks on the current tree; returns (choice, [ms1, ms2, ms4])."""
