@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nside", type=int, default=256)
+    ap.add_argument("--box-mpc", type=float, default=100.0, help="box side, Mpc/h")
+    ap.add_argument("--tpl", type=int, default=0, choices=[0, 1, 2, 4],
+                    help="targets per lane of the group walk (0: autotune)")
     ap.add_argument("--plain-stride", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -177,9 +180,23 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def make_ics(nside, seed):
+def make_ics(nside, seed, box_mpc=100.0):
     from tandav_b200 import ics
-    return ics.zeldovich_box(n_side=nside, seed=seed)
+    return ics.zeldovich_box(n_side=nside, box_mpc=box_mpc, seed=seed)
+
+
+def device_memory_used_gb(index):
+    """Device memory in use on the GPU (NVML), GB."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            return round(pynvml.nvmlDeviceGetMemoryInfo(h).used / 1e9, 2)
+        finally:
+            pynvml.nvmlShutdown()
+    except Exception:         # no NVML on the host: not reported
+        return None
 
 
 def cpu_reference(p, cores, target_s=20.0):
@@ -214,7 +231,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    p = make_ics(args.nside, 1234)
+    p = make_ics(args.nside, 1234, args.box_mpc)
     cb, err = cpu_reference(p, cores)
     if cb is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
@@ -258,7 +275,7 @@ def rung_run(args, p, G, device):
         ctx.timer_start()
         ctx.compute_acceleration(form=G.FORM_GROUP, parts=parts, prepare=True)
         prep_ms = ctx.timer_stop()
-        tpl, _ = ctx.autotune(use_bh=False, parts=parts)
+        tpl = args.tpl or ctx.autotune(use_bh=False, parts=parts)[0]
         steps = []
         for _ in range(args.rung_steps):
             st = ctx.timeline()
@@ -298,7 +315,7 @@ def rung_run(args, p, G, device):
 def workload_config(args, p, ws):
     return {
         "workload": f"zeldovich_{args.nside}^3_periodic_z50",
-        "n_particles": int(p.n), "box_mpc_h": 100.0, "z_start": 50.0,
+        "n_particles": int(p.n), "box_mpc_h": args.box_mpc, "z_start": 50.0,
         "softening_kpc_h": round(float(p.softening), 4),
         "criterion": (f"relative, TREE_OPEN_PARAM_REL {args.open_rel:g} (group form), "
                       f"{args.plain_open_rel:g} (plain form); |a_old| first from a BH (theta^2 "
@@ -314,7 +331,7 @@ def workload_config(args, p, ws):
                  "walks) as one captured CUDA graph launch (tvg_step_graph); |a_old| from the "
                  "previous step"),
         "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-        "l2": "inputs larger than L2 (16.7M particles, ~2 GB of particle state)",
+        "l2": f"inputs larger than L2 ({p.n / 1e6:.1f}M particles, ~{p.n * 120 / 1e9:.1f} GB of particle state)",
     }
 
 
@@ -324,9 +341,11 @@ def main():
         return run_reference_arm(args)
     ws, rank, local = dist_info()
     dist = Dist(ws)
+    if args.tpl:
+        os.environ["TVG_GROUP_TPL"] = str(args.tpl)
     from tandav_b200 import gravity as G
 
-    p = make_ics(args.nside, 1234 + rank)
+    p = make_ics(args.nside, 1234 + rank, args.box_mpc)
     n = p.n
     ctx = G.GravityContext(n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
                            device=local)
@@ -342,7 +361,10 @@ def main():
     ctx.save_last_accel()
     ctx.set_opening(0.25, args.open_rel)
     ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
-    tune_choice, tune_ms = ctx.autotune(use_bh=False, parts=parts)
+    if args.tpl:              # group size fixed (TVG_GROUP_TPL, set before the first walk)
+        tune_choice, tune_ms = args.tpl, None
+    else:
+        tune_choice, tune_ms = ctx.autotune(use_bh=False, parts=parts)
     # warm-up: the first graph step runs directly, the next two capture the
     # step for the two buffer states the sort alternates between
     for _ in range(max(args.warmup, 3)):
@@ -367,6 +389,7 @@ def main():
     total_ms = ctx.timer_stop()
     launches = ctx.launch_count() - l0
     clk = clocks.stop()
+    hbm_gb = device_memory_used_gb(local)
     dist.barrier()
     t_step = dist.max(total_ms / args.steps) / 1e3
     value = dist.sum(n) / t_step
@@ -551,9 +574,11 @@ def main():
                            "evaluation": "Taylor-table K, dK, d2K: 15 float4 loads, ~200 FP32 ops"},
             "plain_form": plain,
             "learned_ewald": learned,
+            "device_memory_used_gb": hbm_gb,
             "accuracy": accuracy,
             "autotune": {"targets_per_lane": tune_choice,
-                         "walk_ms_1_2_4_targets_per_lane": [round(x, 1) for x in tune_ms]},
+                         "walk_ms_1_2_4_targets_per_lane": (None if tune_ms is None
+                                                             else [round(x, 1) for x in tune_ms])},
             "rung_run": rungs,
         }
         print(json.dumps(out))
