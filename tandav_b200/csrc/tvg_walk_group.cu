@@ -66,9 +66,10 @@
 #define GW_ELIST 64
 #define GW_DEFAULT_TPL 2
 // resident blocks per SM the Ewald walk is compiled for; capping its
-// registers for 3 or 4 blocks made it slower (1340, 1442 ms against 1252 ms
-// per step at 256^3): the table gathers need the registers more than the SM
-// needs the warps
+// registers for 3 or 4 blocks made it slower, with the tricubic lookup
+// (1340, 1442 ms against 1252 ms per step at 256^3) and with the Taylor table
+// (3 blocks at 168 registers: 140.4 against 136.9 ms at 128^3): the loads in
+// flight need the registers more than the SM needs the warps
 #ifndef GW_EWALD_MINB
 #define GW_EWALD_MINB 1
 #endif
