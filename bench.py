@@ -46,8 +46,12 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "tree-force particles/s at 256^3 periodic: chosen vs plain GPU form @≤1e-3 rms err"
 UNIT = "particles/s"
-FLOP_PER_GRAV = 20.0      # per monopole / particle interaction (SURVEY measurement convention)
-FLOP_PER_EWALD = 60.0     # per table-Ewald interaction
+# flop counted per interaction (a fixed convention shared by both forms):
+# monopole / particle pair = 3 sub, 5 for r^2, rsqrt, 2 for r^-3, mass,
+# 6 for the accumulation, 2 for the criterion; table Ewald = fold and three
+# 8-corner trilinear interpolations
+FLOP_PER_GRAV = 20.0
+FLOP_PER_EWALD = 60.0
 
 
 def parse():

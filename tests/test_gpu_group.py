@@ -3,9 +3,10 @@ against FP64 direct summation (Ewald-summed in the periodic box) with the
 reference's softened kernel, and agreement with the plain form.
 
 Tolerances: the relative criterion at errtol 0.005 gives rms relative errors
-~1e-3 in the reference (SURVEY probe); the group tests are conservative for
-the whole group, so their rms error must stay at or below the plain form's
-(with 20 % slack) and below 1e-3 where the plain form is below it."""
+~1e-3 in the reference (its own walk, run on small boxes); the group tests
+are conservative for the whole group, so their rms error must stay at or
+below the plain form's (with 20 % slack) and below 1e-3 where the plain form
+is below it."""
 import numpy as np
 import pytest
 
