@@ -1,6 +1,8 @@
 // tvg_step.cu -- one tree-force evaluation on device-resident particles, with
 // per-phase CUDA-event timing on the context stream; and the same evaluation
 // captured as a CUDA graph (tvg_step_graph).
+#include <string.h>
+
 #include "tvg_internal.cuh"
 
 extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
@@ -200,17 +202,43 @@ void tvg_graph_release(tvg_context *ctx)
 	ctx->graph_warm_key = 0;
 }
 
-// the configuration a graph is valid for
+static uint64_t mix(uint64_t k, uint64_t v)
+{
+	k ^= v + 0x9E3779B97F4A7C15ull + (k << 6) + (k >> 2);
+	return k;
+}
+
+static uint64_t mix_d(uint64_t k, double v)
+{
+	uint64_t b;
+	memcpy(&b, &v, 8);
+	return mix(k, b);
+}
+
+// the configuration a graph is valid for: everything the captured launches
+// were given by value (a change forces a direct step and new captures)
 static uint64_t graph_key(const tvg_context *ctx, uint32_t parts, int32_t ewald_kind)
 {
+	const tvg_config &c = ctx->cfg;
 	uint64_t k = 1;
-	k = k * 1000003u + parts;
-	k = k * 1000003u + (uint32_t) ewald_kind;
-	k = k * 1000003u + (uint32_t) ctx->group_tpl;
-	k = k * 1000003u + (ctx->have_timeline ? 1u : 0u);
-	k = k * 1000003u + (uint64_t) ctx->n;
-	k = k * 1000003u + (ctx->mlp_ok ? 1u : 0u);
-	return k;
+	k = mix(k, parts);
+	k = mix(k, (uint32_t) ewald_kind);
+	k = mix(k, (uint32_t) ctx->group_tpl);
+	k = mix(k, ctx->have_timeline ? 1u : 0u);
+	k = mix(k, (uint64_t) ctx->n);
+	k = mix(k, ctx->mlp_ok ? 1u : 0u);
+	k = mix(k, (uint64_t) c.flags);
+	k = mix(k, (uint64_t) c.vector_size);
+	k = mix_d(k, c.open_rel);
+	k = mix_d(k, c.open_bh);
+	k = mix_d(k, c.gravity);
+	k = mix_d(k, c.softening);
+	k = mix_d(k, c.boxsize);
+	k = mix_d(k, ctx->ewald_open_rel);
+	k = mix_d(k, ctx->ewald_open_bh);
+	k = mix_d(k, ctx->dsize);
+	for (int d = 0; d < 3; d++) k = mix_d(k, ctx->origin[d]);
+	return k ? k : 1;
 }
 
 static int capture(tvg_context *ctx, uint32_t parts, int32_t ewald_kind, uint64_t key,

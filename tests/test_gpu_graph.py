@@ -89,3 +89,29 @@ def test_graph_step_in_the_step_loop():
     finally:
         direct.close()
         graph.close()
+
+
+def test_graph_follows_parameter_changes():
+    # the opening parameters are passed to the captured kernels by value: a
+    # change must give a new capture, not a replay with the old values
+    p = ics.zeldovich_box(n_side=32, seed=43)
+    direct, graph = _ctx(p), _ctx(p)
+    try:
+        for c in (direct, graph):
+            c.upload(p.pos, p.mass)
+            c.compute_acceleration(form=G.FORM_GROUP, parts=PARTS, prepare=True)
+        for setting in (None, ("open", 0.25, 5e-4), ("ewald", 1e-3, 0.5), None):
+            if setting and setting[0] == "open":
+                for c in (direct, graph):
+                    c.set_opening(setting[1], setting[2])
+            elif setting:
+                for c in (direct, graph):
+                    c.set_ewald_opening(setting[1], setting[2])
+            for _ in range(3):          # a direct step, then the two captures / replays
+                direct.compute_acceleration(form=G.FORM_GROUP, parts=PARTS)
+                graph.step_graph(PARTS)
+                _same(direct.download(FIELDS), graph.download(FIELDS))
+                assert direct.walk_counters() == graph.walk_counters()
+    finally:
+        direct.close()
+        graph.close()
