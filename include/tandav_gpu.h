@@ -63,7 +63,14 @@ enum {
 	 * VECTOR_SIZE particles) that the walk reaches below the top level, as the
 	 * reference's walks do (tree_accel.c:221-243). Default: such a bundle is a
 	 * monopole like any other node when the opening criterion accepts it. */
-	TVG_CFG_OPEN_BUNDLES = 2
+	TVG_CFG_OPEN_BUNDLES = 2,
+	/* GRAVITY_POTENTIAL: the plain form also computes Grav_Pot (the Dehnen K1
+	 * potential of interact(), tree_accel.c:362-389, plus G m times the
+	 * trilinear lookup of the Ewald potential table, Gravity/periodic.c:
+	 * 115-170, tree_periodic.c:439-447), in the reference's sign convention
+	 * (+G m / r). The group form computes no potential and refuses a walk
+	 * while this flag is set. */
+	TVG_CFG_POTENTIAL = 4
 };
 
 /* Host view of struct Particle_Data (src/Gravity/../particles.h:17-37). Any
@@ -83,6 +90,7 @@ typedef struct {
 	void *grav_acc[3];
 	void *last_acc_mag;
 	int32_t *tree_parent;
+	void *grav_pot;        /* Grav_Pot (TVG_CFG_POTENTIAL) */
 } tvg_particles;
 
 enum {
@@ -90,7 +98,9 @@ enum {
 	TVG_F_IT_KICK = 1 << 3, TVG_F_KEY = 1 << 4, TVG_F_ID = 1 << 5, TVG_F_COST = 1 << 6,
 	TVG_F_POS = 1 << 7, TVG_F_VEL = 1 << 8, TVG_F_ACC = 1 << 9, TVG_F_MASS = 1 << 10,
 	TVG_F_GRAV_ACC = 1 << 11, TVG_F_LAST_ACC = 1 << 12, TVG_F_TREE_PARENT = 1 << 13,
-	TVG_F_ALL = (1 << 14) - 1
+	TVG_F_ALL = (1 << 14) - 1,
+	/* not in TVG_F_ALL: the reference has Grav_Pot only with GRAVITY_POTENTIAL */
+	TVG_F_GRAV_POT = 1 << 14
 };
 
 /* Top node as dumped from union Domain_Node_List (src/domain.h:40-52). */

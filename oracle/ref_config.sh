@@ -2,7 +2,7 @@
 # Generate the reference's config.h for one oracle variant from its own Config
 # file, the same way the reference Makefile does (Makefile:94-96: strip
 # comments/blank lines, prefix "#define"), after switching the hot-path options.
-#   $1 = reference Config file, $2 = variant (iso|per|perc)_(f32|f64)[_t], $3 = out
+#   $1 = reference Config file, $2 = variant (iso|per|perc)_(f32|f64)[_t|_pot], $3 = out
 set -e
 cfg="$1"; variant="$2"; out="$3"
 geom=${variant%%_*}
@@ -20,5 +20,7 @@ case "$geom" in
   *) echo "bad variant $variant" >&2; exit 1 ;;
 esac
 if [ "$prec" = "f64" ]; then echo "DOUBLE_PRECISION" >> "$tmp"; fi
+# suffix _pot: the gravitational potential (GRAVITY_POTENTIAL)
+case "$variant" in *_pot*) echo "GRAVITY_POTENTIAL" >> "$tmp" ;; esac
 sed '/^#/d; /^[[:space:]]*$/d; s/^/#define /g' "$tmp" > "$out"
 rm -f "$tmp"

@@ -150,6 +150,9 @@ static void load_particles(const struct input *in)
 			P.Grav_Acc[k][i] = 0;
 		}
 		P.Mass[i] = (Float) in->mass[i];
+#ifdef GRAVITY_POTENTIAL
+		P.Grav_Pot[i] = 0;
+#endif
 		P.Last_Acc_Mag[i] = 0;
 		P.Tree_Parent[i] = 0;
 	}
@@ -162,10 +165,14 @@ static void zero_accumulators(void)
 		P.Acc[0][i] = P.Acc[1][i] = P.Acc[2][i] = 0;
 		P.Grav_Acc[0][i] = P.Grav_Acc[1][i] = P.Grav_Acc[2][i] = 0;
 		P.Cost[i] = 0;
+#ifdef GRAVITY_POTENTIAL
+		P.Grav_Pot[i] = 0;
+#endif
 	}
 }
 
-/* Dump Acc/Grav_Acc/Cost as doubles under a name prefix. */
+/* Dump Acc/Grav_Acc/Cost (and Grav_Pot with GRAVITY_POTENTIAL) as doubles
+ * under a name prefix. */
 static void dump_forces(const char *prefix, int64_t n)
 {
 	if (!Dump_Bulk) return;
@@ -185,6 +192,12 @@ static void dump_forces(const char *prefix, int64_t n)
 		buf[i] = P.Cost[i];
 	snprintf(name, 16, "%s_cost", prefix);
 	put(name, buf, n * sizeof(double));
+#ifdef GRAVITY_POTENTIAL
+	for (int64_t i = 0; i < n; i++)
+		buf[i] = P.Grav_Pot[i];
+	snprintf(name, 16, "%s_pot", prefix);
+	put(name, buf, n * sizeof(double));
+#endif
 	free(buf);
 }
 

@@ -203,6 +203,7 @@ static void *host_field(const tvg_particles *p, int slot)
 	case FS_GACC0: case FS_GACC1: case FS_GACC2: return p->grav_acc[slot - FS_GACC0];
 	case FS_LAST_ACC: return p->last_acc_mag;
 	case FS_TREE_PARENT: return p->tree_parent;
+	case FS_GRAV_POT: return p->grav_pot;
 	}
 	return nullptr;
 }
@@ -223,6 +224,7 @@ static uint32_t slot_bit(int slot)
 	case FS_GACC0: case FS_GACC1: case FS_GACC2: return TVG_F_GRAV_ACC;
 	case FS_LAST_ACC: return TVG_F_LAST_ACC;
 	case FS_TREE_PARENT: return TVG_F_TREE_PARENT;
+	case FS_GRAV_POT: return TVG_F_GRAV_POT;
 	}
 	return 0;
 }

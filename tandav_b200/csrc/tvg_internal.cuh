@@ -222,7 +222,7 @@ enum {
 	FS_TYPE = 0, FS_TIME_BIN, FS_IT_DRIFT, FS_IT_KICK, FS_ID, FS_COST,
 	FS_POS0, FS_POS1, FS_POS2, FS_VEL0, FS_VEL1, FS_VEL2,
 	FS_ACC0, FS_ACC1, FS_ACC2, FS_MASS, FS_GACC0, FS_GACC1, FS_GACC2,
-	FS_LAST_ACC, FS_TREE_PARENT, FS_NFIELDS
+	FS_LAST_ACC, FS_TREE_PARENT, FS_GRAV_POT, FS_NFIELDS
 };
 
 int tvg_fail(tvg_context *ctx, int code, const char *fmt, ...);

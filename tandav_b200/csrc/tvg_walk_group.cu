@@ -1322,6 +1322,9 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		return tvg_fail(ctx, TVG_E_BADINPUT,
 		                "group form: the gravity and Ewald parts share the particle images; "
 		                "pass TVG_WALK_GRAVITY | TVG_WALK_EWALD");
+	if (ctx->cfg.flags & TVG_CFG_POTENTIAL)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "group form: no potential (TVG_CFG_POTENTIAL); use "
+		                "TVG_FORM_PLAIN");
 	const bool mlp = ewald && ewald_kind == TVG_EWALD_MLP;
 	if (ewald && ewald_kind != TVG_EWALD_TABLE && ewald_kind != TVG_EWALD_MLP)
 		return tvg_fail(ctx, TVG_E_BADINPUT, "unknown Ewald kind %d", ewald_kind);

@@ -8,6 +8,10 @@
 // kept as in the reference: the sign flip of quirk Q1).
 // Ewald part: Gravity_Tree_Periodic (tree_periodic.c:23-450) with the
 // trilinear table lookup of Ewald_Correction (Gravity/periodic.c:35-113).
+// With TVG_CFG_POTENTIAL (GRAVITY_POTENTIAL) the potential of interact()
+// (tree_accel.c:362-389) and of interact_with_ewald_cube (tree_periodic.c:
+// 425-447, Ewald_Potential at Gravity/periodic.c:115-170) are summed in double
+// as the reference's Recv.Grav_Potential.
 // This file is compiled with -fmad=false: every expression rounds in the
 // reference's order (float/double promotion as in C), so given the same tree
 // the accelerations are the reference's bit for bit.
@@ -28,7 +32,7 @@ template <typename F> struct WNode {
 
 struct PlainParams {
 	double gravity, domain_size, boxsize, open_bh, open_rel;
-	double eps2, eps3, box2grid;
+	double eps, eps2, eps3, box2grid;
 	int periodic, use_bh, vsize, ntop, fix_small;
 };
 
@@ -36,7 +40,7 @@ template <typename F> struct PlainCtx {
 	const F *x, *y, *z, *m;
 	const tvg_topnode *top;
 	const WNode<F> *tree;
-	const F *fx, *fy, *fz;
+	const F *fx, *fy, *fz, *fp;
 	F boxhalf;
 	PlainParams p;
 };
@@ -56,23 +60,32 @@ template <typename F> __device__ __forceinline__ F fsqrt(F v);
 template <> __device__ __forceinline__ float fsqrt<float>(float v) { return __fsqrt_rn(v); }
 template <> __device__ __forceinline__ double fsqrt<double>(double v) { return __dsqrt_rn(v); }
 
-// interact(), tree_accel.c:362-394
-template <typename F>
+// interact(), tree_accel.c:362-394; with POT the potential fac_pot, whose
+// inner polynomial is the reference's (u2 * (175 - (u2 * 147 - u2 * 45))
+// - 105) / (32 Epsilon), summed into pot
+template <bool POT, typename F>
 __device__ __forceinline__ void interact(const PlainCtx<F> &c, F mass, const F dr[3], F r2,
-                                         double acc[3], F &cost)
+                                         double acc[3], F &cost, double &pot)
 {
 	F fac = (F) (c.p.gravity * mass);
+	F fac_pot = fac;
 	if (r2 < c.p.eps2) {
 		F u2 = (F) (r2 / c.p.eps2);
 		F poly = (F) 175 - u2 * ((F) 294 - u2 * (F) 135);
 		fac = (F) (fac * (poly / (16 * c.p.eps3)));
+		if (POT) {
+			const F ppoly = u2 * ((F) 175 - (u2 * (F) 147 - u2 * (F) 45)) - (F) 105;
+			fac_pot = (F) (fac_pot * (ppoly / (32 * c.p.eps)));
+		}
 	} else {
 		F r_inv = (F) 1 / fsqrt<F>(r2);
 		fac *= r_inv * r_inv * r_inv;
+		if (POT) fac_pot *= r_inv;
 	}
 	acc[0] += fac * dr[0];
 	acc[1] += fac * dr[1];
 	acc[2] += fac * dr[2];
+	if (POT) pot += fac_pot;
 	cost += 1;
 }
 
@@ -82,8 +95,9 @@ __device__ __forceinline__ F node_size(const PlainCtx<F> &c, int lvl)
 	return (F) (c.p.domain_size / (double) (F) (1ULL << lvl));
 }
 
-template <typename F>
-__device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double acc[3], F &cost)
+template <bool POT, typename F>
+__device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double acc[3], F &cost,
+                             double &pot)
 {
 	const F fac = (F) (sacc / c.p.gravity * c.p.open_rel);
 	for (int j = 0; j < c.p.ntop; j++) {
@@ -102,7 +116,7 @@ __device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double
 			bool open;
 			if (c.p.use_bh) open = (double) (nsize * nsize) > r2 * c.p.open_bh;
 			else open = nmass * nsize * nsize > r2 * r2 * fac;
-			if (!open) { interact(c, nmass, dr, r2, acc, cost); continue; }
+			if (!open) { interact<POT>(c, nmass, dr, r2, acc, cost, pot); continue; }
 		}
 		if (t.npart <= c.p.vsize) {
 			const int64_t f0 = c.p.fix_small ? t.first_part : t.target;
@@ -110,7 +124,7 @@ __device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double
 				F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
 				nearest(c, d);
 				F r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-				if (r2 != 0) interact(c, c.m[jp], d, r2, acc, cost);
+				if (r2 != 0) interact<POT>(c, c.m[jp], d, r2, acc, cost, pot);
 			}
 			continue;
 		}
@@ -126,7 +140,7 @@ __device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double
 					F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
 					nearest(c, d);
 					F r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-					if (r2 != 0) interact(c, c.m[jp], d, r2, acc, cost);
+					if (r2 != 0) interact<POT>(c, c.m[jp], d, r2, acc, cost, pot);
 				}
 				node++;
 				continue;
@@ -145,7 +159,7 @@ __device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double
 				if (fabs((double) ds[0]) < 0.6 * nsz && fabs((double) ds[1]) < 0.6 * nsz
 				    && fabs((double) ds[2]) < 0.6 * nsz) { node++; continue; }
 			}
-			interact(c, nmass, d, r2, acc, cost);
+			interact<POT>(c, nmass, d, r2, acc, cost, pot);
 			node += dn;
 		}
 	}
@@ -186,9 +200,35 @@ __device__ __forceinline__ void ewald_corr(const PlainCtx<F> &c, const F dr[3], 
 	f[2] *= sg[2];
 }
 
+// Ewald_Potential, Gravity/periodic.c:115-170: trilinear in double on the
+// potential table at |dr|, the result stored as Float
 template <typename F>
+__device__ __forceinline__ F ewald_pot(const PlainCtx<F> &c, const F dr[3])
+{
+	const double dx = fabs((double) dr[0]), dy = fabs((double) dr[1]), dz = fabs((double) dr[2]);
+	double u = dx * c.p.box2grid, v = dy * c.p.box2grid, w = dz * c.p.box2grid;
+	int i = (int) u, j = (int) v, k = (int) w;
+	if (i >= 64) i = 63;
+	if (j >= 64) j = 63;
+	if (k >= 64) k = 63;
+	u -= i;
+	v -= j;
+	w -= k;
+	const double wt[8] = { (1 - u) * (1 - v) * (1 - w), (1 - u) * (1 - v) * w,
+	                       (1 - u) * v * (1 - w), (1 - u) * v * w,
+	                       u * (1 - v) * (1 - w), u * (1 - v) * w,
+	                       u * v * (1 - w), u * v * w };
+	const int64_t b = ((int64_t) i * 65 + j) * 65 + k;
+	const F *T = c.fp;
+	return (F) (wt[0] * T[b] + wt[1] * T[b + 1] + wt[2] * T[b + 65] + wt[3] * T[b + 66]
+	            + wt[4] * T[b + 65 * 65] + wt[5] * T[b + 65 * 65 + 1] + wt[6] * T[b + 65 * 65 + 65]
+	            + wt[7] * T[b + 65 * 65 + 66]);
+}
+
+// interact_with_ewald_cube, tree_periodic.c:425-447
+template <bool POT, typename F>
 __device__ __forceinline__ void ewald_cube(const PlainCtx<F> &c, const F dr[3], F mass, double acc[3],
-                                           F &cost)
+                                           F &cost, double &pot)
 {
 	F r[3];
 	ewald_corr(c, dr, r);
@@ -196,10 +236,12 @@ __device__ __forceinline__ void ewald_cube(const PlainCtx<F> &c, const F dr[3], 
 	acc[1] += c.p.gravity * mass * r[1];
 	acc[2] += c.p.gravity * mass * r[2];
 	cost += 1;
+	if (POT) pot += c.p.gravity * mass * ewald_pot(c, dr);
 }
 
-template <typename F>
-__device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double acc[3], F &cost)
+template <bool POT, typename F>
+__device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double acc[3], F &cost,
+                           double &pot)
 {
 	const double box = c.p.boxsize;
 	const F fac = (F) (sacc / c.p.gravity * c.p.open_rel);
@@ -232,13 +274,13 @@ __device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double a
 			    || nsize > 0.2 * box)
 				open = true;
 		}
-		if (!open) { ewald_cube(c, dr, (F) t.mass, acc, cost); continue; }
+		if (!open) { ewald_cube<POT>(c, dr, (F) t.mass, acc, cost, pot); continue; }
 		if (t.npart <= c.p.vsize) {
 			const int64_t f0 = c.p.fix_small ? t.first_part : t.target;
 			for (int64_t jp = f0; jp < f0 + t.npart; jp++) {
 				F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
 				nearest(c, d);
-				if (d[0] != 0 && d[1] != 0 && d[2] != 0) ewald_cube(c, d, c.m[jp], acc, cost);
+				if (d[0] != 0 && d[1] != 0 && d[2] != 0) ewald_cube<POT>(c, d, c.m[jp], acc, cost, pot);
 			}
 			continue;
 		}
@@ -254,7 +296,7 @@ __device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double a
 				for (int64_t jp = f; jp < f + np; jp++) {
 					F d[3] = { c.x[jp] - sp[0], c.y[jp] - sp[1], c.z[jp] - sp[2] };
 					nearest(c, d);
-					if (d[0] != 0 && d[1] != 0 && d[2] != 0) ewald_cube(c, d, c.m[jp], acc, cost);
+					if (d[0] != 0 && d[1] != 0 && d[2] != 0) ewald_cube<POT>(c, d, c.m[jp], acc, cost, pot);
 				}
 				node++;
 				continue;
@@ -280,17 +322,17 @@ __device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double a
 				if (fabs((double) ds[0]) > dl || fabs((double) ds[1]) > dl || fabs((double) ds[2]) > dl
 				    || nsz > 0.2 * box) { node++; continue; }
 			}
-			ewald_cube(c, d, nmass, acc, cost);
+			ewald_cube<POT>(c, d, nmass, acc, cost, pot);
 			node += dn;
 		}
 	}
 }
 
-template <typename F>
+template <bool POT, typename F>
 __global__ void __launch_bounds__(128)
 k_walk_plain(int64_t n_act, const int32_t *__restrict__ active, PlainCtx<F> c, int ewald,
              const F *__restrict__ last_acc, F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1,
-             F *gacc2, F *cost_out, double *counter)
+             F *gacc2, F *cost_out, F *pot_out, double *counter)
 {
 	__shared__ tvg_topnode s_top[TVG_MAX_TOP];
 	for (int j = threadIdx.x; j < c.p.ntop; j += blockDim.x) s_top[j] = c.top[j];
@@ -302,9 +344,9 @@ k_walk_plain(int64_t n_act, const int32_t *__restrict__ active, PlainCtx<F> c, i
 	if (t < n_act) {
 		const int64_t i = active ? active[t] : t;     // Active_Particle_List[t]
 		const F sp[3] = { c.x[i], c.y[i], c.z[i] };
-		double a[3] = { 0, 0, 0 };
-		if (ewald) walk_ewald(cc, sp, last_acc[i], a, cost);
-		else walk_gravity(cc, sp, last_acc[i], a, cost);
+		double a[3] = { 0, 0, 0 }, pot = 0;
+		if (ewald) walk_ewald<POT>(cc, sp, last_acc[i], a, cost, pot);
+		else walk_gravity<POT>(cc, sp, last_acc[i], a, cost, pot);
 		// add_recv_to (tree_accel.c:110-129, tree_periodic.c:91-110)
 		acc0[i] += a[0];
 		acc1[i] += a[1];
@@ -314,11 +356,13 @@ k_walk_plain(int64_t n_act, const int32_t *__restrict__ active, PlainCtx<F> c, i
 			gacc1[i] += a[1];
 			gacc2[i] += a[2];
 			cost_out[i] += cost;
+			if (POT) pot_out[i] += pot;
 		} else {
 			gacc0[i] = (F) a[0];
 			gacc1[i] = (F) a[1];
 			gacc2[i] = (F) a[2];
 			cost_out[i] = cost;
+			if (POT) pot_out[i] = (F) pot;
 		}
 	}
 	// interaction count for the roofline accounting
@@ -343,6 +387,7 @@ static int walk_typed(tvg_context *ctx, int use_bh, uint32_t parts)
 	c.fx = (const F *) ctx->ewald_f[0];
 	c.fy = (const F *) ctx->ewald_f[1];
 	c.fz = (const F *) ctx->ewald_f[2];
+	c.fp = (const F *) ctx->ewald_f[3];
 	const tvg_config &cf = ctx->cfg;
 	c.p.gravity = cf.gravity;
 	c.p.domain_size = ctx->dsize;
@@ -350,6 +395,7 @@ static int walk_typed(tvg_context *ctx, int use_bh, uint32_t parts)
 	c.p.open_bh = cf.open_bh;
 	c.p.open_rel = cf.open_rel;
 	const double eps = -41.0 / 32.0 * cf.softening;    // tree_build.c:136-138
+	c.p.eps = eps;
 	c.p.eps2 = eps * eps;
 	c.p.eps3 = eps * eps * eps;
 	c.p.box2grid = cf.periodic ? 2 * 64 / cf.boxsize : 0;
@@ -366,12 +412,14 @@ static int walk_typed(tvg_context *ctx, int use_bh, uint32_t parts)
 		if (!(parts & (ew ? TVG_WALK_EWALD : TVG_WALK_GRAVITY))) continue;
 		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[0], s));
 		const int64_t n_act = ctx->use_active ? ctx->n_active : n;
-		k_walk_plain<F><<<TVG_CNT(ctx, tvg_blocks(n_act, 128)), 128, 0, s>>>(
+		const bool pot = (cf.flags & TVG_CFG_POTENTIAL) != 0;
+		auto kern = pot ? k_walk_plain<true, F> : k_walk_plain<false, F>;
+		kern<<<TVG_CNT(ctx, tvg_blocks(n_act, 128)), 128, 0, s>>>(
 		    n_act, ctx->use_active ? ctx->active : nullptr, c, ew ? 1 : 0,
 		    (const F *) ctx->f[FS_LAST_ACC], (F *) ctx->f[FS_ACC0],
 		    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0],
 		    (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2], (F *) ctx->f[FS_COST],
-		    ctx->counters + (ew ? 1 : 0));
+		    (F *) ctx->f[FS_GRAV_POT], ctx->counters + (ew ? 1 : 0));
 		TVG_CUDA(ctx, cudaGetLastError());
 		TVG_CUDA(ctx, cudaEventRecord(ctx->ev[1], s));
 		TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
@@ -457,7 +505,7 @@ int tvg_impl_zero_accel(tvg_context *ctx)
 		return TVG_OK;
 	}
 	const size_t b = tvg_fsize(ctx) * ctx->n;
-	const int slots[] = { FS_ACC0, FS_ACC1, FS_ACC2, FS_GACC0, FS_GACC1, FS_GACC2, FS_COST };
+	const int slots[] = { FS_ACC0, FS_ACC1, FS_ACC2, FS_GACC0, FS_GACC1, FS_GACC2, FS_COST, FS_GRAV_POT };
 	for (int s : slots) TVG_CUDA(ctx, cudaMemsetAsync(ctx->f[s], 0, b, ctx->stream));
 	return TVG_OK;
 }

@@ -24,9 +24,11 @@ EWALD_TABLE, EWALD_MLP = 0, 1
 BUILD_EXACT_MOMENTS = 1
 CFG_FIX_SMALL_TOPNODES = 1
 CFG_OPEN_BUNDLES = 2
+CFG_POTENTIAL = 4              # the plain form computes Grav_Pot
 
 F_TYPE, F_TIME_BIN, F_IT_DRIFT, F_IT_KICK, F_KEY, F_ID, F_COST = (1 << k for k in range(7))
 F_POS, F_VEL, F_ACC, F_MASS, F_GRAV_ACC, F_LAST_ACC, F_TREE_PARENT = (1 << k for k in range(7, 14))
+F_GRAV_POT = 1 << 14            # not in TVG_F_ALL
 
 # struct Tree_Node of the reference (src/Gravity/tree.h:23-32)
 TREE_DTYPE = {
@@ -52,7 +54,7 @@ class Particles(C.Structure):
                 ("it_kick_pos", C.c_void_p), ("key", C.c_void_p), ("id", C.c_void_p),
                 ("cost", C.c_void_p), ("pos", C.c_void_p * 3), ("vel", C.c_void_p * 3),
                 ("acc", C.c_void_p * 3), ("mass", C.c_void_p), ("grav_acc", C.c_void_p * 3),
-                ("last_acc_mag", C.c_void_p), ("tree_parent", C.c_void_p)]
+                ("last_acc_mag", C.c_void_p), ("tree_parent", C.c_void_p), ("grav_pot", C.c_void_p)]
 
 
 class TimelineConfig(C.Structure):
@@ -209,6 +211,7 @@ class GravityContext:
         for name, bit, dt in (("mass", F_MASS, ft), ("cost", F_COST, ft),
                               ("last_acc_mag", F_LAST_ACC, ft), ("id", F_ID, np.uint32),
                               ("tree_parent", F_TREE_PARENT, np.int32),
+                              ("grav_pot", F_GRAV_POT, ft),
                               ("time_bin", F_TIME_BIN, np.int32), ("type", F_TYPE, np.int32),
                               ("it_drift_pos", F_IT_DRIFT, np.uint32),
                               ("it_kick_pos", F_IT_KICK, np.uint32)):

@@ -4,7 +4,8 @@ The reference C sources are compiled unmodified by `make -C oracle ref` into
 oracle/_ref/<variant>/ref_harness; this script feeds them seeded inputs and
 stores their outputs (keys, sort permutation, top nodes, tree, Tree_Parent,
 accelerations of the BH and relative passes, Ewald parts) as compressed .npz
-files. Re-run after changing the inputs: `python tests/golden/make_golden.py`.
+files. Re-run after changing the inputs: `python tests/golden/make_golden.py`
+(`... make_golden.py potential` for the potential fixtures only).
 """
 from __future__ import annotations
 
@@ -55,7 +56,7 @@ def force_case(name, variant, p, flags=3):
                topnodes=r["topnodes"], tree=r["tree"], tree_parent=r["tree_parent"],
                last_acc_mag=r["last_acc_mag"])
     for part in ("bh", "rel", "bhew", "relew"):
-        for q in ("gacc", "acc", "cost"):
+        for q in ("gacc", "acc", "cost", "pot"):
             k = f"{part}_{q}"
             if k in r:
                 out[k] = r[k]
@@ -70,5 +71,17 @@ def main():
     force_case("zeldovich_per_f64", "per_f64", ics.zeldovich_box(n_side=20, seed=9))
 
 
+def potential_cases():
+    """The same inputs through the reference built with GRAVITY_POTENTIAL
+    (variants *_pot): forces and Grav_Pot of both passes."""
+    force_case("hernquist_iso_f64_pot", "iso_f64_pot", ics.hernquist(n=2048, seed=5))
+    force_case("hernquist_iso_f32_pot", "iso_f32_pot", ics.hernquist(n=2048, seed=6))
+    force_case("zeldovich_per_f64_pot", "per_f64_pot", ics.zeldovich_box(n_side=20, seed=9))
+
+
 if __name__ == "__main__":
-    main()
+    # `make_golden.py potential` writes only the potential fixtures
+    if sys.argv[1:] == ["potential"]:
+        potential_cases()
+    else:
+        main()

@@ -215,3 +215,39 @@ def test_state_errors():
         with pytest.raises(G.TvgError) as e:
             ctx.walk()                           # no tree
         assert e.value.code == 7
+
+
+POT_CASES = ["hernquist_iso_f64_pot", "hernquist_iso_f32_pot", "zeldovich_per_f64_pot"]
+
+
+@pytest.mark.parametrize("case", POT_CASES)
+def test_potential_matches_reference_golden(golden_dir, case):
+    """TVG_CFG_POTENTIAL: Grav_Pot of the plain form (gravity + Ewald) bit for
+    bit against the reference built with GRAVITY_POTENTIAL, both passes; the
+    forces stay the reference's; the group form refuses the flag."""
+    g = np.load(golden_dir / f"{case}.npz")
+    fsize = int(g["float_size"])
+    box = float(g["box"])
+    n = len(g["mass_in"])
+    with make_ctx(n, fsize, box=box, softening=float(g["softening"]), gravity=float(g["gravity"][0]),
+                  flags=G.CFG_POTENTIAL) as ctx:
+        perm, _, tree, _ = gpu_pipeline(ctx, g["pos_in"], g["mass_in"], g["domain_origin"],
+                                        float(g["domain_size"][0]))
+        assert np.array_equal(perm, g["perm"])
+        assert_struct_equal(tree, g["tree"], TREE_FIELDS, "tree")
+        parts = G.WALK_GRAVITY | (G.WALK_EWALD if box > 0 else 0)
+        if box > 0:
+            ctx.upload_ewald_table(*reference_table(fsize))
+        ctx.zero_accel()
+        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+        bh = ctx.download(G.F_GRAV_ACC | G.F_GRAV_POT)
+        ctx.save_last_accel()
+        ctx.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
+        rel = ctx.download(G.F_GRAV_ACC | G.F_GRAV_POT)
+        for name, got in (("bh", bh), ("rel", rel)):
+            a = got["grav_acc"].astype(np.float64)
+            assert np.array_equal(a, g[name + "_gacc"]), name
+            p, ref = got["grav_pot"].astype(np.float64), g[name + "_pot"]
+            assert np.array_equal(p, ref), f"{name}: max diff {np.abs(p - ref).max()}"
+        with pytest.raises(G.TvgError):
+            ctx.walk(G.FORM_GROUP, use_bh=False, parts=parts)

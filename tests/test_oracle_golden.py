@@ -81,3 +81,16 @@ def test_ewald_table_matches_reference_formula():
     assert np.allclose(f, np.array(ref), rtol=0, atol=1e-15)
     fneg = port.ewald_force(-np.array(pts), nreal=4, nk=4)
     assert np.allclose(fneg, -f, atol=1e-12)
+
+
+@pytest.mark.parametrize("case", ["hernquist_iso_f64", "hernquist_iso_f32", "zeldovich_per_f64"])
+def test_potential_build_changes_nothing_else(golden_dir, case):
+    """The reference built with GRAVITY_POTENTIAL (the *_pot fixtures) gives
+    the same keys, order, tree and forces as without it, plus Grav_Pot."""
+    a = np.load(golden_dir / f"{case}.npz")
+    b = np.load(golden_dir / f"{case}_pot.npz")
+    shared = [k for k in a.files if k in b.files]
+    assert {"perm", "tree", "bh_gacc", "rel_gacc"} <= set(shared)
+    for k in shared:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.all(np.isfinite(b["bh_pot"])) and np.all(np.isfinite(b["rel_pot"]))
