@@ -93,8 +93,10 @@ def tree_build(rev_sorted, pos_sorted, mass_sorted, domain_size, top, fsize=4):
 
 
 def walk(kind, pos_sorted, mass_sorted, last_acc, top, tree, params: WalkParams,
-         ewald_tables=None, fsize=4):
-    """kind = 'gravity' | 'ewald'; returns (acc (3, n) float64, cost (n,))."""
+         ewald_tables=None, fsize=4, potential=False):
+    """kind = 'gravity' | 'ewald'; returns (acc (3, n) float64, cost (n,)),
+    and with potential=True also the double sum of the potential terms (for
+    'ewald' the fourth table of ewald_tables is the potential table)."""
     ft = ftype(fsize)
     x, y, z = (np.ascontiguousarray(pos_sorted[k], dtype=ft) for k in range(3))
     m = np.ascontiguousarray(mass_sorted, dtype=ft)
@@ -104,16 +106,19 @@ def walk(kind, pos_sorted, mass_sorted, last_acc, top, tree, params: WalkParams,
     cost = np.zeros(n)
     top = np.ascontiguousarray(top)
     tree = np.ascontiguousarray(tree)
+    pot = np.zeros(n) if potential else None
     if kind == "gravity":
-        lib().tvo_walk_gravity(C.c_int64(n), C.c_int32(fsize), _p(x), _p(y), _p(z), _p(m),
-                               _p(la), _p(top), C.c_int32(len(top)), _p(tree),
-                               C.byref(params), _p(acc), _p(cost))
+        lib().tvo_walk_gravity_pot(C.c_int64(n), C.c_int32(fsize), _p(x), _p(y), _p(z), _p(m),
+                                   _p(la), _p(top), C.c_int32(len(top)), _p(tree),
+                                   C.byref(params), _p(acc), _p(cost), _p(pot))
     else:
-        fx, fy, fz = (np.ascontiguousarray(t, dtype=ft) for t in ewald_tables)
-        lib().tvo_walk_ewald(C.c_int64(n), C.c_int32(fsize), _p(x), _p(y), _p(z), _p(m),
-                             _p(la), _p(top), C.c_int32(len(top)), _p(tree),
-                             C.byref(params), _p(fx), _p(fy), _p(fz), _p(acc), _p(cost))
-    return acc, cost
+        tabs = [np.ascontiguousarray(t, dtype=ft) for t in ewald_tables]
+        fp = tabs[3] if potential else None
+        lib().tvo_walk_ewald_pot(C.c_int64(n), C.c_int32(fsize), _p(x), _p(y), _p(z), _p(m),
+                                 _p(la), _p(top), C.c_int32(len(top)), _p(tree),
+                                 C.byref(params), _p(tabs[0]), _p(tabs[1]), _p(tabs[2]), _p(fp),
+                                 _p(acc), _p(cost), _p(pot))
+    return (acc, cost, pot) if potential else (acc, cost)
 
 
 def ewald_table(n_ewald=64, potential=False):

@@ -130,10 +130,20 @@ void tvo_walk_gravity(int64_t n, int32_t fsize, const void *x, const void *y, co
                       int32_t ntop, const void *tree, const tvo_walk_params *prm, double *acc,
                       double *cost)
 {
+	tvo_walk_gravity_pot(n, fsize, x, y, z, mass, last_acc, top, ntop, tree, prm, acc, cost, NULL);
+}
+
+void tvo_walk_gravity_pot(int64_t n, int32_t fsize, const void *x, const void *y, const void *z,
+                          const void *mass, const void *last_acc, const tvo_topnode *top,
+                          int32_t ntop, const void *tree, const tvo_walk_params *prm, double *acc,
+                          double *cost, double *pot)
+{
 	if (fsize == 4)
-		walk_all_f32(n, x, y, z, mass, last_acc, top, ntop, tree, prm, NULL, NULL, NULL, 0, acc, cost);
+		walk_all_f32(n, x, y, z, mass, last_acc, top, ntop, tree, prm, NULL, NULL, NULL, NULL, 0,
+		             acc, cost, pot);
 	else
-		walk_all_f64(n, x, y, z, mass, last_acc, top, ntop, tree, prm, NULL, NULL, NULL, 0, acc, cost);
+		walk_all_f64(n, x, y, z, mass, last_acc, top, ntop, tree, prm, NULL, NULL, NULL, NULL, 0,
+		             acc, cost, pot);
 }
 
 void tvo_walk_ewald(int64_t n, int32_t fsize, const void *x, const void *y, const void *z,
@@ -141,10 +151,21 @@ void tvo_walk_ewald(int64_t n, int32_t fsize, const void *x, const void *y, cons
                     const void *tree, const tvo_walk_params *prm, const void *fx, const void *fy,
                     const void *fz, double *acc, double *cost)
 {
+	tvo_walk_ewald_pot(n, fsize, x, y, z, mass, last_acc, top, ntop, tree, prm, fx, fy, fz, NULL, acc,
+	                   cost, NULL);
+}
+
+void tvo_walk_ewald_pot(int64_t n, int32_t fsize, const void *x, const void *y, const void *z,
+                        const void *mass, const void *last_acc, const tvo_topnode *top, int32_t ntop,
+                        const void *tree, const tvo_walk_params *prm, const void *fx, const void *fy,
+                        const void *fz, const void *fp, double *acc, double *cost, double *pot)
+{
 	if (fsize == 4)
-		walk_all_f32(n, x, y, z, mass, last_acc, top, ntop, tree, prm, fx, fy, fz, 1, acc, cost);
+		walk_all_f32(n, x, y, z, mass, last_acc, top, ntop, tree, prm, fx, fy, fz, fp, 1, acc, cost,
+		             pot);
 	else
-		walk_all_f64(n, x, y, z, mass, last_acc, top, ntop, tree, prm, fx, fy, fz, 1, acc, cost);
+		walk_all_f64(n, x, y, z, mass, last_acc, top, ntop, tree, prm, fx, fy, fz, fp, 1, acc, cost,
+		             pot);
 }
 
 /*

@@ -87,6 +87,23 @@ void tvo_walk_ewald(int64_t n, int32_t fsize, const void *x, const void *y,
                     const void *ewald_fy, const void *ewald_fz, double *acc,
                     double *cost);
 
+/* The two walks with GRAVITY_POTENTIAL: pot[i] = the double sum of the
+ * potential terms of particle i (interact(), tree_accel.c:362-389;
+ * interact_with_ewald_cube with Ewald_Potential, tree_periodic.c:439-447,
+ * Gravity/periodic.c:115-170; ewald_fp is the potential table divided by
+ * Boxsize). pot may be NULL. */
+void tvo_walk_gravity_pot(int64_t n, int32_t fsize, const void *x, const void *y,
+                          const void *z, const void *mass, const void *last_acc,
+                          const tvo_topnode *top, int32_t ntop, const void *tree,
+                          const tvo_walk_params *prm, double *acc, double *cost,
+                          double *pot);
+void tvo_walk_ewald_pot(int64_t n, int32_t fsize, const void *x, const void *y,
+                        const void *z, const void *mass, const void *last_acc,
+                        const tvo_topnode *top, int32_t ntop, const void *tree,
+                        const tvo_walk_params *prm, const void *ewald_fx,
+                        const void *ewald_fy, const void *ewald_fz, const void *ewald_fp,
+                        double *acc, double *cost, double *pot);
+
 /* compute_ewald_force / compute_ewald_potential (Gravity/periodic.c:235-461)
  * in box units on the (N_EWALD+1)^3 octant grid, FP64 (not yet divided by
  * Boxsize^2 / Boxsize). */

@@ -94,3 +94,39 @@ def test_potential_build_changes_nothing_else(golden_dir, case):
     for k in shared:
         assert np.array_equal(a[k], b[k]), k
     assert np.all(np.isfinite(b["bh_pot"])) and np.all(np.isfinite(b["rel_pot"]))
+
+
+@pytest.mark.parametrize("case", ["hernquist_iso_f64_pot", "hernquist_iso_f32_pot",
+                                  "zeldovich_per_f64_pot"])
+def test_oracle_potential_matches_reference(golden_dir, case):
+    """The restatement's potential (port.walk(potential=True)) against the
+    reference built with GRAVITY_POTENTIAL, both passes, bit for bit: the
+    gravity pass assigns Grav_Pot (tree_accel.c:122-124), the Ewald pass adds
+    to it (tree_periodic.c:103-105)."""
+    g = np.load(golden_dir / f"{case}.npz")
+    fsize = int(g["float_size"])
+    ft = port.ftype(fsize)
+    box = float(g["box"])
+    pos = g["pos_in"].astype(ft)[:, g["perm"]]
+    mass = g["mass_in"].astype(ft)[g["perm"]]
+    prm = port.WalkParams(gravity=float(g["gravity"][0]), softening=float(g["softening"]),
+                          domain_size=float(g["domain_size"][0]), boxsize=box, open_bh=0.25,
+                          open_rel=0.005, use_bh=1, vector_size=64)
+    tabs = None
+    if box > 0:
+        fx, fy, fz, fp = port.ewald_table(potential=True)
+        tabs = [(t.astype(ft).astype(np.float64) / (box * box)).astype(ft) for t in (fx, fy, fz)]
+        tabs.append((fp.astype(ft).astype(np.float64) / box).astype(ft))
+    for name, use_bh, last in (("bh", 1, np.zeros(len(mass), ft)),
+                               ("rel", 0, g["last_acc_mag"].astype(ft))):
+        prm.use_bh = use_bh
+        _, _, pg = port.walk("gravity", pos, mass, last, g["topnodes"], g["tree"], prm,
+                             fsize=fsize, potential=True)
+        pot = pg.astype(ft)
+        if box > 0:
+            _, _, pe = port.walk("ewald", pos, mass, last, g["topnodes"], g["tree"], prm, tabs,
+                                 fsize=fsize, potential=True)
+            pot = (pot.astype(np.float64) + pe).astype(ft)
+        ref = g[name + "_pot"]
+        assert np.array_equal(pot.astype(np.float64), ref), \
+            f"{name}: max diff {np.abs(pot.astype(np.float64) - ref).max()}"
