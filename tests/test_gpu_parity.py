@@ -251,3 +251,50 @@ def test_potential_matches_reference_golden(golden_dir, case):
             assert np.array_equal(p, ref), f"{name}: max diff {np.abs(p - ref).max()}"
         with pytest.raises(G.TvgError):
             ctx.walk(G.FORM_GROUP, use_bh=False, parts=parts)
+
+
+@pytest.mark.parametrize("kind,fsize,n", [("hernquist", 8, 32768), ("zeldovich", 4, 32 ** 3)])
+def test_potential_vs_oracle(kind, fsize, n):
+    """TVG_CFG_POTENTIAL at larger sizes against the restatement
+    (port.walk(potential=True), itself pinned to the reference's golden
+    potential): the plain form's Grav_Pot bit for bit, both passes. In FP32
+    with the Ewald part both take the separation in double (the reference
+    leaves that case undefined)."""
+    p, origin, size = make_case(kind, n)
+    ft = port.ftype(fsize)
+    o = oracle_pipeline(p.pos, p.mass, origin, size, fsize, box=p.box, softening=p.softening,
+                        passes=())
+    prm = port.WalkParams(gravity=43007.1, softening=p.softening, domain_size=size, boxsize=p.box,
+                          open_bh=0.25, open_rel=0.005, use_bh=1, vector_size=64)
+    tabs = None
+    if p.box > 0:
+        fx, fy, fz, fpt = reference_table(fsize)
+        tabs = [(t.astype(np.float64) / (p.box * p.box)).astype(ft) for t in (fx, fy, fz)]
+        tabs.append((fpt.astype(np.float64) / p.box).astype(ft))
+
+    def oracle_pass(use_bh, last):
+        prm.use_bh = use_bh
+        _, _, pg = port.walk("gravity", o["pos"], o["mass"], last, o["top"], o["tree"], prm,
+                             fsize=fsize, potential=True)
+        pot = pg.astype(ft)
+        if p.box > 0:
+            _, _, pe = port.walk("ewald", o["pos"], o["mass"], last, o["top"], o["tree"], prm, tabs,
+                                 fsize=fsize, potential=True)
+            pot = (pot.astype(np.float64) + pe).astype(ft)
+        return pot
+
+    with make_ctx(p.n, fsize, box=p.box, softening=p.softening, flags=G.CFG_POTENTIAL) as ctx:
+        gpu_pipeline(ctx, p.pos, p.mass, origin, size)
+        parts = G.WALK_GRAVITY | (G.WALK_EWALD if p.box > 0 else 0)
+        if p.box > 0:
+            ctx.upload_ewald_table(*reference_table(fsize))
+        ctx.zero_accel()
+        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+        bh = ctx.download(G.F_GRAV_POT)["grav_pot"]
+        ctx.save_last_accel()
+        last = ctx.download(G.F_LAST_ACC)["last_acc_mag"]
+        ctx.walk(G.FORM_PLAIN, use_bh=False, parts=parts)
+        rel = ctx.download(G.F_GRAV_POT)["grav_pot"]
+    for name, got, ref in (("bh", bh, oracle_pass(1, np.zeros(p.n, ft))),
+                           ("rel", rel, oracle_pass(0, last.astype(ft)))):
+        assert np.array_equal(got, ref), f"{name}: max diff {np.abs(got.astype(float) - ref).max()}"
