@@ -441,6 +441,42 @@ int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, double *t);
  * the max error is at most max_allowed. */
 int tvg_ewald_mlp_judge(tvg_context *ctx, double max_allowed, double *max_err, double *rms_err);
 
+/* ---------------------------------------------------------- snapshots */
+
+/* Header of a Gadget format-2 snapshot (struct gadget_header, IO/io.h:24-44):
+ * particles per type in this file and in the simulation, mass per type (0:
+ * the MASS block holds it), Time, Redshift (the reference writes
+ * 1/Time - 1 with COMOVING), the number of files, and the box and cosmology
+ * constants. */
+typedef struct {
+	uint32_t npart[6];
+	uint64_t nall[6];
+	double massarr[6];
+	double time;
+	double redshift;
+	int32_t num_files;
+	double boxsize, omega0, omega_lambda, hubble_param;
+} tvg_snapshot_header;
+
+/* Optional blocks after POS, VEL, ID, MASS (IO/io.h:69-84). */
+enum {
+	TVG_SNAP_ACC = 1,      /* "ACC ": one component, Acc[0], as the reference's table declares */
+	TVG_SNAP_GACC = 2,     /* "GACC": Grav_Acc[3] (OUTPUT_PARTIAL_ACCELERATIONS) */
+	TVG_SNAP_GPOT = 4      /* "GPOT": Grav_Pot (OUTPUT_GRAV_POTENTIAL) */
+};
+
+/* Write_Snapshot (IO/write_snapshot.c:13-328) for one rank and one file:
+ * the header and the blocks in the reference's format (4-byte Fortran record
+ * markers, format-2 label records, 32-bit IDs, fields interleaved per
+ * particle) of the n particles in the host arrays of p (Float of
+ * float_bytes). The header's 64 fill and padding bytes are written as zero. */
+int tvg_write_snapshot_host(const char *path, const tvg_snapshot_header *header, int64_t n,
+                            int32_t float_bytes, const tvg_particles *p, uint32_t blocks);
+/* The same for the context's particles, downloaded from the device in their
+ * current order (PH order after a sort, as the reference writes them). */
+int tvg_write_snapshot(tvg_context *ctx, const char *path, const tvg_snapshot_header *header,
+                       uint32_t blocks);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,8 @@ case "$geom" in
   *) echo "bad variant $variant" >&2; exit 1 ;;
 esac
 if [ "$prec" = "f64" ]; then echo "DOUBLE_PRECISION" >> "$tmp"; fi
-# suffix _pot: the gravitational potential (GRAVITY_POTENTIAL)
-case "$variant" in *_pot*) echo "GRAVITY_POTENTIAL" >> "$tmp" ;; esac
+# suffix _pot: the gravitational potential (GRAVITY_POTENTIAL) and its
+# snapshot block (OUTPUT_GRAV_POTENTIAL, which changes nothing but the I/O)
+case "$variant" in *_pot*) printf 'GRAVITY_POTENTIAL\nOUTPUT_GRAV_POTENTIAL\n' >> "$tmp" ;; esac
 sed '/^#/d; /^[[:space:]]*$/d; s/^/#define /g' "$tmp" > "$out"
 rm -f "$tmp"

@@ -414,10 +414,48 @@ static int run_force(const struct input *in)
 	return 0;
 }
 
+/* Write_Snapshot (IO/write_snapshot.c:13-60) of the input particles in
+ * input order, to "<output>_000", with Acc[k] = (k+1) Pos[k] and
+ * Grav_Acc[k] = (k+2) Vel[k] (and Grav_Pot = Pos[0] - 3 Mass). In this mode the input's size field is
+ * Time.Current and box is Sim.Boxsize; the Cosmo constants (compile-time in
+ * the reference) are reported as the record "cosmo" in <output>. */
+static int run_snap(const struct input *in, const char *out_base)
+{
+	int64_t n = in->n;
+	set_particle_counts(n);
+	sizeof_P = 0;
+	for (int i = 0; i < NP_Fields; i++) sizeof_P += P_Fields[i].Bytes * P_Fields[i].N;
+	init_memory(n);
+	Allocate_Particle_Structures();
+	load_particles(in);
+	for (int64_t i = 0; i < n; i++)    /* distinct per component, for the ACC/GACC blocks */
+		for (int k = 0; k < 3; k++) {
+			P.Acc[k][i] = (Float) ((k + 1) * in->pos[k * n + i]);
+			P.Grav_Acc[k][i] = (Float) ((k + 2) * in->vel[k * n + i]);
+		}
+#ifdef GRAVITY_POTENTIAL
+	for (int64_t i = 0; i < n; i++) P.Grav_Pot[i] = (Float) (in->pos[i] - 3 * in->mass[i]);
+#endif
+	for (int t = 0; t < NPARTYPE; t++) Sim.Mpart[t] = 0;
+	Sim.Boxsize[0] = Sim.Boxsize[1] = Sim.Boxsize[2] = in->box;
+	Time.Current = in->size;
+	Time.NSnap = 10;
+	Time.Snap_Counter = 0;
+	Param.Num_Output_Files = 1;
+	Param.Num_IO_Tasks = 1;
+	snprintf(Param.Output_File_Base, sizeof(Param.Output_File_Base), "%s", out_base);
+	Write_Snapshot();
+	double cosmo[3] = { Cosmo.Omega_0, Cosmo.Omega_Lambda, Cosmo.Hubble_Constant };
+	put("cosmo", cosmo, sizeof(cosmo));
+	int32_t fsize = (int32_t) sizeof(Float);
+	put("float_size", &fsize, 4);
+	return 0;
+}
+
 int main(int argc, char *argv[])
 {
 	if (argc != 4) {
-		fprintf(stderr, "usage: %s force|keys input.bin output.bin\n", argv[0]);
+		fprintf(stderr, "usage: %s force|keys|snap input.bin output.bin\n", argv[0]);
 		return 1;
 	}
 	preamble();
@@ -429,6 +467,8 @@ int main(int argc, char *argv[])
 		rc = run_keys(&in);
 	else if (!strcmp(argv[1], "force"))
 		rc = run_force(&in);
+	else if (!strcmp(argv[1], "snap"))
+		rc = run_snap(&in, argv[3]);
 	fclose(Out);
 	return rc;
 }

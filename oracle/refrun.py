@@ -98,7 +98,12 @@ def run(variant: str, mode: str, pos, vel=None, mass=None, box=0.0, softening=0.
             raise RuntimeError(f"ref_harness failed ({proc.returncode}): "
                                f"{proc.stderr.decode()[-2000:]}{proc.stdout.decode()[-2000:]}")
         rec = read_output(fout)
-    return decode(rec, n)
+        snap = Path(str(fout) + "_000")
+        snap_bytes = snap.read_bytes() if mode == "snap" and snap.exists() else None
+    out = decode(rec, n)
+    if snap_bytes is not None:
+        out["snapshot"] = snap_bytes       # the file Write_Snapshot wrote
+    return out
 
 
 def decode(rec: dict, n: int) -> dict:

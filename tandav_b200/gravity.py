@@ -89,6 +89,76 @@ class MlpTrainConfig(C.Structure):
 
 MLP_NPARAM = 4672
 
+# optional blocks of a snapshot after POS, VEL, ID, MASS (src/IO/io.h:74-85)
+SNAP_ACC, SNAP_GACC, SNAP_GPOT = 1, 2, 4
+
+
+class SnapshotHeader(C.Structure):
+    """struct gadget_header of the reference (src/IO/io.h:24-44), less its fill."""
+    _fields_ = [("npart", C.c_uint32 * 6), ("nall", C.c_uint64 * 6), ("massarr", C.c_double * 6),
+                ("time", C.c_double), ("redshift", C.c_double), ("num_files", C.c_int32),
+                ("boxsize", C.c_double), ("omega0", C.c_double), ("omega_lambda", C.c_double),
+                ("hubble_param", C.c_double)]
+
+
+def snapshot_header(npart, time, boxsize, omega0=1.0, omega_lambda=0.0, hubble_param=0.7,
+                    comoving=True, nall=None, massarr=None, num_files=1):
+    """Header as Write_Snapshot fills it (src/IO/write_snapshot.c:183-219).
+
+    ``npart`` / ``nall`` are six per-type counts (an int means all type 1);
+    Redshift is 1/Time - 1 for a comoving run and 0 otherwise."""
+    def six(v):
+        return [0, int(v), 0, 0, 0, 0] if np.isscalar(v) else [int(x) for x in v]
+    h = SnapshotHeader()
+    h.npart[:] = six(npart)
+    h.nall[:] = six(npart if nall is None else nall)
+    h.massarr[:] = [0.0] * 6 if massarr is None else [float(m) for m in massarr]
+    h.time = time
+    h.redshift = 1.0 / time - 1.0 if comoving else 0.0
+    h.num_files = num_files
+    h.boxsize, h.omega0, h.omega_lambda, h.hubble_param = boxsize, omega0, omega_lambda, hubble_param
+    return h
+
+
+def write_snapshot_host(path, header, pos, vel, ids, mass, acc=None, grav_acc=None,
+                        grav_pot=None):
+    """Write a snapshot of host arrays (tvg_write_snapshot_host): pos, vel
+    (and acc, grav_acc) shaped (3, n), ids uint32, all Floats of one width."""
+    ft = np.asarray(pos).dtype
+    n = np.asarray(mass).shape[0]
+
+    def f(a, shape):
+        a = np.ascontiguousarray(a, dtype=ft)
+        assert a.shape == shape, (a.shape, shape)
+        return a
+
+    keep = [f(pos, (3, n)), f(vel, (3, n)), np.ascontiguousarray(ids, dtype=np.uint32),
+            f(mass, (n,))]
+    p = Particles()
+    for k in range(3):
+        p.pos[k] = keep[0][k].ctypes.data
+        p.vel[k] = keep[1][k].ctypes.data
+    p.id, p.mass = keep[2].ctypes.data, keep[3].ctypes.data
+    blocks = 0
+    if acc is not None:
+        keep.append(f(acc, (3, n)))
+        for k in range(3):
+            p.acc[k] = keep[-1][k].ctypes.data
+        blocks |= SNAP_ACC
+    if grav_acc is not None:
+        keep.append(f(grav_acc, (3, n)))
+        for k in range(3):
+            p.grav_acc[k] = keep[-1][k].ctypes.data
+        blocks |= SNAP_GACC
+    if grav_pot is not None:
+        keep.append(f(grav_pot, (n,)))
+        p.grav_pot = keep[-1].ctypes.data
+        blocks |= SNAP_GPOT
+    rc = lib().tvg_write_snapshot_host(str(path).encode(), C.byref(header), C.c_int64(n),
+                                       C.c_int32(ft.itemsize), C.byref(p), C.c_uint32(blocks))
+    if rc != TVG_OK:
+        raise TvgError(rc, f"tvg_write_snapshot_host({path})")
+
 
 class TvgError(RuntimeError):
     def __init__(self, code, msg):
@@ -494,6 +564,11 @@ class GravityContext:
         self._check(self.lib.tvg_upload(self.ctx, C.c_int64(n), C.byref(p), C.c_uint32(fields)),
                     "upload")
         self.n = n
+
+    def write_snapshot(self, path, header, blocks=0):
+        """Write_Snapshot of the resident particles in their device order."""
+        self._check(self.lib.tvg_write_snapshot(self.ctx, str(path).encode(), C.byref(header),
+                                                C.c_uint32(blocks)), "write_snapshot")
 
     def download_into(self, grav_acc=None, ids=None):
         """Download into pre-allocated (e.g. pinned) arrays."""

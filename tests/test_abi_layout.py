@@ -17,7 +17,8 @@ ROOT = Path(__file__).resolve().parents[1]
 
 STRUCTS = [("tvg_config", G.Config), ("tvg_particles", G.Particles),
            ("tvg_timeline_config", G.TimelineConfig), ("tvg_timeline_state", G.TimelineState),
-           ("tvg_mlp_train_config", G.MlpTrainConfig)]
+           ("tvg_mlp_train_config", G.MlpTrainConfig),
+           ("tvg_snapshot_header", G.SnapshotHeader)]
 
 
 def _c_layout(tmp_path):

@@ -1,0 +1,139 @@
+"""Snapshot output (Write_Snapshot, src/IO/write_snapshot.c:13-328): the
+library's writer against the file the reference's own Write_Snapshot writes
+for the same particles (the reference harness, mode "snap", which also sets
+Acc[k] = (k+1) Pos[k], Grav_Acc[k] = (k+2) Vel[k] and Grav_Pot = Pos[0] -
+3 Mass so that every block carries distinct data).
+
+Byte for byte, except the header's 64 fill and padding bytes (the reference
+leaves them unset) and, without COMOVING, Redshift (also unset there)."""
+import ctypes as C
+import struct
+
+import numpy as np
+import pytest
+
+from oracle import refrun
+from tandav_b200 import gravity as G
+
+HEAD = 20            # label record (16 bytes) + the record marker before the header
+
+
+def _blocks(buf: bytes):
+    """Format-2 blocks as (label, payload) with every marker checked."""
+    out, off = [], 0
+    while off < len(buf):
+        m0, label, size8, m1 = struct.unpack_from("<I4sII", buf, off)
+        assert (m0, m1) == (8, 8), off
+        off += 16
+        (a,) = struct.unpack_from("<I", buf, off)
+        assert a + 8 == size8, label
+        data = buf[off + 4:off + 4 + a]
+        (b,) = struct.unpack_from("<I", buf, off + 4 + a)
+        assert b == a, label
+        out.append((label.decode(), data))
+        off += 8 + a
+    return out
+
+
+def _particles(n, box, seed):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0, box, (3, n))
+    vel = rng.normal(0, 30.0, (3, n))
+    mass = rng.uniform(0.5, 1.5, n) / n
+    return pos, vel, mass
+
+
+def _fields(pos, vel, mass, ft, with_pot):
+    k = np.arange(1, 4)[:, None]
+    out = dict(pos=pos.astype(ft), vel=vel.astype(ft), ids=np.arange(pos.shape[1], dtype=np.uint32),
+               mass=mass.astype(ft), acc=(k * pos).astype(ft), grav_acc=((k + 1) * vel).astype(ft))
+    if with_pot:
+        out["grav_pot"] = (pos[0] - 3 * mass).astype(ft)
+    return out
+
+
+VARIANTS = [("perc_f32", True, False), ("per_f64", False, False), ("per_f64_pot", False, True),
+            ("iso_f32", False, False)]
+
+
+@pytest.mark.parametrize("variant,comoving,with_pot", VARIANTS)
+def test_snapshot_matches_reference_write_snapshot(tmp_path, variant, comoving, with_pot):
+    if not refrun.available(variant):
+        pytest.skip(f"oracle/_ref/{variant} not built")
+    n, box, time = 777, 100.0, 0.02
+    pos, vel, mass = _particles(n, box, seed=len(variant))
+    ref = refrun.run(variant, "snap", pos, vel, mass, box=box, size=time)
+    fb = ref["float_size"]
+    ft = np.float32 if fb == 4 else np.float64
+    om0, oml, hub = ref["cosmo"]
+    h = G.snapshot_header(n, time, box, om0, oml, hub, comoving=comoving)
+    f = _fields(pos, vel, mass, ft, with_pot)
+    path = tmp_path / "snap_000"
+    G.write_snapshot_host(path, h, f["pos"], f["vel"], f["ids"], f["mass"], acc=f["acc"],
+                          grav_acc=f["grav_acc"], grav_pot=f.get("grav_pot"))
+    ours, theirs = path.read_bytes(), ref["snapshot"]
+    labels = ["HEAD", "POS ", "VEL ", "ID  ", "MASS", "ACC ", "GACC"] + (["GPOT"] if with_pot else [])
+    assert [b[0] for b in _blocks(theirs)] == labels
+    assert [b[0] for b in _blocks(ours)] == labels
+    assert len(ours) == len(theirs)
+    mask = np.ones(len(ours), bool)
+    mask[HEAD + 192:HEAD + 256] = False
+    if not comoving:
+        mask[HEAD + 80:HEAD + 88] = False
+    a, b = np.frombuffer(ours, np.uint8), np.frombuffer(theirs, np.uint8)
+    bad = np.flatnonzero((a != b) & mask)
+    assert bad.size == 0, f"{bad.size} bytes differ, first at {bad[:8]}"
+    # the ACC block is one component, Acc[0], as the reference declares it
+    acc_block = dict(_blocks(ours))["ACC "]
+    np.testing.assert_array_equal(np.frombuffer(acc_block, ft), f["acc"][0])
+
+
+def test_snapshot_header_fields(tmp_path):
+    """Per-type counts, the 64-bit total split into Nall and Nall_High_Word,
+    Massarr, and zero fill; an empty snapshot still has every block."""
+    h = G.snapshot_header([0, 0, 0, 0, 0, 0], 0.5, 1000.0, 0.3, 0.7, 0.68,
+                          nall=[0, 5_000_000_000, 0, 0, 0, 3], massarr=[0, 2.5, 0, 0, 0, 0],
+                          num_files=4)
+    z = np.zeros((3, 0))
+    path = tmp_path / "empty"
+    G.write_snapshot_host(path, h, z, z, np.zeros(0, np.uint32), np.zeros(0))
+    blocks = _blocks(path.read_bytes())
+    assert [b[0] for b in blocks] == ["HEAD", "POS ", "VEL ", "ID  ", "MASS"]
+    assert all(len(b[1]) == 0 for b in blocks[1:])
+    head = blocks[0][1]
+    assert len(head) == 256
+    assert struct.unpack_from("<6I", head, 0) == (0,) * 6
+    assert struct.unpack_from("<6d", head, 24) == (0, 2.5, 0, 0, 0, 0)
+    assert struct.unpack_from("<dd", head, 72) == (0.5, 1.0)
+    assert struct.unpack_from("<6I", head, 96) == (0, 5_000_000_000 & 0xFFFFFFFF, 0, 0, 0, 3)
+    assert struct.unpack_from("<6I", head, 168) == (0, 5_000_000_000 >> 32, 0, 0, 0, 0)
+    assert struct.unpack_from("<ii", head, 88) == (0, 0)                  # Sfr, Feedback
+    assert struct.unpack_from("<ii", head, 120) == (0, 4)                 # Cooling, Num_Files
+    assert struct.unpack_from("<4d", head, 128) == (1000.0, 0.3, 0.7, 0.68)
+    assert struct.unpack_from("<ii", head, 160) == (0, 0)                 # Age, Metals
+    assert head[192:] == bytes(64)
+
+
+def test_snapshot_rejects_bad_requests(tmp_path):
+    """A requested block whose array is NULL, a Float width other than 4/8,
+    and an unwritable path are errors (TVG_E_BADINPUT), not crashes."""
+    lib = G.lib()
+    n = 8
+    pos = np.zeros((3, n), np.float32)
+    ids = np.arange(n, dtype=np.uint32)
+    mass = np.ones(n, np.float32)
+    p = G.Particles()
+    for k in range(3):
+        p.pos[k] = p.vel[k] = pos[k].ctypes.data
+    p.id, p.mass = ids.ctypes.data, mass.ctypes.data
+    h = G.snapshot_header(n, 1.0, 1.0)
+
+    def call(path, fb, blocks):
+        return lib.tvg_write_snapshot_host(str(path).encode(), C.byref(h), C.c_int64(n),
+                                           C.c_int32(fb), C.byref(p), C.c_uint32(blocks))
+
+    assert call(tmp_path / "ok", 4, 0) == G.TVG_OK
+    assert call(tmp_path / "gacc", 4, G.SNAP_GACC) == 5
+    assert call(tmp_path / "pot", 4, G.SNAP_GPOT) == 5
+    assert call(tmp_path / "fb", 2, 0) == 5
+    assert call(tmp_path / "no" / "such" / "dir", 4, 0) == 5
