@@ -21,6 +21,9 @@
  *   mode "force": the sequence above.
  *   mode "keys":  Peano_Key / Reversed_Peano_Key for the input positions with
  *                 the domain taken from the input header (no decomposition).
+ *   mode "update": "force" with the tree updates between rebuilds applied
+ *                 to the built tree before the walks (tree_update_sequence).
+ *   mode "snap":  Write_Snapshot of the input particles (run_snap).
  *
  * Input  (little endian): "TVIN", int32 version(1), int64 n, double box
  *   (<=0: isolated), double softening, double origin[3], double size,
@@ -232,7 +235,63 @@ static int run_keys(const struct input *in)
 	return 0;
 }
 
-static int run_force(const struct input *in)
+/* The top nodes and the tree under a name prefix ("<p>_top", "<p>_tree"). */
+static void dump_tree_state(const char *prefix)
+{
+	char name[16];
+	struct dump_topnode *tn = calloc(NTop_Nodes, sizeof(*tn));
+	for (uint32_t j = 0; j < NTop_Nodes; j++) {
+		tn[j].key = D[j].TNode.Key;
+		tn[j].target = D[j].TNode.Target;
+		tn[j].level = D[j].TNode.Level;
+		tn[j].first_part = D[j].TNode.First_Part;
+		tn[j].npart = D[j].TNode.Npart;
+		for (int k = 0; k < 3; k++) {
+			tn[j].pos[k] = D[j].TNode.Pos[k];
+			tn[j].com[k] = D[j].TNode.CoM[k];
+			tn[j].dp[k] = D[j].TNode.Dp[k];
+		}
+		tn[j].mass = D[j].TNode.Mass;
+	}
+	snprintf(name, 16, "%s_top", prefix);
+	put(name, tn, (int64_t) NTop_Nodes * sizeof(*tn));
+	free(tn);
+	snprintf(name, 16, "%s_tree", prefix);
+	put(name, Tree, (int64_t) NNodes * sizeof(struct Tree_Node));
+}
+
+/* Mode "update": the tree updates between rebuilds (Gravity/tree_update.c,
+ * called from kick.c:31-32,61-62 and drift.c:41-42) on the tree just built.
+ * Acc = Vel; the active particles are those with ID % 3 != 1, in index
+ * order; two kick passes of Gravity_Tree_Update_Kicks, with the Float kick
+ * step size * (1 + ID % 4) / 4 and then size * (1 + ID % 3) / 3; then
+ * Gravity_Tree_Update_Drift(origin[0]). The state after the kicks is dumped
+ * as "upk_*", after the drift as "upd_*"; the walks then run on the updated
+ * tree for all particles. */
+static void tree_update_sequence(const struct input *in, int64_t n)
+{
+	for (int64_t i = 0; i < n; i++)
+		for (int k = 0; k < 3; k++) P.Acc[k][i] = P.Vel[k][i];
+	int na = 0;
+	for (int64_t i = 0; i < n; i++)
+		if (P.ID[i] % 3 != 1) Active_Particle_List[na++] = (int) i;
+	for (int pass = 0; pass < 2; pass++) {
+		const int q = pass == 0 ? 4 : 3;
+		for (int j = 0; j < na; j++) {
+			const int ipart = Active_Particle_List[j];
+			const Float dt = (Float) (in->size * (1 + P.ID[ipart] % q) / q);
+			Gravity_Tree_Update_Kicks(ipart, dt);
+		}
+	}
+	dump_tree_state("upk");
+	#pragma omp parallel
+	Gravity_Tree_Update_Drift(in->origin[0]);
+	dump_tree_state("upd");
+	for (int64_t i = 0; i < n; i++) Active_Particle_List[i] = (int) i;
+	NActive_Particles = (int) n;
+}
+
+static int run_force(const struct input *in, bool update)
 {
 	int64_t n = in->n;
 	bool periodic = in->box > 0;
@@ -339,6 +398,7 @@ static int run_force(const struct input *in)
 		int32_t fsize = (int32_t) sizeof(Float);
 		put("float_size", &fsize, 4);
 	}
+	if (update) tree_update_sequence(in, n);
 
 	#pragma omp parallel
 	{
@@ -455,7 +515,7 @@ static int run_snap(const struct input *in, const char *out_base)
 int main(int argc, char *argv[])
 {
 	if (argc != 4) {
-		fprintf(stderr, "usage: %s force|keys|snap input.bin output.bin\n", argv[0]);
+		fprintf(stderr, "usage: %s force|keys|snap|update input.bin output.bin\n", argv[0]);
 		return 1;
 	}
 	preamble();
@@ -466,7 +526,9 @@ int main(int argc, char *argv[])
 	if (!strcmp(argv[1], "keys"))
 		rc = run_keys(&in);
 	else if (!strcmp(argv[1], "force"))
-		rc = run_force(&in);
+		rc = run_force(&in, false);
+	else if (!strcmp(argv[1], "update"))
+		rc = run_force(&in, true);
 	else if (!strcmp(argv[1], "snap"))
 		rc = run_snap(&in, argv[3]);
 	fclose(Out);

@@ -114,9 +114,9 @@ def decode(rec: dict, n: int) -> dict:
             out[name] = keys_u128(buf)
         elif name in ("perm",):
             out[name] = np.frombuffer(buf, dtype="<u4").copy()
-        elif name == "tree":
+        elif name == "tree" or name.endswith("_tree"):
             out[name] = np.frombuffer(buf, dtype=TREE_DTYPE[fsize]).copy()
-        elif name == "topnodes":
+        elif name == "topnodes" or name.endswith("_top"):
             out[name] = np.frombuffer(buf, dtype=TOPNODE_DTYPE).copy()
         elif name == "tree_parent":
             out[name] = np.frombuffer(buf, dtype="<i4").copy()
