@@ -359,13 +359,29 @@ int tvg_kick_drift_factors(tvg_context *ctx, uint32_t it_curr, uint32_t it_next,
 int tvg_set_new_timesteps(tvg_context *ctx);
 /* Kick_First_Halfstep / Kick_Second_Halfstep (kick.c:9-70) over the active
  * particles; the second also ends the step (Sig.First_Step = false, as
- * Update(AFTER_STEP) does). The GPU path rebuilds the tree every force
- * computation, so the node kicks of the reference have no counterpart. */
+ * Update(AFTER_STEP) does). After tvg_time_for_domain_update, and while no
+ * domain update is due, each kick also adds the particles' momentum to the
+ * kept tree (Gravity_Tree_Update_Kicks, tree_update.c:12-54): Dp of every
+ * node above them and of their top node, summed in particle order. */
 int tvg_kick_first_halfstep(tvg_context *ctx);
 int tvg_kick_second_halfstep(tvg_context *ctx);
 /* Drift_To_Sync_Point (drift.c:12-62): drifts the active particles to
- * Int_Time.Next, wraps all particles into the box, advances the clock. */
+ * Int_Time.Next, wraps all particles into the box, advances the clock; with
+ * tree updates and no domain update due, moves the kicked nodes by
+ * Time.Step * Dp (Gravity_Tree_Update_Drift, tree_update.c:62-101). */
 int tvg_drift_to_sync_point(tvg_context *ctx);
+/* Time_For_Domain_Update (signal.c:85-116): adds NActive_Particles to the
+ * particle updates since the last domain decomposition; a decomposition (and
+ * a new tree) is due at a sync point or when they exceed
+ * domain_update_param * N (DOMAIN_UPDATE_PARAM, 0.1 in the reference's
+ * Config). *domain_update receives Sig.Domain_Update. The first call turns on
+ * the reference's tree updates between rebuilds for this context: until a
+ * due update, the kicks and the drift update the kept tree and
+ * tvg_compute_acceleration / tvg_step_graph walk it without keys, sort or
+ * build. A context that never calls it rebuilds at every force computation.
+ * The node sums follow the particle order, which is the order of the
+ * Active_Particle_List that Set_New_Timesteps makes. */
+int tvg_time_for_domain_update(tvg_context *ctx, double domain_update_param, int32_t *domain_update);
 /* Reads / replaces the timeline state (e.g. to restart). */
 int tvg_timeline_get(tvg_context *ctx, tvg_timeline_state *st);
 int tvg_timeline_set(tvg_context *ctx, const tvg_timeline_state *st);
@@ -376,7 +392,9 @@ int tvg_rung_histogram(tvg_context *ctx, int32_t *hist);
  * the Active_Particle_List, peano.c:42), top nodes, tree build, then for the
  * active particles safe_last_accel (Last_Acc_Mag = |Acc|, Acc = 0), with
  * prepare (Sig.Prepare_Step) a Barnes-Hut walk and safe_last_accel again, and
- * the relative-criterion walk. Without a timeline every particle is active. */
+ * the relative-criterion walk. Without a timeline every particle is active.
+ * With tree updates (tvg_time_for_domain_update) and no domain update due,
+ * the walks run on the kept, updated tree (accel.c:53). */
 int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t parts, int32_t ewald_kind,
                              int32_t prepare);
 /* tvg_compute_acceleration of the group form (prepare = 0) with the step's

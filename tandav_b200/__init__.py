@@ -30,7 +30,7 @@ EXPORTS = (
     "tvg_rung_histogram", "tvg_compute_acceleration", "tvg_step_graph", "tvg_step_graph_reset",
     "tvg_ewald_mlp_train",
     "tvg_ewald_mlp_weights", "tvg_ewald_mlp_grad", "tvg_ewald_mlp_eval", "tvg_ewald_mlp_judge",
-    "tvg_autotune", "tvg_write_snapshot", "tvg_write_snapshot_host",
+    "tvg_autotune", "tvg_write_snapshot", "tvg_write_snapshot_host", "tvg_time_for_domain_update",
 )
 
 

@@ -24,7 +24,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", str(ROOT / "include")]
 # translation units that replay the reference's rounding order
-NO_FMA = {"tvg_walk_plain.cu", "tvg_tree.cu", "tvg_ewald.cu", "tvg_keys.cu", "tvg_integrate.cu"}
+NO_FMA = {"tvg_walk_plain.cu", "tvg_tree.cu", "tvg_ewald.cu", "tvg_keys.cu", "tvg_integrate.cu",
+          "tvg_tree_update.cu"}
 # FP32 walks with no parity constraint: denormals flushed (rsqrtf and the
 # divisions then need no range fix-up around MUFU)
 FTZ = {"tvg_walk_group.cu"}

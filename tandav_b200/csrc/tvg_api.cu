@@ -37,6 +37,8 @@ int tvg_sync_status(tvg_context *ctx, const char *phase)
 		return tvg_fail(ctx, TVG_E_TIMEOUT, "%s: bounded device wait expired", phase);
 	if (st & TVG_ST_LIST_OVERFLOW)
 		return tvg_fail(ctx, TVG_E_TREE_FULL, "%s: interaction list overflow", phase);
+	if (st & TVG_ST_TREE_STALE)
+		return tvg_fail(ctx, TVG_E_STATE, "%s: the kept tree does not fit the particles", phase);
 	if (st & TVG_ST_TIMESTEP)
 		return tvg_fail(ctx, TVG_E_BADINPUT, "%s: time step below the integer timeline's resolution "
 		                "or not finite (timestep.c:219-222)", phase);
@@ -178,7 +180,7 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->ewald_ext, ctx->active, ctx->kd_x, ctx->kd_kick, ctx->kd_drift,
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
 	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
-	                 ctx->d_topinfo, ctx->d_topplace };
+	                 ctx->d_topinfo, ctx->d_topplace, ctx->tu_first, ctx->tu_dp };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

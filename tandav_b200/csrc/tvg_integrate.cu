@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "tvg_internal.cuh"
+#include "tvg_tree_update.cuh"
 
 #define KD_TABLE 512
 #define KD_GL 16
@@ -192,6 +193,28 @@ __global__ void k_kick(int64_t n_act, const int32_t *__restrict__ active, TimePa
 	v1[i] += dt * a1[i];
 	v2[i] += dt * a2[i];
 	it_kick[i] += it_step >> 1;
+}
+
+// the momentum change of each active particle for the tree updates
+// (tree_update.c:14-17), stored by its slot in particle order; taken with the
+// kick step of k_kick, before k_kick advances It_Kick_Pos
+template <typename F>
+__global__ void k_kick_dp(int64_t n, const int32_t *__restrict__ flag, const int32_t *__restrict__ off,
+                          TimeParams p, const int32_t *__restrict__ bin, const uint32_t *__restrict__ it_kick,
+                          const F *__restrict__ mass, const F *__restrict__ a0, const F *__restrict__ a1,
+                          const F *__restrict__ a2, F *dp0, F *dp1, F *dp2)
+{
+	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n || !flag[i]) return;
+	const uint32_t it_step = 1u << bin[i];
+	const uint32_t it_curr = it_kick[i], it_next = it_curr + (it_step >> 1);
+	const F dt = (F) kick_step(p, it_curr, it_next);
+	F d[3];
+	tu_particle_dp(mass[i], dt, a0[i], a1[i], a2[i], d);
+	const int64_t k = off[i];
+	dp0[k] = d[0];
+	dp1[k] = d[1];
+	dp2[k] = d[2];
 }
 
 // Drift_To_Sync_Point (drift.c:12-40): the active particles only
@@ -633,12 +656,29 @@ static int kick_typed(tvg_context *ctx)
 {
 	const int64_t na = ctx->use_active ? ctx->n_active : ctx->n;
 	if (na == 0) return TVG_OK;
+	// Gravity_Tree_Update_Kicks (kick.c:31-32, 61-62) without a due domain update
+	const bool nodes = tvg_tree_update_due(ctx);
+	int64_t slots = 0;
+	if (nodes) {
+		TVG_CHECK(tvg_tree_update_check(ctx, "kick"));
+		TVG_CHECK(tvg_impl_active_slots(ctx, &slots));
+		void *dpv = nullptr;
+		TVG_CHECK(tvg_impl_tree_dp_buffer(ctx, &dpv));
+		F *dp = (F *) dpv;
+		const int64_t cap = ctx->cap;
+		k_kick_dp<F><<<TVG_CNT(ctx, tvg_blocks(ctx->n, 256)), 256, 0, ctx->stream>>>(
+		    ctx->n, ctx->act_flag, ctx->act_off, time_params(ctx), (const int32_t *) ctx->f[FS_TIME_BIN],
+		    (const uint32_t *) ctx->f[FS_IT_KICK], (const F *) ctx->f[FS_MASS], (const F *) ctx->f[FS_ACC0],
+		    (const F *) ctx->f[FS_ACC1], (const F *) ctx->f[FS_ACC2], dp, dp + cap, dp + 2 * cap);
+		TVG_CUDA(ctx, cudaGetLastError());
+	}
 	k_kick<F><<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, ctx->stream>>>(
 	    na, ctx->use_active ? ctx->active : nullptr, time_params(ctx),
 	    (const int32_t *) ctx->f[FS_TIME_BIN], (uint32_t *) ctx->f[FS_IT_KICK],
 	    (const F *) ctx->f[FS_ACC0], (const F *) ctx->f[FS_ACC1], (const F *) ctx->f[FS_ACC2],
 	    (F *) ctx->f[FS_VEL0], (F *) ctx->f[FS_VEL1], (F *) ctx->f[FS_VEL2]);
 	TVG_CUDA(ctx, cudaGetLastError());
+	if (nodes) TVG_CHECK(tvg_impl_tree_kick(ctx, slots));
 	return TVG_OK;
 }
 
@@ -680,6 +720,11 @@ static int drift_typed(tvg_context *ctx)
 		    (F *) ctx->f[FS_POS2], ctx->status);
 		TVG_CUDA(ctx, cudaGetLastError());
 	}
+	// Gravity_Tree_Update_Drift(Time.Step) (drift.c:41-42)
+	if (tvg_tree_update_due(ctx)) {
+		TVG_CHECK(tvg_tree_update_check(ctx, "drift"));
+		TVG_CHECK(tvg_impl_tree_drift(ctx, st.time_step));
+	}
 	if (ctx->cfg.periodic) {
 		k_wrap<F><<<TVG_CNT(ctx, tvg_blocks(ctx->n, 256)), 256, 0, s>>>(
 		    ctx->n, (F) ctx->cfg.boxsize, (F *) ctx->f[FS_POS0], (F *) ctx->f[FS_POS1],
@@ -695,8 +740,13 @@ static int drift_typed(tvg_context *ctx)
 	st.time_next = host_it2time(ctx, st.next);
 	st.step_counter++;
 	set_current_cosmology(ctx);
-	// positions moved: keys, order and tree are stale
-	ctx->keys_std = ctx->sorted = ctx->have_top = ctx->have_tree = ctx->have_walktree = false;
+	if (ctx->tree_updates) {
+		// the reference walks the tree it keeps until the next domain update
+		ctx->have_walktree = false;
+	} else {
+		// positions moved: keys, order and tree are stale
+		ctx->keys_std = ctx->sorted = ctx->have_top = ctx->have_tree = ctx->have_walktree = false;
+	}
 	return TVG_OK;
 }
 

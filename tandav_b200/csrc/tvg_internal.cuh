@@ -46,7 +46,8 @@ enum {
 	TVG_ST_TREE_FULL = 4,
 	TVG_ST_TIMEOUT = 8,
 	TVG_ST_LIST_OVERFLOW = 16,
-	TVG_ST_TIMESTEP = 32
+	TVG_ST_TIMESTEP = 32,
+	TVG_ST_TREE_STALE = 64     // a kept tree's ranges do not fit the particles
 };
 
 struct tvg_buf {
@@ -200,6 +201,13 @@ struct tvg_context {
 	void *tl_scratch = nullptr;        // reductions (256 B)
 	int32_t *act_flag = nullptr, *act_off = nullptr;
 
+	// tree updates between rebuilds (tvg_tree_update.cu)
+	bool tree_updates = false;         // tvg_time_for_domain_update has been called
+	bool domain_update = true;         // Sig.Domain_Update (= Sig.Tree_Update)
+	int64_t npart_updates = 0;         // Local_NPart_Updates (signal.c:80)
+	int32_t *tu_first = nullptr;       // first particle of every tree node
+	void *tu_dp = nullptr;             // dp of the active particles by slot, 3 x cap Float
+
 	// device-resident counts and top-node tables of the step
 	tvg_devcount *dc = nullptr;
 	TopInfo *d_topinfo = nullptr;
@@ -240,6 +248,16 @@ int tvg_walk_group_results(tvg_context *ctx);
 // the active-bin limit of the timeline into the device counts
 int tvg_set_device_max_bin(tvg_context *ctx);
 void tvg_graph_release(tvg_context *ctx);
+// tree updates between rebuilds (tvg_tree_update.cu): due when the context
+// follows Time_For_Domain_Update and no domain update is due
+bool tvg_tree_update_due(const tvg_context *ctx);
+int tvg_tree_update_check(tvg_context *ctx, const char *what);
+// active flags and their exclusive scan (act_flag, act_off) for the current
+// active set, in particle order; *na = its size
+int tvg_impl_active_slots(tvg_context *ctx, int64_t *na);
+int tvg_impl_tree_dp_buffer(tvg_context *ctx, void **dp);
+int tvg_impl_tree_kick(tvg_context *ctx, int64_t na);
+int tvg_impl_tree_drift(tvg_context *ctx, double dt);
 
 // phase implementations (one translation unit each)
 int tvg_impl_keys(tvg_context *ctx, bool reversed);

@@ -62,25 +62,35 @@ static int accel_phases(tvg_context *ctx, int32_t form, uint32_t parts, int32_t 
                         int32_t prepare)
 {
 	cudaEvent_t *ev = ctx->ev;
+	// without a due domain update the kept tree is walked (accel.c:53, main.c:73-78)
+	const bool keep_tree = tvg_tree_update_due(ctx);
+	if (keep_tree) TVG_CHECK(tvg_tree_update_check(ctx, "compute_acceleration"));
 	TVG_CUDA(ctx, tvg_record(ctx, ev[8]));
-	TVG_CHECK(tvg_impl_keys(ctx, false));
-	ctx->keys_std = true;
-	TVG_CUDA(ctx, tvg_record(ctx, ev[9]));
-	TVG_CHECK(tvg_impl_sort(ctx, nullptr));
-	ctx->sorted = true;
-	// Sort_Particles_By_Peano_Key ends with Make_Active_Particle_List (peano.c:42)
-	if (ctx->have_timeline) {
-		TVG_CHECK(tvg_impl_active_from_bins(ctx));
+	if (keep_tree) {
+		TVG_CUDA(ctx, tvg_record(ctx, ev[9]));
+		TVG_CUDA(ctx, tvg_record(ctx, ev[10]));
+		TVG_CUDA(ctx, tvg_record(ctx, ev[11]));
+		ctx->have_walktree = false;
 	} else {
-		ctx->use_active = false;
+		TVG_CHECK(tvg_impl_keys(ctx, false));
+		ctx->keys_std = true;
+		TVG_CUDA(ctx, tvg_record(ctx, ev[9]));
+		TVG_CHECK(tvg_impl_sort(ctx, nullptr));
+		ctx->sorted = true;
+		// Sort_Particles_By_Peano_Key ends with Make_Active_Particle_List (peano.c:42)
+		if (ctx->have_timeline) {
+			TVG_CHECK(tvg_impl_active_from_bins(ctx));
+		} else {
+			ctx->use_active = false;
+		}
+		TVG_CUDA(ctx, tvg_record(ctx, ev[10]));
+		TVG_CHECK(tvg_impl_top_nodes(ctx));
+		ctx->have_top = true;
+		TVG_CUDA(ctx, tvg_record(ctx, ev[11]));
+		TVG_CHECK(tvg_impl_tree_build(ctx, form == TVG_FORM_PLAIN ? TVG_BUILD_EXACT_MOMENTS : 0));
+		ctx->have_tree = true;
+		ctx->have_walktree = false;
 	}
-	TVG_CUDA(ctx, tvg_record(ctx, ev[10]));
-	TVG_CHECK(tvg_impl_top_nodes(ctx));
-	ctx->have_top = true;
-	TVG_CUDA(ctx, tvg_record(ctx, ev[11]));
-	TVG_CHECK(tvg_impl_tree_build(ctx, form == TVG_FORM_PLAIN ? TVG_BUILD_EXACT_MOMENTS : 0));
-	ctx->have_tree = true;
-	ctx->have_walktree = false;
 	TVG_CUDA(ctx, tvg_record(ctx, ev[12]));
 	// safe_last_accel, accel.c:28-43 (the active particles)
 	TVG_CHECK(tvg_impl_save_last_accel(ctx));
@@ -286,6 +296,8 @@ extern "C" int tvg_step_graph(tvg_context *ctx, uint32_t parts, int32_t ewald_ki
 {
 	TVG_CHECK(accel_check(ctx, TVG_FORM_GROUP));
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	// a step on the kept tree (no keys, sort or build) runs directly
+	if (tvg_tree_update_due(ctx)) return tvg_compute_acceleration(ctx, TVG_FORM_GROUP, parts, ewald_kind, 0);
 	const uint64_t key = graph_key(ctx, parts, ewald_kind);
 	if (key != ctx->graph_warm_key) {
 		// a new configuration: one direct step, which also makes every

@@ -1,0 +1,201 @@
+// tvg_tree_update.cu -- the reference's tree updates between rebuilds.
+//
+// Time_For_Domain_Update (src/signal.c:85-116) decides when the particles
+// are decomposed, sorted and given a new tree: at a sync point, or once the
+// active particles of the steps since the last decomposition exceed
+// DOMAIN_UPDATE_PARAM * N. In between, the tree is kept: every kick adds the
+// particles' momentum change to the nodes above them
+// (Gravity_Tree_Update_Kicks, tree_update.c:12-54, from kick.c:31-32,61-62),
+// every drift moves the kicked nodes (Gravity_Tree_Update_Drift,
+// tree_update.c:62-101, from drift.c:41-42), and the force walks run on that
+// tree (accel.c:53). A context enters this mode with its first
+// tvg_time_for_domain_update call; until then every force computation
+// rebuilds.
+//
+// Kernels (one thread per node, the arithmetic in tvg_tree_update.cuh): the
+// first particle of every node, the node kicks, the top-node kicks, the node
+// and top-node drifts. Roofline: a kick reads each active particle's dp once
+// per tree level above it (L2-resident for the few-percent active sets the
+// mode runs with); a drift reads and writes the 48 B (FP32) node records.
+#include "tvg_internal.cuh"
+#include "tvg_tree_update.cuh"
+
+template <typename F>
+__global__ void k_node_first(const tvg_devcount *__restrict__ dc, int64_t tcap,
+                             const TuNode<F> *__restrict__ tree, int32_t *__restrict__ first)
+{
+	const int64_t nn = dc->nnodes < tcap ? dc->nnodes : tcap;
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nn; i += (int64_t) gridDim.x * blockDim.x)
+		first[i] = tu_node_first(tree, nn, i);
+}
+
+template <typename F>
+__global__ void k_kick_nodes(const tvg_devcount *__restrict__ dc, int64_t tcap, TuNode<F> *tree,
+                             const int32_t *__restrict__ first, const int32_t *__restrict__ act_off, int64_t n,
+                             int64_t na, const F *__restrict__ dp0, const F *__restrict__ dp1,
+                             const F *__restrict__ dp2, int *status)
+{
+	const int64_t nn = dc->nnodes < tcap ? dc->nnodes : tcap;
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nn; i += (int64_t) gridDim.x * blockDim.x)
+		if (!tu_kick_node_at(tree, i, first, act_off, n, na, dp0, dp1, dp2)) atomicOr(status, TVG_ST_TREE_STALE);
+}
+
+template <typename F>
+__global__ void k_kick_top(const tvg_devcount *__restrict__ dc, tvg_topnode *top,
+                           const int32_t *__restrict__ act_off, int64_t n, int64_t na, const F *__restrict__ dp0,
+                           const F *__restrict__ dp1, const F *__restrict__ dp2, int *status)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= dc->ntop || t >= TVG_MAX_TOP) return;
+	if (!tu_kick_top_at(top, t, act_off, n, na, dp0, dp1, dp2)) atomicOr(status, TVG_ST_TREE_STALE);
+}
+
+template <typename F>
+__global__ void k_drift_nodes(const tvg_devcount *__restrict__ dc, int64_t tcap, TuNode<F> *tree, double dt)
+{
+	const int64_t nn = dc->nnodes < tcap ? dc->nnodes : tcap;
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nn; i += (int64_t) gridDim.x * blockDim.x)
+		tu_drift_node(tree[i], dt);
+}
+
+__global__ void k_drift_top(const tvg_devcount *__restrict__ dc, tvg_topnode *top, double dt)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= dc->ntop || t >= TVG_MAX_TOP) return;
+	tu_drift_top(top[t], dt);
+}
+
+// flag[active[k]] = 1 (indices outside [0, n) are reported, not written)
+__global__ void k_flag_list(int64_t na, const int32_t *__restrict__ active, int64_t n, int32_t *flag, int *status)
+{
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k >= na) return;
+	const int32_t i = active[k];
+	if (i < 0 || i >= n) {
+		atomicOr(status, TVG_ST_TREE_STALE);
+		return;
+	}
+	flag[i] = 1;
+}
+
+__global__ void k_fill_i32(int64_t n, int32_t v, int32_t *a)
+{
+	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i < n) a[i] = v;
+}
+
+static int alloc_once(tvg_context *ctx, void **p, size_t bytes)
+{
+	if (*p) return TVG_OK;
+	if (cudaMalloc(p, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		*p = nullptr;
+		return tvg_fail(ctx, TVG_E_NOMEM, "tree update: cannot allocate %zu bytes", bytes);
+	}
+	return TVG_OK;
+}
+
+bool tvg_tree_update_due(const tvg_context *ctx)
+{
+	return ctx->tree_updates && !ctx->domain_update;
+}
+
+int tvg_tree_update_check(tvg_context *ctx, const char *what)
+{
+	if (!ctx->have_tree || !ctx->have_top)
+		return tvg_fail(ctx, TVG_E_STATE, "%s: no tree to update (the tree of the last domain update "
+		                "is kept until the next one)", what);
+	return TVG_OK;
+}
+
+int tvg_impl_active_slots(tvg_context *ctx, int64_t *na_out)
+{
+	const int64_t n = ctx->n, cap = ctx->cap;
+	cudaStream_t s = ctx->stream;
+	TVG_CHECK(alloc_once(ctx, (void **) &ctx->act_flag, 4 * (size_t) cap));
+	TVG_CHECK(alloc_once(ctx, (void **) &ctx->act_off, 4 * (size_t) cap));
+	const int64_t na = ctx->use_active ? ctx->n_active : n;
+	if (ctx->use_active) {
+		TVG_CUDA(ctx, cudaMemsetAsync(ctx->act_flag, 0, 4 * (size_t) n, s));
+		if (na > 0)
+			k_flag_list<<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, s>>>(na, ctx->active, n, ctx->act_flag,
+			                                                              ctx->status);
+	} else {
+		k_fill_i32<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, 1, ctx->act_flag);
+	}
+	TVG_CUDA(ctx, cudaGetLastError());
+	int64_t total = 0;
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->act_flag, ctx->act_off, n, &total));
+	TVG_CHECK(tvg_sync_status(ctx, "tree update: active list"));
+	if (total != na)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "tree update: the active list repeats particles (%lld of %lld distinct)",
+		                (long long) total, (long long) na);
+	*na_out = na;
+	return TVG_OK;
+}
+
+template <typename F>
+static int tree_kick_typed(tvg_context *ctx, int64_t na, const F *dp)
+{
+	const int64_t n = ctx->n, cap = ctx->cap, tcap = ctx->tcap;
+	cudaStream_t s = ctx->stream;
+	TVG_CHECK(alloc_once(ctx, (void **) &ctx->tu_first, 4 * (size_t) tcap));
+	TuNode<F> *tree = (TuNode<F> *) ctx->tree;
+	const int grid = (int) (tvg_blocks(tcap, 256) < 148 * 16 ? tvg_blocks(tcap, 256) : 148 * 16);
+	k_node_first<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(ctx->dc, tcap, tree, ctx->tu_first);
+	k_kick_nodes<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(ctx->dc, tcap, tree, ctx->tu_first, ctx->act_off, n, na,
+	                                                   dp, dp + cap, dp + 2 * cap, ctx->status);
+	k_kick_top<F><<<TVG_CNT(ctx, 1), TVG_MAX_TOP, 0, s>>>(ctx->dc, ctx->d_top, ctx->act_off, n, na, dp, dp + cap,
+	                                                       dp + 2 * cap, ctx->status);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return tvg_sync_status(ctx, "tree update: kicks");
+}
+
+int tvg_impl_tree_kick(tvg_context *ctx, int64_t na)
+{
+	if (ctx->cfg.float_bytes == 4) return tree_kick_typed<float>(ctx, na, (const float *) ctx->tu_dp);
+	return tree_kick_typed<double>(ctx, na, (const double *) ctx->tu_dp);
+}
+
+int tvg_impl_tree_dp_buffer(tvg_context *ctx, void **dp)
+{
+	TVG_CHECK(alloc_once(ctx, &ctx->tu_dp, 3 * (size_t) ctx->cap * tvg_fsize(ctx)));
+	*dp = ctx->tu_dp;
+	return TVG_OK;
+}
+
+template <typename F>
+static int tree_drift_typed(tvg_context *ctx, double dt)
+{
+	cudaStream_t s = ctx->stream;
+	const int64_t tcap = ctx->tcap;
+	const int grid = (int) (tvg_blocks(tcap, 256) < 148 * 16 ? tvg_blocks(tcap, 256) : 148 * 16);
+	k_drift_nodes<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(ctx->dc, tcap, (TuNode<F> *) ctx->tree, dt);
+	k_drift_top<<<TVG_CNT(ctx, 1), TVG_MAX_TOP, 0, s>>>(ctx->dc, ctx->d_top, dt);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
+}
+
+int tvg_impl_tree_drift(tvg_context *ctx, double dt)
+{
+	if (ctx->cfg.float_bytes == 4) return tree_drift_typed<float>(ctx, dt);
+	return tree_drift_typed<double>(ctx, dt);
+}
+
+extern "C" int tvg_time_for_domain_update(tvg_context *ctx, double domain_update_param, int32_t *domain_update)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!(domain_update_param >= 0)) return tvg_fail(ctx, TVG_E_BADINPUT, "domain_update_param must be >= 0");
+	ctx->tree_updates = true;
+	// signal.c:89-113 (one rank: the global count is the local one)
+	ctx->domain_update = false;
+	ctx->npart_updates += ctx->have_timeline ? ctx->tl.state.n_active : ctx->n;
+	const double max_updates = domain_update_param * (double) ctx->n;
+	const bool sync = ctx->have_timeline && ctx->tl.state.sync_point;
+	if (sync || (double) ctx->npart_updates > max_updates) {
+		ctx->npart_updates = 0;
+		ctx->domain_update = true;
+	}
+	if (domain_update) *domain_update = ctx->domain_update ? 1 : 0;
+	return TVG_OK;
+}

@@ -401,6 +401,15 @@ class GravityContext:
                                                     C.byref(k), C.byref(d)), "kd_factors")
         return k.value, d.value
 
+    def time_for_domain_update(self, domain_update_param=0.1):
+        """Time_For_Domain_Update (src/signal.c:85-116); returns
+        Sig.Domain_Update. The first call turns on the tree updates between
+        rebuilds for this context."""
+        flag = C.c_int32()
+        self._check(self.lib.tvg_time_for_domain_update(self.ctx, C.c_double(domain_update_param),
+                                                        C.byref(flag)), "time_for_domain_update")
+        return bool(flag.value)
+
     def set_new_timesteps(self):
         self._check(self.lib.tvg_set_new_timesteps(self.ctx), "set_new_timesteps")
 

@@ -1,0 +1,124 @@
+"""The tree updates between rebuilds on the GPU (tvg_tree_update.cu) in the
+step loop of src/main.c:43-78 with Time_For_Domain_Update, on a Hernquist
+sphere whose particles fill eight time bins. Without a due domain update:
+
+* each kick adds the active particles' momentum to the kept tree: every
+  node and top-node field equals the restatement (oracle/tree_update.py,
+  pinned to the reference's Gravity_Tree_Update_Kicks) applied to the tree
+  downloaded before the kick, with the GPU's own kick factors;
+* each drift moves the kicked nodes by Time.Step * Dp, bit for bit;
+* the force computation keeps the particle order and walks the updated
+  tree: the plain form's accelerations equal the restatement's walk
+  (port.walk) on the downloaded tree, bit for bit, and the group form on the
+  same tree agrees within its accuracy."""
+import numpy as np
+import pytest
+
+import port
+import tree_update as TU
+from pipeline import assert_struct_equal
+from tandav_b200 import gravity as G
+from tandav_b200 import ics
+
+pytestmark = pytest.mark.gpu
+
+TREE_FIELDS = ("DNext", "Bitfield", "DUp", "Npart", "Pos", "Mass", "CoM", "Dp")
+TOP_FIELDS = ("Key", "Target", "Level", "First_Part", "Npart", "Pos", "Mass", "CoM", "Dp")
+DOMAIN_UPDATE_PARAM = 0.1           # the reference's Config value
+
+
+def _timeline():
+    return dict(comoving=0, time_begin=0.0, time_end=0.02, hubble_constant=0.1, omega_matter=0.3,
+                omega_lambda=0.7, omega_rad=0.0, omega_0=1.0, omega_baryon=0.0, rho_crit0=1.0,
+                time_int_accuracy=0.025, max_timestep=2e-3, displ_constraint=0.25)
+
+
+def _expected_kick(ctx):
+    """The kept tree after the coming kick, restated from the device state."""
+    d = ctx.download(G.F_MASS | G.F_ACC | G.F_TIME_BIN | G.F_IT_KICK | G.F_TREE_PARENT)
+    tree, top = ctx.download_tree()
+    st = ctx.timeline()
+    active = np.flatnonzero(d["time_bin"] <= st.max_active_bin)
+    dt = np.zeros(len(d["mass"]), np.float32)
+    factors = {}
+    for i in active:
+        c = int(d["it_kick_pos"][i])
+        nx = c + ((1 << int(d["time_bin"][i])) >> 1)
+        if (c, nx) not in factors:
+            factors[(c, nx)] = ctx.kick_drift_factors(c, nx)[0]
+        dt[i] = np.float32(factors[(c, nx)])
+    dp = TU.particle_dp(d["mass"], dt, d["acc"], 4)
+    return TU.kicks(tree, top, d["tree_parent"], active, dp, 4)
+
+
+def _assert_tree(ctx, expected, what):
+    tree, top = ctx.download_tree()
+    assert_struct_equal(tree, expected[0], TREE_FIELDS, f"tree {what}")
+    assert_struct_equal(top, expected[1], TOP_FIELDS, f"top nodes {what}")
+
+
+def test_tree_updates_in_the_step_loop():
+    p = ics.hernquist(n=8192, seed=21)
+    c = np.median(p.pos, axis=1)
+    size = 2.001 * np.abs(p.pos - c[:, None]).max()
+    n = p.n
+    prm = port.WalkParams(gravity=ics.GRAVITY, softening=p.softening, domain_size=size, boxsize=0.0,
+                          open_bh=0.25, open_rel=0.005, use_bh=0, vector_size=64)
+    seen = dict(kick=0, drift=0, walk=0, group=0)
+    with G.GravityContext(n, float_bytes=4, periodic=False, softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32),
+                   time_bin=np.zeros(n, np.int32), it_drift=np.zeros(n, np.uint32),
+                   it_kick=np.zeros(n, np.uint32))
+        ctx.set_domain(c - 0.5 * size, size)
+        ctx.timeline_init(**_timeline())
+        # Update(BEFORE_MAIN_LOOP), update.c:13-34
+        ctx.compute_acceleration(form=G.FORM_PLAIN, parts=G.WALK_GRAVITY, prepare=True)
+        dom = ctx.time_for_domain_update(DOMAIN_UPDATE_PARAM)
+        assert dom                                    # every particle was active
+        for _ in range(16):
+            ctx.set_new_timesteps()
+            st = ctx.timeline()
+            exp = None if dom else _expected_kick(ctx)
+            ctx.kick_first_halfstep()
+            if exp is not None:
+                _assert_tree(ctx, exp, "after the first kick")
+                seen["kick"] += 1
+            drifted = not dom
+            if drifted:
+                tree, top = ctx.download_tree()
+                exp = TU.drift(tree, top, st.time_step, 4)
+            ctx.drift_to_sync_point()
+            if drifted:
+                _assert_tree(ctx, exp, "after the drift")
+                seen["drift"] += 1
+            ids = ctx.download(G.F_ID)["id"]
+            dom = ctx.time_for_domain_update(DOMAIN_UPDATE_PARAM)
+            ctx.compute_acceleration(form=G.FORM_PLAIN, parts=G.WALK_GRAVITY)
+            if not dom:
+                d = ctx.download(G.F_ID | G.F_POS | G.F_MASS | G.F_GRAV_ACC | G.F_LAST_ACC
+                                 | G.F_TIME_BIN)
+                assert np.array_equal(d["id"], ids)   # no sort without a domain update
+                tree, top = ctx.download_tree()
+                act = d["time_bin"] <= ctx.timeline().max_active_bin
+                g, _ = port.walk("gravity", d["pos"], d["mass"], d["last_acc_mag"], top, tree, prm,
+                                 fsize=4)
+                want, got = g.astype(np.float32)[:, act], d["grav_acc"][:, act]
+                assert np.array_equal(got, want), f"walk on the kept tree: max diff " \
+                                                  f"{np.abs(got.astype(float) - want).max()}"
+                if drifted:
+                    seen["walk"] += 1
+                    if not seen["group"]:
+                        # the group form on the same tree (it assigns Grav_Acc)
+                        ctx.walk(G.FORM_GROUP, use_bh=False, parts=G.WALK_GRAVITY)
+                        grp = ctx.download(G.F_GRAV_ACC)["grav_acc"][:, act].astype(np.float64)
+                        ref = got.astype(np.float64)
+                        err = np.sqrt(((grp - ref) ** 2).sum(0).mean() / (ref ** 2).sum(0).mean())
+                        assert err < 1e-2, f"group form on the kept tree: rms {err:.2e}"
+                        seen["group"] += 1
+            exp = None if dom else _expected_kick(ctx)
+            ctx.kick_second_halfstep()
+            if exp is not None:
+                _assert_tree(ctx, exp, "after the second kick")
+                seen["kick"] += 1
+    print(seen)
+    assert seen["kick"] >= 6 and seen["drift"] >= 3 and seen["walk"] >= 2 and seen["group"] == 1

@@ -5,7 +5,14 @@ over a subset of the particles and Gravity_Tree_Update_Drift on the tree it
 has just built, then both walks on the updated tree. Every tree and top-node
 field after the kicks (Dp, the UPDATED bits, negative top-node levels) and
 after the drift (CoM), and the accelerations of the walks on the updated
-tree (port.walk), must agree bit for bit."""
+tree (port.walk), must agree bit for bit. The library's own per-node
+functions (tandav_b200/csrc/tvg_tree_update.cuh, built for the host by
+tests/tree_update_host.cu) are held against the same reference output."""
+import ctypes as C
+import shutil
+import subprocess
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -47,13 +54,25 @@ def _restated(ref, fsize, pos, vel, mass):
     return upk, TU.drift(tree, top, DRIFT_DT, fsize)
 
 
-@pytest.mark.parametrize("variant,kind", CASES)
-def test_tree_update_matches_reference(variant, kind):
+ROOT = Path(__file__).resolve().parents[1]
+_RUNS = {}
+
+
+def _reference(variant, kind):
+    """The harness's update run (cached: two tests read it)."""
     if not refrun.available(variant):
         pytest.skip(f"oracle/_ref/{variant} not built")
-    pos, vel, mass, box, soft = _case(kind)
-    ref = refrun.run(variant, "update", pos, vel, mass, box=box, softening=soft,
-                     origin=(DRIFT_DT, 0.0, 0.0), size=KICK_DT)
+    if variant not in _RUNS:
+        pos, vel, mass, box, soft = _case(kind)
+        _RUNS[variant] = (refrun.run(variant, "update", pos, vel, mass, box=box, softening=soft,
+                                     origin=(DRIFT_DT, 0.0, 0.0), size=KICK_DT),
+                          pos, vel, mass, box, soft)
+    return _RUNS[variant]
+
+
+@pytest.mark.parametrize("variant,kind", CASES)
+def test_tree_update_matches_reference(variant, kind):
+    ref, pos, vel, mass, box, soft = _reference(variant, kind)
     fsize = ref["float_size"]
     (kt, ktop), (dt_, dtop) = _restated(ref, fsize, pos, vel, mass)
     # the kicks reached nodes and top nodes, and the drift moved them
@@ -84,6 +103,54 @@ def test_tree_update_matches_reference(variant, kind):
         assert np.array_equal(got, want), f"{name}: max diff {np.abs(got - want).max()}"
         if name == "bh":
             last = np.sqrt(gacc[0] * gacc[0] + gacc[1] * gacc[1] + gacc[2] * gacc[2]).astype(ft)
+
+
+@pytest.fixture(scope="module")
+def host_lib(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("nvcc not found")
+    out = tmp_path_factory.mktemp("tree_update_host") / "libtuhost.so"
+    subprocess.run([nvcc, "-x", "cu", "-std=c++17", "-O2", "-shared", "-Xcompiler",
+                    "-fPIC,-ffp-contract=off", "-I", str(ROOT / "include"),
+                    str(ROOT / "tests" / "tree_update_host.cu"), "-o", str(out)],
+                   check=True, capture_output=True)
+    return C.CDLL(str(out))
+
+
+@pytest.mark.parametrize("variant,kind", CASES)
+def test_library_node_functions_match_reference(host_lib, variant, kind):
+    """The per-node functions the kernels run (first particle of a node,
+    active slots by the scan of the active flags, dp, node and top-node
+    kicks and drifts), looped on the CPU, against the reference."""
+    ref, pos, vel, mass, box, soft = _reference(variant, kind)
+    fsize = ref["float_size"]
+    ft = port.ftype(fsize)
+    ids = ref["perm"]
+    n = len(ids)
+    flag = (ids % 3 != 1).astype(np.int32)
+    off = np.zeros(n, np.int32)
+    off[1:] = np.cumsum(flag)[:-1]
+    na = int(flag.sum())
+    m = np.ascontiguousarray(mass.astype(ft)[ids])
+    acc = np.ascontiguousarray(vel.astype(ft)[:, ids])
+    tree, top = ref["tree"].copy(), ref["topnodes"].copy()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    for q in (4, 3):
+        dt = np.ascontiguousarray((KICK_DT * (1 + ids % q) / q).astype(ft))
+        dp = np.zeros((3, n), ft)
+        host_lib.tu_host_dp(C.c_int(fsize), C.c_int64(n), p(flag), p(off), p(m), p(dt), p(acc),
+                            p(dp), C.c_int64(n))
+        bad = host_lib.tu_host_kick(C.c_int(fsize), p(tree), C.c_int64(len(tree)), p(top),
+                                    C.c_int(len(top)), p(off), C.c_int64(n), C.c_int64(na), p(dp),
+                                    C.c_int64(n))
+        assert bad == 0
+    assert_struct_equal(tree, ref["upk_tree"], TREE_FIELDS, "tree after the kicks")
+    assert_struct_equal(top, ref["upk_top"], TOP_FIELDS, "top nodes after the kicks")
+    host_lib.tu_host_drift(C.c_int(fsize), p(tree), C.c_int64(len(tree)), p(top), C.c_int(len(top)),
+                           C.c_double(DRIFT_DT))
+    assert_struct_equal(tree, ref["upd_tree"], TREE_FIELDS, "tree after the drift")
+    assert_struct_equal(top, ref["upd_top"], TOP_FIELDS, "top nodes after the drift")
 
 
 def test_kicks_reach_top_node_without_subtree():
