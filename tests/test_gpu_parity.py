@@ -11,6 +11,7 @@ import pytest
 import port
 from pipeline import oracle_pipeline, oracle_ewald_tables, assert_struct_equal
 from tandav_b200 import gravity as G
+from tree_audit import audit
 from tandav_b200 import ics
 
 pytestmark = pytest.mark.gpu
@@ -156,6 +157,23 @@ def test_fast_moments_close_to_exact():
     assert_struct_equal(exact, fast, ["DNext", "Bitfield", "DUp", "Npart", "Pos"], "topology")
     assert np.allclose(exact["Mass"], fast["Mass"], rtol=1e-5)
     assert np.allclose(exact["CoM"], fast["CoM"], rtol=0, atol=1e-4 * p.box)
+
+
+@pytest.mark.parametrize("kind,fsize,n,exact", [("zeldovich", 4, 128 ** 3, True),
+                                               ("zeldovich", 4, 128 ** 3, False),
+                                               ("hernquist", 8, 1 << 20, True)])
+def test_tree_audit_large(kind, fsize, n, exact):
+    """The reference's node audit (tree_build.c:620-685, tests/tree_audit.py)
+    over every node of trees built on the GPU at sizes beyond the oracle
+    comparisons: branches against DNext, contiguous particle ranges and
+    Npart, mass and centre of mass (exact Float sums or FP64 warp sums),
+    octant geometry, every particle inside its bundle's cube."""
+    p, origin, size = make_case(kind, n)
+    ft = port.ftype(fsize)
+    with make_ctx(p.n, fsize, box=p.box, softening=p.softening) as ctx:
+        perm, _, tree, top = gpu_pipeline(ctx, p.pos, p.mass, origin, size, exact=exact)
+    figures = audit(tree, top, p.pos.astype(ft)[:, perm], p.mass.astype(ft)[perm], size, fsize)
+    print(kind, n, "exact" if exact else "fast", figures)
 
 
 @pytest.mark.parametrize("fsize", [4, 8])

@@ -7,6 +7,7 @@ import pytest
 
 import port
 from pipeline import oracle_pipeline, oracle_ewald_tables, assert_struct_equal
+from tree_audit import audit
 
 FORCE_CASES = ["hernquist_iso_f64", "hernquist_iso_f32", "box_per_f32", "zeldovich_per_f64"]
 TREE_FIELDS = ["DNext", "Bitfield", "DUp", "Npart", "Pos", "Mass", "CoM", "Dp"]
@@ -130,3 +131,27 @@ def test_oracle_potential_matches_reference(golden_dir, case):
         ref = g[name + "_pot"]
         assert np.array_equal(pot.astype(np.float64), ref), \
             f"{name}: max diff {np.abs(pot.astype(np.float64) - ref).max()}"
+
+
+@pytest.mark.parametrize("case", FORCE_CASES)
+def test_tree_audit_on_reference_trees(golden_dir, case):
+    """The reference's node audit (tree_build.c:620-685, tests/tree_audit.py)
+    passes on the reference's own trees, and catches a mistake planted in a
+    copy of one (Npart, DNext, CoM or a node centre changed)."""
+    g = np.load(golden_dir / f"{case}.npz")
+    fsize = int(g["float_size"])
+    ft = port.ftype(fsize)
+    pos = g["pos_in"].astype(ft)[:, g["perm"]]
+    mass = g["mass_in"].astype(ft)[g["perm"]]
+    size = float(g["domain_size"][0])
+    audit(g["tree"], g["topnodes"], pos, mass, size, fsize)
+    i = np.flatnonzero(g["tree"]["DNext"] > 0)[3]
+    for field, k, delta in (("Npart", None, 1), ("DNext", None, 1), ("CoM", 0, 0.05 * size),
+                            ("Pos", 1, 1e-4 * size)):
+        bad = g["tree"].copy()
+        if k is None:
+            bad[field][i] += delta
+        else:
+            bad[field][i + 1, k] += delta
+        with pytest.raises(AssertionError):
+            audit(bad, g["topnodes"], pos, mass, size, fsize)
