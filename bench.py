@@ -460,14 +460,14 @@ def main():
             pass
 
     # ---- the same step with the learned Ewald correction: trained here by the
-    # library's own kernels, judged by the exact table, then run in the walk
+    # library's own kernels, validated against the exact table, then run in the walk
     learned = None
     if not args.no_mlp:
         ctx.timer_start()
         loss = ctx.mlp_train(steps=20000, batch=16384, n_samples=1 << 20, lr=2e-3, lr_final=1e-6,
                              seed=3)
         train_ms = ctx.timer_stop()
-        mx, rms = ctx.mlp_judge(max_allowed=1.0)
+        mx, rms = ctx.mlp_validate(max_allowed=1.0)
         for _ in range(3):                     # direct step, then the two captures
             ctx.step_graph(parts, G.EWALD_MLP)
         ml_ms = ml_ew = 0.0

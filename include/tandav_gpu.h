@@ -442,8 +442,8 @@ typedef struct {
 
 /* Trains on the device (fits C and s first unless resume != 0);
  * final_loss = mean square error per component of T (box units) with the
- * FP32 weights over all samples. Leaves the weights unjudged (see
- * tvg_ewald_mlp_judge). */
+ * FP32 weights over all samples. Leaves the weights unvalidated (see
+ * tvg_ewald_mlp_validate). */
 int tvg_ewald_mlp_train(tvg_context *ctx, const tvg_mlp_train_config *cfg, float *final_loss);
 /* Copies the FP32 parameters out (set = 0) or in (set != 0). */
 int tvg_ewald_mlp_weights(tvg_context *ctx, float *params, int32_t set);
@@ -454,10 +454,10 @@ int tvg_ewald_mlp_grad(tvg_context *ctx, int64_t n, const float *x, const float 
                        float *loss);
 /* T(x) at n octant points x[3n] (box units) from the BF16 weights. */
 int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, double *t);
-/* The exact FP64 table (tvg_ewald_init) judges the BF16 network at its 65^3
+/* The exact FP64 table (tvg_ewald_init) validates the BF16 network at its 65^3
  * nodes: max and rms |T_mlp - T|; the walk accepts TVG_EWALD_MLP only while
  * the max error is at most max_allowed. */
-int tvg_ewald_mlp_judge(tvg_context *ctx, double max_allowed, double *max_err, double *rms_err);
+int tvg_ewald_mlp_validate(tvg_context *ctx, double max_allowed, double *max_err, double *rms_err);
 
 /* ---------------------------------------------------------- snapshots */
 

@@ -29,7 +29,7 @@ EXPORTS = (
     "tvg_kick_second_halfstep", "tvg_drift_to_sync_point", "tvg_timeline_get", "tvg_timeline_set",
     "tvg_rung_histogram", "tvg_compute_acceleration", "tvg_step_graph", "tvg_step_graph_reset",
     "tvg_ewald_mlp_train",
-    "tvg_ewald_mlp_weights", "tvg_ewald_mlp_grad", "tvg_ewald_mlp_eval", "tvg_ewald_mlp_judge",
+    "tvg_ewald_mlp_weights", "tvg_ewald_mlp_grad", "tvg_ewald_mlp_eval", "tvg_ewald_mlp_validate",
     "tvg_autotune", "tvg_write_snapshot", "tvg_write_snapshot_host", "tvg_time_for_domain_update",
 )
 

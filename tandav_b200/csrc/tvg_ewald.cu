@@ -9,7 +9,7 @@
 // point and axis-sum. Stored as Float, then divided by Boxsize^2 (force) and
 // Boxsize (potential) as the reference does after loading (periodic.c:215-228).
 // The raw FP64 values stay on the device as the training target and max-error
-// judge of the learned correction.
+// reference for validating the learned correction.
 #include "tvg_internal.cuh"
 #include "tvg_ewald_sum.cuh"
 

@@ -26,8 +26,8 @@
 // (deterministic), then Adam.
 //
 // Inference: BF16 weights (rounded once after training), FP32 arithmetic and
-// accumulation. The exact FP64 table (the reference's 65^3 nodes) is the
-// judge: tvg_ewald_mlp_judge measures the max and rms error there, and the
+// accumulation. The exact FP64 table (the reference's 65^3 nodes) validates
+// it: tvg_ewald_mlp_validate measures the max and rms error there, and the
 // walk refuses the learned correction when the max error is above the limit
 // the caller gives.
 #include <math.h>
@@ -401,7 +401,7 @@ static int refresh_bf16(tvg_context *ctx)
 	k_mlp_to_bf16<<<TVG_CNT(ctx, (MLP_NPARAM + 255) / 256), 256, 0, ctx->stream>>>(ctx->mlp_prm, (__nv_bfloat16 *) ctx->mlp_bf16);
 	TVG_CUDA(ctx, cudaGetLastError());
 	ctx->have_mlp = true;
-	ctx->mlp_ok = false;          // until judged
+	ctx->mlp_ok = false;          // until validated
 	return TVG_OK;
 }
 
@@ -576,7 +576,7 @@ extern "C" int tvg_ewald_mlp_eval(tvg_context *ctx, int64_t n, const double *x, 
 // errors of the walk's evaluation of the model at the 65^3 nodes of the
 // exact FP64 table
 __global__ void __launch_bounds__(128)
-k_mlp_judge(const double *__restrict__ raw, const __nv_bfloat16 *__restrict__ w,
+k_mlp_validate(const double *__restrict__ raw, const __nv_bfloat16 *__restrict__ w,
             const float *__restrict__ f32, double *err)
 {
 	__shared__ float P[MLP_NPARAM];
@@ -599,25 +599,25 @@ k_mlp_judge(const double *__restrict__ raw, const __nv_bfloat16 *__restrict__ w,
 	err[idx] = sqrt(e2);
 }
 
-extern "C" int tvg_ewald_mlp_judge(tvg_context *ctx, double max_allowed, double *max_err,
+extern "C" int tvg_ewald_mlp_validate(tvg_context *ctx, double max_allowed, double *max_err,
                                    double *rms_err)
 {
 	if (!ctx) return TVG_E_BADINPUT;
 	if (!ctx->have_mlp) return tvg_fail(ctx, TVG_E_STATE, "mlp: no weights");
 	if (!ctx->have_ewald || !ctx->ewald_raw)
-		return tvg_fail(ctx, TVG_E_STATE, "mlp judge: exact Ewald table not initialised");
+		return tvg_fail(ctx, TVG_E_STATE, "mlp validate: exact Ewald table not initialised");
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	const int npt = 65 * 65 * 65;
 	double *d;
 	TVG_CUDA(ctx, cudaMalloc((void **) &d, 8 * (size_t) npt));
-	k_mlp_judge<<<TVG_CNT(ctx, (npt + 127) / 128), 128, 0, ctx->stream>>>(ctx->ewald_raw, (const __nv_bfloat16 *) ctx->mlp_bf16,
+	k_mlp_validate<<<TVG_CNT(ctx, (npt + 127) / 128), 128, 0, ctx->stream>>>(ctx->ewald_raw, (const __nv_bfloat16 *) ctx->mlp_bf16,
 	                                                                       ctx->mlp_prm, d);
 	std::vector<double> h(npt);
 	cudaError_t e = cudaGetLastError();
 	if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, 8 * (size_t) npt, cudaMemcpyDeviceToHost, ctx->stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
 	cudaFree(d);
-	if (e != cudaSuccess) return tvg_fail(ctx, TVG_E_CUDA, "mlp judge: %s", cudaGetErrorString(e));
+	if (e != cudaSuccess) return tvg_fail(ctx, TVG_E_CUDA, "mlp validate: %s", cudaGetErrorString(e));
 	double mx = 0, s2 = 0;
 	for (double q : h) { mx = q > mx ? q : mx; s2 += q * q; }
 	if (max_err) *max_err = mx;

@@ -78,7 +78,7 @@ __device__ __forceinline__ void mlp_net(const float *P, const float v[3], float 
 	o[2] = o2;
 }
 
-// the walk's and the judge's copy of the parameters: network in BF16 (as
+// the walk's and the validation's copy of the parameters: network in BF16 (as
 // inference uses it), the fitted polynomial and the scale in FP32
 __device__ __forceinline__ float mlp_param(const __nv_bfloat16 *w, const float *f32, int e)
 {

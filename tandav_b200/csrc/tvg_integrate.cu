@@ -137,7 +137,7 @@ struct KDTables {
 	double a0, da;       // knot i >= 1 at a0 exp(i da)
 };
 
-// spline value at a (interval [x_i, x_{i+1}) with the knots as the judge)
+// spline value at a, in the knot interval [x_i, x_{i+1}) that holds a
 __device__ __forceinline__ double spline_eval(const KDTables &t, const double *y,
                                               const double *m2, double a)
 {

@@ -1330,7 +1330,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		return tvg_fail(ctx, TVG_E_BADINPUT, "unknown Ewald kind %d", ewald_kind);
 	if (mlp && !(ctx->have_mlp && ctx->mlp_ok))
 		return tvg_fail(ctx, TVG_E_STATE, "learned Ewald correction not trained or not accepted by "
-		                "the table (tvg_ewald_mlp_judge)");
+		                "the table (tvg_ewald_mlp_validate)");
 	cudaStream_t s = ctx->stream;
 	if (!ctx->have_walktree) TVG_CHECK(prepare_typed<F>(ctx));
 	if (ewald && !ctx->ewald_ext) TVG_CHECK(tvg_impl_ewald_ext(ctx));

@@ -495,10 +495,10 @@ class GravityContext:
                                                 C.c_void_p(_ptr(t))), "mlp_eval")
         return t
 
-    def mlp_judge(self, max_allowed=1e-2):
+    def mlp_validate(self, max_allowed=1e-2):
         mx, rms = C.c_double(), C.c_double()
-        self._check(self.lib.tvg_ewald_mlp_judge(self.ctx, C.c_double(max_allowed), C.byref(mx),
-                                                 C.byref(rms)), "mlp_judge")
+        self._check(self.lib.tvg_ewald_mlp_validate(self.ctx, C.c_double(max_allowed), C.byref(mx),
+                                                 C.byref(rms)), "mlp_validate")
         return mx.value, rms.value
 
     def set_ewald_opening(self, rel_alpha=2.5e-4, bh_factor=0.5):

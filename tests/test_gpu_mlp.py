@@ -1,6 +1,6 @@
 """The learned Ewald correction (tvg_ewald_mlp.cu): the training kernels'
 gradient against the FP64 oracle (oracle/mlp.py); a network trained on the
-GPU, judged by the exact table and compared with the reference's trilinear
+GPU, validated against the exact table and compared with the reference's trilinear
 interpolation of that table (Gravity/periodic.c:35-113); and the walk with
 the learned correction against the same walk without a correction and with
 the table, by the FP64 Ewald-summed direct force."""
@@ -23,7 +23,7 @@ def trained():
         ctx.set_domain((0, 0, 0), 1.0)
         ctx.ewald_init()
         loss = ctx.mlp_train(**TRAIN)
-        mx, rms = ctx.mlp_judge(max_allowed=1.0)
+        mx, rms = ctx.mlp_validate(max_allowed=1.0)
         return ctx.mlp_weights(), loss, mx, rms
 
 
@@ -44,7 +44,7 @@ def test_mlp_gradient_matches_oracle():
         assert np.abs(go[lo_:hi_]).max() > 0, name
 
 
-def test_mlp_training_judged_by_table(trained):
+def test_mlp_training_validated_by_table(trained):
     w, loss, mx, rms = trained
     rng = np.random.default_rng(8)
     xs = rng.random((2000, 3)) * 0.5
@@ -57,7 +57,7 @@ def test_mlp_training_judged_by_table(trained):
     t_fp32 = O.forward(w.astype(np.float64), xs)
     e = {k: np.sqrt(((v - t_ref) ** 2).sum(1)) for k, v in
          (("mlp_bf16", t_mlp), ("mlp_fp32", t_fp32), ("trilinear", t_tri))}
-    print(f"train loss {loss:.3e}; judge (65^3 nodes): max {mx:.3e} rms {rms:.3e}; "
+    print(f"train loss {loss:.3e}; validation (65^3 nodes): max {mx:.3e} rms {rms:.3e}; "
           + "; ".join(f"{k}: max {v.max():.3e} rms {np.sqrt((v ** 2).mean()):.3e}" for k, v in e.items())
           + f"; max |T| {np.abs(t_ref).max():.2f}")
     assert loss < 1e-7
@@ -81,9 +81,9 @@ def test_walk_with_learned_correction(trained):
         ctx.set_domain((0, 0, 0), p.box)
         ctx.ewald_init()
         ctx.mlp_weights(w)
-        with pytest.raises(G.TvgError):         # not judged yet
+        with pytest.raises(G.TvgError):         # not validated yet
             ctx.force_step(form=G.FORM_GROUP, parts=parts, ewald_kind=G.EWALD_MLP)
-        ctx.mlp_judge(max_allowed=1.0)
+        ctx.mlp_validate(max_allowed=1.0)
         ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
         ctx.save_last_accel()
         tgt = np.sort(np.random.default_rng(1).choice(p.n, 2000, replace=False))
