@@ -100,6 +100,14 @@ struct TopPlace {
 
 struct tvg_graph_entry;
 
+// field slots in ctx->f[]
+enum {
+	FS_TYPE = 0, FS_TIME_BIN, FS_IT_DRIFT, FS_IT_KICK, FS_ID, FS_COST,
+	FS_POS0, FS_POS1, FS_POS2, FS_VEL0, FS_VEL1, FS_VEL2,
+	FS_ACC0, FS_ACC1, FS_ACC2, FS_MASS, FS_GACC0, FS_GACC1, FS_GACC2,
+	FS_LAST_ACC, FS_TREE_PARENT, FS_GRAV_POT, FS_NFIELDS
+};
+
 struct tvg_context {
 	int device = 0;
 	tvg_config cfg{};
@@ -118,8 +126,8 @@ struct tvg_context {
 	char err[512] = { 0 };
 
 	// particle fields (two buffers each for the permutation)
-	void *f[TVG_MAX_TOP] = { nullptr };
-	void *falt[TVG_MAX_TOP] = { nullptr };
+	void *f[FS_NFIELDS] = { nullptr };
+	void *falt[FS_NFIELDS] = { nullptr };
 	// key split for the sort
 	uint64_t *key_hi = nullptr, *key_lo = nullptr, *key_tmp = nullptr;
 	uint32_t *perm = nullptr, *perm_tmp = nullptr;
@@ -225,13 +233,6 @@ struct tvg_context {
 	double last_counts[2] = { 0, 0 };
 };
 
-// field slots in ctx->f[]
-enum {
-	FS_TYPE = 0, FS_TIME_BIN, FS_IT_DRIFT, FS_IT_KICK, FS_ID, FS_COST,
-	FS_POS0, FS_POS1, FS_POS2, FS_VEL0, FS_VEL1, FS_VEL2,
-	FS_ACC0, FS_ACC1, FS_ACC2, FS_MASS, FS_GACC0, FS_GACC1, FS_GACC2,
-	FS_LAST_ACC, FS_TREE_PARENT, FS_GRAV_POT, FS_NFIELDS
-};
 
 int tvg_fail(tvg_context *ctx, int code, const char *fmt, ...);
 int tvg_sync_status(tvg_context *ctx, const char *phase);
