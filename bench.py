@@ -75,6 +75,10 @@ def parse():
                     help="opening of the group form's Ewald walk (relative to |a_old|)")
     ap.add_argument("--plain-open-rel", type=float, default=0.005,
                     help="TREE_OPEN_PARAM_REL of the plain form (the reference's value)")
+    ap.add_argument("--domain-update-param", type=float, default=None,
+                    help="rung run: follow Time_For_Domain_Update with this DOMAIN_UPDATE_PARAM "
+                         "(the reference's 0.1), keeping and updating the tree between domain "
+                         "updates; default: rebuild at every step")
     ap.add_argument("--rung-steps", type=int, default=0,
                     help="also run this many hierarchical time steps from z = 50 (rung workload)")
     ap.add_argument("--time-int-accuracy", type=float, default=0.025)
@@ -279,6 +283,9 @@ def rung_run(args, p, G, device):
         ctx.timer_start()
         ctx.compute_acceleration(form=G.FORM_GROUP, parts=parts, prepare=True)
         prep_ms = ctx.timer_stop()
+        dup = args.domain_update_param
+        if dup is not None:
+            ctx.time_for_domain_update(dup)          # Update(BEFORE_MAIN_LOOP)
         tpl = args.tpl or ctx.autotune(use_bh=False, parts=parts)[0]
         steps = []
         for _ in range(args.rung_steps):
@@ -290,6 +297,7 @@ def rung_run(args, p, G, device):
             st = ctx.timeline()
             ctx.kick_first_halfstep()
             ctx.drift_to_sync_point()
+            rebuilt = ctx.time_for_domain_update(dup) if dup is not None else True
             ctx.step_graph(parts)              # Compute_Acceleration, one graph launch
             ctx.kick_second_halfstep()
             ms = ctx.timer_stop()
@@ -297,7 +305,8 @@ def rung_run(args, p, G, device):
             ph = ctx.phase_times()
             g_i, e_i = ctx.walk_counters()
             steps.append({"a": round(st.time_current, 6), "n_active": int(st.n_active),
-                          "max_active_bin": int(st.max_active_bin), "ms": round(ms, 2),
+                          "max_active_bin": int(st.max_active_bin), "rebuilt": bool(rebuilt),
+                          "ms": round(ms, 2),
                           "walk_ms": round(ph["walk"], 1), "ewald_ms": round(ph["ewald"], 1),
                           "interactions_per_active": round(g_i / max(st.n_active, 1)),
                           "ewald_evals_per_active": round(e_i / max(st.n_active, 1), 1),
@@ -307,6 +316,8 @@ def rung_run(args, p, G, device):
         tot_act = sum(s["n_active"] for s in steps)
         return {"workload": f"zeldovich_{args.nside}^3 from z = 50, hierarchical steps, "
                             f"TimeIntAccuracy {args.time_int_accuracy}",
+                "tree": ("rebuilt every step" if dup is None else
+                         f"kept between domain updates, DOMAIN_UPDATE_PARAM {dup}"),
                 "prepare_ms": round(prep_ms, 1), "targets_per_lane": tpl,
                 "steps": len(steps), "total_ms": round(tot_ms, 1),
                 "active_particles_per_s": round(tot_act / (tot_ms * 1e-3)) if tot_ms else None,
