@@ -137,3 +137,27 @@ def test_snapshot_rejects_bad_requests(tmp_path):
     assert call(tmp_path / "pot", 4, G.SNAP_GPOT) == 5
     assert call(tmp_path / "fb", 2, 0) == 5
     assert call(tmp_path / "no" / "such" / "dir", 4, 0) == 5
+
+
+def test_snapshot_many_particles_matches_numpy_rendering(tmp_path):
+    """200,001 particles (the writer interleaves in chunks of 65,536, the last
+    one ragged) against the format rendered with numpy: label record, record
+    markers, components interleaved per particle."""
+    n = 200001
+    rng = np.random.default_rng(1)
+    pos, vel, gacc = (rng.random((3, n)).astype(np.float32) for _ in range(3))
+    ids = np.arange(n, dtype=np.uint32)
+    mass = rng.random(n).astype(np.float32)
+    h = G.snapshot_header(n, 0.5, 10.0)
+    path = tmp_path / "big"
+    G.write_snapshot_host(path, h, pos, vel, ids, mass, grav_acc=gacc)
+    got = path.read_bytes()
+
+    def rec(label, data):
+        return (struct.pack("<I4sII", 8, label, len(data) + 8, 8) + struct.pack("<I", len(data))
+                + data + struct.pack("<I", len(data)))
+
+    want = (got[:HEAD + 256 + 4] + rec(b"POS ", pos.T.tobytes()) + rec(b"VEL ", vel.T.tobytes())
+            + rec(b"ID  ", ids.tobytes()) + rec(b"MASS", mass.tobytes())
+            + rec(b"GACC", gacc.T.tobytes()))
+    assert got == want
