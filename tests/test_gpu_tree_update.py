@@ -1,6 +1,8 @@
 """The tree updates between rebuilds on the GPU (tvg_tree_update.cu) in the
 step loop of src/main.c:43-78 with Time_For_Domain_Update, on a Hernquist
-sphere whose particles fill eight time bins. Without a due domain update:
+sphere (isolated) and on clumps in a periodic box (particles wrapped into
+the box every drift), both filling six to eight time bins. Without a due
+domain update:
 
 * each kick adds the active particles' momentum to the kept tree: every
   node and top-node field equals the restatement (oracle/tree_update.py,
@@ -9,8 +11,9 @@ sphere whose particles fill eight time bins. Without a due domain update:
 * each drift moves the kicked nodes by Time.Step * Dp, bit for bit;
 * the force computation keeps the particle order and walks the updated
   tree: the plain form's accelerations equal the restatement's walk
-  (port.walk) on the downloaded tree, bit for bit, and (FP32) the group form
-  on the same tree agrees within its accuracy.
+  (port.walk) on the downloaded tree, bit for bit (gravity part; nearest
+  images in the box), and (FP32, isolated) the group form on the same tree
+  agrees within its accuracy.
 
 FP32 and FP64 (the reference's DOUBLE_PRECISION) builds."""
 import numpy as np
@@ -29,10 +32,21 @@ TOP_FIELDS = ("Key", "Target", "Level", "First_Part", "Npart", "Pos", "Mass", "C
 DOMAIN_UPDATE_PARAM = 0.1           # the reference's Config value
 
 
-def _timeline():
-    return dict(comoving=0, time_begin=0.0, time_end=0.02, hubble_constant=0.1, omega_matter=0.3,
-                omega_lambda=0.7, omega_rad=0.0, omega_0=1.0, omega_baryon=0.0, rho_crit0=1.0,
-                time_int_accuracy=0.025, max_timestep=2e-3, displ_constraint=0.25)
+def _case(kind):
+    """Particles, domain and a Newtonian timeline whose time bins spread over
+    six to eight rungs (chosen from the oracle's accelerations)."""
+    if kind == "hernquist":
+        p = ics.hernquist(n=8192, seed=21)
+        c = np.median(p.pos, axis=1)
+        size = 2.001 * np.abs(p.pos - c[:, None]).max()
+        origin, t_end, dt_max = c - 0.5 * size, 0.02, 2e-3
+    else:                                   # clumps in a periodic box
+        p = ics.random_box(8192, box=2000.0, seed=22, clumps=9)
+        origin, size, t_end, dt_max = np.zeros(3), p.box, 30.5, 1.9
+    tl = dict(comoving=0, time_begin=0.0, time_end=t_end, hubble_constant=0.1, omega_matter=0.3,
+              omega_lambda=0.7, omega_rad=0.0, omega_0=1.0, omega_baryon=0.0, rho_crit0=1.0,
+              time_int_accuracy=0.025, max_timestep=dt_max, displ_constraint=0.25)
+    return p, origin, size, tl
 
 
 def _expected_kick(ctx, fsize):
@@ -60,22 +74,22 @@ def _assert_tree(ctx, expected, what):
     assert_struct_equal(top, expected[1], TOP_FIELDS, f"top nodes {what}")
 
 
-@pytest.mark.parametrize("fsize", [4, 8])
-def test_tree_updates_in_the_step_loop(fsize):
-    p = ics.hernquist(n=8192, seed=21)
+@pytest.mark.parametrize("kind,fsize", [("hernquist", 4), ("hernquist", 8), ("clumps", 4)])
+def test_tree_updates_in_the_step_loop(kind, fsize):
+    p, origin, size, timeline = _case(kind)
     ft = port.ftype(fsize)
-    c = np.median(p.pos, axis=1)
-    size = 2.001 * np.abs(p.pos - c[:, None]).max()
     n = p.n
-    prm = port.WalkParams(gravity=ics.GRAVITY, softening=p.softening, domain_size=size, boxsize=0.0,
+    prm = port.WalkParams(gravity=ics.GRAVITY, softening=p.softening, domain_size=size, boxsize=p.box,
                           open_bh=0.25, open_rel=0.005, use_bh=0, vector_size=64)
+    group_check = fsize == 4 and p.box == 0
     seen = dict(kick=0, drift=0, walk=0, group=0)
-    with G.GravityContext(n, float_bytes=fsize, periodic=False, softening=p.softening) as ctx:
+    with G.GravityContext(n, float_bytes=fsize, periodic=p.box > 0, boxsize=p.box,
+                          softening=p.softening) as ctx:
         ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32),
                    time_bin=np.zeros(n, np.int32), it_drift=np.zeros(n, np.uint32),
                    it_kick=np.zeros(n, np.uint32))
-        ctx.set_domain(c - 0.5 * size, size)
-        ctx.timeline_init(**_timeline())
+        ctx.set_domain(origin, size)
+        ctx.timeline_init(**timeline)
         # Update(BEFORE_MAIN_LOOP), update.c:13-34
         ctx.compute_acceleration(form=G.FORM_PLAIN, parts=G.WALK_GRAVITY, prepare=True)
         dom = ctx.time_for_domain_update(DOMAIN_UPDATE_PARAM)
@@ -112,7 +126,7 @@ def test_tree_updates_in_the_step_loop(fsize):
                                                   f"{np.abs(got.astype(float) - want).max()}"
                 if drifted:
                     seen["walk"] += 1
-                    if fsize == 4 and not seen["group"]:
+                    if group_check and not seen["group"]:
                         # the group form on the same tree (it assigns Grav_Acc)
                         ctx.walk(G.FORM_GROUP, use_bh=False, parts=G.WALK_GRAVITY)
                         grp = ctx.download(G.F_GRAV_ACC)["grav_acc"][:, act].astype(np.float64)
@@ -127,4 +141,4 @@ def test_tree_updates_in_the_step_loop(fsize):
                 seen["kick"] += 1
     print(seen)
     assert seen["kick"] >= 6 and seen["drift"] >= 3 and seen["walk"] >= 2
-    assert seen["group"] == (1 if fsize == 4 else 0)
+    assert seen["group"] == (1 if group_check else 0)
