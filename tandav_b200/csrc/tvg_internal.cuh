@@ -18,6 +18,7 @@
 #include "../../include/tandav_gpu.h"
 
 #define TVG_MAX_TOP 64
+#define TVG_MAX_DEVICES 64         // per-device caches of launch attributes
 #define TVG_MAX_LEVEL 42
 
 // ---------------------------------------------------------------- errors

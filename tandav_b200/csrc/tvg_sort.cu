@@ -20,6 +20,8 @@
 // unspecified order).
 // Roofline: HBM bound; per pass 8 B read (histogram) + 12 B read + 12 B write
 // per key.
+#include <mutex>
+
 #include "tvg_internal.cuh"
 
 #define RS_THREADS 256
@@ -251,6 +253,24 @@ __global__ void k_gather_fields(int64_t n, const uint32_t *__restrict__ perm, Ga
 	}
 }
 
+// k_radix_scatter's dynamic shared memory (above the 48 KB default) is a
+// function attribute of each device: set it once for every device the
+// process sorts on
+static cudaError_t radix_smem_attr(size_t smem)
+{
+	static std::mutex mu;
+	static bool done[TVG_MAX_DEVICES] = { false };
+	int device = 0;
+	cudaError_t e = cudaGetDevice(&device);
+	if (e != cudaSuccess) return e;
+	if (device < 0 || device >= TVG_MAX_DEVICES) return cudaErrorInvalidDevice;
+	std::lock_guard<std::mutex> lock(mu);
+	if (done[device]) return cudaSuccess;
+	e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+	if (e == cudaSuccess) done[device] = true;
+	return e;
+}
+
 int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 {
 	const int64_t n = ctx->n;
@@ -263,13 +283,8 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 	int32_t *skip = ctx->dc->sort_skip;
 	k_digit_skip<<<TVG_CNT(ctx, 1), 32, 0, s>>>(n, ctx->digit_count, skip);
 	TVG_CUDA(ctx, cudaGetLastError());
-	static bool attr_set = false;
 	const size_t smem = RS_TILE * 12 + (RS_WARPS * 256 + 3 * 256 + 33) * 4;
-	if (!attr_set) {
-		TVG_CUDA(ctx, cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                                   (int) smem));
-		attr_set = true;
-	}
+	TVG_CUDA(ctx, radix_smem_attr(smem));
 	uint64_t *kin = ctx->key_hi, *kout = ctx->key_tmp;
 	uint32_t *vin = ctx->perm, *vout = ctx->perm_tmp;
 	for (int d = 0; d < 8; d++) {
@@ -324,8 +339,6 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 // nothing has to start at zero. Two calls that overlap on the same GPU (from
 // two host threads, or on two streams) corrupt each other's scratch.
 // ------------------------------------------------------------------------
-
-#include <mutex>
 
 #define NOALLOC_TILES (TVG_NOALLOC_MAX_KEYS / RS_TILE)
 
@@ -412,14 +425,8 @@ extern "C" int tvg_sort_keys_noalloc(const uint64_t *key_hi, const uint64_t *key
 	if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return TVG_E_CUDA; }
 	NoallocScratch *S = noalloc_scratch(device);
 	if (!S) return TVG_E_CUDA;
-	static std::once_flag smem_once;
 	const size_t smem = RS_TILE * 12 + (RS_WARPS * 256 + 3 * 256 + 33) * 4;
-	cudaError_t attr_err = cudaSuccess;
-	std::call_once(smem_once, [&] {
-		attr_err = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                                (int) smem);
-	});
-	if (attr_err != cudaSuccess) { cudaGetLastError(); return TVG_E_CUDA; }
+	if (radix_smem_attr(smem) != cudaSuccess) { cudaGetLastError(); return TVG_E_CUDA; }
 	const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
 	cudaStream_t s = 0;
 	k_iota<<<tvg_blocks(n, 256), 256, 0, s>>>(n, S->idx[0]);

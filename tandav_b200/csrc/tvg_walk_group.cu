@@ -1238,6 +1238,15 @@ static int build_groups(tvg_context *ctx, int gsize)
 	return TVG_OK;
 }
 
+// the dynamic shared-memory attribute and the occupancy belong to a device:
+// the launch helpers cache them per device index
+static int device_slot(tvg_context *ctx)
+{
+	if (ctx->device < 0 || ctx->device >= TVG_MAX_DEVICES)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "device index %d out of range", ctx->device);
+	return TVG_OK;
+}
+
 template <typename K>
 static int blocks_for(tvg_context *ctx, K kernel, size_t smem, int *cache)
 {
@@ -1255,7 +1264,9 @@ template <int MODE, int TPL, typename F>
 static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
                        double *counter)
 {
-	static int nblk = 0;
+	static int nblk_dev[TVG_MAX_DEVICES] = { 0 };
+	TVG_CHECK(device_slot(ctx));
+	int &nblk = nblk_dev[ctx->device];
 	const size_t smem = sizeof(WarpSmem) * GW_WARPS;
 	TVG_CHECK(blocks_for(ctx, k_walk_group<MODE, TPL, F>, smem, &nblk));
 	k_walk_group<MODE, TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
@@ -1272,7 +1283,9 @@ template <int TPL, bool MLP, typename F>
 static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
                         double *counter)
 {
-	static int nblk = 0;
+	static int nblk_dev[TVG_MAX_DEVICES] = { 0 };
+	TVG_CHECK(device_slot(ctx));
+	int &nblk = nblk_dev[ctx->device];
 	const size_t smem = sizeof(EwaldSmem) * GW_WARPS + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : 0);
 	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
 	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
