@@ -36,6 +36,9 @@ enum {
 	TVG_E_STATE = 7        /* call out of order (e.g. walk before tree build) */
 };
 
+/* Largest capacity a context accepts: node and particle indices are 32-bit. */
+#define TVG_MAX_PARTICLES (((int64_t) 1 << 30) - 4096)
+
 typedef struct tvg_context tvg_context;
 
 /* Compile-time Config and run-time parameters of the reference that the hot
@@ -50,7 +53,7 @@ typedef struct {
 	double open_rel;       /* TREE_OPEN_PARAM_REL */
 	int32_t vector_size;   /* VECTOR_SIZE */
 	int32_t flags;         /* TVG_CFG_* */
-	int64_t max_particles; /* device capacity (Task.Npart_Total_Max) */
+	int64_t max_particles; /* device capacity (Task.Npart_Total_Max), <= TVG_MAX_PARTICLES */
 } tvg_config;
 
 enum {

@@ -68,7 +68,9 @@ extern "C" int tvg_init(int device, const tvg_config *cfg, tvg_context **out)
 	if (!out || !cfg) return TVG_E_BADINPUT;
 	*out = nullptr;
 	if (cfg->float_bytes != 4 && cfg->float_bytes != 8) return TVG_E_BADINPUT;
-	if (cfg->max_particles <= 0 || cfg->max_particles > (int64_t) 1 << 30) return TVG_E_BADINPUT;
+	// node and particle indices are 32-bit: the uncollapsed-node capacity
+	// 2 max_particles + 4096 must stay below 2^31
+	if (cfg->max_particles <= 0 || cfg->max_particles > TVG_MAX_PARTICLES) return TVG_E_BADINPUT;
 	if (cfg->periodic && !(cfg->boxsize > 0)) return TVG_E_BADINPUT;
 	if (cfg->vector_size <= 0 || cfg->vector_size > 64) return TVG_E_BADINPUT;
 	int ndev = 0;
