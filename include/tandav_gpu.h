@@ -240,6 +240,14 @@ int tvg_launch_count(tvg_context *ctx, int64_t *count);
 /* Page-locked host memory for transfers that overlap with device work. */
 int tvg_host_alloc(size_t bytes, void **ptr);
 int tvg_host_free(void *ptr);
+/* Page-locks an existing host range (cudaHostRegister), so that uploads from
+ * and downloads into it run as direct transfers: the reference's memory pool
+ * (`Memory`, posix_memalign in Init_Memory_Management, memory.c:209), which
+ * holds P, is registered once after it is allocated and unregistered before
+ * it is freed. TVG_E_BADINPUT for a NULL or empty range, TVG_E_STATE when
+ * (part of) the range is registered already, TVG_E_CUDA otherwise. */
+int tvg_host_register(void *ptr, size_t bytes);
+int tvg_host_unregister(void *ptr);
 
 /* Measured FP32 FFMA throughput of the device (TFLOP/s, FMA = 2 flop) over
  * `ms_target` milliseconds: the denominator of the walk's roofline. */

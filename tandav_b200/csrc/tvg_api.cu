@@ -553,6 +553,24 @@ extern "C" int tvg_host_alloc(size_t bytes, void **ptr)
 	return TVG_OK;
 }
 
+extern "C" int tvg_host_register(void *ptr, size_t bytes)
+{
+	if (!ptr || !bytes) return TVG_E_BADINPUT;
+	const cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+	if (e == cudaSuccess) return TVG_OK;
+	cudaGetLastError();
+	return e == cudaErrorHostMemoryAlreadyRegistered ? TVG_E_STATE : TVG_E_CUDA;
+}
+
+extern "C" int tvg_host_unregister(void *ptr)
+{
+	if (!ptr) return TVG_E_BADINPUT;
+	const cudaError_t e = cudaHostUnregister(ptr);
+	if (e == cudaSuccess) return TVG_OK;
+	cudaGetLastError();
+	return e == cudaErrorHostMemoryNotRegistered ? TVG_E_STATE : TVG_E_CUDA;
+}
+
 extern "C" int tvg_host_free(void *ptr)
 {
 	return cudaFreeHost(ptr) == cudaSuccess ? TVG_OK : TVG_E_CUDA;

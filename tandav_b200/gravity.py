@@ -593,6 +593,22 @@ class GravityContext:
         self._check(self.lib.tvg_download(self.ctx, C.byref(p), C.c_uint32(fields)), "download")
 
 
+def host_register(a):
+    """Page-lock the memory of a contiguous numpy array (tvg_host_register)."""
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("host_register needs a contiguous array")
+    rc = lib().tvg_host_register(C.c_void_p(a.ctypes.data), C.c_size_t(a.nbytes))
+    if rc != TVG_OK:
+        raise TvgError(rc, "tvg_host_register failed")
+
+
+def host_unregister(a):
+    """Release a range registered with host_register."""
+    rc = lib().tvg_host_unregister(C.c_void_p(a.ctypes.data))
+    if rc != TVG_OK:
+        raise TvgError(rc, "tvg_host_unregister failed")
+
+
 class PinnedArray:
     """numpy view of page-locked host memory (tvg_host_alloc)."""
 

@@ -51,3 +51,18 @@ def test_init_without_gpu_reports_cuda_error():
     assert lib.tvg_init(0, C.byref(cfg), C.byref(ctx)) == 1      # TVG_E_CUDA
     with pytest.raises(gravity.TvgError):
         gravity.GravityContext(100)
+
+
+def test_init_rejects_capacity_beyond_32bit_indices():
+    lib = tandav_b200.lib()
+    ctx = C.c_void_p()
+    cfg = gravity.Config(4, 0, 0.0, 1.0, 0.01, 0.25, 0.005, 64, 0, (1 << 30) - 4095)
+    assert lib.tvg_init(0, C.byref(cfg), C.byref(ctx)) == 5      # > TVG_MAX_PARTICLES
+
+
+def test_host_register_rejects_null_or_empty_ranges():
+    lib = tandav_b200.lib()
+    buf = (C.c_char * 64)()
+    assert lib.tvg_host_register(None, C.c_size_t(64)) == 5
+    assert lib.tvg_host_register(buf, C.c_size_t(0)) == 5
+    assert lib.tvg_host_unregister(None) == 5
