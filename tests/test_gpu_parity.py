@@ -159,6 +159,7 @@ def test_fast_moments_close_to_exact():
     assert np.allclose(exact["CoM"], fast["CoM"], rtol=0, atol=1e-4 * p.box)
 
 
+@pytest.mark.late
 @pytest.mark.parametrize("kind,fsize,n,exact", [("zeldovich", 4, 128 ** 3, True),
                                                ("zeldovich", 4, 128 ** 3, False),
                                                ("hernquist", 8, 1 << 20, True)])

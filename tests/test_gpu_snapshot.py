@@ -10,7 +10,7 @@ import pytest
 from tandav_b200 import gravity as G
 from tandav_b200 import ics
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.late]
 
 
 @pytest.mark.parametrize("fb", [4, 8])
