@@ -347,12 +347,20 @@ static int run_force(const struct input *in, bool update)
 		t_build = now() - t0;
 	}
 
-	/* bounded CPU sample (flags bits 8..31 = stride s > 1): the walks run for
-	 * every s-th particle only, as a reduced Active_Particle_List */
-	const int stride = (flags >> 8) > 1 ? (flags >> 8) : 1;
+	/* bounded CPU sample (flags bits 8..23 = stride s > 1): the walks run for
+	 * every s-th particle only, as a reduced Active_Particle_List. Bits 24..30
+	 * = repetitions R <= s: the BH pass runs for the particles i with
+	 * i % s < R, then the relative pass R times, repetition r for the
+	 * particles i % s == r, each timed ("rel_times") */
+	const int stride = ((flags >> 8) & 0xFFFF) > 1 ? ((flags >> 8) & 0xFFFF) : 1;
+	int reps = (flags >> 24) & 0x7F;
+	if (reps < 1) reps = 1;
+	if (reps > stride) reps = stride;
+	double rel_times[128] = { 0 };
 	if (stride > 1) {
 		int na = 0;
-		for (int64_t i = 0; i < n; i += stride) Active_Particle_List[na++] = (int) i;
+		for (int64_t i = 0; i < n; i++)
+			if (i % stride < reps) Active_Particle_List[na++] = (int) i;
 		NActive_Particles = na;
 	}
 	const bool dump_bulk = (flags & 4) == 0;
@@ -437,15 +445,28 @@ static int run_force(const struct input *in, bool update)
 			}
 		}
 		if (flags & 2) {
-			zero_accumulators();
-			#pragma omp master
-			t0 = now();
-			Sig.Use_BH_Criterion = false;
-			Gravity_Tree_Acceleration();
-			#pragma omp barrier
-			#pragma omp master
-			{ t_rel = now() - t0; dump_forces("rel", n); }
-			#pragma omp barrier
+			for (int r = 0; r < reps; r++) {
+				if (reps > 1) {
+					#pragma omp single
+					{
+						int na = 0;
+						for (int64_t i = r; i < n; i += stride) Active_Particle_List[na++] = (int) i;
+						NActive_Particles = na;
+					}
+				}
+				zero_accumulators();
+				#pragma omp master
+				t0 = now();
+				Sig.Use_BH_Criterion = false;
+				Gravity_Tree_Acceleration();
+				#pragma omp barrier
+				#pragma omp master
+				{
+					rel_times[r] = now() - t0;
+					if (r == 0) { t_rel = rel_times[0]; dump_forces("rel", n); }
+				}
+				#pragma omp barrier
+			}
 			if (periodic && dump_bulk) {
 				zero_accumulators();
 				#pragma omp master
@@ -466,6 +487,7 @@ static int run_force(const struct input *in, bool update)
 	}
 	double timings[8] = { t_ewald_init, t_dd, t_build, t_bh, t_bh_ew, t_rel, t_rel_ew, (double) NThreads };
 	put("timings", timings, sizeof(timings));
+	put("rel_times", rel_times, (int64_t) reps * sizeof(double));
 	double gconst = Const.Gravity;
 	put("gravity", &gconst, sizeof(double));
 	double eps[3] = { Epsilon[1], Epsilon2[1], Epsilon3[1] };
