@@ -1,6 +1,7 @@
 """Snapshot of the resident particles (tvg_write_snapshot): after a force step
 (keys, sort, build, walks on the device) the file holds the particles in
-their Peano-Hilbert order with their IDs, Acc[0] and Grav_Acc, and equals
+their Peano-Hilbert order with their IDs, Acc[0], Grav_Acc and (FP64 with
+GRAVITY_POTENTIAL) Grav_Pot, and equals
 byte for byte the file the host writer makes from the downloaded fields. The
 host writer itself is pinned to the reference's Write_Snapshot in
 test_snapshot.py."""
@@ -13,24 +14,26 @@ from tandav_b200 import ics
 pytestmark = [pytest.mark.gpu, pytest.mark.late]
 
 
-@pytest.mark.parametrize("fb", [4, 8])
-def test_device_snapshot_equals_host_writer(tmp_path, fb):
+@pytest.mark.parametrize("fb,potential", [(4, False), (8, True)])
+def test_device_snapshot_equals_host_writer(tmp_path, fb, potential):
     p = ics.zeldovich_box(n_side=24, seed=17)
     ft = np.float32 if fb == 4 else np.float64
     ids = np.arange(p.n, dtype=np.uint32)
+    flags = G.CFG_POTENTIAL if potential else 0
     with G.GravityContext(p.n, float_bytes=fb, periodic=True, boxsize=p.box,
-                          softening=p.softening) as ctx:
+                          softening=p.softening, flags=flags) as ctx:
         ctx.upload(p.pos, p.mass, vel=p.vel, ids=ids)
         ctx.set_domain((0, 0, 0), p.box)
         ctx.ewald_init()
         form = G.FORM_GROUP if fb == 4 else G.FORM_PLAIN
         ctx.force_step(form=form, use_bh=True, parts=G.WALK_GRAVITY | G.WALK_EWALD)
         h = G.snapshot_header(p.n, p.a_start, p.box, 0.3, 0.7, 0.7)
-        blocks = G.SNAP_ACC | G.SNAP_GACC
+        blocks = G.SNAP_ACC | G.SNAP_GACC | (G.SNAP_GPOT if potential else 0)
         ctx.write_snapshot(tmp_path / "dev_000", h, blocks)
-        d = ctx.download(G.F_POS | G.F_VEL | G.F_ID | G.F_MASS | G.F_ACC | G.F_GRAV_ACC)
+        d = ctx.download(G.F_POS | G.F_VEL | G.F_ID | G.F_MASS | G.F_ACC | G.F_GRAV_ACC
+                         | (G.F_GRAV_POT if potential else 0))
     G.write_snapshot_host(tmp_path / "host_000", h, d["pos"], d["vel"], d["id"], d["mass"],
-                          acc=d["acc"], grav_acc=d["grav_acc"])
+                          acc=d["acc"], grav_acc=d["grav_acc"], grav_pot=d.get("grav_pot"))
     assert (tmp_path / "dev_000").read_bytes() == (tmp_path / "host_000").read_bytes()
     # sorted order: the IDs are a permutation and carry their particles along
     assert np.array_equal(np.sort(d["id"]), ids)
@@ -38,3 +41,5 @@ def test_device_snapshot_equals_host_writer(tmp_path, fb):
     np.testing.assert_array_equal(d["pos"], p.pos.astype(ft)[:, d["id"]])
     np.testing.assert_array_equal(d["vel"], p.vel.astype(ft)[:, d["id"]])
     assert np.all(np.isfinite(d["grav_acc"])) and np.any(d["grav_acc"] != 0)
+    if potential:
+        assert np.all(np.isfinite(d["grav_pot"])) and np.any(d["grav_pot"] != 0)
