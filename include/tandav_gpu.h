@@ -491,7 +491,8 @@ typedef struct {
 enum {
 	TVG_SNAP_ACC = 1,      /* "ACC ": one component, Acc[0], as the reference's table declares */
 	TVG_SNAP_GACC = 2,     /* "GACC": Grav_Acc[3] (OUTPUT_PARTIAL_ACCELERATIONS) */
-	TVG_SNAP_GPOT = 4      /* "GPOT": Grav_Pot (OUTPUT_GRAV_POTENTIAL) */
+	TVG_SNAP_GPOT = 4,     /* "GPOT": Grav_Pot (OUTPUT_GRAV_POTENTIAL) */
+	TVG_SNAP_MASS = 8      /* reading: the MASS block was present */
 };
 
 /* Write_Snapshot (IO/write_snapshot.c:13-328) for one rank and one file:
@@ -505,6 +506,27 @@ int tvg_write_snapshot_host(const char *path, const tvg_snapshot_header *header,
  * current order (PH order after a sort, as the reference writes them). */
 int tvg_write_snapshot(tvg_context *ctx, const char *path, const tvg_snapshot_header *header,
                        uint32_t blocks);
+/* read_header_data (IO/read_snapshot.c:313-402): the header of the snapshot
+ * `path`, or of `path.0` when the snapshot is split into files path.0,
+ * path.1, ... (find_files, :544-575); *num_files receives their number.
+ * Files of either byte order are read. */
+int tvg_read_snapshot_header(const char *path, tvg_snapshot_header *header, int32_t *num_files);
+/* Read_Snapshot (IO/read_snapshot.c:19-123) for one rank: the particles of
+ * all files into the host arrays of p (cap entries each, Float of
+ * float_bytes; IDs 32-bit). POS, VEL and ID are required; MASS, ACC
+ * (component 0), GACC and GPOT are read when present and p has the array.
+ * As the reference stores them (Reallocate_P): one section per type in
+ * increasing type order, each in file order. Masses come from the header's
+ * Massarr of the type's section when any Massarr is nonzero
+ * (generate_masses_from_header, :412-437), else from the MASS block; p->type
+ * from the ID ranges of the header's per-type totals (set_particle_types,
+ * :444-474), or the section's type where no range holds the ID (the
+ * reference leaves it unset). *n receives the particle count, *blocks the
+ * TVG_SNAP_* bits of the optional blocks found in every file. A block whose
+ * size disagrees with the file's particle count and the Float width, a
+ * missing required block or n > cap are TVG_E_BADINPUT. */
+int tvg_read_snapshot_host(const char *path, int32_t float_bytes, int64_t cap, tvg_particles *p,
+                           int64_t *n, uint32_t *blocks);
 
 #ifdef __cplusplus
 }

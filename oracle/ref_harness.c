@@ -24,6 +24,8 @@
  *   mode "update": "force" with the tree updates between rebuilds applied
  *                 to the built tree before the walks (tree_update_sequence).
  *   mode "snap":  Write_Snapshot of the input particles (run_snap).
+ *   mode "read":  Read_Snapshot of a snapshot file given in place of the
+ *                 input file (run_read).
  *
  * Input  (little endian): "TVIN", int32 version(1), int64 n, double box
  *   (<=0: isolated), double softening, double origin[3], double size,
@@ -39,6 +41,7 @@
 #include "Gravity/periodic.h"
 #include "periodic.h"
 #include "vector.h"
+#include "IO/io.h"
 
 void Init_Memory_Management(void);
 void Setup_Leaf_Vectors(void);
@@ -534,13 +537,80 @@ static int run_snap(const struct input *in, const char *out_base)
 	return 0;
 }
 
+/* Read_Snapshot (IO/read_snapshot.c:19-123) of the snapshot at `path` (or
+ * path.0, path.1, ...): the memory pool is sized from the header's totals,
+ * then the reference reads the file(s) into P. Dumps the particles in the
+ * order read (ID, Type, Pos, Vel, Mass, Acc[0], Grav_Acc as doubles) and
+ * Sim's per-type counts and masses. */
+static int run_read(const char *path)
+{
+	char first[CHARBUFSIZE];
+	snprintf(first, sizeof(first), "%s", path);
+	FILE *fp = fopen(first, "rb");
+	if (!fp) {
+		snprintf(first, sizeof(first), "%s.0", path);
+		fp = fopen(first, "rb");
+	}
+	if (!fp) { fprintf(stderr, "cannot open %s\n", path); return 2; }
+	unsigned char head[20 + 256];
+	if (fread(head, 1, sizeof(head), fp) != sizeof(head)) { fclose(fp); return 2; }
+	fclose(fp);
+	int64_t total = 0;
+	for (int t = 0; t < 6; t++) {
+		uint32_t lo, hi;
+		memcpy(&lo, head + 20 + 96 + 4 * t, 4);
+		memcpy(&hi, head + 20 + 168 + 4 * t, 4);
+		total += (int64_t) lo + ((int64_t) hi << 32);
+	}
+	sizeof_P = 0;
+	for (int i = 0; i < NP_Fields; i++) sizeof_P += P_Fields[i].Bytes * P_Fields[i].N;
+	init_memory(total > 0 ? total : 1);
+	Param.Num_IO_Tasks = 1;
+	Read_Snapshot((char *) path);
+	const int64_t n = Task.Npart_Total;
+	put("read_n", &n, 8);
+	uint32_t *id = malloc((n ? n : 1) * sizeof(uint32_t));
+	int32_t *type = malloc((n ? n : 1) * sizeof(int32_t));
+	double *buf = malloc((n ? 3 * n : 1) * sizeof(double));
+	for (int64_t i = 0; i < n; i++) { id[i] = (uint32_t) P.ID[i]; type[i] = P.Type[i]; }
+	put("read_id", id, n * sizeof(uint32_t));
+	put("read_type", type, n * sizeof(int32_t));
+	for (int k = 0; k < 3; k++) for (int64_t i = 0; i < n; i++) buf[k * n + i] = P.Pos[k][i];
+	put("read_pos", buf, 3 * n * sizeof(double));
+	for (int k = 0; k < 3; k++) for (int64_t i = 0; i < n; i++) buf[k * n + i] = P.Vel[k][i];
+	put("read_vel", buf, 3 * n * sizeof(double));
+	for (int64_t i = 0; i < n; i++) buf[i] = P.Mass[i];
+	put("read_mass", buf, n * sizeof(double));
+	for (int64_t i = 0; i < n; i++) buf[i] = P.Acc[0][i];
+	put("read_acc0", buf, n * sizeof(double));
+	for (int k = 0; k < 3; k++) for (int64_t i = 0; i < n; i++) buf[k * n + i] = P.Grav_Acc[k][i];
+	put("read_gacc", buf, 3 * n * sizeof(double));
+	int64_t npart[6];
+	double mpart[6];
+	for (int t = 0; t < 6; t++) { npart[t] = (int64_t) Sim.Npart[t]; mpart[t] = Sim.Mpart[t]; }
+	put("sim_npart", npart, sizeof(npart));
+	put("sim_mpart", mpart, sizeof(mpart));
+	int32_t fsize = (int32_t) sizeof(Float);
+	put("float_size", &fsize, 4);
+	free(id); free(type); free(buf);
+	return 0;
+}
+
 int main(int argc, char *argv[])
 {
 	if (argc != 4) {
-		fprintf(stderr, "usage: %s force|keys|snap|update input.bin output.bin\n", argv[0]);
+		fprintf(stderr, "usage: %s force|keys|snap|update input.bin output.bin\n"
+		                "       %s read snapshot output.bin\n", argv[0], argv[0]);
 		return 1;
 	}
 	preamble();
+	if (!strcmp(argv[1], "read")) {       /* argv[2] is a snapshot, not an input file */
+		Out = fopen(argv[3], "wb");
+		if (!Out) { fprintf(stderr, "cannot write %s\n", argv[3]); return 2; }
+		int rc = run_read(argv[2]);
+		fclose(Out);
+		return rc;
+	}
 	struct input in = read_input(argv[2]);
 	Out = fopen(argv[3], "wb");
 	if (!Out) { fprintf(stderr, "cannot write %s\n", argv[3]); return 2; }

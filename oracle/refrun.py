@@ -106,6 +106,35 @@ def run(variant: str, mode: str, pos, vel=None, mass=None, box=0.0, softening=0.
     return out
 
 
+def read_snapshot(variant: str, path, threads: int = 1, timeout: float = 600.0) -> dict:
+    """Run the reference's Read_Snapshot (``ref_harness read``) on a snapshot
+    file (or the files path.0, path.1, ...) and return what it loaded."""
+    exe = harness_path(variant)
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref`")
+    with tempfile.TemporaryDirectory() as td:
+        fout = Path(td) / "out.bin"
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        proc = subprocess.run([str(exe), "read", str(path), str(fout)], cwd=td, env=env,
+                              stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"ref_harness read failed ({proc.returncode}): "
+                               f"{proc.stderr.decode()[-2000:]}{proc.stdout.decode()[-2000:]}")
+        rec = read_output(fout)
+    n = struct.unpack("<q", rec["read_n"])[0]
+    fsize = struct.unpack("<i", rec["float_size"])[0]
+    return dict(n=n, float_size=fsize,
+                id=np.frombuffer(rec["read_id"], "<u4").copy(),
+                type=np.frombuffer(rec["read_type"], "<i4").copy(),
+                pos=np.frombuffer(rec["read_pos"], "<f8").reshape(3, n).copy(),
+                vel=np.frombuffer(rec["read_vel"], "<f8").reshape(3, n).copy(),
+                mass=np.frombuffer(rec["read_mass"], "<f8").copy(),
+                acc0=np.frombuffer(rec["read_acc0"], "<f8").copy(),
+                grav_acc=np.frombuffer(rec["read_gacc"], "<f8").reshape(3, n).copy(),
+                sim_npart=np.frombuffer(rec["sim_npart"], "<i8").copy(),
+                sim_mpart=np.frombuffer(rec["sim_mpart"], "<f8").copy())
+
+
 def decode(rec: dict, n: int) -> dict:
     out = {}
     fsize = struct.unpack("<i", rec["float_size"])[0] if "float_size" in rec else 4

@@ -12,6 +12,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <array>
+#include <string>
 #include <vector>
 
 #include "tvg_internal.cuh"
@@ -218,4 +220,250 @@ extern "C" int tvg_write_snapshot(tvg_context *ctx, const char *path, const tvg_
 		return f.rc;
 	}
 	return rc;
+}
+
+// ------------------------------------------------------------------ reading
+
+namespace {
+
+uint32_t bswap32(uint32_t v) { return __builtin_bswap32(v); }
+
+void swap_words(unsigned char *d, size_t bytes, size_t word)
+{
+	for (size_t o = 0; o + word <= bytes; o += word)
+		for (size_t a = 0, b = word - 1; a < b; a++, b--) {
+			const unsigned char t = d[o + a];
+			d[o + a] = d[o + b];
+			d[o + b] = t;
+		}
+}
+
+// one format-2 file: its blocks by label (payload offset and size)
+struct SnapFile {
+	FILE *fp = nullptr;
+	bool swap = false;
+	struct Blk { char label[4]; long off; uint32_t size; };
+	std::vector<Blk> blocks;
+	~SnapFile() { if (fp) fclose(fp); }
+
+	bool u32(uint32_t *v)
+	{
+		if (fread(v, 4, 1, fp) != 1) return false;
+		if (swap) *v = bswap32(*v);
+		return true;
+	}
+	// the byte order from the first record marker (find_endianess,
+	// read_snapshot.c:519-541), then every block's label record
+	bool open(const char *path)
+	{
+		fp = fopen(path, "rb");
+		if (!fp) return false;
+		uint32_t first = 0;
+		if (fread(&first, 4, 1, fp) != 1) return false;
+		if (first == 8) swap = false;
+		else if (bswap32(first) == 8) swap = true;
+		else return false;                      // not a format-2 file
+		rewind(fp);
+		for (;;) {
+			uint32_t m0, size8, m1, a, b;
+			Blk k;
+			if (!u32(&m0)) break;                   // end of file
+			if (m0 != 8 || fread(k.label, 1, 4, fp) != 4 || !u32(&size8) || !u32(&m1) || m1 != 8)
+				return false;
+			if (!u32(&a) || a + 8 != size8) return false;
+			k.off = ftell(fp);
+			k.size = a;
+			if (fseek(fp, (long) a, SEEK_CUR) != 0 || !u32(&b) || b != a) return false;
+			blocks.push_back(k);
+		}
+		return true;
+	}
+	const Blk *find(const char *label) const
+	{
+		for (const Blk &k : blocks)
+			if (!memcmp(k.label, label, 4)) return &k;
+		return nullptr;
+	}
+	bool read(const Blk *k, void *dst, size_t word)
+	{
+		if (fseek(fp, k->off, SEEK_SET) != 0 || fread(dst, 1, k->size, fp) != k->size) return false;
+		if (swap) swap_words((unsigned char *) dst, k->size, word);
+		return true;
+	}
+};
+
+// the 256-byte header (struct gadget_header, io.h:24-44)
+bool parse_header(SnapFile &f, tvg_snapshot_header *h, uint32_t npart[6])
+{
+	const SnapFile::Blk *k = f.find("HEAD");
+	if (!k || k->size != 256) return false;
+	unsigned char b[256];
+	if (fseek(f.fp, k->off, SEEK_SET) != 0 || fread(b, 1, 256, f.fp) != 256) return false;
+	if (f.swap) {
+		swap_words(b, 24, 4);                  // Npart
+		swap_words(b + 24, 64, 8);             // Massarr, Time, Redshift
+		swap_words(b + 88, 40, 4);             // Flag_Sfr .. Num_Files
+		swap_words(b + 128, 32, 8);            // Boxsize .. Hubble_Param
+		swap_words(b + 160, 32, 4);            // Flag_Age, Flag_Metals, Nall_High_Word
+	}
+	memset(h, 0, sizeof(*h));
+	for (int t = 0; t < 6; t++) {
+		uint32_t lo, hi;
+		memcpy(&npart[t], b + 4 * t, 4);
+		memcpy(&h->massarr[t], b + 24 + 8 * t, 8);
+		memcpy(&lo, b + 96 + 4 * t, 4);
+		memcpy(&hi, b + 168 + 4 * t, 4);
+		h->npart[t] = npart[t];
+		h->nall[t] = (uint64_t) lo | ((uint64_t) hi << 32);
+	}
+	memcpy(&h->time, b + 72, 8);
+	memcpy(&h->redshift, b + 80, 8);
+	memcpy(&h->num_files, b + 124, 4);
+	memcpy(&h->boxsize, b + 128, 8);
+	memcpy(&h->omega0, b + 136, 8);
+	memcpy(&h->omega_lambda, b + 144, 8);
+	memcpy(&h->hubble_param, b + 152, 8);
+	return true;
+}
+
+// find_files (read_snapshot.c:544-575): path itself, else path.0, path.1, ...
+std::vector<std::string> snapshot_files(const char *path)
+{
+	std::vector<std::string> out;
+	if (FILE *fp = fopen(path, "rb")) {
+		fclose(fp);
+		out.push_back(path);
+		return out;
+	}
+	for (int i = 0; i < 10000; i++) {
+		std::string name = std::string(path) + "." + std::to_string(i);
+		FILE *fp = fopen(name.c_str(), "rb");
+		if (!fp) break;
+		fclose(fp);
+		out.push_back(name);
+	}
+	return out;
+}
+
+} // namespace
+
+extern "C" int tvg_read_snapshot_header(const char *path, tvg_snapshot_header *header, int32_t *num_files)
+{
+	if (!path || !header) return TVG_E_BADINPUT;
+	const std::vector<std::string> files = snapshot_files(path);
+	if (files.empty()) return TVG_E_BADINPUT;
+	SnapFile f;
+	uint32_t np[6];
+	if (!f.open(files[0].c_str()) || !parse_header(f, header, np)) return TVG_E_BADINPUT;
+	if (num_files) *num_files = (int32_t) files.size();
+	return TVG_OK;
+}
+
+extern "C" int tvg_read_snapshot_host(const char *path, int32_t float_bytes, int64_t cap, tvg_particles *p,
+                                      int64_t *n_out, uint32_t *blocks_out)
+{
+	if (!path || !p || cap < 0 || (float_bytes != 4 && float_bytes != 8)) return TVG_E_BADINPUT;
+	if (!p->pos[0] || !p->pos[1] || !p->pos[2] || !p->vel[0] || !p->vel[1] || !p->vel[2] || !p->id)
+		return TVG_E_BADINPUT;
+	const std::vector<std::string> files = snapshot_files(path);
+	if (files.empty()) return TVG_E_BADINPUT;
+	const size_t fb = (size_t) float_bytes;
+	// per-file and total counts per type; the first file's header gives the
+	// masses and the ID ranges (Sim.Mpart, Sim.Npart)
+	std::vector<std::array<uint32_t, 6>> per_file(files.size());
+	tvg_snapshot_header h0;
+	uint64_t total[6] = { 0 };
+	for (size_t f = 0; f < files.size(); f++) {
+		SnapFile sf;
+		tvg_snapshot_header h;
+		uint32_t np[6];
+		if (!sf.open(files[f].c_str()) || !parse_header(sf, &h, np)) return TVG_E_BADINPUT;
+		if (f == 0) h0 = h;
+		for (int t = 0; t < 6; t++) {
+			per_file[f][t] = np[t];
+			total[t] += np[t];
+		}
+	}
+	uint64_t n = 0, off[6];
+	for (int t = 0; t < 6; t++) {
+		off[t] = n;
+		n += total[t];
+	}
+	if ((int64_t) n > cap) return TVG_E_BADINPUT;
+	// blocks: label, components, bytes per component, destinations
+	struct Want { const char *label; int ncomp; size_t bytes; void *dst[3]; uint32_t bit; bool required; };
+	Want want[] = {
+		{ "POS ", 3, fb, { p->pos[0], p->pos[1], p->pos[2] }, 0, true },
+		{ "VEL ", 3, fb, { p->vel[0], p->vel[1], p->vel[2] }, 0, true },
+		{ "ID  ", 1, 4, { p->id, nullptr, nullptr }, 0, true },
+		{ "MASS", 1, fb, { p->mass, nullptr, nullptr }, TVG_SNAP_MASS, false },
+		{ "ACC ", 1, fb, { p->acc[0], nullptr, nullptr }, TVG_SNAP_ACC, false },
+		{ "GACC", 3, fb, { p->grav_acc[0], p->grav_acc[1], p->grav_acc[2] }, TVG_SNAP_GACC, false },
+		{ "GPOT", 1, fb, { p->grav_pot, nullptr, nullptr }, TVG_SNAP_GPOT, false },
+	};
+	uint32_t found = TVG_SNAP_MASS | TVG_SNAP_ACC | TVG_SNAP_GACC | TVG_SNAP_GPOT;
+	uint64_t run[6] = { 0 };
+	std::vector<unsigned char> buf;
+	for (size_t f = 0; f < files.size(); f++) {
+		SnapFile sf;
+		if (!sf.open(files[f].c_str())) return TVG_E_BADINPUT;
+		uint64_t nf = 0, first[6];
+		for (int t = 0; t < 6; t++) {
+			first[t] = nf;
+			nf += per_file[f][t];
+		}
+		for (const Want &w : want) {
+			const SnapFile::Blk *k = sf.find(w.label);
+			if (!k) {
+				if (w.required) return TVG_E_BADINPUT;   // "Can't find required block"
+				found &= ~w.bit;
+				continue;
+			}
+			if ((uint64_t) k->size != nf * w.ncomp * w.bytes) return TVG_E_BADINPUT;
+			if (!w.dst[0]) continue;                    // present, not wanted
+			buf.resize(k->size > 0 ? k->size : 1);
+			if (k->size && !sf.read(k, buf.data(), w.bytes)) return TVG_E_BADINPUT;
+			// particle j of type t goes to its type's section, after the
+			// particles of that type from the earlier files
+			for (int t = 0; t < 6; t++)
+				for (uint64_t j = 0; j < per_file[f][t]; j++) {
+					const uint64_t src = first[t] + j, dst = off[t] + run[t] + j;
+					for (int c = 0; c < w.ncomp; c++)
+						memcpy((unsigned char *) w.dst[c] + dst * w.bytes,
+						       &buf[(src * w.ncomp + c) * w.bytes], w.bytes);
+				}
+		}
+		for (int t = 0; t < 6; t++) run[t] += per_file[f][t];
+	}
+	// masses from the header (generate_masses_from_header)
+	bool header_mass = false;
+	for (int t = 0; t < 6; t++) header_mass |= h0.massarr[t] != 0;
+	if (header_mass && p->mass)
+		for (int t = 0; t < 6; t++)
+			for (uint64_t i = off[t]; i < off[t] + total[t]; i++) {
+				if (fb == 4) ((float *) p->mass)[i] = (float) h0.massarr[t];
+				else ((double *) p->mass)[i] = h0.massarr[t];
+			}
+	// types from the ID ranges of the header's totals (set_particle_types)
+	if (p->type) {
+		uint64_t lo[6], hi[6], r = 0;
+		bool any[6];
+		for (int t = 0; t < 6; t++) {
+			any[t] = h0.nall[t] != 0;
+			lo[t] = r;
+			r += h0.nall[t];
+			hi[t] = r - 1;
+		}
+		for (int t = 0; t < 6; t++)
+			for (uint64_t i = off[t]; i < off[t] + total[t]; i++) {
+				const uint64_t id = p->id[i];
+				int32_t type = t;
+				for (int u = 0; u < 6; u++)
+					if (any[u] && id >= lo[u] && id <= hi[u]) type = u;
+				p->type[i] = type;
+			}
+	}
+	if (n_out) *n_out = (int64_t) n;
+	if (blocks_out) *blocks_out = found;
+	return TVG_OK;
 }

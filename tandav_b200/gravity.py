@@ -89,8 +89,9 @@ class MlpTrainConfig(C.Structure):
 
 MLP_NPARAM = 4672
 
-# optional blocks of a snapshot after POS, VEL, ID, MASS (src/IO/io.h:74-85)
-SNAP_ACC, SNAP_GACC, SNAP_GPOT = 1, 2, 4
+# optional blocks of a snapshot after POS, VEL, ID, MASS (src/IO/io.h:74-85);
+# SNAP_MASS: a read found the MASS block
+SNAP_ACC, SNAP_GACC, SNAP_GPOT, SNAP_MASS = 1, 2, 4, 8
 
 
 class SnapshotHeader(C.Structure):
@@ -591,6 +592,50 @@ class GravityContext:
             p.id = ids.ctypes.data
             fields |= F_ID
         self._check(self.lib.tvg_download(self.ctx, C.byref(p), C.c_uint32(fields)), "download")
+
+
+def read_snapshot_header(path):
+    """The header of a snapshot (or of path.0 of a split one) and the number
+    of files (tvg_read_snapshot_header)."""
+    h = SnapshotHeader()
+    nf = C.c_int32()
+    rc = lib().tvg_read_snapshot_header(str(path).encode(), C.byref(h), C.byref(nf))
+    if rc != TVG_OK:
+        raise TvgError(rc, f"tvg_read_snapshot_header({path})")
+    return h, nf.value
+
+
+def read_snapshot(path, float_bytes=4):
+    """Read_Snapshot into numpy arrays (tvg_read_snapshot_host): pos, vel
+    (3, n), id, mass, type, and acc0, grav_acc, grav_pot when the file has
+    them; the particles in the reference's order (type sections, each in
+    file order)."""
+    h, nf = read_snapshot_header(path)
+    cap = int(sum(h.nall))
+    ft = np.float32 if float_bytes == 4 else np.float64
+    a = dict(pos=np.zeros((3, cap), ft), vel=np.zeros((3, cap), ft), id=np.zeros(cap, np.uint32),
+             mass=np.zeros(cap, ft), type=np.zeros(cap, np.int32), acc0=np.zeros(cap, ft),
+             grav_acc=np.zeros((3, cap), ft), grav_pot=np.zeros(cap, ft))
+    p = Particles()
+    for k in range(3):
+        p.pos[k] = a["pos"][k].ctypes.data
+        p.vel[k] = a["vel"][k].ctypes.data
+        p.grav_acc[k] = a["grav_acc"][k].ctypes.data
+    p.acc[0] = a["acc0"].ctypes.data
+    p.id, p.mass, p.type = a["id"].ctypes.data, a["mass"].ctypes.data, a["type"].ctypes.data
+    p.grav_pot = a["grav_pot"].ctypes.data
+    n, blocks = C.c_int64(), C.c_uint32()
+    rc = lib().tvg_read_snapshot_host(str(path).encode(), C.c_int32(float_bytes), C.c_int64(cap),
+                                      C.byref(p), C.byref(n), C.byref(blocks))
+    if rc != TVG_OK:
+        raise TvgError(rc, f"tvg_read_snapshot_host({path})")
+    m, b = n.value, blocks.value
+    out = {k: v[..., :m] for k, v in a.items()}
+    for name, bit in (("acc0", SNAP_ACC), ("grav_acc", SNAP_GACC), ("grav_pot", SNAP_GPOT)):
+        if not b & bit:
+            del out[name]
+    out.update(header=h, num_files=nf, n=m, blocks=b)
+    return out
 
 
 def host_register(a):
