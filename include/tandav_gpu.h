@@ -527,6 +527,10 @@ int tvg_read_snapshot_header(const char *path, tvg_snapshot_header *header, int3
  * missing required block or n > cap are TVG_E_BADINPUT. */
 int tvg_read_snapshot_host(const char *path, int32_t float_bytes, int64_t cap, tvg_particles *p,
                            int64_t *n, uint32_t *blocks);
+/* tvg_read_snapshot_host into host staging, then tvg_upload of Pos, Vel, ID,
+ * Mass, Type and the optional fields found (Acc with Acc[0] from the ACC
+ * block, Grav_Acc, Grav_Pot) to the context. */
+int tvg_read_snapshot(tvg_context *ctx, const char *path, int64_t *n, uint32_t *blocks);
 
 #ifdef __cplusplus
 }

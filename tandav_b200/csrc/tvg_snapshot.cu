@@ -467,3 +467,43 @@ extern "C" int tvg_read_snapshot_host(const char *path, int32_t float_bytes, int
 	if (blocks_out) *blocks_out = found;
 	return TVG_OK;
 }
+
+extern "C" int tvg_read_snapshot(tvg_context *ctx, const char *path, int64_t *n_out, uint32_t *blocks_out)
+{
+	if (!ctx || !path) return TVG_E_BADINPUT;
+	tvg_snapshot_header h;
+	int32_t nfiles = 0;
+	if (tvg_read_snapshot_header(path, &h, &nfiles) != TVG_OK)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "read_snapshot: cannot read the header of %s", path);
+	uint64_t cap = 0;
+	for (int t = 0; t < 6; t++) cap += h.nall[t];
+	if ((int64_t) cap > ctx->cap)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "read_snapshot: %llu particles > capacity %lld",
+		                (unsigned long long) cap, (long long) ctx->cap);
+	const size_t fb = tvg_fsize(ctx), m = cap > 0 ? (size_t) cap : 1;
+	// staging: pos 3, vel 3, mass 1, acc 3, grav_acc 3, grav_pot 1 Floats; id, type 4 B
+	std::vector<unsigned char> fl(14 * m * fb, 0), id(4 * m), type(4 * m);
+	tvg_particles p;
+	memset(&p, 0, sizeof(p));
+	unsigned char *q = fl.data();
+	for (int k = 0; k < 3; k++) p.pos[k] = q + (size_t) k * m * fb;
+	for (int k = 0; k < 3; k++) p.vel[k] = q + (size_t) (3 + k) * m * fb;
+	p.mass = q + 6 * m * fb;
+	for (int k = 0; k < 3; k++) p.acc[k] = q + (size_t) (7 + k) * m * fb;
+	for (int k = 0; k < 3; k++) p.grav_acc[k] = q + (size_t) (10 + k) * m * fb;
+	p.grav_pot = q + 13 * m * fb;
+	p.id = (uint32_t *) id.data();
+	p.type = (int32_t *) type.data();
+	int64_t n = 0;
+	uint32_t blocks = 0;
+	if (tvg_read_snapshot_host(path, (int32_t) fb, (int64_t) cap, &p, &n, &blocks) != TVG_OK)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "read_snapshot: cannot read %s", path);
+	uint32_t fields = TVG_F_POS | TVG_F_VEL | TVG_F_ID | TVG_F_MASS | TVG_F_TYPE;
+	if (blocks & TVG_SNAP_ACC) fields |= TVG_F_ACC;
+	if (blocks & TVG_SNAP_GACC) fields |= TVG_F_GRAV_ACC;
+	if (blocks & TVG_SNAP_GPOT) fields |= TVG_F_GRAV_POT;
+	TVG_CHECK(tvg_upload(ctx, n, &p, fields));
+	if (n_out) *n_out = n;
+	if (blocks_out) *blocks_out = blocks;
+	return TVG_OK;
+}

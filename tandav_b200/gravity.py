@@ -575,6 +575,15 @@ class GravityContext:
                     "upload")
         self.n = n
 
+    def read_snapshot(self, path):
+        """Read_Snapshot onto the device (tvg_read_snapshot); returns the
+        particle count and the optional blocks found."""
+        n, b = C.c_int64(), C.c_uint32()
+        self._check(self.lib.tvg_read_snapshot(self.ctx, str(path).encode(), C.byref(n), C.byref(b)),
+                    "read_snapshot")
+        self.n = n.value
+        return n.value, b.value
+
     def write_snapshot(self, path, header, blocks=0):
         """Write_Snapshot of the resident particles in their device order."""
         self._check(self.lib.tvg_write_snapshot(self.ctx, str(path).encode(), C.byref(header),

@@ -43,3 +43,27 @@ def test_device_snapshot_equals_host_writer(tmp_path, fb, potential):
     assert np.all(np.isfinite(d["grav_acc"])) and np.any(d["grav_acc"] != 0)
     if potential:
         assert np.all(np.isfinite(d["grav_pot"])) and np.any(d["grav_pot"] != 0)
+
+
+def test_read_snapshot_to_device(tmp_path):
+    """tvg_read_snapshot: a two-type snapshot read onto the device holds the
+    particles the host reader returns, field for field and in its order."""
+    rng = np.random.default_rng(8)
+    n1, n4 = 3000, 1000
+    n = n1 + n4
+    pos = rng.uniform(0, 100.0, (3, n)).astype(np.float32)
+    vel = rng.normal(0, 30.0, (3, n)).astype(np.float32)
+    mass = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    gacc = rng.normal(0, 1.0, (3, n)).astype(np.float32)
+    ids = np.concatenate([rng.permutation(n1), n1 + rng.permutation(n4)]).astype(np.uint32)
+    h = G.snapshot_header([0, n1, 0, 0, n4, 0], 0.5, 100.0)
+    path = tmp_path / "ics"
+    G.write_snapshot_host(path, h, pos, vel, ids, mass, grav_acc=gacc)
+    host = G.read_snapshot(path, 4)
+    with G.GravityContext(n, float_bytes=4, periodic=True, boxsize=100.0, softening=0.1) as ctx:
+        got_n, blocks = ctx.read_snapshot(path)
+        d = ctx.download(G.F_POS | G.F_VEL | G.F_ID | G.F_MASS | G.F_TYPE | G.F_GRAV_ACC)
+    assert got_n == n and blocks == G.SNAP_MASS | G.SNAP_GACC
+    for k in ("pos", "vel", "id", "mass", "type", "grav_acc"):
+        np.testing.assert_array_equal(d[k], host[k], err_msg=k)
+    np.testing.assert_array_equal(np.unique(d["type"]), [1, 4])
