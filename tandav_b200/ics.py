@@ -200,7 +200,7 @@ def zeldovich_box(n_side: int = 128, box_mpc: float = 100.0, z_start: float = 50
     g = (np.arange(n) + 0.5) * spacing
     qx, qy, qz = np.meshgrid(g, g, g, indexing="ij")
     pos = np.stack([qx, qy, qz]).reshape(3, -1) + disp.reshape(3, -1)
-    pos = np.mod(pos, L)
+    pos = inside_box(np.mod(pos, L), L)
     # peculiar velocity a*H*f*D-scaled displacement; internal variable a^2 dx/dt
     hub = 0.1 * cosmo.E(a)                           # km/s per kpc/h
     vel = disp.reshape(3, -1) * (a * hub * frate) * a
@@ -209,6 +209,18 @@ def zeldovich_box(n_side: int = 128, box_mpc: float = 100.0, z_start: float = 50
     mass = np.full(n ** 3, mpart)
     return Particles(pos=pos, vel=vel, mass=mass, box=L,
                      softening=spacing * softening_frac, a_start=a)
+
+
+def inside_box(pos: np.ndarray, box: float) -> np.ndarray:
+    """Positions in [0, box) in float64 and in float32 alike. np.mod can return
+    box itself for tiny negative inputs, and a float64 position just below the
+    box can round up to box in float32; such coordinates become the largest
+    float32 below box. The reference wraps positions into the box before its
+    first keys (Periodic_Constrain_Particles_To_Box, periodic.c:30-55): a
+    coordinate equal to the box would otherwise take the key of coordinate 0
+    and break the tree's PH contiguity."""
+    below = float(np.nextafter(np.float32(box), np.float32(0.0)))
+    return np.where(pos.astype(np.float32) >= np.float32(box), below, pos)
 
 
 def random_box(n: int, box: float = 1000.0, seed: int = 7, clumps: int = 0) -> Particles:
@@ -220,6 +232,7 @@ def random_box(n: int, box: float = 1000.0, seed: int = 7, clumps: int = 0) -> P
         centres = rng.uniform(0.0, box, (3, clumps))
         which = rng.integers(0, clumps, m)
         pos[:, :m] = np.mod(centres[:, which] + rng.normal(0.0, 0.02 * box, (3, m)), box)
+    pos = inside_box(pos, box)
     vel = rng.normal(0.0, 1.0, (3, n))
     mass = np.full(n, 1.0 / n)
     return Particles(pos=pos, vel=vel, mass=mass, box=box,
