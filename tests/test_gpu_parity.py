@@ -160,6 +160,24 @@ def test_fast_moments_close_to_exact():
 
 
 @pytest.mark.late
+def test_keys_and_sort_of_the_256_box():
+    """The 256^3 benchmark box (16.7M particles): every 128-bit key and the
+    sort permutation bit for bit against the oracle (C restatement, pinned
+    to the reference's keys and sort on the golden cases)."""
+    p, origin, size = make_case("zeldovich", 256 ** 3)
+    std, _ = port.peano_keys(p.pos.astype(np.float32), origin, size, 4)
+    perm_o = port.sort_keys(std)
+    with make_ctx(p.n, 4, box=p.box, softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain(origin, size)
+        ctx.peano_keys()
+        perm = ctx.sort_particles()
+        keys = ctx.download(G.F_KEY)["key"]
+    assert np.array_equal(perm, perm_o)
+    assert np.array_equal(keys, std[perm_o])
+
+
+@pytest.mark.late
 @pytest.mark.parametrize("kind,fsize,n,exact", [("zeldovich", 4, 128 ** 3, True),
                                                ("zeldovich", 4, 128 ** 3, False),
                                                ("hernquist", 8, 1 << 20, True),
