@@ -160,21 +160,26 @@ def test_fast_moments_close_to_exact():
 
 
 @pytest.mark.late
-def test_keys_and_sort_of_the_256_box():
-    """The 256^3 benchmark box (16.7M particles): every 128-bit key and the
-    sort permutation bit for bit against the oracle (C restatement, pinned
-    to the reference's keys and sort on the golden cases)."""
+def test_keys_sort_and_tree_of_the_256_box():
+    """The 256^3 benchmark box (16.7M particles): every 128-bit key, the sort
+    permutation, the top nodes, every field of the 913k tree nodes and
+    Tree_Parent bit for bit against the oracle (C restatement, pinned to the
+    reference on the golden cases)."""
     p, origin, size = make_case("zeldovich", 256 ** 3)
-    std, _ = port.peano_keys(p.pos.astype(np.float32), origin, size, 4)
+    pos_f = p.pos.astype(np.float32)
+    std, rev = port.peano_keys(pos_f, origin, size, 4)
     perm_o = port.sort_keys(std)
+    pos_s, mass_s = pos_f[:, perm_o], p.mass.astype(np.float32)[perm_o]
+    top_o = port.top_nodes(std[perm_o], pos_s, origin, size, 4)
+    tree_o, top_o, parent_o = port.tree_build(rev[perm_o], pos_s, mass_s, size, top_o, 4)
     with make_ctx(p.n, 4, box=p.box, softening=p.softening) as ctx:
-        ctx.upload(p.pos, p.mass)
-        ctx.set_domain(origin, size)
-        ctx.peano_keys()
-        perm = ctx.sort_particles()
-        keys = ctx.download(G.F_KEY)["key"]
+        perm, keys, tree, top = gpu_pipeline(ctx, p.pos, p.mass, origin, size, exact=True)
+        parent = ctx.download(G.F_TREE_PARENT)["tree_parent"]
     assert np.array_equal(perm, perm_o)
     assert np.array_equal(keys, std[perm_o])
+    assert_struct_equal(top, top_o, TOP_FIELDS, "topnodes")
+    assert_struct_equal(tree, tree_o, TREE_FIELDS, "tree")
+    assert np.array_equal(parent, parent_o)
 
 
 @pytest.mark.late
