@@ -49,3 +49,26 @@ def test_ctypes_structs_match_the_header(tmp_path):
         assert c["size"] == C.sizeof(cls), cname
         for field, _ in cls._fields_:
             assert c[field] == getattr(cls, field).offset, f"{cname}.{field}"
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
+def test_topnode_dtype_matches_the_header(tmp_path):
+    """gravity.TOPNODE_DTYPE (what tvg_download_tree fills) against
+    tvg_topnode: size and the offset of every field."""
+    names = {"Key": "key", "Target": "target", "Level": "level", "First_Part": "first_part",
+             "Npart": "npart", "Pos": "pos", "Mass": "mass", "CoM": "com", "Dp": "dp"}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "tandav_gpu.h"',
+             "int main(void) {", '  printf("%zu", sizeof(tvg_topnode));']
+    for c in names.values():
+        lines.append(f'  printf(" %zu", offsetof(tvg_topnode, {c}));')
+    lines += ['  printf("\\n");', "  return 0;", "}"]
+    src = tmp_path / "top.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "top"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True,
+                                           text=True).stdout.split()]
+    dt = G.TOPNODE_DTYPE
+    assert vals[0] == dt.itemsize
+    assert vals[1:] == [dt.fields[f][1] for f in names]
