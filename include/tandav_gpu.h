@@ -136,6 +136,13 @@ int tvg_download(tvg_context *ctx, tvg_particles *p, uint32_t fields);
 /* Domain.Origin / Domain.Size used by the keys (set_computational_domain,
  * src/domain.c:732-762). */
 int tvg_set_domain(tvg_context *ctx, const double origin[3], double size);
+/* set_computational_domain (domain.c:732-847) from the resident positions,
+ * then tvg_set_domain with the result. Periodic: origin 0, size the box.
+ * Isolated: centre = the median of each coordinate as the reference's Median
+ * computes it (the (n >> 1)-th smallest of particles 1 .. n-1 in the current
+ * order, kept in Float; select.c:19-107), size = 2.001 * the largest
+ * |x - centre| over particles and axes (double), origin = centre - size / 2. */
+int tvg_find_domain(tvg_context *ctx, double origin[3], double *size);
 
 /* Replaces the Peano_Key loop of Sort_Particles_By_Peano_Key
  * (src/peano.c:27-30): P.Key = standard 128-bit key of P.Pos. */

@@ -146,3 +146,26 @@ def direct(pos, mass, targets, gravity, softening, box=0.0, corr_table=None, cor
                      C.c_double(gravity), C.c_double(softening), C.c_double(box), _p(ct),
                      C.c_int32(corr_n), _p(acc))
     return acc
+
+
+def find_domain(pos, fsize=4, box=0.0):
+    """set_computational_domain (src/domain.c:732-847) restated: periodic ->
+    (origin 0, size box); isolated -> centre = Median of each coordinate as
+    select.c computes it, Select(n >> 1, n, data) with the 1-based Numerical
+    Recipes bounds on a 0-based array, i.e. the (n >> 1)-th smallest of
+    data[1 .. n-1] (data[0] for n = 1), kept in Float; size = 2.001 * the
+    largest |x - centre| (double); origin = centre - size / 2."""
+    if box > 0:
+        return np.zeros(3), float(box)
+    p = np.asarray(pos, dtype=ftype(fsize))
+    n = p.shape[1]
+    center = np.zeros(3)
+    for d in range(3):
+        if n == 1:
+            center[d] = float(p[d, 0])
+        else:
+            k = n >> 1
+            center[d] = float(np.partition(p[d, 1:], k - 1)[k - 1])
+    maxd = float(np.abs(p.astype(np.float64) - center[:, None]).max())
+    size = 2.001 * maxd
+    return center - 0.5 * size, size

@@ -32,7 +32,8 @@ EXPORTS = (
     "tvg_ewald_mlp_train",
     "tvg_ewald_mlp_weights", "tvg_ewald_mlp_grad", "tvg_ewald_mlp_eval", "tvg_ewald_mlp_validate",
     "tvg_autotune", "tvg_write_snapshot", "tvg_write_snapshot_host",
-    "tvg_read_snapshot_header", "tvg_read_snapshot_host", "tvg_read_snapshot", "tvg_time_for_domain_update",
+    "tvg_read_snapshot_header", "tvg_read_snapshot_host", "tvg_read_snapshot",
+    "tvg_find_domain", "tvg_time_for_domain_update",
 )
 
 

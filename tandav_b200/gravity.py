@@ -303,6 +303,14 @@ class GravityContext:
         o = (C.c_double * 3)(*origin)
         self._check(self.lib.tvg_set_domain(self.ctx, o, C.c_double(size)), "set_domain")
 
+    def find_domain(self):
+        """set_computational_domain on the device (tvg_find_domain); sets and
+        returns (origin, size)."""
+        o = (C.c_double * 3)()
+        s = C.c_double()
+        self._check(self.lib.tvg_find_domain(self.ctx, o, C.byref(s)), "find_domain")
+        return np.array(o[:]), s.value
+
     def peano_keys(self):
         self._check(self.lib.tvg_peano_keys(self.ctx), "peano_keys")
 

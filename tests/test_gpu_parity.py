@@ -160,6 +160,33 @@ def test_fast_moments_close_to_exact():
 
 
 @pytest.mark.late
+@pytest.mark.parametrize("case", ["hernquist_iso_f32", "hernquist_iso_f64", "hernquist_2^18"])
+def test_find_domain_matches_reference(golden_dir, case):
+    """tvg_find_domain as the reference's setup runs it: on the input order,
+    then (after the keys and the sort) on the PH order. The golden cases
+    match the reference's Domain.Origin/Size bit for bit; a 2^18 sphere
+    matches the restatement (port.find_domain) in FP32."""
+    if case.startswith("hernquist_iso"):
+        g = np.load(golden_dir / f"{case}.npz")
+        fs, pos, mass = int(g["float_size"]), g["pos_in"], g["mass_in"]
+        want_o, want_s = g["domain_origin"], float(g["domain_size"][0])
+    else:
+        p = ics.hernquist(n=1 << 18, seed=9)
+        fs, pos, mass = 4, p.pos, p.mass
+        pf = pos.astype(np.float32)
+        o1, s1 = port.find_domain(pf, 4)
+        std, _ = port.peano_keys(pf, o1, s1, 4)
+        want_o, want_s = port.find_domain(pf[:, port.sort_keys(std)], 4)
+    with make_ctx(pos.shape[1], fs) as ctx:
+        ctx.upload(pos, mass)
+        ctx.find_domain()                         # Setup_Domain_Decomposition
+        ctx.peano_keys()
+        ctx.sort_particles()
+        o, s = ctx.find_domain()                  # Domain_Decomposition
+    assert np.array_equal(o, want_o) and s == want_s
+
+
+@pytest.mark.late
 def test_keys_sort_and_tree_of_the_256_box():
     """The 256^3 benchmark box (16.7M particles): every 128-bit key, the sort
     permutation, the top nodes, every field of the 913k tree nodes and

@@ -155,3 +155,23 @@ def test_tree_audit_on_reference_trees(golden_dir, case):
             bad[field][i + 1, k] += delta
         with pytest.raises(AssertionError):
             audit(bad, g["topnodes"], pos, mass, size, fsize)
+
+
+@pytest.mark.parametrize("case", ["hernquist_iso_f32", "hernquist_iso_f64"])
+def test_domain_matches_reference(golden_dir, case):
+    """set_computational_domain restated (port.find_domain) against the
+    reference's Domain.Origin/Size. The reference computes it twice before
+    its first tree: in Setup_Domain_Decomposition on the input order, then,
+    after that sort, in Domain_Decomposition on the PH order
+    (domain.c:67-71, 150-172). Its Median leaves out the first particle of
+    the current order (select.c:19-107), so the second pass differs from the
+    first; the restatement reproduces the second bit for bit."""
+    g = np.load(golden_dir / f"{case}.npz")
+    fs = int(g["float_size"])
+    pos = g["pos_in"].astype(port.ftype(fs))
+    o1, s1 = port.find_domain(pos, fs)
+    std, _ = port.peano_keys(pos, o1, s1, fs)
+    perm = port.sort_keys(std)
+    o2, s2 = port.find_domain(pos[:, perm], fs)
+    assert np.array_equal(o2, g["domain_origin"]) and s2 == float(g["domain_size"][0])
+    assert not np.array_equal(o1, o2)
