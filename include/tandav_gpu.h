@@ -73,7 +73,13 @@ enum {
 	 * 115-170, tree_periodic.c:439-447), in the reference's sign convention
 	 * (+G m / r). The group form computes no potential and refuses a walk
 	 * while this flag is set. */
-	TVG_CFG_POTENTIAL = 4
+	TVG_CFG_POTENTIAL = 4,
+	/* Isolated runs: every domain decomposition of tvg_compute_acceleration
+	 * and tvg_force_step first recomputes the domain from the current order
+	 * (tvg_find_domain), as Domain_Decomposition does (domain.c:67-71);
+	 * tvg_step_graph then runs such steps directly. Without it the domain is
+	 * the one last set (tvg_set_domain / tvg_find_domain). */
+	TVG_CFG_FIND_DOMAIN = 8
 };
 
 /* Host view of struct Particle_Data (src/Gravity/../particles.h:17-37). Any

@@ -5,14 +5,25 @@
 
 #include "tvg_internal.cuh"
 
+// set_computational_domain at every decomposition (TVG_CFG_FIND_DOMAIN, isolated)
+static bool find_domain_each_step(const tvg_context *ctx)
+{
+	return (ctx->cfg.flags & TVG_CFG_FIND_DOMAIN) && !ctx->cfg.periodic;
+}
+
 extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
                               int32_t ewald_kind)
 {
 	if (!ctx) return TVG_E_BADINPUT;
-	if (!ctx->have_domain) return tvg_fail(ctx, TVG_E_STATE, "force_step: domain not set");
+	if (!ctx->have_domain && !find_domain_each_step(ctx))
+		return tvg_fail(ctx, TVG_E_STATE, "force_step: domain not set");
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	cudaStream_t s = ctx->stream;
 	cudaEvent_t *ev = ctx->ev;
+	if (find_domain_each_step(ctx)) {
+		double o[3], sz;
+		TVG_CHECK(tvg_find_domain(ctx, o, &sz));
+	}
 	TVG_CUDA(ctx, cudaEventRecord(ev[8], s));
 	TVG_CHECK(tvg_impl_keys(ctx, false));
 	ctx->keys_std = true;
@@ -72,6 +83,12 @@ static int accel_phases(tvg_context *ctx, int32_t form, uint32_t parts, int32_t 
 		TVG_CUDA(ctx, tvg_record(ctx, ev[11]));
 		ctx->have_walktree = false;
 	} else {
+		// set_computational_domain (domain.c:67-71), on the current order
+		if (find_domain_each_step(ctx)) {
+			if (ctx->capturing) return tvg_fail(ctx, TVG_E_STATE, "find_domain cannot be captured");
+			double o[3], sz;
+			TVG_CHECK(tvg_find_domain(ctx, o, &sz));
+		}
 		TVG_CHECK(tvg_impl_keys(ctx, false));
 		ctx->keys_std = true;
 		TVG_CUDA(ctx, tvg_record(ctx, ev[9]));
@@ -127,7 +144,8 @@ static int accel_times(tvg_context *ctx)
 static int accel_check(tvg_context *ctx, int32_t form)
 {
 	if (!ctx) return TVG_E_BADINPUT;
-	if (!ctx->have_domain) return tvg_fail(ctx, TVG_E_STATE, "compute_acceleration: domain not set");
+	if (!ctx->have_domain && !find_domain_each_step(ctx))
+		return tvg_fail(ctx, TVG_E_STATE, "compute_acceleration: domain not set");
 	if (form != TVG_FORM_PLAIN && form != TVG_FORM_GROUP)
 		return tvg_fail(ctx, TVG_E_BADINPUT, "unknown form %d", form);
 	return TVG_OK;
@@ -296,8 +314,10 @@ extern "C" int tvg_step_graph(tvg_context *ctx, uint32_t parts, int32_t ewald_ki
 {
 	TVG_CHECK(accel_check(ctx, TVG_FORM_GROUP));
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
-	// a step on the kept tree (no keys, sort or build) runs directly
-	if (tvg_tree_update_due(ctx)) return tvg_compute_acceleration(ctx, TVG_FORM_GROUP, parts, ewald_kind, 0);
+	// a step on the kept tree (no keys, sort or build), or one that finds its
+	// domain first (host synchronisations), runs directly
+	if (tvg_tree_update_due(ctx) || find_domain_each_step(ctx))
+		return tvg_compute_acceleration(ctx, TVG_FORM_GROUP, parts, ewald_kind, 0);
 	const uint64_t key = graph_key(ctx, parts, ewald_kind);
 	if (key != ctx->graph_warm_key) {
 		// a new configuration: one direct step, which also makes every

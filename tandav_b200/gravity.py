@@ -25,6 +25,7 @@ BUILD_EXACT_MOMENTS = 1
 CFG_FIX_SMALL_TOPNODES = 1
 CFG_OPEN_BUNDLES = 2
 CFG_POTENTIAL = 4              # the plain form computes Grav_Pot
+CFG_FIND_DOMAIN = 8            # isolated: the domain is found at every decomposition
 
 F_TYPE, F_TIME_BIN, F_IT_DRIFT, F_IT_KICK, F_KEY, F_ID, F_COST = (1 << k for k in range(7))
 F_POS, F_VEL, F_ACC, F_MASS, F_GRAV_ACC, F_LAST_ACC, F_TREE_PARENT = (1 << k for k in range(7, 14))

@@ -187,6 +187,34 @@ def test_find_domain_matches_reference(golden_dir, case):
 
 
 @pytest.mark.late
+@pytest.mark.parametrize("case", ["hernquist_iso_f32", "hernquist_iso_f64"])
+def test_isolated_setup_finds_the_reference_domain(golden_dir, case):
+    """The isolated pipeline from the input order with TVG_CFG_FIND_DOMAIN, run
+    as the reference's setup runs it: tvg_find_domain, keys and sort
+    (Setup_Domain_Decomposition), then a force step that finds the domain
+    again on the PH order (Domain_Decomposition), builds and walks. The
+    particle order, the top nodes, every tree field and the Barnes-Hut
+    accelerations equal the reference's golden output bit for bit, with no
+    domain given by the host."""
+    g = np.load(golden_dir / f"{case}.npz")
+    fsize = int(g["float_size"])
+    n = len(g["mass_in"])
+    with make_ctx(n, fsize, softening=float(g["softening"]), gravity=float(g["gravity"][0]),
+                  flags=G.CFG_FIND_DOMAIN) as ctx:
+        ctx.upload(g["pos_in"], g["mass_in"], ids=np.arange(n, dtype=np.uint32))
+        ctx.find_domain()
+        ctx.peano_keys()
+        ctx.sort_particles()
+        ctx.force_step(form=G.FORM_PLAIN, use_bh=True, parts=G.WALK_GRAVITY)
+        d = ctx.download(G.F_ID | G.F_GRAV_ACC)
+        tree, top = ctx.download_tree()
+    assert np.array_equal(d["id"], g["perm"])
+    assert_struct_equal(top, g["topnodes"], TOP_FIELDS, "topnodes")
+    assert_struct_equal(tree, g["tree"], TREE_FIELDS, "tree")
+    assert np.array_equal(d["grav_acc"].astype(np.float64), g["bh_gacc"])
+
+
+@pytest.mark.late
 def test_keys_sort_and_tree_of_the_256_box():
     """The 256^3 benchmark box (16.7M particles): every 128-bit key, the sort
     permutation, the top nodes, every field of the 913k tree nodes and
