@@ -273,17 +273,18 @@ int tvg_fp32_peak(tvg_context *ctx, double ms_target, double *tflops);
 
 /* This entry point has no counterpart in the reference. It is the PH-key
  * sort of tvg_sort_particles for callers that cannot allocate device memory:
- * a host code whose memory pool already owns the GPU's memory, a caller that
- * is recording a CUDA stream (where cudaMalloc is not allowed), or one that
- * cannot afford the device-wide synchronisation of an allocation. It needs
- * no context.
+ * a host code whose own memory manager reserves the GPU's memory up front and
+ * admits no allocation behind its back (as the reference reserves its whole
+ * host pool once), or a step loop that cannot take the device-wide
+ * synchronisation that cudaMalloc and cudaFree imply. It needs no context.
  *
  * key_hi, key_lo: n 128-bit keys (high and low 64-bit words), device memory;
  * perm: n uint32, device memory, receives the permutation that orders the
  * keys ascending (perm[i] = input index of the i-th smallest key; equal keys
  * keep input order) -- the same permutation tvg_sort_particles returns.
- * Runs on the calling thread's current device and its default stream, and
- * returns when the result is in perm.
+ * Runs on the calling thread's current device, on the legacy default stream
+ * (stream 0), and synchronises that stream before it returns, so the result
+ * is in perm on return.
  *
  * Its scratch (about 6.4 MB) is one statically sized device array that every
  * GPU loading this library holds until the process exits; nothing is

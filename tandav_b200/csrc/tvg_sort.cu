@@ -324,11 +324,11 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 // ------------------------------------------------------------------------
 // Sort without any allocation (tvg_sort_keys_noalloc).
 //
-// Some callers cannot allocate device memory: a host code whose memory pool
-// already owns the GPU's memory and forbids other allocations, a caller in the
-// middle of recording a CUDA stream (cudaMalloc is not allowed there), or a
-// latency-bound caller that cannot pay the device-wide synchronisation an
-// allocation implies. For them this variant of the sort keeps its scratch (the
+// Some callers cannot allocate device memory: a host code whose own memory
+// manager reserves the GPU's memory up front and forbids allocations behind
+// its back, or a latency-bound step loop that cannot pay the device-wide
+// synchronisation that cudaMalloc and cudaFree imply. For them this variant
+// of the sort keeps its scratch (the
 // key and index ping-pong buffers and the digit histograms) in one file-scope
 // device array of fixed size, so a call allocates nothing; the caller passes
 // the keys and receives the permutation in its own device buffers.

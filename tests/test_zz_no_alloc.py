@@ -1,13 +1,14 @@
 """The sort entry point that allocates nothing (tvg_sort_keys_noalloc).
 
 It exists for callers that cannot allocate device memory -- a host code whose
-memory pool owns the GPU, a caller recording a CUDA stream, a caller that
-cannot afford the synchronisation of an allocation -- and keeps its scratch
-in a fixed device array instead. Here the caller's device buffers are torch
-tensors; the permutation must equal the one the context-based sort
-(tvg_sort_particles) returns for the same keys, bit for bit, on two calls in
-a row (the second on different, smaller input, so stale scratch from the
-first call would show).
+own memory manager reserves the GPU's memory up front and admits no other
+allocation, or a step loop that cannot take the device-wide synchronisation
+of cudaMalloc and cudaFree -- and keeps its scratch in a fixed device array
+instead. Here the caller's device buffers are torch tensors; the permutation
+must equal the one the context-based sort (tvg_sort_particles) returns for
+the same keys, bit for bit, on two calls in a row (the second on different,
+smaller input, so stale scratch from the first call would show), and a call
+must leave the device's free memory unchanged.
 """
 import ctypes as C
 
@@ -36,16 +37,20 @@ def context_keys_and_perm(p):
 
 
 def noalloc_perm(keys):
+    """Permutation from tvg_sort_keys_noalloc, and the device's free memory
+    just before and just after the call (all buffers made beforehand)."""
     import torch
     n = keys.shape[0]
     hi = torch.from_numpy(np.ascontiguousarray(keys[:, 0]).view(np.int64)).cuda()
     lo = torch.from_numpy(np.ascontiguousarray(keys[:, 1]).view(np.int64)).cuda()
     out = torch.full((n,), -1, dtype=torch.int32, device="cuda")
     torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
     rc = tandav_b200.lib().tvg_sort_keys_noalloc(C.c_void_p(hi.data_ptr()), C.c_void_p(lo.data_ptr()),
                                                  C.c_int64(n), C.c_void_p(out.data_ptr()))
+    free_after = torch.cuda.mem_get_info()[0]
     assert rc == 0, f"tvg_sort_keys_noalloc returned {rc}"
-    return out.cpu().numpy().view(np.uint32)
+    return out.cpu().numpy().view(np.uint32), free_before, free_after
 
 
 def test_noalloc_sort_matches_context_sort_twice():
@@ -53,10 +58,12 @@ def test_noalloc_sort_matches_context_sort_twice():
     second = ics.random_box(150001, box=1000.0, seed=42, clumps=3)
     # coincident particles: equal 128-bit keys keep input order in both paths
     second.pos[:, 100:110] = second.pos[:, 5:6]
-    for p in (first, second):
+    for k, p in enumerate((first, second)):
         keys, perm_ref = context_keys_and_perm(p)
-        perm = noalloc_perm(keys)
+        perm, free_before, free_after = noalloc_perm(keys)
         assert np.array_equal(perm, perm_ref)
+        if k > 0:     # the first call may load the module; later calls allocate nothing
+            assert free_after == free_before, (free_before, free_after)
 
 
 def test_noalloc_rejects_oversized_input():
