@@ -120,8 +120,9 @@ int find_domain_typed(tvg_context *ctx, double origin[3], double *size)
 	const int64_t n = ctx->n;
 	cudaStream_t s = ctx->stream;
 	const F *x[3] = { (const F *) ctx->f[FS_POS0], (const F *) ctx->f[FS_POS1], (const F *) ctx->f[FS_POS2] };
-	void *scratch = nullptr;
-	TVG_CUDA(ctx, cudaMalloc(&scratch, 256 * 4 + 8));
+	// scratch: the sort's tile histograms (at least 2 x 1 KB, free between
+	// sorts) hold the 256 digit counts and the maximum distance
+	void *scratch = ctx->sort_hist;
 	uint32_t *d_hist = (uint32_t *) scratch;
 	unsigned long long *d_max = (unsigned long long *) ((char *) scratch + 256 * 4);
 	double center[3];
@@ -133,11 +134,13 @@ int find_domain_typed(tvg_context *ctx, double origin[3], double *size)
 	}
 	if (rc == TVG_OK) {
 		const int grid = (int) (tvg_blocks(n, 256) < 148 * 8 ? tvg_blocks(n, 256) : 148 * 8);
-		cudaMemsetAsync(d_max, 0, 8, s);
-		k_max_distance<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(n, x[0], x[1], x[2], center[0], center[1],
-		                                                       center[2], d_max);
 		unsigned long long m = 0;
-		cudaError_t e = cudaGetLastError();
+		cudaError_t e = cudaMemsetAsync(d_max, 0, 8, s);
+		if (e == cudaSuccess) {
+			k_max_distance<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(n, x[0], x[1], x[2], center[0],
+			                                                       center[1], center[2], d_max);
+			e = cudaGetLastError();
+		}
 		if (e == cudaSuccess) e = cudaMemcpyAsync(&m, d_max, 8, cudaMemcpyDeviceToHost, s);
 		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
 		if (e != cudaSuccess) rc = tvg_fail(ctx, TVG_E_CUDA, "find_domain: %s", cudaGetErrorString(e));
@@ -146,8 +149,6 @@ int find_domain_typed(tvg_context *ctx, double origin[3], double *size)
 		*size = 2.001 * maxd;                           // domain.c:832
 		for (int d = 0; d < 3; d++) origin[d] = center[d] - 0.5 * *size;
 	}
-	cudaStreamSynchronize(s);
-	cudaFree(scratch);
 	return rc;
 }
 
