@@ -11,7 +11,7 @@ import pytest
 from tandav_b200 import gravity as G
 from tandav_b200 import ics
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 
 def test_registered_pool_round_trip():

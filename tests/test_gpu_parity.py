@@ -159,7 +159,6 @@ def test_fast_moments_close_to_exact():
     assert np.allclose(exact["CoM"], fast["CoM"], rtol=0, atol=1e-4 * p.box)
 
 
-@pytest.mark.late
 @pytest.mark.parametrize("case", ["hernquist_iso_f32", "hernquist_iso_f64", "hernquist_2^18"])
 def test_find_domain_matches_reference(golden_dir, case):
     """tvg_find_domain as the reference's setup runs it: on the input order,
@@ -186,7 +185,6 @@ def test_find_domain_matches_reference(golden_dir, case):
     assert np.array_equal(o, want_o) and s == want_s
 
 
-@pytest.mark.late
 @pytest.mark.parametrize("case", ["hernquist_iso_f32", "hernquist_iso_f64"])
 def test_isolated_setup_finds_the_reference_domain(golden_dir, case):
     """The isolated pipeline from the input order with TVG_CFG_FIND_DOMAIN, run
@@ -214,7 +212,6 @@ def test_isolated_setup_finds_the_reference_domain(golden_dir, case):
     assert np.array_equal(d["grav_acc"].astype(np.float64), g["bh_gacc"])
 
 
-@pytest.mark.late
 def test_keys_sort_and_tree_of_the_256_box():
     """The 256^3 benchmark box (16.7M particles): every 128-bit key, the sort
     permutation, the top nodes, every field of the 913k tree nodes and
@@ -237,7 +234,6 @@ def test_keys_sort_and_tree_of_the_256_box():
     assert np.array_equal(parent, parent_o)
 
 
-@pytest.mark.late
 @pytest.mark.parametrize("kind,fsize,n,exact", [("zeldovich", 4, 128 ** 3, True),
                                                ("zeldovich", 4, 128 ** 3, False),
                                                ("hernquist", 8, 1 << 20, True),

@@ -11,7 +11,7 @@ import pytest
 from tandav_b200 import gravity as G
 from tandav_b200 import ics
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("fb,potential", [(4, False), (8, True)])

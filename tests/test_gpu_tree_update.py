@@ -25,7 +25,7 @@ from pipeline import assert_struct_equal
 from tandav_b200 import gravity as G
 from tandav_b200 import ics
 
-pytestmark = [pytest.mark.gpu, pytest.mark.late]
+pytestmark = pytest.mark.gpu
 
 TREE_FIELDS = ("DNext", "Bitfield", "DUp", "Npart", "Pos", "Mass", "CoM", "Dp")
 TOP_FIELDS = ("Key", "Target", "Level", "First_Part", "Npart", "Pos", "Mass", "CoM", "Dp")
