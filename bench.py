@@ -64,7 +64,11 @@ def parse():
     ap.add_argument("--box-mpc", type=float, default=100.0, help="box side, Mpc/h")
     ap.add_argument("--tpl", type=int, default=0, choices=[0, 1, 2, 4],
                     help="targets per lane of the group walk (0: autotune)")
-    ap.add_argument("--plain-stride", type=int, default=64)
+    ap.add_argument("--plain-stride", type=int, default=1,
+                    help="walk every s-th particle in the plain form (1: all particles, no "
+                         "extrapolation)")
+    ap.add_argument("--no-matched", action="store_true",
+                    help="skip the group form at the plain form's opening parameter")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-mlp", action="store_true", help="skip the learned-Ewald step")
@@ -350,6 +354,8 @@ def workload_config(args, p, ws):
         "criterion": (f"relative, TREE_OPEN_PARAM_REL {args.open_rel:g} (group form), "
                       f"{args.plain_open_rel:g} (plain form); |a_old| first from a BH (theta^2 "
                       f"0.25) pass"),
+        "ewald_headline": ("Taylor table (the faster evaluator at the same force error); the "
+                           "learned correction runs the same step in learned_ewald"),
         "ewald": (f"group form: per-group Ewald walk, Taylor table of the lattice sum (33^3 nodes, "
                   f"third order; K, dK, d2K at node centres of mass, second-order expansion about "
                   f"the group centre plus the exact uniform-cube remainder), opening "
@@ -488,6 +494,42 @@ def main():
         except (OSError, ValueError):
             pass
 
+    # ---- the group form at the plain form's opening parameter (same
+    # criterion, same particles): one pair of numbers at matched opening
+    matched = None
+    if not args.no_matched:
+        m_err = None
+        try:
+            ctx.set_opening(0.25, args.plain_open_rel)
+            for _ in range(3):                     # direct step, then the two captures
+                ctx.step_graph(parts)
+            m_ms = 0.0
+            for _ in range(args.steps):
+                ctx.timer_start()
+                ctx.step_graph(parts)
+                m_ms += ctx.timer_stop()
+            mg, _ = ctx.walk_counters()
+        except Exception as e:       # every rank still takes the collective steps below
+            m_err, m_ms = str(e), math.inf
+        t_m = dist.max(m_ms / args.steps) / 1e3
+        n_all_m = dist.sum(n)
+        if m_err is not None or not math.isfinite(t_m):
+            matched = {"error": m_err or "failed on another rank"}
+        else:
+            matched = {"open_rel": args.plain_open_rel, "particles_per_s": n_all_m / t_m,
+                       "ms_per_step": round(t_m * 1e3, 2),
+                       "interactions_per_particle": round(mg / n, 1)}
+            if tgt_ids is not None:
+                try:
+                    ids_m = ctx.download(G.F_ID)["id"]
+                    inv = np.empty(n, np.int64)
+                    inv[ids_m] = np.arange(n)
+                    _, _, err_m = ctx.forcetest(np.sort(inv[tgt_ids]))
+                    matched["force_error"] = {k: float(f"{v:.4e}") for k, v in err_m.items()}
+                except Exception as e:
+                    matched["force_error"] = {"error": str(e)}
+        ctx.set_opening(0.25, args.open_rel)
+
     # ---- the same step with the learned Ewald correction: trained here by the
     # library's own kernels, validated against the exact table, then run in the walk
     learned = None
@@ -581,11 +623,16 @@ def main():
             t_plain = pre_ms * 1e-3 + w_ms * 1e-3 * n / len(act)
             plain = {"value": n / t_plain, "unit": UNIT,
                      "form": "plain: reference walk, one thread per particle, FP64, table Ewald",
-                     "sample": f"walk of every {args.plain_stride}th particle ({len(act)}), "
-                               f"keys/sort/build for all, extrapolated",
+                     "sample": ("keys, sort, build and the relative walk (incl. Ewald) of all "
+                                f"{n} particles, measured" if args.plain_stride == 1 else
+                                f"walk of every {args.plain_stride}th particle ({len(act)}), "
+                                f"keys/sort/build for all, extrapolated"),
                      "ms_keys_sort_build": round(pre_ms, 2), "ms_walk_sample": round(w_ms, 2),
                      "interactions_per_particle": round((g_pl + e_pl) / len(act), 1),
                      "speedup_group_over_plain": round(value / ws / (n / t_plain), 2)}
+            if matched and "particles_per_s" in matched:
+                plain["speedup_group_over_plain_at_matched_opening"] = round(
+                    matched["particles_per_s"] / ws / (n / t_plain), 2)
         except Exception as e:       # the headline line is printed all the same
             plain = {"error": str(e)}
         finally:
@@ -631,6 +678,7 @@ def main():
                            "evaluations_per_group": round(ew_i / args.steps / (n / (32 * tune_choice)), 1),
                            "evaluation": "Taylor-table K, dK, d2K: 15 float4 loads, ~200 FP32 ops"},
             "plain_form": plain,
+            "group_form_at_plain_opening": matched,
             "learned_ewald": learned,
             "device_memory_used_gb": hbm_gb,
             "accuracy": accuracy,
