@@ -163,10 +163,26 @@ int tvg_sort_particles(tvg_context *ctx, uint32_t *perm);
 /* Replaces Reverse_Peano_Keys (src/peano.c:84-97): P.Key = reversed key. */
 int tvg_reverse_keys(tvg_context *ctx);
 
-/* Top nodes of the single-target decomposition (src/domain.c:67-145,
- * 220-250 with NTarget = 1): every non-empty level-2 cell, in descending key
- * order. Particles must be sorted. ntop receives the count (<= 64). */
+/* Replaces the bunch loop of Domain_Decomposition (src/domain.c:67-145) and
+ * transform_bunches_into_top_nodes (:220-250): the top nodes, in descending
+ * key order, for the particles sorted by standard keys. With one target
+ * (NTask = 1, the default, or NTask >= 65 on one rank, domain.c:151-156)
+ * every non-empty level-2 cell; with NTask = 2 .. 64 targets (set by
+ * tvg_set_domain_decomposition) the cells balanced by P.Cost as the
+ * reference balances them over its threads. ntop receives the count. */
 int tvg_top_nodes(tvg_context *ctx, int32_t *ntop);
+
+/* NTask of Setup_Domain_Decomposition (src/domain.c:151-156; one rank: the
+ * OpenMP threads of the reference's team), Param.Part_Alloc_Factor and
+ * DOMAIN_IMBAL_CEIL (Config). The decomposition then weighs the particles by
+ * cost_metric (domain.c:533-536: the integer part of max(1, P.Cost), P.Cost as
+ * left by the last walk or uploaded with TVG_F_COST) and sums the costs as
+ * the reference's threads do: each of NTask static shares of a range in
+ * float, the shares added in thread order. Defaults: 1, 1.1, 0.05. */
+int tvg_set_domain_decomposition(tvg_context *ctx, int32_t ntask, double part_alloc_factor,
+                                 double imbal_ceil);
+/* Refinement rounds of the last balanced decomposition. */
+int tvg_decomposition_rounds(tvg_context *ctx, int32_t *rounds);
 
 /* ----------------------------------------------------------- tree build */
 
@@ -329,6 +345,14 @@ int tvg_set_opening(tvg_context *ctx, double open_bh, double open_rel);
  * h2 s^2 / L^2 exceeds bh_factor times TREE_OPEN_PARAM_BH (Barnes-Hut mode).
  * Defaults 2.5e-4 and 0.5. */
 int tvg_set_ewald_opening(tvg_context *ctx, double rel_alpha, double bh_factor);
+
+/* Iteration limit of the group form's traversal loops (no reference
+ * counterpart; the reference's walks run unbounded, tree_accel.c:211-353):
+ * a warp that pops more than `max_iterations` node batches for one group
+ * stops, and the walk returns TVG_E_TIMEOUT with the context still usable.
+ * Default 2^24, far above any walk (a group pops at most a few 10^4
+ * batches). Accepts 1 .. 2^31 - 1. */
+int tvg_set_walk_limit(tvg_context *ctx, int64_t max_iterations);
 
 /* ------------------------------------------- hierarchical time stepping */
 

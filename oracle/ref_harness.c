@@ -21,6 +21,9 @@
  *   mode "force": the sequence above.
  *   mode "keys":  Peano_Key / Reversed_Peano_Key for the input positions with
  *                 the domain taken from the input header (no decomposition).
+ *   mode "force2": one force computation on the first tree, then a second
+ *                 Domain_Decomposition (balanced on the P.Cost it left) and
+ *                 tree; the dumps and walks are those of the second.
  *   mode "update": "force" with the tree updates between rebuilds applied
  *                 to the built tree before the walks (tree_update_sequence).
  *   mode "snap":  Write_Snapshot of the input particles (run_snap).
@@ -294,7 +297,29 @@ static void tree_update_sequence(const struct input *in, int64_t n)
 	NActive_Particles = (int) n;
 }
 
-static int run_force(const struct input *in, bool update)
+/* One force computation on the current tree as Compute_Acceleration does it
+ * with Sig.Prepare_Step (accel.c:15-71): Barnes-Hut pass, |Acc| into
+ * Last_Acc_Mag, zeroed accumulators, relative pass. P.Cost then holds the
+ * relative pass's interaction counts (incl. the Ewald walk when periodic),
+ * the cost the next Domain_Decomposition balances (domain.c:533-536). */
+static void force_for_cost(void)
+{
+	#pragma omp parallel
+	{
+		zero_accumulators();
+		Sig.Use_BH_Criterion = true;
+		Gravity_Tree_Acceleration();
+		#pragma omp barrier
+		#pragma omp for
+		for (int i = 0; i < Task.Npart_Total; i++)
+			P.Last_Acc_Mag[i] = SQRT(p2(P.Acc[0][i]) + p2(P.Acc[1][i]) + p2(P.Acc[2][i]));
+		zero_accumulators();
+		Sig.Use_BH_Criterion = false;
+		Gravity_Tree_Acceleration();
+	}
+}
+
+static int run_force(const struct input *in, bool update, bool redecompose)
 {
 	int64_t n = in->n;
 	bool periodic = in->box > 0;
@@ -348,6 +373,35 @@ static int run_force(const struct input *in, bool update)
 		#pragma omp barrier
 		#pragma omp master
 		t_build = now() - t0;
+	}
+
+	/* mode "force2": one force computation, then the next decomposition and
+	 * tree (the main loop's second step, main.c:43-70): the dumps below
+	 * describe that second decomposition, balanced on P.Cost. cost_in / id_in
+	 * are P.Cost and P.ID in the order the second decomposition starts from. */
+	if (redecompose) {
+		force_for_cost();
+		const int64_t nn = Task.Npart_Total;
+		double *c = malloc(nn * sizeof(double));
+		uint32_t *ids = malloc(nn * sizeof(uint32_t));
+		for (int64_t i = 0; i < nn; i++) { c[i] = P.Cost[i]; ids[i] = (uint32_t) P.ID[i]; }
+		put("cost_in", c, nn * sizeof(double));
+		put("id_in", ids, nn * sizeof(uint32_t));
+		free(c);
+		free(ids);
+		#pragma omp parallel
+		{
+			Sig.Domain_Update = true;
+			Domain_Decomposition();
+		}
+		/* Gravity_Tree_Build places each subtree where its thread reserves
+		 * memory (tree_build.c:59-96), so with several threads the node
+		 * indices (Target, Tree_Parent, and through quirk Q3 the particles a
+		 * small top node's walk reads) depend on the threads' timing. A
+		 * one-thread team places the subtrees in top-node order, as every
+		 * run with one thread does; the subtrees themselves do not change. */
+		#pragma omp parallel num_threads(1)
+		Gravity_Tree_Build();
 	}
 
 	/* bounded CPU sample (flags bits 8..23 = stride s > 1): the walks run for
@@ -618,9 +672,11 @@ int main(int argc, char *argv[])
 	if (!strcmp(argv[1], "keys"))
 		rc = run_keys(&in);
 	else if (!strcmp(argv[1], "force"))
-		rc = run_force(&in, false);
+		rc = run_force(&in, false, false);
+	else if (!strcmp(argv[1], "force2"))
+		rc = run_force(&in, false, true);
 	else if (!strcmp(argv[1], "update"))
-		rc = run_force(&in, true);
+		rc = run_force(&in, true, false);
 	else if (!strcmp(argv[1], "snap"))
 		rc = run_snap(&in, argv[3]);
 	fclose(Out);

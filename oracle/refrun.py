@@ -141,7 +141,7 @@ def decode(rec: dict, n: int) -> dict:
     for name, buf in rec.items():
         if name in ("std_key", "rev_key"):
             out[name] = keys_u128(buf)
-        elif name in ("perm",):
+        elif name in ("perm", "id_in"):
             out[name] = np.frombuffer(buf, dtype="<u4").copy()
         elif name == "tree" or name.endswith("_tree"):
             out[name] = np.frombuffer(buf, dtype=TREE_DTYPE[fsize]).copy()

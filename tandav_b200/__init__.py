@@ -19,13 +19,13 @@ _lib = None
 EXPORTS = (
     "tvg_init", "tvg_finalize", "tvg_last_error", "tvg_version", "tvg_upload", "tvg_download",
     "tvg_set_domain", "tvg_peano_keys", "tvg_sort_particles", "tvg_reverse_keys",
-    "tvg_top_nodes", "tvg_tree_build", "tvg_download_tree", "tvg_ewald_init",
+    "tvg_top_nodes", "tvg_set_domain_decomposition", "tvg_decomposition_rounds", "tvg_tree_build", "tvg_download_tree", "tvg_ewald_init",
     "tvg_download_ewald_table", "tvg_upload_ewald_table", "tvg_walk", "tvg_save_last_accel", "tvg_zero_accel",
     "tvg_force_step", "tvg_phase_times", "tvg_walk_counters", "tvg_set_active", "tvg_timer",
     "tvg_launch_count", "tvg_host_alloc", "tvg_host_free",
     "tvg_host_register", "tvg_host_unregister", "tvg_fp32_peak",
     "tvg_sort_keys_noalloc", "tvg_forcetest", "tvg_set_opening",
-    "tvg_set_ewald_opening", "tvg_timeline_init", "tvg_download_kick_drift_table",
+    "tvg_set_ewald_opening", "tvg_set_walk_limit", "tvg_timeline_init", "tvg_download_kick_drift_table",
     "tvg_kick_drift_factors", "tvg_set_new_timesteps", "tvg_kick_first_halfstep",
     "tvg_kick_second_halfstep", "tvg_drift_to_sync_point", "tvg_timeline_get", "tvg_timeline_set",
     "tvg_rung_histogram", "tvg_compute_acceleration", "tvg_step_graph", "tvg_step_graph_reset",

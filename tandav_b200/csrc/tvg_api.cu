@@ -39,6 +39,10 @@ int tvg_sync_status(tvg_context *ctx, const char *phase)
 		return tvg_fail(ctx, TVG_E_TREE_FULL, "%s: interaction list overflow", phase);
 	if (st & TVG_ST_TREE_STALE)
 		return tvg_fail(ctx, TVG_E_STATE, "%s: the kept tree does not fit the particles", phase);
+	if (st & TVG_ST_OFF_GRID)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "%s: a particle lies more than half a domain size "
+		                "outside the domain of the last decomposition (the group form's integer grid); "
+		                "a domain update is due", phase);
 	if (st & TVG_ST_TIMESTEP)
 		return tvg_fail(ctx, TVG_E_BADINPUT, "%s: time step below the integer timeline's resolution "
 		                "or not finite (timestep.c:219-222)", phase);
@@ -134,8 +138,9 @@ extern "C" int tvg_init(int device, const tvg_config *cfg, tvg_context **out)
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->work_counter, 64));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->counters, 8 * 8));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->dc, sizeof(tvg_devcount)));
-	TVG_CHECK(dalloc(ctx, (void **) &ctx->d_topinfo, sizeof(TopInfo)));
-	TVG_CHECK(dalloc(ctx, (void **) &ctx->d_topplace, sizeof(TopPlace)));
+	TVG_CHECK(dalloc(ctx, (void **) &ctx->d_toptab, 4 * sizeof(int32_t) * TVG_MAX_TOP));
+	TVG_CUDA(ctx, cudaMemset(ctx->d_toptab, 0, 4 * sizeof(int32_t) * TVG_MAX_TOP));
+	TVG_CHECK(dalloc(ctx, (void **) &ctx->top_of, 4 * cap));
 	TVG_CUDA(ctx, cudaMemset(ctx->dc, 0, sizeof(tvg_devcount)));
 	return TVG_OK;
 }
@@ -144,10 +149,8 @@ extern "C" int tvg_init(int device, const tvg_config *cfg, tvg_context **out)
 int tvg_read_counts(tvg_context *ctx)
 {
 	tvg_devcount h;
-	TopPlace tp;
 	cudaStream_t s = ctx->stream;
 	TVG_CUDA(ctx, cudaMemcpyAsync(&h, ctx->dc, sizeof(h), cudaMemcpyDeviceToHost, s));
-	TVG_CUDA(ctx, cudaMemcpyAsync(&tp, ctx->d_topplace, sizeof(tp), cudaMemcpyDeviceToHost, s));
 	TVG_CUDA(ctx, cudaStreamSynchronize(s));
 	ctx->ntop = h.ntop;
 	ctx->nu = h.nu;
@@ -156,11 +159,6 @@ int tvg_read_counts(tvg_context *ctx)
 		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->h_top, ctx->d_top, sizeof(tvg_topnode) * ctx->ntop,
 		                              cudaMemcpyDeviceToHost, s));
 	TVG_CUDA(ctx, cudaStreamSynchronize(s));
-	for (int t = 0; t < TVG_MAX_TOP; t++) {
-		const bool ok = t < ctx->ntop;
-		ctx->h_target[t] = ok ? tp.target[t] : 0;
-		ctx->h_nsurv[t] = ok ? tp.nsurv[t] : 0;
-	}
 	return TVG_OK;
 }
 
@@ -182,7 +180,7 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->ewald_ext, ctx->active, ctx->kd_x, ctx->kd_kick, ctx->kd_drift,
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
 	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
-	                 ctx->d_topinfo, ctx->d_topplace, ctx->tu_first, ctx->tu_dp };
+	                 ctx->d_toptab, ctx->top_of, ctx->dd_scratch, ctx->tu_first, ctx->tu_dp };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -512,6 +510,16 @@ extern "C" int tvg_set_ewald_opening(tvg_context *ctx, double rel_alpha, double 
 		return tvg_fail(ctx, TVG_E_BADINPUT, "set_ewald_opening: parameters must be > 0");
 	ctx->ewald_open_rel = rel_alpha;
 	ctx->ewald_open_bh = bh_factor;
+	return TVG_OK;
+}
+
+extern "C" int tvg_set_walk_limit(tvg_context *ctx, int64_t max_iterations)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (max_iterations < 1 || max_iterations > 0x7FFFFFFF)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "set_walk_limit: %lld outside 1 .. 2^31 - 1",
+		                (long long) max_iterations);
+	ctx->walk_limit = (int32_t) max_iterations;
 	return TVG_OK;
 }
 

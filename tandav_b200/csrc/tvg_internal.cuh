@@ -17,7 +17,9 @@
 
 #include "../../include/tandav_gpu.h"
 
-#define TVG_MAX_TOP 64
+// top nodes: 64 level-2 cells on one target; up to 512 + 20 rounds x 64
+// splits x 7 when Domain_Decomposition balances 64 targets
+#define TVG_MAX_TOP 16384
 #define TVG_MAX_DEVICES 64         // per-device caches of launch attributes
 #define TVG_MAX_LEVEL 42
 
@@ -48,7 +50,8 @@ enum {
 	TVG_ST_TIMEOUT = 8,
 	TVG_ST_LIST_OVERFLOW = 16,
 	TVG_ST_TIMESTEP = 32,
-	TVG_ST_TREE_STALE = 64     // a kept tree's ranges do not fit the particles
+	TVG_ST_TREE_STALE = 64,    // a kept tree's ranges do not fit the particles
+	TVG_ST_OFF_GRID = 128      // group form: a position off its integer grid
 };
 
 struct tvg_buf {
@@ -83,21 +86,17 @@ struct tvg_devcount {
 	int32_t sort_skip[8];    // radix digit d is the same for all keys
 };
 
-// level-2 cells and their top nodes (tree build), on the device
-struct TopInfo {            // per level-2 cell c (0..63)
-	int32_t first[64];      // first particle, -1 if empty
-	int32_t count[64];
-	int32_t tidx[64];       // index in the top node list (descending key order)
-	int32_t big[64];        // count > VECTOR_SIZE: has a subtree
+// Per top node tables of the tree build, on the device (TVG_MAX_TOP
+// entries each, one allocation): the subtree's first node and node count,
+// the offset from a node's rank among the build's survivors to its tree
+// index, and the first particle after the top node.
+struct TopTables {
+	int32_t *target;
+	int32_t *nsurv;
+	int32_t *toff;
+	int32_t *end;
 };
 
-struct TopPlace {
-	int32_t tidx[64];       // by level-2 cell
-	int32_t toff[64];       // by top index: G = toff + F[u]
-	int32_t target[64];
-	int32_t nsurv[64];
-	int32_t end[64];        // by top index: first particle after the node
-};
 
 struct tvg_graph_entry;
 
@@ -146,6 +145,13 @@ struct tvg_context {
 	tvg_topnode h_top[TVG_MAX_TOP];
 	int32_t *top_first = nullptr;      // [64] first particle of level-2 cell c
 	int32_t *top_count = nullptr;      // [64]
+	int32_t *top_of = nullptr;         // top node of every particle (cap)
+	// Domain_Decomposition balanced over NTask targets (tvg_set_domain_decomposition)
+	int32_t dd_ntask = 1;
+	double dd_part_alloc_factor = 1.1; // Param.Part_Alloc_Factor
+	double dd_imbal_ceil = 0.05;       // DOMAIN_IMBAL_CEIL
+	void *dd_scratch = nullptr;        // fill jobs, bunch keys and partial sums
+	int32_t dd_rounds = 0;             // refinement rounds of the last decomposition
 
 	// tree build scratch
 	uint8_t *lvl = nullptr;            // LCA level with the previous particle
@@ -162,8 +168,7 @@ struct tvg_context {
 	void *tree = nullptr;              // reference layout
 	int32_t *tree_u = nullptr;         // final node -> uncollapsed index
 	double *pref = nullptr;            // prefix sums of m, m*x, m*y, m*z (FP64)
-	int32_t h_target[TVG_MAX_TOP];
-	int32_t h_nsurv[TVG_MAX_TOP];
+
 
 	// Ewald tables (Float, divided by box^2) and raw FP64
 	void *ewald_f[4] = { nullptr, nullptr, nullptr, nullptr };
@@ -176,6 +181,8 @@ struct tvg_context {
 	// h2 s^2 / L^2 in units of TREE_OPEN_PARAM_BH (Barnes-Hut mode)
 	double ewald_open_rel = 2.5e-4;
 	double ewald_open_bh = 0.5;
+	// iteration limit of the group walks' traversal loops (tvg_set_walk_limit)
+	int32_t walk_limit = 1 << 24;
 
 	// group walk data
 	uint32_t *ipos[3] = { nullptr, nullptr, nullptr };
@@ -219,8 +226,7 @@ struct tvg_context {
 
 	// device-resident counts and top-node tables of the step
 	tvg_devcount *dc = nullptr;
-	TopInfo *d_topinfo = nullptr;
-	TopPlace *d_topplace = nullptr;
+	int32_t *d_toptab = nullptr;       // TopTables storage: 4 x TVG_MAX_TOP
 	// stream capture in progress: the step's functions skip every host read
 	// and synchronisation
 	bool capturing = false;
@@ -265,6 +271,10 @@ int tvg_impl_tree_drift(tvg_context *ctx, double dt);
 int tvg_impl_keys(tvg_context *ctx, bool reversed);
 int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out);
 int tvg_impl_top_nodes(tvg_context *ctx);
+// Domain_Decomposition's cost-driven top nodes for NTask > 1 (tvg_decompose.cu)
+int tvg_impl_top_nodes_balanced(tvg_context *ctx);
+// the top node of every particle (top_of) from the device top-node list
+int tvg_impl_top_of(tvg_context *ctx);
 int tvg_impl_tree_build(tvg_context *ctx, uint32_t flags);
 int tvg_impl_download_tree(tvg_context *ctx, void *tree, int64_t cap, int64_t *nnodes);
 int tvg_impl_ewald_init(tvg_context *ctx);
@@ -281,6 +291,16 @@ int tvg_impl_zero_accel(tvg_context *ctx);
 int tvg_impl_active_from_bins(tvg_context *ctx);
 
 static inline size_t tvg_fsize(const tvg_context *ctx) { return (size_t) ctx->cfg.float_bytes; }
+
+static inline TopTables tvg_top_tables(const tvg_context *ctx)
+{
+	TopTables t;
+	t.target = ctx->d_toptab;
+	t.nsurv = ctx->d_toptab + TVG_MAX_TOP;
+	t.toff = ctx->d_toptab + 2 * TVG_MAX_TOP;
+	t.end = ctx->d_toptab + 3 * TVG_MAX_TOP;
+	return t;
+}
 
 // records a timing event on the context stream; while a capture is in
 // progress as an event-record node of the graph (a plain record would only

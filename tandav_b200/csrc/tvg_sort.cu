@@ -14,7 +14,9 @@
 //  2. Runs of equal high words are ordered by the low word (insertion sort
 //     per run, one thread per run; runs are rare and short unless positions
 //     coincide).
-//  3. Every particle field is gathered through the permutation in one launch.
+//  3. Every particle field is gathered through the permutation in one launch,
+//     four particles per thread with 128-bit stores (and 128-bit loads where
+//     the permutation keeps an aligned run of four in place).
 // The resulting order is the ascending 128-bit key order, equal keys in
 // input order (the reference's quicksort leaves equal keys in an
 // unspecified order).
@@ -239,17 +241,50 @@ struct GatherList {
 	int nf;
 };
 
-// all particle fields through the permutation in one pass (perm read once)
+// All particle fields through the permutation in one pass (perm read once).
+// A thread moves four consecutive particles i .. i+3 (i a multiple of 4):
+// their permutation entries come in one 128-bit load, and every field is
+// written with 128-bit stores (one per 4-byte field, two per 8-byte field).
+// Where the four sources are one aligned run (perm[i] a multiple of 4 and
+// perm[i+k] = perm[i] + k: particles that kept their place in the order,
+// nearly all of them between the steps of a run) the loads are 128-bit too;
+// elsewhere the four elements are gathered one by one. Buffers start
+// 256-byte aligned, so every vector access is aligned.
 __global__ void k_gather_fields(int64_t n, const uint32_t *__restrict__ perm, GatherList g)
 {
-	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	const int64_t i = 4 * (blockIdx.x * (int64_t) blockDim.x + threadIdx.x);
 	if (i >= n) return;
-	const uint32_t src = perm[i];
+	if (i + 4 > n) {                               // ragged end: scalar
+		for (int64_t j = i; j < n; j++) {
+			const uint32_t src = perm[j];
+			for (int f = 0; f < g.nf; f++) {
+				if (g.bytes[f] == 8) ((uint64_t *) g.out[f])[j] = ((const uint64_t *) g.in[f])[src];
+				else ((uint32_t *) g.out[f])[j] = ((const uint32_t *) g.in[f])[src];
+			}
+		}
+		return;
+	}
+	const uint4 p = *(const uint4 *) (perm + i);
+	const bool run = (p.x & 3u) == 0 && p.y == p.x + 1 && p.z == p.x + 2 && p.w == p.x + 3;
 	for (int f = 0; f < g.nf; f++) {
-		if (g.bytes[f] == 8)
-			((uint64_t *) g.out[f])[i] = ((const uint64_t *) g.in[f])[src];
-		else
-			((uint32_t *) g.out[f])[i] = ((const uint32_t *) g.in[f])[src];
+		if (g.bytes[f] == 8) {
+			const uint64_t *in = (const uint64_t *) g.in[f];
+			uint4 *out = (uint4 *) ((uint64_t *) g.out[f] + i);
+			if (run) {
+				const uint4 *v = (const uint4 *) (in + p.x);
+				out[0] = __ldg(v);
+				out[1] = __ldg(v + 1);
+			} else {
+				const uint64_t a = in[p.x], b = in[p.y], c = in[p.z], d = in[p.w];
+				out[0] = make_uint4((uint32_t) a, (uint32_t) (a >> 32), (uint32_t) b, (uint32_t) (b >> 32));
+				out[1] = make_uint4((uint32_t) c, (uint32_t) (c >> 32), (uint32_t) d, (uint32_t) (d >> 32));
+			}
+		} else {
+			const uint32_t *in = (const uint32_t *) g.in[f];
+			uint4 *out = (uint4 *) ((uint32_t *) g.out[f] + i);
+			if (run) *out = __ldg((const uint4 *) (in + p.x));
+			else *out = make_uint4(in[p.x], in[p.y], in[p.z], in[p.w]);
+		}
 	}
 }
 
@@ -313,7 +348,7 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 		g.bytes[g.nf] = (int) tvg_field_bytes(ctx, f);
 		g.nf++;
 	}
-	k_gather_fields<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->perm, g);
+	k_gather_fields<<<TVG_CNT(ctx, tvg_blocks((n + 3) / 4, 256)), 256, 0, s>>>(n, ctx->perm, g);
 	TVG_CUDA(ctx, cudaGetLastError());
 	for (int f = 0; f < FS_NFIELDS; f++) { void *t = ctx->f[f]; ctx->f[f] = ctx->falt[f]; ctx->falt[f] = t; }
 	if (perm_out)

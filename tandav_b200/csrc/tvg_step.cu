@@ -264,6 +264,7 @@ static uint64_t graph_key(const tvg_context *ctx, uint32_t parts, int32_t ewald_
 	k = mix_d(k, c.boxsize);
 	k = mix_d(k, ctx->ewald_open_rel);
 	k = mix_d(k, ctx->ewald_open_bh);
+	k = mix(k, (uint32_t) ctx->walk_limit);
 	k = mix_d(k, ctx->dsize);
 	for (int d = 0; d < 3; d++) k = mix_d(k, ctx->origin[d]);
 	return k ? k : 1;
@@ -315,8 +316,10 @@ extern "C" int tvg_step_graph(tvg_context *ctx, uint32_t parts, int32_t ewald_ki
 	TVG_CHECK(accel_check(ctx, TVG_FORM_GROUP));
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	// a step on the kept tree (no keys, sort or build), or one that finds its
-	// domain first (host synchronisations), runs directly
-	if (tvg_tree_update_due(ctx) || find_domain_each_step(ctx))
+	// domain first or balances its top nodes over several targets (host
+	// synchronisations), runs directly
+	const bool balanced = ctx->dd_ntask > 1 && ctx->dd_ntask < 65;
+	if (tvg_tree_update_due(ctx) || find_domain_each_step(ctx) || balanced)
 		return tvg_compute_acceleration(ctx, TVG_FORM_GROUP, parts, ewald_kind, 0);
 	const uint64_t key = graph_key(ctx, parts, ewald_kind);
 	if (key != ctx->graph_warm_key) {

@@ -7,11 +7,14 @@
 // evaluates with one thread per particle / node:
 //
 //   l_i   = level of the deepest common cell of sorted particles i-1 and i
-//           (leading equal key triplets), l = L-1 at a top node's first
-//           particle (L = top level 2).
+//           (leading equal key triplets); at a top node's first particle l
+//           is 0, a boundary below every level, whatever the top node's
+//           level L (>= 2; all 64 level-2 cells on one target, deeper cells
+//           where Domain_Decomposition balances several).
 //   nodes = the top cell, and every cell whose parent cell holds >= 2
 //           particles. The cells that start at particle i are levels
-//           l_i+1 .. max(l_i, l_{i+1})+1; pre-order = (first particle, level).
+//           lo_i .. max(l_i, l_{i+1})+1, lo_i = L at a top node's first
+//           particle and l_i+1 elsewhere; pre-order = (first particle, level).
 //   event = particle e with l_e < l_{e-1}: the reference sees it as a new
 //           branch. At e the cell A (level l_e+1, holding e-1) becomes a
 //           bundle if it has <= VECTOR_SIZE particles, else the cell B (level
@@ -31,8 +34,8 @@
 // Roofline: HBM/L2 bound (1 B level + 16 B key per particle, ~O(nodes)).
 #include "tvg_internal.cuh"
 
-#define TOP_LEVEL 2
-#define LVL_START 1         // l at a top node's first particle (L - 1)
+#define TOP_LEVEL 2         // MIN_LEVEL (domain.c:3): the top level on one target
+#define LVL_START 0         // l at a top node's first particle
 #define LVL_SMALL 0xFF      // particle of a top node without subtree
 
 template <typename F> struct TNode {
@@ -60,12 +63,11 @@ __global__ void k_top_first(int64_t n, const uint64_t *__restrict__ key_hi, int3
 // domain.c:678-684), centre from the first particle (domain.c:237-246)
 template <typename F>
 __global__ void k_make_top(int64_t n, const int32_t *first, const F *x, const F *y, const F *z,
-                           double ox, double oy, double oz, double size, int vsize, tvg_topnode *top,
-                           int32_t *count, TopInfo *ti, tvg_devcount *dc)
+                           double ox, double oy, double oz, double size, tvg_topnode *top,
+                           int32_t *count, tvg_devcount *dc)
 {
 	if (threadIdx.x || blockIdx.x) return;
 	int nt = 0;
-	for (int c = 0; c < 64; c++) { ti->first[c] = -1; ti->count[c] = 0; ti->tidx[c] = -1; ti->big[c] = 0; }
 	for (int c = 63; c >= 0; c--) {
 		if (first[c] < 0) { count[c] = 0; continue; }
 		int64_t e = n;
@@ -86,33 +88,52 @@ __global__ void k_make_top(int64_t n, const int32_t *first, const F *x, const F 
 		t.pos[2] = (float) __dadd_rn(__dmul_rn(floor(pz / sz) + 0.5, sz), oz);
 		t.mass = 0;
 		for (int k = 0; k < 3; k++) { t.com[k] = 0; t.dp[k] = 0; }
-		ti->first[c] = t.first_part;
-		ti->count[c] = t.npart;
-		ti->tidx[c] = nt;
-		ti->big[c] = t.npart > vsize;
 		top[nt++] = t;
 	}
 	dc->ntop = nt;
 }
 
+// top node of every particle: block b takes top nodes b, b + grid, ...
+__global__ void k_top_of(const tvg_devcount *__restrict__ dc, const tvg_topnode *__restrict__ top,
+                         int32_t *__restrict__ top_of)
+{
+	const int ntop = dc->ntop;
+	for (int t = blockIdx.x; t < ntop; t += gridDim.x) {
+		const int64_t f = top[t].first_part, e = f + top[t].npart;
+		for (int64_t i = f + threadIdx.x; i < e; i += blockDim.x) top_of[i] = t;
+	}
+}
+
+int tvg_impl_top_of(tvg_context *ctx)
+{
+	k_top_of<<<TVG_CNT(ctx, 148 * 4), 256, 0, ctx->stream>>>(ctx->dc, ctx->d_top, ctx->top_of);
+	TVG_CUDA(ctx, cudaGetLastError());
+	return TVG_OK;
+}
+
+// One target (NTask = 1, or >= 65 tasks on one rank, domain.c:151-156): the
+// reference's loop stops at once with every non-empty level-2 cell as a top
+// node, which needs no host round trip (the step graph captures it). More
+// targets: the cost-balanced refinement of tvg_decompose.cu.
 int tvg_impl_top_nodes(tvg_context *ctx)
 {
+	if (ctx->dd_ntask > 1 && ctx->dd_ntask < 65) return tvg_impl_top_nodes_balanced(ctx);
 	const int64_t n = ctx->n;
 	cudaStream_t s = ctx->stream;
-	TVG_CUDA(ctx, cudaMemsetAsync(ctx->top_first, 0xFF, 4 * TVG_MAX_TOP, s));
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->top_first, 0xFF, 4 * 64, s));
 	k_top_first<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->top_first);
-	const int vsize = ctx->cfg.vector_size;
 	if (ctx->cfg.float_bytes == 4)
 		k_make_top<float><<<TVG_CNT(ctx, 1), 1, 0, s>>>(n, ctx->top_first, (const float *) ctx->f[FS_POS0],
 		                                  (const float *) ctx->f[FS_POS1], (const float *) ctx->f[FS_POS2],
-		                                  ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize, vsize,
-		                                  ctx->d_top, ctx->top_count, ctx->d_topinfo, ctx->dc);
+		                                  ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
+		                                  ctx->d_top, ctx->top_count, ctx->dc);
 	else
 		k_make_top<double><<<TVG_CNT(ctx, 1), 1, 0, s>>>(n, ctx->top_first, (const double *) ctx->f[FS_POS0],
 		                                   (const double *) ctx->f[FS_POS1], (const double *) ctx->f[FS_POS2],
-		                                   ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize, vsize,
-		                                   ctx->d_top, ctx->top_count, ctx->d_topinfo, ctx->dc);
+		                                   ctx->origin[0], ctx->origin[1], ctx->origin[2], ctx->dsize,
+		                                   ctx->d_top, ctx->top_count, ctx->dc);
 	TVG_CUDA(ctx, cudaGetLastError());
+	TVG_CHECK(tvg_impl_top_of(ctx));
 	if (ctx->capturing) return TVG_OK;
 	return tvg_read_counts(ctx);
 }
@@ -127,31 +148,29 @@ __device__ __forceinline__ int lca_level(const uint64_t *hi, const uint64_t *lo,
 }
 
 __global__ void k_levels(int64_t n, const uint64_t *__restrict__ hi, const uint64_t *__restrict__ lo,
-                         const TopInfo *__restrict__ tip, uint8_t *__restrict__ lvl,
-                         int32_t *__restrict__ ncnt, uint8_t *__restrict__ lvl_min64, int *status)
+                         const tvg_topnode *__restrict__ top, const int32_t *__restrict__ top_of,
+                         int vsize, uint8_t *__restrict__ lvl, int32_t *__restrict__ ncnt,
+                         uint8_t *__restrict__ lvl_min64, int *status)
 {
 	__shared__ uint8_t s_min[256 / 32];
-	__shared__ TopInfo ti;
-	for (int e = threadIdx.x; e < 256; e += blockDim.x)
-		((int32_t *) &ti)[e] = ((const int32_t *) tip)[e];
-	__syncthreads();
 	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	unsigned my = 0xFF;
 	if (i < n) {
-		const int c = (int) (hi[i] >> 58);
-		const int64_t f = ti.first[c], e = f + ti.count[c];
+		const tvg_topnode &tn = top[top_of[i]];
+		const int64_t f = tn.first_part, e = f + tn.npart;
+		const bool big = tn.npart > vsize;
 		int l, cnt = 0;
 		if (i == f) {
 			l = LVL_START;
-		} else if (!ti.big[c]) {
+		} else if (!big) {
 			l = LVL_SMALL;
 		} else {
 			l = lca_level(hi, lo, i - 1, i);
 			if (l >= TVG_MAX_LEVEL - 1) atomicOr(status, TVG_ST_COINCIDENT);
 		}
-		if (ti.big[c]) {
+		if (big) {
 			int lnext = (i + 1 < e) ? lca_level(hi, lo, i, i + 1) : -1;
-			int lo_l = l + 1;
+			int lo_l = i == f ? tn.level : l + 1;
 			int hi_l = (l > lnext ? l : lnext) + 1;
 			cnt = hi_l - lo_l + 1;
 		}
@@ -214,8 +233,19 @@ __device__ int64_t prev_smaller(const uint8_t *__restrict__ lvl, const uint8_t *
 enum { UF_COLLAPSED = 1, UF_LEAF = 2, UF_ROOT = 4 };
 
 // every uncollapsed node: range, collapse decision, removal marks
+// first level of the nodes that start at particle s (the top node's level at
+// its first particle, whose l is LVL_START)
+__device__ __forceinline__ int first_level(const uint8_t *__restrict__ lvl,
+                                           const tvg_topnode *__restrict__ top,
+                                           const int32_t *__restrict__ top_of, int64_t s)
+{
+	const int ls = lvl[s];
+	return ls == LVL_START ? top[top_of[s]].level : ls + 1;
+}
+
 __global__ void k_nodes(int64_t n, const uint8_t *__restrict__ lvl, const uint8_t *__restrict__ m64,
-                        const int32_t *__restrict__ base, int vsize, int32_t *__restrict__ u_start,
+                        const int32_t *__restrict__ base, const tvg_topnode *__restrict__ top,
+                        const int32_t *__restrict__ top_of, int vsize, int32_t *__restrict__ u_start,
                         uint8_t *__restrict__ u_level, int32_t *__restrict__ u_count,
                         int32_t *__restrict__ u_endu, uint8_t *__restrict__ u_flag,
                         int32_t *__restrict__ u_diff, int64_t ucap, int *status)
@@ -224,15 +254,15 @@ __global__ void k_nodes(int64_t n, const uint8_t *__restrict__ lvl, const uint8_
 	if (s >= n) return;
 	const int32_t b0 = base[s], nc = base[s + 1] - b0;
 	if (nc == 0) return;
-	const int ls = lvl[s];
-	const int lo_l = ls + 1;
+	const bool top_start = lvl[s] == LVL_START;
+	const int lo_l = first_level(lvl, top, top_of, s);
 	for (int k = 0; k < nc; k++) {
 		const int l = lo_l + k;
 		const int64_t u = b0 + k;
 		const int64_t e = next_smaller(lvl, m64, n, s, l);
 		const int32_t cnt = (int32_t) (e - s);
 		uint8_t flag = 0;
-		if (l == TOP_LEVEL) flag |= UF_ROOT;
+		if (top_start && k == 0) flag |= UF_ROOT;
 		if (cnt == 1) flag |= UF_LEAF;
 		if (cnt <= vsize && e < n && cnt > 1) {
 			const int le = lvl[e], lp = lvl[e - 1];
@@ -282,26 +312,23 @@ __global__ void k_survivors(const tvg_devcount *__restrict__ dc, int64_t ucap,
 // one thread: subtree placement in top-node order (tree_build.c:59-96); the
 // placement table for the emission and the node count, on the device
 __global__ void k_place_subtrees(tvg_devcount *dc, tvg_topnode *top, const int32_t *__restrict__ base,
-                                 const int32_t *__restrict__ F, int vsize, const TopInfo *__restrict__ ti,
-                                 TopPlace *tp, int64_t ucap, int64_t tcap, int *status)
+                                 const int32_t *__restrict__ F, int vsize, TopTables tp, int64_t ucap,
+                                 int64_t tcap, int *status)
 {
 	if (threadIdx.x || blockIdx.x) return;
 	const int ntop = dc->ntop;
 	int64_t run = 0;
-	for (int t = 0; t < 64; t++) {
-		tp->tidx[t] = ti->tidx[t];
-		tp->toff[t] = tp->target[t] = tp->nsurv[t] = tp->end[t] = 0;
-	}
 	for (int t = 0; t < ntop; t++) {
 		top[t].target = (int32_t) run;       // also for small top nodes (quirk Q3)
-		tp->target[t] = (int32_t) run;
-		tp->end[t] = top[t].first_part + top[t].npart;
+		tp.target[t] = (int32_t) run;
+		tp.end[t] = top[t].first_part + top[t].npart;
+		tp.nsurv[t] = tp.toff[t] = 0;
 		if (top[t].npart > vsize) {
 			int64_t f = top[t].first_part, e = f + top[t].npart;
 			// base <= nu; past the capacity the build has failed (status set)
 			int32_t fs = F[min((int64_t) base[f], ucap)], fe = F[min((int64_t) base[e], ucap)];
-			tp->nsurv[t] = fe - fs;
-			tp->toff[t] = (int32_t) (run - fs);
+			tp.nsurv[t] = fe - fs;
+			tp.toff[t] = (int32_t) (run - fs);
 			run += (fe - fs) + 1;             // + terminator
 		}
 	}
@@ -323,14 +350,11 @@ __global__ void k_emit_nodes(const tvg_devcount *__restrict__ dc, int64_t ucap, 
                              const int32_t *__restrict__ u_count, const int32_t *__restrict__ u_endu,
                              const uint8_t *__restrict__ u_flag, const int32_t *__restrict__ surv,
                              const int32_t *__restrict__ Fidx, const uint64_t *__restrict__ hi,
-                             const uint64_t *__restrict__ lo, const TopPlace *__restrict__ tpp,
+                             const uint64_t *__restrict__ lo, const tvg_topnode *__restrict__ top,
+                             const int32_t *__restrict__ top_of, TopTables tp,
                              TNode<F> *tree, int32_t *__restrict__ tree_u,
                              int32_t *__restrict__ tree_parent, int64_t tcap, int *status)
 {
-	__shared__ TopPlace tp;
-	for (int e = threadIdx.x; e < 5 * 64; e += blockDim.x)
-		((int32_t *) &tp)[e] = ((const int32_t *) tpp)[e];
-	__syncthreads();
 	const int64_t nu = min(dc->nu, ucap);
 	const int64_t u = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (u >= nu || !surv[u]) return;
@@ -338,8 +362,7 @@ __global__ void k_emit_nodes(const tvg_devcount *__restrict__ dc, int64_t ucap, 
 	const int l = u_level[u];
 	const int32_t cnt = u_count[u];
 	const uint8_t flag = u_flag[u];
-	const int c = (int) (hi[s] >> 58);
-	const int t = tp.tidx[c];
+	const int t = top_of[s];
 	const int64_t G = (int64_t) tp.toff[t] + Fidx[u];
 	if (G < 0 || G >= tcap) { atomicOr(status, TVG_ST_TREE_FULL); return; }
 	TNode<F> nd;
@@ -363,7 +386,7 @@ __global__ void k_emit_nodes(const tvg_devcount *__restrict__ dc, int64_t ucap, 
 		} else {
 			const int ls = lvl[s];
 			const int64_t p = prev_smaller(lvl, m64, s, ls);
-			pu = base[p] + (ls - (lvl[p] + 1));
+			pu = base[p] + (ls - first_level(lvl, top, top_of, p));
 		}
 		nd.DUp = (int32_t) (G - ((int64_t) tp.toff[t] + Fidx[pu]));
 	}
@@ -377,13 +400,14 @@ __global__ void k_emit_nodes(const tvg_devcount *__restrict__ dc, int64_t ucap, 
 
 // particles of top nodes without subtree point to their top node (-t-1),
 // set_tree_parent_pointers, tree_build.c:226-242
-__global__ void k_small_parent(int64_t n, const uint64_t *__restrict__ hi, const TopInfo *__restrict__ ti,
+__global__ void k_small_parent(int64_t n, const tvg_topnode *__restrict__ top,
+                               const int32_t *__restrict__ top_of, int vsize,
                                int32_t *__restrict__ tree_parent)
 {
 	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	int c = (int) (hi[i] >> 58);
-	if (!ti->big[c]) tree_parent[i] = -ti->tidx[c] - 1;
+	const int t = top_of[i];
+	if (top[t].npart <= vsize) tree_parent[i] = -t - 1;
 }
 
 // reference arithmetic for a child centre (tree_build.c:542-550)
@@ -542,13 +566,13 @@ __global__ void k_moments_warp(const tvg_devcount *__restrict__ dc, int64_t tcap
 // terminators (tree_build.c:468-474); small top nodes sum their particles
 template <typename F>
 __global__ void k_finish_top(const tvg_devcount *__restrict__ dc, tvg_topnode *top, TNode<F> *tree,
-                             const TopPlace *__restrict__ tp, int64_t tcap, const F *__restrict__ x,
+                             TopTables tp, int64_t tcap, const F *__restrict__ x,
                              const F *__restrict__ y, const F *__restrict__ z, const F *__restrict__ m,
                              int vsize)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= dc->ntop) return;
-	const int32_t *nsurv = tp->nsurv;
+	const int32_t *nsurv = tp.nsurv;
 	F o[4];
 	if (top[t].npart > vsize) {
 		const TNode<F> &r = tree[top[t].target];
@@ -583,13 +607,16 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 	const int64_t ucap = ctx->ucap, tcap = ctx->tcap;
 	tvg_devcount *dc = ctx->dc;
 
-	k_levels<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->d_topinfo,
-	                                                          ctx->lvl, ctx->ncnt, ctx->lvl_min64, ctx->status);
+	const TopTables tp = tvg_top_tables(ctx);
+	k_levels<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->d_top,
+	                                                          ctx->top_of, vsize, ctx->lvl, ctx->ncnt,
+	                                                          ctx->lvl_min64, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	if (!ctx->capturing) TVG_CHECK(tvg_sync_status(ctx, "tree_build(levels)"));
 	TVG_CHECK(tvg_device_scan_i32_dev(ctx, ctx->ncnt, ctx->ncnt, n + 1, &dc->nu));
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->u_diff, 0, 4 * (ucap + 1), s));
-	k_nodes<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, s>>>(n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, vsize,
+	k_nodes<<<TVG_CNT(ctx, tvg_blocks(n, 128)), 128, 0, s>>>(n, ctx->lvl, ctx->lvl_min64, ctx->ncnt,
+	                                            ctx->d_top, ctx->top_of, vsize,
 	                                            ctx->u_start, ctx->u_level, ctx->u_count, ctx->u_endu,
 	                                            ctx->u_flag, ctx->u_diff, ucap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
@@ -600,16 +627,17 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->u_diff, ctx->u_final, ucap + 1, nullptr));
 	// placement of the subtrees
-	k_place_subtrees<<<TVG_CNT(ctx, 1), 1, 0, s>>>(dc, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, ctx->d_topinfo,
-	                                               ctx->d_topplace, ucap, tcap, ctx->status);
+	k_place_subtrees<<<TVG_CNT(ctx, 1), 1, 0, s>>>(dc, ctx->d_top, ctx->ncnt, ctx->u_final, vsize, tp,
+	                                               ucap, tcap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	TNode<F> *tree = (TNode<F> *) ctx->tree;
 	k_emit_nodes<F><<<TVG_CNT(ctx, tvg_blocks(ucap, 256)), 256, 0, s>>>(
 	    dc, ucap, n, ctx->lvl, ctx->lvl_min64, ctx->ncnt, ctx->u_start, ctx->u_level, ctx->u_count,
-	    ctx->u_endu, ctx->u_flag, ctx->u_diff, ctx->u_final, ctx->key_hi, ctx->key_lo, ctx->d_topplace, tree,
-	    ctx->tree_u, tree_parent, tcap, ctx->status);
+	    ctx->u_endu, ctx->u_flag, ctx->u_diff, ctx->u_final, ctx->key_hi, ctx->key_lo, ctx->d_top,
+	    ctx->top_of, tp, tree, ctx->tree_u, tree_parent, tcap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
-	k_small_parent<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->d_topinfo, tree_parent);
+	k_small_parent<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->d_top, ctx->top_of, vsize,
+	                                                                tree_parent);
 	TVG_CUDA(ctx, cudaGetLastError());
 	const unsigned gs = 148 * 16;      // grid-stride launches over the node count
 	k_node_pos<F><<<TVG_CNT(ctx, gs), 128, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z,
@@ -620,8 +648,8 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 	if (!exact)
 		k_moments_warp<F><<<TVG_CNT(ctx, gs), 256, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z, m);
 	TVG_CUDA(ctx, cudaGetLastError());
-	k_finish_top<F><<<TVG_CNT(ctx, 1), 64, 0, s>>>(dc, ctx->d_top, tree, ctx->d_topplace, tcap, x, y, z, m,
-	                                                vsize);
+	k_finish_top<F><<<TVG_CNT(ctx, TVG_MAX_TOP / 128), 128, 0, s>>>(dc, ctx->d_top, tree, tp, tcap, x, y,
+	                                                                 z, m, vsize);
 	TVG_CUDA(ctx, cudaGetLastError());
 	if (ctx->capturing) return TVG_OK;
 	TVG_CHECK(tvg_read_counts(ctx));

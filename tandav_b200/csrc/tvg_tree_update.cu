@@ -145,7 +145,7 @@ static int tree_kick_typed(tvg_context *ctx, int64_t na, const F *dp)
 	k_node_first<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(ctx->dc, tcap, tree, ctx->tu_first);
 	k_kick_nodes<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(ctx->dc, tcap, tree, ctx->tu_first, ctx->act_off, n, na,
 	                                                   dp, dp + cap, dp + 2 * cap, ctx->status);
-	k_kick_top<F><<<TVG_CNT(ctx, 1), TVG_MAX_TOP, 0, s>>>(ctx->dc, ctx->d_top, ctx->act_off, n, na, dp, dp + cap,
+	k_kick_top<F><<<TVG_CNT(ctx, TVG_MAX_TOP / 128), 128, 0, s>>>(ctx->dc, ctx->d_top, ctx->act_off, n, na, dp, dp + cap,
 	                                                       dp + 2 * cap, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return tvg_sync_status(ctx, "tree update: kicks");
@@ -171,7 +171,7 @@ static int tree_drift_typed(tvg_context *ctx, double dt)
 	const int64_t tcap = ctx->tcap;
 	const int grid = (int) (tvg_blocks(tcap, 256) < 148 * 16 ? tvg_blocks(tcap, 256) : 148 * 16);
 	k_drift_nodes<F><<<TVG_CNT(ctx, grid), 256, 0, s>>>(ctx->dc, tcap, (TuNode<F> *) ctx->tree, dt);
-	k_drift_top<<<TVG_CNT(ctx, 1), TVG_MAX_TOP, 0, s>>>(ctx->dc, ctx->d_top, dt);
+	k_drift_top<<<TVG_CNT(ctx, TVG_MAX_TOP / 128), 128, 0, s>>>(ctx->dc, ctx->d_top, dt);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }

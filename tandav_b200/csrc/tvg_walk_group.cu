@@ -56,13 +56,20 @@
 #include "tvg_internal.cuh"
 #include "tvg_ewald_mlp.cuh"
 
+// warps per block and far-list depth (sources per flush); compile-time
+// choices, measured flat around these values
+#ifndef GW_WARPS
 #define GW_WARPS 4
+#endif
 #define GW_THREADS (GW_WARPS * 32)
 #define GW_STACK 1024
 #define GW_RESERVE (7 * (TVG_MAX_LEVEL - 2) + 8)
+#ifndef GW_LIST
 #define GW_LIST 256
+#endif
 #define GW_WLIST 64
 #define GW_BQ 64
+#define GW_ROOTS 256        // top nodes pushed at a time
 #define GW_ELIST 64
 #define GW_DEFAULT_TPL 2
 // resident blocks per SM the Ewald walk is compiled for; capping its
@@ -73,19 +80,42 @@
 #ifndef GW_EWALD_MINB
 #define GW_EWALD_MINB 1
 #endif
+// resident blocks per SM the gravity walk is compiled for, and the unroll of
+// its far-list loop (source pairs per iteration)
+#ifndef GW_WALK_MINB
+#define GW_WALK_MINB 1
+#endif
+#ifndef GW_FAR_UNROLL
+#define GW_FAR_UNROLL 2
+#endif
+constexpr int kFarUnroll = GW_FAR_UNROLL;
 
 // -------------------------------------------------- integer coordinates
+
+// A coordinate off the integer grid (isolated runs: more than half a domain
+// size below the domain of the last decomposition, or 1.5 sizes above it) is
+// clamped to the grid's edge and reported (TVG_ST_OFF_GRID): the group form
+// would misplace it, so the walk fails instead of returning wrong forces.
+__device__ __forceinline__ uint32_t grid_coord(double v, int *bad)
+{
+	if (!(v >= 0.0)) { *bad = 1; return 0u; }
+	if (v >= 4294967296.0) { *bad = 1; return 0xFFFFFFFFu; }
+	return (uint32_t) (uint64_t) v;
+}
 
 template <typename F>
 __global__ void k_int_pos(int64_t n, const F *__restrict__ x, const F *__restrict__ y,
                           const F *__restrict__ z, double ox, double oy, double oz, double fac,
-                          uint32_t *__restrict__ ix, uint32_t *__restrict__ iy, uint32_t *__restrict__ iz)
+                          uint32_t *__restrict__ ix, uint32_t *__restrict__ iy, uint32_t *__restrict__ iz,
+                          int *status)
 {
 	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	ix[i] = (uint32_t) (uint64_t) (((double) x[i] - ox) * fac);
-	iy[i] = (uint32_t) (uint64_t) (((double) y[i] - oy) * fac);
-	iz[i] = (uint32_t) (uint64_t) (((double) z[i] - oz) * fac);
+	int bad = 0;
+	ix[i] = grid_coord(((double) x[i] - ox) * fac, &bad);
+	iy[i] = grid_coord(((double) y[i] - oy) * fac, &bad);
+	iz[i] = grid_coord(((double) z[i] - oz) * fac, &bad);
+	if (bad) atomicOr(status, TVG_ST_OFF_GRID);
 }
 
 // ----------------------------------------------------- walk tree (CSR)
@@ -237,6 +267,7 @@ struct GroupParams {
 	int periodic;
 	int use_bh;
 	int open_bundles;   // TVG_CFG_OPEN_BUNDLES
+	int max_iter;       // iteration limit of a group's traversal (tvg_set_walk_limit)
 	float scale;        // length per integer unit
 	float box, half_box;
 	float theta2;       // TREE_OPEN_PARAM_BH
@@ -253,12 +284,27 @@ struct GroupParams {
 	double uniform_g;   // G / L^2: times the total mass, the scale of the uniform-background remainder
 };
 
+// The far list keeps sources in pairs: entries 2q and 2q + 1 share the two
+// float4 slots lxy[q] = (x0, x1, y0, y1) and lzw[q] = (z0, z1, w0, w1), so that
+// each lane meets two sources with one packed f32x2 instruction per operation
+// while its target's coordinates stay in registers as (t, t) pairs.
 struct WarpSmem {
 	int32_t stack[GW_STACK];
-	float4 list[GW_LIST];      // far sources: bare 1/r^2 kernel
+	float4 lxy[GW_LIST / 2];   // far sources (bare 1/r^2 kernel): x, y of a pair
+	float4 lzw[GW_LIST / 2];   // far sources: z, G m of a pair
 	float4 wlist[GW_WLIST];    // near sources (w > 0) and, per-target image, half-box-plane sources (w < 0)
 	int2 bq[GW_BQ];
 };
+
+__device__ __forceinline__ void far_put(WarpSmem &S, int i, float4 e)
+{
+	float *a = (float *) &S.lxy[i >> 1], *b = (float *) &S.lzw[i >> 1];
+	const int o = i & 1;
+	a[o] = e.x;
+	a[2 + o] = e.y;
+	b[o] = e.z;
+	b[2 + o] = e.w;
+}
 
 struct EwaldSmem {
 	int32_t stack[GW_STACK];
@@ -411,19 +457,6 @@ __device__ __forceinline__ void push_children(int32_t *stack, int &sp, bool open
 	sp += tot;
 }
 
-// a source certainly outside the softening length of every target: 1/r^2 law
-__device__ __forceinline__ void pair_far(float4 s, float tx, float ty, float tz, float &ax,
-                                         float &ay, float &az)
-{
-	const float dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
-	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-	const float ri = rsqrtf(r2);
-	const float f = (s.w * ri) * (ri * ri);
-	ax = fmaf(f, dx, ax);
-	ay = fmaf(f, dy, ay);
-	az = fmaf(f, dz, az);
-}
-
 // softened monopole, reference kernel (Dehnen K1 with h = -41/32 eps,
 // tree_accel.c:362-394) in FP32 for a separation d; the r2 = 0 self term
 // selects the inner branch and adds exactly zero
@@ -441,36 +474,53 @@ __device__ __forceinline__ void pair_full(const GroupParams &p, float dx, float 
 	az = fmaf(f, dz, az);
 }
 
+// Far-list flush: for every target of the lane, two sources per packed
+// (f32x2) step -- 3 FADD2, FMUL2 + 2 FFMA2 for r^2, two MUFU.RSQ, 3 FMUL2 and
+// 3 FFMA2 for two interactions, against 24 scalar FP32 instructions -- so the
+// loop is bound by the FMA pipe rather than by instruction issue. The even
+// and odd sources are summed separately and added at the end of the flush.
+// An odd count is padded with a massless source far away (adds exactly 0).
 template <int TPL>
-__device__ __forceinline__ void flush_far(const float4 *list, int nl, Target (&t)[TPL])
+__device__ __forceinline__ void flush_far(WarpSmem &S, int nl, Target (&t)[TPL])
 {
-	float ax[TPL], ay[TPL], az[TPL];
+	if (nl & 1) {
+		if ((threadIdx.x & 31) == 0) far_put(S, nl, make_float4(1.0e15f, 0.f, 0.f, 0.f));
+		__syncwarp();
+	}
+	const int np = (nl + 1) >> 1;
+	float2 ax[TPL], ay[TPL], az[TPL], mx[TPL], my[TPL], mz[TPL];
 #pragma unroll
-	for (int k = 0; k < TPL; k++) ax[k] = ay[k] = az[k] = 0.f;
-	int e = 0;
-#pragma unroll 1
-	for (; e + 4 <= nl; e += 4) {
-		const float4 s0 = list[e], s1 = list[e + 1], s2 = list[e + 2], s3 = list[e + 3];
+	for (int k = 0; k < TPL; k++) {
+		ax[k] = ay[k] = az[k] = make_float2(0.f, 0.f);
+		mx[k] = make_float2(-t[k].tx, -t[k].tx);
+		my[k] = make_float2(-t[k].ty, -t[k].ty);
+		mz[k] = make_float2(-t[k].tz, -t[k].tz);
+	}
+#pragma unroll kFarUnroll
+	for (int q = 0; q < np; q++) {
+		const float4 a = S.lxy[q], b = S.lzw[q];
+		const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w),
+		             sz = make_float2(b.x, b.y), sw = make_float2(b.z, b.w);
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
-			pair_far(s0, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
-			pair_far(s1, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
-			pair_far(s2, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
-			pair_far(s3, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
+			const float2 dx = __fadd2_rn(sx, mx[k]), dy = __fadd2_rn(sy, my[k]),
+			             dz = __fadd2_rn(sz, mz[k]);
+			const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+			const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+			const float2 f = __fmul2_rn(__fmul2_rn(sw, ri), __fmul2_rn(ri, ri));
+			ax[k] = __ffma2_rn(f, dx, ax[k]);
+			ay[k] = __ffma2_rn(f, dy, ay[k]);
+			az[k] = __ffma2_rn(f, dz, az[k]);
 		}
-	}
-	for (; e < nl; e++) {
-		const float4 s = list[e];
-#pragma unroll
-		for (int k = 0; k < TPL; k++) pair_far(s, t[k].tx, t[k].ty, t[k].tz, ax[k], ay[k], az[k]);
 	}
 #pragma unroll
 	for (int k = 0; k < TPL; k++) {
-		t[k].ax += (double) ax[k];
-		t[k].ay += (double) ay[k];
-		t[k].az += (double) az[k];
+		t[k].ax += (double) ax[k].x + (double) ax[k].y;
+		t[k].ay += (double) ay[k].x + (double) ay[k].y;
+		t[k].az += (double) az[k].x + (double) az[k].y;
 		t[k].cost += (float) nl;
 	}
+	__syncwarp();
 }
 
 __device__ __forceinline__ float wrap_half(float d, float box, float half)
@@ -534,108 +584,114 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 
 	int sp = 0, nl = 0, nw = 0;
 	const int ntop = p.dc->ntop;
-	for (int r = lane; r < ntop; r += 32) S.stack[r] = r;
-	sp = ntop;
-	__syncwarp();
 	int guard = 0;
-	while (sp > 0) {
-		if (++guard > (1 << 24)) { atomicOr(status, TVG_ST_TIMEOUT); break; }
-		bool stop;
-		const int node = pop_nodes(S.stack, sp, status, stop);
-		if (stop) break;
-		bool accept = false, open_int = false, open_bundle = false, wrap = false, near = false;
-		float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
-		int nchild = 0, child = 0;
-		if (node >= 0) {
-			const tvg_wnode nd = wt[node];
-			const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
-			            dz = ioff(nd.cz, g.cz, p.scale);
-			float r2;
-			const bool open = gravity_opens(p, g, nd, node, dx, dy, dz, ioff(nd.gx, g.cx, p.scale),
-			                                ioff(nd.gy, g.cy, p.scale), ioff(nd.gz, g.cz, p.scale), r2);
-			if (!open) {
-				accept = true;
-				entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
-				wrap = per_target && (fabsf(dx) > wlimx || fabsf(dy) > wlimy || fabsf(dz) > wlimz);
-				near = r2 < p.near2;
-			} else if (nd.nchild > 0) {
-				open_int = true;
-				nchild = nd.nchild;
-				child = nd.child;
-			} else {
-				open_bundle = true;
-				nchild = -nd.nchild;
-				child = nd.child;
-			}
-		}
-		// accepted nodes -> interaction lists
-		const bool to_far = accept && !wrap && !near;
-		const bool to_slow = accept && (wrap || near);
-		if (wrap) entry.w = -entry.w;
-		const unsigned bm = __ballot_sync(0xFFFFFFFFu, to_far);
-		const unsigned bw = __ballot_sync(0xFFFFFFFFu, to_slow);
-		if (nl + __popc(bm) > GW_LIST) {
-			flush_far<TPL>(S.list, nl, t);
-			nl = 0;
-			__syncwarp();
-		}
-		if (nw + __popc(bw) > GW_WLIST) {
-			flush_slow<TPL>(p, S.wlist, nw, t);
-			nw = 0;
-			__syncwarp();
-		}
-		if (to_far) S.list[nl + __popc(bm & lt)] = entry;
-		if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
-		nl += __popc(bm);
-		nw += __popc(bw);
-		push_children(S.stack, sp, open_int, nchild, child);
-		// opened bundles -> bundle queue
-		const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
-		if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
+	bool halt = false;
+	// the roots in chunks of GW_ROOTS (a balanced decomposition can have
+	// thousands of top nodes, more than the stack holds at once)
+	for (int r0 = 0; r0 < ntop && !halt; r0 += GW_ROOTS) {
+		const int nr = min(GW_ROOTS, ntop - r0);
+		for (int r = lane; r < nr; r += 32) S.stack[r] = r0 + r;
+		sp = nr;
 		__syncwarp();
-		const int nb = __popc(bb);
-		for (int b = 0; b < nb; b++) {
-			const int2 q = S.bq[b];
-			for (int o = 0; o < q.y; o += 32) {
-				const int j = o + lane;
-				const bool have = j < q.y;
-				float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-				bool wr = false, nr = false;
-				if (have) {
-					const int64_t jp = (int64_t) q.x + j;
-					e.x = ioff(ix[jp], g.cx, p.scale);
-					e.y = ioff(iy[jp], g.cy, p.scale);
-					e.z = ioff(iz[jp], g.cz, p.scale);
-					e.w = p.gravity * mass_f[jp];
-					const float ax = fmaxf(fabsf(e.x) - g.hx, 0.f), ay = fmaxf(fabsf(e.y) - g.hy, 0.f),
-					            az = fmaxf(fabsf(e.z) - g.hz, 0.f);
-					nr = ax * ax + ay * ay + az * az < p.near2;
-					wr = per_target && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz);
+		while (sp > 0) {
+			if (++guard > p.max_iter) { atomicOr(status, TVG_ST_TIMEOUT); halt = true; break; }
+			bool stop;
+			const int node = pop_nodes(S.stack, sp, status, stop);
+			if (stop) { halt = true; break; }
+			bool accept = false, open_int = false, open_bundle = false, wrap = false, near = false;
+			float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
+			int nchild = 0, child = 0;
+			if (node >= 0) {
+				const tvg_wnode nd = wt[node];
+				const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
+				            dz = ioff(nd.cz, g.cz, p.scale);
+				float r2;
+				const bool open = gravity_opens(p, g, nd, node, dx, dy, dz, ioff(nd.gx, g.cx, p.scale),
+				                                ioff(nd.gy, g.cy, p.scale), ioff(nd.gz, g.cz, p.scale), r2);
+				if (!open) {
+					accept = true;
+					entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
+					wrap = per_target && (fabsf(dx) > wlimx || fabsf(dy) > wlimy || fabsf(dz) > wlimz);
+					near = r2 < p.near2;
+				} else if (nd.nchild > 0) {
+					open_int = true;
+					nchild = nd.nchild;
+					child = nd.child;
+				} else {
+					open_bundle = true;
+					nchild = -nd.nchild;
+					child = nd.child;
 				}
-				const bool tm = have && !wr && !nr, tw = have && (wr || nr);
-				if (wr) e.w = -e.w;
-				const unsigned m1 = __ballot_sync(0xFFFFFFFFu, tm), m2 = __ballot_sync(0xFFFFFFFFu, tw);
-				if (nl + __popc(m1) > GW_LIST) {
-					flush_far<TPL>(S.list, nl, t);
-					nl = 0;
-					__syncwarp();
-				}
-				if (nw + __popc(m2) > GW_WLIST) {
-					flush_slow<TPL>(p, S.wlist, nw, t);
-					nw = 0;
-					__syncwarp();
-				}
-				if (tm) S.list[nl + __popc(m1 & lt)] = e;
-				if (tw) S.wlist[nw + __popc(m2 & lt)] = e;
-				nl += __popc(m1);
-				nw += __popc(m2);
+			}
+			// accepted nodes -> interaction lists
+			const bool to_far = accept && !wrap && !near;
+			const bool to_slow = accept && (wrap || near);
+			if (wrap) entry.w = -entry.w;
+			const unsigned bm = __ballot_sync(0xFFFFFFFFu, to_far);
+			const unsigned bw = __ballot_sync(0xFFFFFFFFu, to_slow);
+			if (nl + __popc(bm) > GW_LIST) {
+				flush_far<TPL>(S, nl, t);
+				nl = 0;
 				__syncwarp();
 			}
+			if (nw + __popc(bw) > GW_WLIST) {
+				flush_slow<TPL>(p, S.wlist, nw, t);
+				nw = 0;
+				__syncwarp();
+			}
+			if (to_far) far_put(S, nl + __popc(bm & lt), entry);
+			if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
+			nl += __popc(bm);
+			nw += __popc(bw);
+			push_children(S.stack, sp, open_int, nchild, child);
+			// opened bundles -> bundle queue
+			const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
+			if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
+			__syncwarp();
+			const int nb = __popc(bb);
+			for (int b = 0; b < nb; b++) {
+				const int2 q = S.bq[b];
+				for (int o = 0; o < q.y; o += 32) {
+					const int j = o + lane;
+					const bool have = j < q.y;
+					float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+					bool wr = false, nr = false;
+					if (have) {
+						const int64_t jp = (int64_t) q.x + j;
+						e.x = ioff(ix[jp], g.cx, p.scale);
+						e.y = ioff(iy[jp], g.cy, p.scale);
+						e.z = ioff(iz[jp], g.cz, p.scale);
+						e.w = p.gravity * mass_f[jp];
+						const float ax = fmaxf(fabsf(e.x) - g.hx, 0.f), ay = fmaxf(fabsf(e.y) - g.hy, 0.f),
+						            az = fmaxf(fabsf(e.z) - g.hz, 0.f);
+						nr = ax * ax + ay * ay + az * az < p.near2;
+						wr = per_target && (fabsf(e.x) > wlimx || fabsf(e.y) > wlimy || fabsf(e.z) > wlimz);
+					}
+					const bool tm = have && !wr && !nr, tw = have && (wr || nr);
+					if (wr) e.w = -e.w;
+					const unsigned m1 = __ballot_sync(0xFFFFFFFFu, tm), m2 = __ballot_sync(0xFFFFFFFFu, tw);
+					if (nl + __popc(m1) > GW_LIST) {
+						flush_far<TPL>(S, nl, t);
+						nl = 0;
+						__syncwarp();
+					}
+					if (nw + __popc(m2) > GW_WLIST) {
+						flush_slow<TPL>(p, S.wlist, nw, t);
+						nw = 0;
+						__syncwarp();
+					}
+					if (tm) far_put(S, nl + __popc(m1 & lt), e);
+					if (tw) S.wlist[nw + __popc(m2 & lt)] = e;
+					nl += __popc(m1);
+					nw += __popc(m2);
+					__syncwarp();
+				}
+			}
+			__syncwarp();
 		}
-		__syncwarp();
 	}
 	__syncwarp();
-	flush_far<TPL>(S.list, nl, t);
+	flush_far<TPL>(S, nl, t);
 	flush_slow<TPL>(p, S.wlist, nw, t);
 #pragma unroll
 	for (int k = 0; k < TPL; k++) t[k].cost -= 1.f;     // the self pair, which the reference skips
@@ -643,7 +699,7 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 }
 
 template <int MODE, int TPL, typename F>
-__global__ void __launch_bounds__(GW_THREADS)
+__global__ void __launch_bounds__(GW_THREADS, GW_WALK_MINB)
 k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
              const tvg_wnode *__restrict__ wt,
              const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
@@ -964,88 +1020,94 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 
 	int sp = 0, nl = 0;
 	const int ntop = p.dc->ntop;
-	for (int r = lane; r < ntop; r += 32) S.stack[r] = r;
-	sp = ntop;
-	__syncwarp();
 	int guard = 0;
-	while (sp > 0) {
-		if (++guard > (1 << 24)) { atomicOr(status, TVG_ST_TIMEOUT); break; }
-		bool stop;
-		const int node = pop_nodes(S.stack, sp, status, stop);
-		if (stop) break;
-		bool accept = false, open_int = false, open_bundle = false;
-		float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
-		int nchild = 0, child = 0;
-		if (node >= 0) {
-			const tvg_wnode nd = wt[node];
-			const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
-			            dz = ioff(nd.cz, g.cz, p.scale);
-			const float gx = ioff(nd.gx, g.cx, p.scale), gy = ioff(nd.gy, g.cy, p.scale),
-			            gz = ioff(nd.gz, g.cz, p.scale);
-			const float hs = 0.5f * nd.size + margin;
-			const bool straddle = fabsf(gx) + hs + ex > p.half_box || fabsf(gy) + hs + ey > p.half_box
-			                   || fabsf(gz) + hs + ez > p.half_box;
-			bool open;
-			if (straddle) {
-				float r2;
-				open = gravity_opens(p, g, nd, node, dx, dy, dz, gx, gy, gz, r2);
-			} else {
-				// monopole error of K: G M h2 s^2 / (8 L^4) (s^2 / 4: the mean square
-				// offset of a uniform cube's mass from its centre)
-				const float rfar = (sqrtf(gx * gx + gy * gy + gz * gz) + nd.size + hmax) * p.inv_box;
-				const float l2 = p.inv_box * p.inv_box;
-				const float hs2 = ewald_h2(rfar) * nd.size2 * l2;     // h2 s^2 / L^2
-				if (p.use_bh) open = hs2 > p.ew_bh;
-				else open = nd.mass * hs2 * 0.125f * l2 > p.ew_rel * g.fac;
-			}
-			if (!open) {
-				accept = true;
-				entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
-			} else if (nd.nchild > 0) {
-				open_int = true;
-				nchild = nd.nchild;
-				child = nd.child;
-			} else {
-				open_bundle = true;
-				nchild = -nd.nchild;
-				child = nd.child;
-			}
-		}
-		const unsigned bm = __ballot_sync(0xFFFFFFFFu, accept);
-		if (accept) S.list[nl + __popc(bm & lt)] = entry;
-		nl += __popc(bm);
+	bool halt = false;
+	// the roots in chunks of GW_ROOTS (a balanced decomposition can have
+	// thousands of top nodes, more than the stack holds at once)
+	for (int r0 = 0; r0 < ntop && !halt; r0 += GW_ROOTS) {
+		const int nr = min(GW_ROOTS, ntop - r0);
+		for (int r = lane; r < nr; r += 32) S.stack[r] = r0 + r;
+		sp = nr;
 		__syncwarp();
-		if (nl >= 32) {
-			ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
-			nl -= 32;
-		}
-		push_children(S.stack, sp, open_int, nchild, child);
-		const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
-		if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
-		__syncwarp();
-		const int nb = __popc(bb);
-		for (int b = 0; b < nb; b++) {
-			const int2 q = S.bq[b];
-			for (int o = 0; o < q.y; o += 32) {
-				const int jj = o + lane;
-				const bool have = jj < q.y;
-				float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-				if (have) {
-					const int64_t jp = (int64_t) q.x + jj;
-					e = make_float4(ioff(ix[jp], g.cx, p.scale), ioff(iy[jp], g.cy, p.scale),
-					                ioff(iz[jp], g.cz, p.scale), p.gravity * mass_f[jp]);
+		while (sp > 0) {
+			if (++guard > p.max_iter) { atomicOr(status, TVG_ST_TIMEOUT); halt = true; break; }
+			bool stop;
+			const int node = pop_nodes(S.stack, sp, status, stop);
+			if (stop) { halt = true; break; }
+			bool accept = false, open_int = false, open_bundle = false;
+			float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
+			int nchild = 0, child = 0;
+			if (node >= 0) {
+				const tvg_wnode nd = wt[node];
+				const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
+				            dz = ioff(nd.cz, g.cz, p.scale);
+				const float gx = ioff(nd.gx, g.cx, p.scale), gy = ioff(nd.gy, g.cy, p.scale),
+				            gz = ioff(nd.gz, g.cz, p.scale);
+				const float hs = 0.5f * nd.size + margin;
+				const bool straddle = fabsf(gx) + hs + ex > p.half_box || fabsf(gy) + hs + ey > p.half_box
+				                   || fabsf(gz) + hs + ez > p.half_box;
+				bool open;
+				if (straddle) {
+					float r2;
+					open = gravity_opens(p, g, nd, node, dx, dy, dz, gx, gy, gz, r2);
+				} else {
+					// monopole error of K: G M h2 s^2 / (8 L^4) (s^2 / 4: the mean square
+					// offset of a uniform cube's mass from its centre)
+					const float rfar = (sqrtf(gx * gx + gy * gy + gz * gz) + nd.size + hmax) * p.inv_box;
+					const float l2 = p.inv_box * p.inv_box;
+					const float hs2 = ewald_h2(rfar) * nd.size2 * l2;     // h2 s^2 / L^2
+					if (p.use_bh) open = hs2 > p.ew_bh;
+					else open = nd.mass * hs2 * 0.125f * l2 > p.ew_rel * g.fac;
 				}
-				const unsigned mb = __ballot_sync(0xFFFFFFFFu, have);
-				if (have) S.list[nl + __popc(mb & lt)] = e;
-				nl += __popc(mb);
-				__syncwarp();
-				if (nl >= 32) {
-					ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
-					nl -= 32;
+				if (!open) {
+					accept = true;
+					entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
+				} else if (nd.nchild > 0) {
+					open_int = true;
+					nchild = nd.nchild;
+					child = nd.child;
+				} else {
+					open_bundle = true;
+					nchild = -nd.nchild;
+					child = nd.child;
 				}
 			}
+			const unsigned bm = __ballot_sync(0xFFFFFFFFu, accept);
+			if (accept) S.list[nl + __popc(bm & lt)] = entry;
+			nl += __popc(bm);
+			__syncwarp();
+			if (nl >= 32) {
+				ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
+				nl -= 32;
+			}
+			push_children(S.stack, sp, open_int, nchild, child);
+			const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
+			if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
+			__syncwarp();
+			const int nb = __popc(bb);
+			for (int b = 0; b < nb; b++) {
+				const int2 q = S.bq[b];
+				for (int o = 0; o < q.y; o += 32) {
+					const int jj = o + lane;
+					const bool have = jj < q.y;
+					float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+					if (have) {
+						const int64_t jp = (int64_t) q.x + jj;
+						e = make_float4(ioff(ix[jp], g.cx, p.scale), ioff(iy[jp], g.cy, p.scale),
+						                ioff(iz[jp], g.cz, p.scale), p.gravity * mass_f[jp]);
+					}
+					const unsigned mb = __ballot_sync(0xFFFFFFFFu, have);
+					if (have) S.list[nl + __popc(mb & lt)] = e;
+					nl += __popc(mb);
+					__syncwarp();
+					if (nl >= 32) {
+						ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
+						nl -= 32;
+					}
+				}
+			}
+			__syncwarp();
 		}
-		__syncwarp();
 	}
 	__syncwarp();
 	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, 0, nl, per_target, c, t, nev);
@@ -1157,15 +1219,28 @@ __global__ void k_to_float(int64_t n, const F *__restrict__ a, float *__restrict
 	if (i < n) b[i] = (float) a[i];
 }
 
+// Origin of the integer grid: the box origin when periodic (2^32 units per
+// box, wrap-around = nearest image); isolated, half a domain size below the
+// domain's origin (2^31 units per domain size, so the grid spans
+// [origin - size/2, origin + 3 size/2) and particles that drift out of the
+// domain between decompositions stay on it).
+static void grid_origin(const tvg_context *ctx, double o[3])
+{
+	for (int d = 0; d < 3; d++)
+		o[d] = ctx->cfg.periodic ? ctx->origin[d] : ctx->origin[d] - 0.5 * ctx->dsize;
+}
+
 template <typename F>
 static int prepare_typed(tvg_context *ctx)
 {
 	const int64_t n = ctx->n;
 	cudaStream_t s = ctx->stream;
 	const double fac = ctx->cfg.periodic ? 4294967296.0 / ctx->dsize : 2147483648.0 / ctx->dsize;
+	double go[3];
+	grid_origin(ctx, go);
 	k_int_pos<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(
 	    n, (const F *) ctx->f[FS_POS0], (const F *) ctx->f[FS_POS1], (const F *) ctx->f[FS_POS2],
-	    ctx->origin[0], ctx->origin[1], ctx->origin[2], fac, ctx->ipos[0], ctx->ipos[1], ctx->ipos[2]);
+	    go[0], go[1], go[2], fac, ctx->ipos[0], ctx->ipos[1], ctx->ipos[2], ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	// node count from the device: grid-stride launches, and a scan over the
 	// capacity (zeros past the count)
@@ -1175,12 +1250,11 @@ static int prepare_typed(tvg_context *ctx)
 	k_wt_nchild<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, lscan, tree, nch);
 	TVG_CUDA(ctx, cudaGetLastError());
 	TVG_CHECK(tvg_device_scan_i32(ctx, nch, choff, lscan, nullptr));
-	k_wt_emit<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, tree, nch, choff, ctx->origin[0],
-	                                                   ctx->origin[1], ctx->origin[2], fac, ctx->dsize,
-	                                                   ctx->wtree);
+	k_wt_emit<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, tree, nch, choff, go[0], go[1],
+	                                                   go[2], fac, ctx->dsize, ctx->wtree);
 	TVG_CUDA(ctx, cudaGetLastError());
-	k_wt_small_top<<<TVG_CNT(ctx, 1), 64, 0, s>>>(ctx->dc, ctx->d_top, ctx->cfg.vector_size, ctx->origin[0],
-	                                 ctx->origin[1], ctx->origin[2], fac, ctx->dsize, ctx->wtree);
+	k_wt_small_top<<<TVG_CNT(ctx, TVG_MAX_TOP / 128), 128, 0, s>>>(ctx->dc, ctx->d_top, ctx->cfg.vector_size, go[0], go[1],
+	                                 go[2], fac, ctx->dsize, ctx->wtree);
 	TVG_CUDA(ctx, cudaGetLastError());
 	ctx->have_walktree = true;
 	return TVG_OK;
@@ -1363,6 +1437,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	GroupParams p;
 	p.n = n;
 	p.dc = ctx->dc;
+	p.max_iter = ctx->walk_limit;
 	p.gsize = 32 * tpl;
 	if (ctx->use_active) {
 		TVG_CHECK(build_groups(ctx, p.gsize));

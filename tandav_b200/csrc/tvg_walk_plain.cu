@@ -42,6 +42,7 @@ template <typename F> struct PlainCtx {
 	const WNode<F> *tree;
 	const F *fx, *fy, *fz, *fp;
 	F boxhalf;
+	int64_t tree_cap;    // node capacity: the walks never read past it
 	PlainParams p;
 };
 
@@ -130,7 +131,9 @@ __device__ void walk_gravity(const PlainCtx<F> &c, const F sp[3], F sacc, double
 		}
 		const int start = t.target;
 		int node = start;
-		while (c.tree[node].DNext != 0 || node == start) {
+		// (a valid tree ends every subtree with a terminator, DNext = 0, well
+		// inside the capacity; the bound only keeps a damaged one in memory)
+		while (node < c.tree_cap && (c.tree[node].DNext != 0 || node == start)) {
 			const WNode<F> &nd = c.tree[node];
 			const int32_t dn = nd.DNext;
 			if (dn < 0) {
@@ -287,7 +290,7 @@ __device__ void walk_ewald(const PlainCtx<F> &c, const F sp[3], F sacc, double a
 		const int start = t.target;
 		const int end = start + c.tree[start].DNext;
 		int node = start;
-		while (node != end) {
+		while (node < end && node < c.tree_cap) {
 			const WNode<F> &nd = c.tree[node];
 			const int32_t dn = nd.DNext;
 			if (dn < 0) {
@@ -334,11 +337,15 @@ k_walk_plain(int64_t n_act, const int32_t *__restrict__ active, PlainCtx<F> c, i
              const F *__restrict__ last_acc, F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1,
              F *gacc2, F *cost_out, F *pot_out, double *counter)
 {
-	__shared__ tvg_topnode s_top[TVG_MAX_TOP];
-	for (int j = threadIdx.x; j < c.p.ntop; j += blockDim.x) s_top[j] = c.top[j];
-	__syncthreads();
+	// every thread reads every top node: staged in shared memory when they
+	// fit (one target: <= 64 level-2 cells), else read through L1
+	__shared__ tvg_topnode s_top[64];
 	PlainCtx<F> cc = c;
-	cc.top = s_top;
+	if (c.p.ntop <= 64) {
+		for (int j = threadIdx.x; j < c.p.ntop; j += blockDim.x) s_top[j] = c.top[j];
+		__syncthreads();
+		cc.top = s_top;
+	}
 	const int64_t t = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
 	F cost = 0;
 	if (t < n_act) {
@@ -384,6 +391,7 @@ static int walk_typed(tvg_context *ctx, int use_bh, uint32_t parts)
 	c.m = (const F *) ctx->f[FS_MASS];
 	c.top = ctx->d_top;
 	c.tree = (const WNode<F> *) ctx->tree;
+	c.tree_cap = ctx->tcap;
 	c.fx = (const F *) ctx->ewald_f[0];
 	c.fy = (const F *) ctx->ewald_f[1];
 	c.fz = (const F *) ctx->ewald_f[2];

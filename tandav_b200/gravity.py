@@ -218,7 +218,7 @@ class GravityContext:
     # ------------------------------------------------------------ data
 
     def upload(self, pos, mass, vel=None, ids=None, last_acc=None, types=None, time_bin=None,
-               it_drift=None, it_kick=None, acc=None, grav_acc=None):
+               it_drift=None, it_kick=None, acc=None, grav_acc=None, cost=None):
         ft = self.ft
         n = int(np.asarray(mass).shape[0])
         self._keep = []
@@ -258,6 +258,11 @@ class GravityContext:
         self._keep.append(ids)
         p.id = ids.ctypes.data
         fields |= F_ID
+        if cost is not None:          # P.Cost: what a balanced decomposition weighs
+            c_arr = np.ascontiguousarray(cost, dtype=ft)
+            self._keep.append(c_arr)
+            p.cost = c_arr.ctypes.data
+            fields |= F_COST
         la = np.zeros(n, ft) if last_acc is None else np.ascontiguousarray(last_acc, dtype=ft)
         self._keep.append(la)
         p.last_acc_mag = la.ctypes.data
@@ -323,6 +328,17 @@ class GravityContext:
         self._check(self.lib.tvg_sort_particles(self.ctx, C.c_void_p(_ptr(perm))), "sort")
         return perm
 
+    def set_domain_decomposition(self, ntask=1, part_alloc_factor=1.1, imbal_ceil=0.05):
+        """Domain_Decomposition over NTask targets (tvg_set_domain_decomposition)."""
+        self._check(self.lib.tvg_set_domain_decomposition(
+            self.ctx, C.c_int32(ntask), C.c_double(part_alloc_factor), C.c_double(imbal_ceil)),
+            "set_domain_decomposition")
+
+    def decomposition_rounds(self):
+        r = C.c_int32()
+        self._check(self.lib.tvg_decomposition_rounds(self.ctx, C.byref(r)), "decomposition_rounds")
+        return r.value
+
     def top_nodes(self):
         nt = C.c_int32()
         self._check(self.lib.tvg_top_nodes(self.ctx, C.byref(nt)), "top_nodes")
@@ -338,10 +354,10 @@ class GravityContext:
         self._check(self.lib.tvg_download_tree(self.ctx, None, C.c_int64(0), C.byref(nn), None,
                                                C.c_int32(0), C.byref(nt)), "download_tree")
         tree = np.zeros(max(nn.value, 1), TREE_DTYPE[self.fb])
-        top = np.zeros(64, TOPNODE_DTYPE)
+        top = np.zeros(max(nt.value, 1), TOPNODE_DTYPE)
         self._check(self.lib.tvg_download_tree(self.ctx, C.c_void_p(tree.ctypes.data),
                                                C.c_int64(len(tree)), C.byref(nn),
-                                               C.c_void_p(top.ctypes.data), C.c_int32(64),
+                                               C.c_void_p(top.ctypes.data), C.c_int32(len(top)),
                                                C.byref(nt)), "download_tree")
         return tree[:nn.value].copy(), top[:nt.value].copy()
 
@@ -515,6 +531,11 @@ class GravityContext:
         """Opening of the group form's Ewald walk (see tvg_set_ewald_opening)."""
         self._check(self.lib.tvg_set_ewald_opening(self.ctx, C.c_double(rel_alpha),
                                                    C.c_double(bh_factor)), "set_ewald_opening")
+
+    def set_walk_limit(self, max_iterations=1 << 24):
+        """Iteration limit of the group walks (see tvg_set_walk_limit)."""
+        self._check(self.lib.tvg_set_walk_limit(self.ctx, C.c_int64(max_iterations)),
+                    "set_walk_limit")
 
     def forcetest(self, targets, parts=None):
         """Gravity_Forcetest: FP64 direct force on the targets (sorted-order

@@ -5,7 +5,8 @@ oracle/_ref/<variant>/ref_harness; this script feeds them seeded inputs and
 stores their outputs (keys, sort permutation, top nodes, tree, Tree_Parent,
 accelerations of the BH and relative passes, Ewald parts) as compressed .npz
 files. Re-run after changing the inputs: `python tests/golden/make_golden.py`
-(`... make_golden.py potential` for the potential fixtures only).
+(`... make_golden.py potential` for the potential fixtures only,
+`... make_golden.py decomposition` for the balanced decompositions only).
 """
 from __future__ import annotations
 
@@ -63,6 +64,32 @@ def force_case(name, variant, p, flags=3):
     np.savez_compressed(HERE / f"{name}.npz", **out)
 
 
+def decomposition_case(name, variant, p, ntask):
+    """The reference's second Domain_Decomposition (mode force2) at `ntask`
+    OpenMP threads: top nodes balanced by the P.Cost of a first force
+    computation, the tree and both passes on them."""
+    r = refrun.run(variant, "force2", p.pos, p.vel, p.mass, box=p.box, softening=p.softening,
+                   flags=3, threads=ntask)
+    out = dict(pos_in=p.pos, mass_in=p.mass, box=np.array(p.box), softening=np.array(p.softening),
+               ntask=np.array(ntask), float_size=np.array(r["float_size"]), gravity=r["gravity"],
+               domain_size=r["domain_size"], domain_origin=r["domain_origin"],
+               cost_in=r["cost_in"], id_in=r["id_in"], perm=r["perm"], std_key=r["std_key"],
+               rev_key=r["rev_key"], topnodes=r["topnodes"], tree=r["tree"],
+               tree_parent=r["tree_parent"], last_acc_mag=r["last_acc_mag"])
+    for part in ("bh", "rel", "bhew", "relew"):
+        for q in ("gacc", "cost"):
+            k = f"{part}_{q}"
+            if k in r:
+                out[k] = r[k]
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+
+
+def decomposition_cases():
+    decomposition_case("decomp_hernquist_iso_f64_t3", "iso_f64", ics.hernquist(n=16384, seed=43), 3)
+    decomposition_case("decomp_clumpy_per_f32_t8", "per_f32",
+                       ics.random_box(20000, box=1000.0, seed=44, clumps=5), 8)
+
+
 def main():
     keys_case()
     force_case("hernquist_iso_f64", "iso_f64", ics.hernquist(n=2048, seed=5))
@@ -83,5 +110,7 @@ if __name__ == "__main__":
     # `make_golden.py potential` writes only the potential fixtures
     if sys.argv[1:] == ["potential"]:
         potential_cases()
+    elif sys.argv[1:] == ["decomposition"]:
+        decomposition_cases()
     else:
         main()

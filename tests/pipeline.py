@@ -5,11 +5,31 @@ from __future__ import annotations
 import numpy as np
 
 import port
+from refrun import TOPNODE_DTYPE
+
+
+def balanced_top_nodes(std_s, pos_s, cost_s, origin, size, ntask):
+    """Top nodes of the reference's decomposition over `ntask` targets
+    (oracle/decomposition.py), with the centres transform_bunches_into_top_nodes
+    gives them (domain.c:220-250)."""
+    import decomposition
+    bunches, _ = decomposition.decompose(std_s[:, 0], cost_s, ntask)
+    top = np.zeros(len(bunches), TOPNODE_DTYPE)
+    for t, (key, level, first, npart) in enumerate(bunches):
+        top[t]["Key"], top[t]["Level"], top[t]["First_Part"], top[t]["Npart"] = key, level, first, npart
+        top[t]["Target"] = -1
+        sz = size / float(1 << level)
+        for k in range(3):
+            px = float(pos_s[k, first]) - float(origin[k])
+            top[t]["Pos"][k] = np.float32((np.floor(px / sz) + 0.5) * sz + float(origin[k]))
+    return top
 
 
 def oracle_pipeline(pos, mass, origin, size, fsize, box=0.0, softening=0.01, gravity=43007.1,
-                    ewald=None, passes=("bh", "rel")):
-    """Keys -> sort -> top nodes -> tree -> walks, as the reference runs them."""
+                    ewald=None, passes=("bh", "rel"), ntask=1, cost=None):
+    """Keys -> sort -> top nodes -> tree -> walks, as the reference runs them
+    (top nodes balanced over `ntask` targets by `cost`, in input order, when
+    ntask > 1)."""
     ft = port.ftype(fsize)
     pos_f = np.asarray(pos).astype(ft)
     std, rev = port.peano_keys(pos_f, origin, size, fsize)
@@ -17,7 +37,10 @@ def oracle_pipeline(pos, mass, origin, size, fsize, box=0.0, softening=0.01, gra
     std_s, rev_s = std[perm], rev[perm]
     pos_s = pos_f[:, perm]
     mass_s = np.asarray(mass).astype(ft)[perm]
-    top = port.top_nodes(std_s, pos_s, origin, size, fsize)
+    if ntask > 1:
+        top = balanced_top_nodes(std_s, pos_s, np.asarray(cost, np.float64)[perm], origin, size, ntask)
+    else:
+        top = port.top_nodes(std_s, pos_s, origin, size, fsize)
     tree, top, parent = port.tree_build(rev_s, pos_s, mass_s, size, top, fsize)
     out = dict(perm=perm, std_key=std_s, rev_key=rev_s, pos=pos_s, mass=mass_s, top=top,
                tree=tree, tree_parent=parent)

@@ -85,3 +85,37 @@ def test_group_accuracy(kind):
         assert rms_g <= 1.2 * rms_p + 1e-6
         if rms_p < 1e-3:
             assert rms_g < 1e-3
+
+
+def test_walk_limit_times_out_and_the_context_recovers():
+    """The group walks' traversal loops are bounded (tvg_set_walk_limit): with
+    a limit of a few iterations both the gravity and the Ewald walk stop,
+    tvg_walk returns TVG_E_TIMEOUT, and the context stays usable -- with the
+    limit restored the same walk gives the accelerations of a walk that never
+    timed out."""
+    # 32^3: 512 particles per level-2 cell, so every top node has a subtree
+    # and a group needs many node batches
+    p = ics.zeldovich_box(n_side=32, seed=34)
+    parts = G.WALK_GRAVITY | G.WALK_EWALD
+    with G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box,
+                          softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.peano_keys()
+        ctx.sort_particles()
+        ctx.top_nodes()
+        ctx.tree_build()
+        ctx.ewald_init()
+        ctx.zero_accel()
+        ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
+        first = ctx.download(G.F_GRAV_ACC)["grav_acc"].copy()
+        for part in (G.WALK_GRAVITY, G.WALK_EWALD):
+            ctx.set_walk_limit(2)
+            ctx.zero_accel()
+            with pytest.raises(G.TvgError) as e:
+                ctx.walk(G.FORM_GROUP, use_bh=True, parts=part)
+            assert e.value.code == 4, e.value          # TVG_E_TIMEOUT
+        ctx.set_walk_limit()
+        ctx.zero_accel()
+        ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
+        assert np.array_equal(ctx.download(G.F_GRAV_ACC)["grav_acc"], first)

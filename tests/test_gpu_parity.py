@@ -105,6 +105,83 @@ def test_pipeline_matches_reference_golden(golden_dir, case):
         assert np.array_equal(ctx.download(G.F_KEY)["key"], g["rev_key"])
 
 
+def test_config1_hernquist_65536_fp64_vs_reference():
+    """The CPU-runnable configuration exactly: an isolated Hernquist halo of
+    65,536 equal-mass particles (a = 1, truncated at 100 a, eps = 0.01 a), FP64,
+    one tree build and both passes -- Barnes-Hut (theta^2 0.25), then the
+    relative criterion (errtol 0.005) with |a_old| from the first pass
+    (accel.c:15-71). The reference itself (oracle/_ref/iso_f64, the unmodified
+    sources) runs on the same input here; keys, permutation, top nodes, every
+    tree field, Tree_Parent, both passes' accelerations and interaction counts
+    and Last_Acc_Mag must equal its output bit for bit."""
+    import refrun
+    if not refrun.available("iso_f64"):
+        pytest.skip("reference harness oracle/_ref/iso_f64 not built (make -C oracle ref)")
+    p = ics.hernquist(n=65536, seed=31)
+    r = refrun.run("iso_f64", "force", p.pos, p.vel, p.mass, softening=p.softening, flags=3)
+    assert r["float_size"] == 8
+    with make_ctx(p.n, 8, softening=p.softening, gravity=float(r["gravity"][0])) as ctx:
+        perm, keys, tree, top = gpu_pipeline(ctx, p.pos, p.mass, r["domain_origin"],
+                                             float(r["domain_size"][0]))
+        assert np.array_equal(perm, r["perm"])
+        assert np.array_equal(keys, r["std_key"])
+        assert_struct_equal(top, r["topnodes"], TOP_FIELDS, "topnodes")
+        assert_struct_equal(tree, r["tree"], TREE_FIELDS, "tree")
+        assert np.array_equal(ctx.download(G.F_TREE_PARENT)["tree_parent"], r["tree_parent"])
+        bh, last, rel = walks(ctx, False, 8)
+        for name, got in (("bh", bh), ("rel", rel)):
+            assert np.array_equal(got["cost"].astype(np.float64), r[name + "_cost"]), name
+            a = got["grav_acc"].astype(np.float64)
+            assert np.array_equal(a, r[name + "_gacc"]), \
+                f"{name}: max diff {np.abs(a - r[name + '_gacc']).max()}"
+        assert np.array_equal(last.astype(np.float64), r["last_acc_mag"])
+        ctx.reverse_keys()
+        assert np.array_equal(ctx.download(G.F_KEY)["key"], r["rev_key"])
+
+
+BALANCED_CASES = ["decomp_hernquist_iso_f64_t3", "decomp_clumpy_per_f32_t8"]
+
+
+@pytest.mark.parametrize("case", BALANCED_CASES)
+def test_balanced_decomposition_matches_reference(golden_dir, case):
+    """Top nodes balanced over NTask = 3 and 8 targets by the P.Cost of a
+    first force computation, as the reference's second Domain_Decomposition
+    makes them (domain.c:67-145, 151-156; levels 2 to 6, up to several hundred
+    top nodes), then the tree and both passes on them: permutation, keys, top
+    nodes, every tree field, Tree_Parent, forces and interaction counts equal
+    the reference's bit for bit."""
+    g = np.load(golden_dir / f"{case}.npz")
+    fsize, box = int(g["float_size"]), float(g["box"])
+    n = len(g["mass_in"])
+    cost = np.empty(n)
+    cost[g["id_in"].astype(np.int64)] = g["cost_in"]
+    with make_ctx(n, fsize, box=box, softening=float(g["softening"]),
+                  gravity=float(g["gravity"][0])) as ctx:
+        ctx.set_domain_decomposition(int(g["ntask"]))
+        ctx.upload(g["pos_in"], g["mass_in"], cost=cost)
+        ctx.set_domain(g["domain_origin"], float(g["domain_size"][0]))
+        ctx.peano_keys()
+        perm = ctx.sort_particles()
+        keys = ctx.download(G.F_KEY)["key"]
+        ntop = ctx.top_nodes()
+        assert ctx.decomposition_rounds() > 0
+        ctx.tree_build(exact_moments=True)
+        tree, top = ctx.download_tree()
+        assert ntop == len(g["topnodes"])
+        assert np.array_equal(perm, g["perm"])
+        assert np.array_equal(keys, g["std_key"])
+        assert_struct_equal(top, g["topnodes"], TOP_FIELDS, "topnodes")
+        assert_struct_equal(tree, g["tree"], TREE_FIELDS, "tree")
+        assert np.array_equal(ctx.download(G.F_TREE_PARENT)["tree_parent"], g["tree_parent"])
+        bh, last, rel = walks(ctx, box > 0, fsize)
+        for name, got in (("bh", bh), ("rel", rel)):
+            assert np.array_equal(got["cost"].astype(np.float64), g[name + "_cost"]), name
+            a = got["grav_acc"].astype(np.float64)
+            assert np.array_equal(a, g[name + "_gacc"]), \
+                f"{name}: max diff {np.abs(a - g[name + '_gacc']).max()}"
+        assert np.array_equal(last.astype(np.float64), g["last_acc_mag"])
+
+
 RANDOM_CASES = [
     ("hernquist", 8, 32768),
     ("hernquist", 4, 65536),
@@ -131,22 +208,21 @@ def test_tree_and_plain_walk_vs_oracle(kind, fsize, n):
     p, origin, size = make_case(kind, n)
     ew = oracle_ewald_tables(fsize, p.box) if p.box > 0 else None
     o = oracle_pipeline(p.pos, p.mass, origin, size, fsize, box=p.box, softening=p.softening,
-                        ewald=ew, passes=("bh",))
+                        ewald=ew, passes=("bh", "rel"))
     with make_ctx(p.n, fsize, box=p.box, softening=p.softening) as ctx:
         perm, keys, tree, top = gpu_pipeline(ctx, p.pos, p.mass, origin, size)
         assert np.array_equal(perm, o["perm"])
         assert_struct_equal(top, o["top"], TOP_FIELDS, "topnodes")
         assert_struct_equal(tree, o["tree"], TREE_FIELDS, "tree")
         assert np.array_equal(ctx.download(G.F_TREE_PARENT)["tree_parent"], o["tree_parent"])
-        parts = G.WALK_GRAVITY | (G.WALK_EWALD if p.box > 0 else 0)
-        if p.box > 0:
-            ctx.upload_ewald_table(*reference_table(fsize))
-        ctx.zero_accel()
-        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
-        got = ctx.download(G.F_GRAV_ACC | G.F_COST)
-        assert np.array_equal(got["cost"], o["bh_cost"])
-        a, ref = got["grav_acc"].astype(np.float64), o["bh_gacc"].astype(np.float64)
-        assert np.array_equal(a, ref), f"max diff {np.abs(a - ref).max()}"
+        # both passes: Barnes-Hut, then the relative criterion with |a_old|
+        # from the first (accel.c:15-71)
+        bh, last, rel = walks(ctx, p.box > 0, fsize)
+        for name, got in (("bh", bh), ("rel", rel)):
+            assert np.array_equal(got["cost"], o[name + "_cost"]), name
+            a, ref = got["grav_acc"].astype(np.float64), o[name + "_gacc"].astype(np.float64)
+            assert np.array_equal(a, ref), f"{name}: max diff {np.abs(a - ref).max()}"
+        assert np.array_equal(last, o["last_acc_mag"])
 
 
 def test_fast_moments_close_to_exact():
