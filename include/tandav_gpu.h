@@ -460,10 +460,11 @@ int tvg_step_graph_reset(tvg_context *ctx);
 
 /* Autotuner of the group form (no reference counterpart): on the current tree
  * and active set, times the gravity + Ewald walks with 32-, 64- and
- * 128-particle groups (one, two or four targets per lane) and keeps the
+ * 128-particle groups (one, two or four targets per lane) over a sample --
+ * the active particles in every 8th window of 128 particles -- and keeps the
  * fastest for the later walks of this context. choice receives 1, 2 or 4,
- * ms[3] the three times. The chosen walk runs last: the accelerations left
- * are its result. */
+ * ms[3] the three sample times. The chosen walk then runs over the whole
+ * active set: the accelerations left are its result. */
 int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
                  int32_t *choice, double *ms);
 

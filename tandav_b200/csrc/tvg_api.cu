@@ -180,7 +180,8 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->ewald_ext, ctx->active, ctx->kd_x, ctx->kd_kick, ctx->kd_drift,
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
 	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
-	                 ctx->d_toptab, ctx->top_of, ctx->dd_scratch, ctx->tu_first, ctx->tu_dp };
+	                 ctx->d_toptab, ctx->top_of, ctx->dd_scratch, ctx->tu_first, ctx->tu_dp,
+	                 ctx->tune_active };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

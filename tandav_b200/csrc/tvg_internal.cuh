@@ -195,6 +195,7 @@ struct tvg_context {
 
 	// active particles (Active_Particle_List); all particles when !use_active
 	int32_t *active = nullptr;
+	int32_t *tune_active = nullptr;    // the autotuner's sample of the active set
 	int64_t n_active = 0;
 	bool use_active = false;
 	int64_t launches = 0;              // kernels launched by this context

@@ -312,6 +312,56 @@ struct EwaldSmem {
 	int2 bq[GW_BQ];
 };
 
+// Per-warp stage of the Ewald walk's Taylor records (table evaluation): a
+// full batch of 32 accepted sources has its 32 records (256 B each) copied
+// from the table in global memory into shared memory by the bulk-copy (TMA)
+// engine, cp.async.bulk completing on an mbarrier, while the warp goes on
+// walking; the batch is evaluated from shared memory when the next one is
+// issued. Two buffers: a new batch is issued before the pending one is
+// evaluated. Sources are this GPU's own memory; no multicast.
+struct EwaldStage {
+	float4 rec[2][32][16];     // the batches' records
+	float4 pend[2][32];        // the batches' sources
+	uint64_t bar[2];           // completion barriers (arrival count 1 + transaction bytes)
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+	return (uint32_t) __cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+	             : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+	uint32_t done;
+	asm volatile("{\n\t.reg .pred p;\n\t"
+	             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+	             "selp.u32 %0, 1, 0, p;\n\t}"
+	             : "=r"(done)
+	             : "r"(smem_addr(bar)), "r"(parity)
+	             : "memory");
+	return done != 0;
+}
+
+// 1-D bulk copy global -> shared (16-byte aligned addresses, size a multiple
+// of 16), completing `bytes` transactions on the mbarrier
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+	             ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+	             : "memory");
+}
+
 // per-lane sums over accepted sources of m K, m J and m H (about the group
 // centre), FP32 (a few hundred terms per lane)
 struct CorrSum {
@@ -786,9 +836,20 @@ __device__ __forceinline__ void lagrange4(float t, float w[4], float d[4], float
 // K_a = -s_a T_a, J_ab = -s_a s_b g dT_a/du_b, H_abc = -s_a s_b s_c g^2
 // d2T_a/du_b du_c, all times G m / L^2 (s the signs of d, g node spacings per
 // length).
-template <bool OVR>
+// index of the Taylor-table record nearest to |d| (node units)
+__device__ __forceinline__ int taylor_record(const GroupParams &p, float4 e)
+{
+	const int i = min(__float2int_rn(fabsf(e.x) * p.tay_grid), TVG_TAYLOR_NODES - 1);
+	const int j = min(__float2int_rn(fabsf(e.y) * p.tay_grid), TVG_TAYLOR_NODES - 1);
+	const int l = min(__float2int_rn(fabsf(e.z) * p.tay_grid), TVG_TAYLOR_NODES - 1);
+	return (i * TVG_TAYLOR_NODES + j) * TVG_TAYLOR_NODES + l;
+}
+
+// STAGED: the record is `staged` (shared memory) instead of the table entry
+template <bool OVR, bool STAGED = false>
 __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const float4 *__restrict__ tay,
-                                                 float4 e, CorrSum &c, const float *ovr)
+                                                 float4 e, CorrSum &c, const float *ovr,
+                                                 const float4 *staged = nullptr)
 {
 	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
 	const float u = fabsf(e.x) * p.tay_grid, v = fabsf(e.y) * p.tay_grid, w = fabsf(e.z) * p.tay_grid;
@@ -796,12 +857,17 @@ __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const flo
 	const int j = min(__float2int_rn(v), TVG_TAYLOR_NODES - 1);
 	const int l = min(__float2int_rn(w), TVG_TAYLOR_NODES - 1);
 	const float du = u - (float) i, dv = v - (float) j, dw = w - (float) l;
-	const float4 *rec = tay + 16 * ((i * TVG_TAYLOR_NODES + j) * TVG_TAYLOR_NODES + l);
+	const float4 *rec = STAGED ? staged : tay + 16 * ((i * TVG_TAYLOR_NODES + j) * TVG_TAYLOR_NODES + l);
 	const float m0 = -e.w * p.inv_box * p.inv_box, m1 = m0 * p.tay_grid, m2 = m1 * p.tay_grid;
 #pragma unroll
 	for (int q = 0; q < 3; q++) {
-		const float4 r0 = __ldg(rec + 5 * q), r1 = __ldg(rec + 5 * q + 1), r2 = __ldg(rec + 5 * q + 2),
-		             r3 = __ldg(rec + 5 * q + 3), r4 = __ldg(rec + 5 * q + 4);
+		float4 r0, r1, r2, r3, r4;
+		if (STAGED) {
+			r0 = rec[5 * q]; r1 = rec[5 * q + 1]; r2 = rec[5 * q + 2]; r3 = rec[5 * q + 3]; r4 = rec[5 * q + 4];
+		} else {
+			r0 = __ldg(rec + 5 * q); r1 = __ldg(rec + 5 * q + 1); r2 = __ldg(rec + 5 * q + 2);
+			r3 = __ldg(rec + 5 * q + 3); r4 = __ldg(rec + 5 * q + 4);
+		}
 		// D_bc = sum_d d3T_bcd du_d
 		const float dxx = fmaf(r2.z, du, fmaf(r3.y, dv, r3.z * dw));
 		const float dyy = fmaf(r3.w, du, fmaf(r2.w, dv, r4.x * dw));
@@ -989,6 +1055,68 @@ __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *
 	}
 }
 
+// pipeline state of a warp's record stage (uniform across its lanes)
+struct StageState {
+	uint32_t phase;    // bit b: parity of buffer b's next completion
+	int cur;           // the buffer the next batch goes to
+	bool pending;      // the other buffer holds an issued batch
+	bool ok;           // false after a wait gave up: no more staging
+};
+
+// bounded wait for buffer b's copies (TVG_ST_TIMEOUT when they never land)
+__device__ __forceinline__ bool stage_wait(EwaldStage *st, int b, StageState &ss, int *status)
+{
+	const uint32_t par = (ss.phase >> b) & 1u;
+	for (int it = 0; !mbar_try_wait(&st->bar[b], par);) {
+		if (++it > (1 << 20)) {
+			atomicOr(status, TVG_ST_TIMEOUT);
+			ss.ok = false;
+			return false;
+		}
+	}
+	ss.phase ^= 1u << b;
+	return true;
+}
+
+__device__ __forceinline__ void stage_eval(const GroupParams &p, EwaldStage *st, int b, CorrSum &c, float &nev)
+{
+	const int lane = threadIdx.x & 31;
+	ewald_kjh_taylor<false, true>(p, nullptr, st->pend[b][lane], c, nullptr, &st->rec[b][lane][0]);
+	nev += 1.f;
+}
+
+// a full batch of 32 sources (list[from + lane]) goes to the free buffer;
+// then the batch issued before it is evaluated. Every lane copies its own
+// record; lane 0 posts the batch's 8 KB on the buffer's barrier first.
+__device__ __forceinline__ void stage_batch(const GroupParams &p, const float4 *__restrict__ tay,
+                                            EwaldStage *st, const float4 *list, int from, StageState &ss,
+                                            CorrSum &c, float &nev, int *status)
+{
+	const int lane = threadIdx.x & 31;
+	const float4 e = list[from + lane];
+	const int b = ss.cur;
+	if (lane == 0) mbar_arrive_expect_tx(&st->bar[b], 32 * 16 * sizeof(float4));
+	__syncwarp();
+	st->pend[b][lane] = e;
+	// this lane read the slot as generic memory when the buffer was last
+	// evaluated: order that before the bulk copy writes it
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	bulk_g2s(&st->rec[b][lane][0], tay + 16 * taylor_record(p, e), 16 * sizeof(float4), &st->bar[b]);
+	if (ss.pending && stage_wait(st, b ^ 1, ss, status)) stage_eval(p, st, b ^ 1, c, nev);
+	ss.pending = true;
+	ss.cur = b ^ 1;
+	__syncwarp();
+}
+
+// evaluates the batch still in flight (end of a group)
+__device__ __forceinline__ void stage_drain(const GroupParams &p, EwaldStage *st, StageState &ss, CorrSum &c,
+                                            float &nev, int *status)
+{
+	if (ss.pending && stage_wait(st, ss.cur ^ 1, ss, status)) stage_eval(p, st, ss.cur ^ 1, c, nev);
+	ss.pending = false;
+	__syncwarp();
+}
+
 template <int TPL, bool MLP>
 __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode *__restrict__ wt,
                             const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
@@ -996,7 +1124,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
                             const float *__restrict__ last_acc, const float4 *__restrict__ tab,
                             const float4 *__restrict__ tay, const float *mlp, const uint32_t *w2b,
                             int64_t first, int cnt, const int32_t *__restrict__ active,
-                            Target (&t)[TPL], float &nev, int *status)
+                            Target (&t)[TPL], float &nev, EwaldStage *st, StageState &ss, int *status)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned lt = (1u << lane) - 1u;
@@ -1077,7 +1205,8 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 			nl += __popc(bm);
 			__syncwarp();
 			if (nl >= 32) {
-				ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
+				if (st && ss.ok && !per_target) stage_batch(p, tay, st, S.list, nl - 32, ss, c, nev, status);
+				else ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
 				nl -= 32;
 			}
 			push_children(S.stack, sp, open_int, nchild, child);
@@ -1101,7 +1230,8 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 					nl += __popc(mb);
 					__syncwarp();
 					if (nl >= 32) {
-						ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
+						if (st && ss.ok && !per_target) stage_batch(p, tay, st, S.list, nl - 32, ss, c, nev, status);
+						else ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
 						nl -= 32;
 					}
 				}
@@ -1110,6 +1240,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 		}
 	}
 	__syncwarp();
+	if (st && ss.ok) stage_drain(p, st, ss, c, nev, status);
 	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, 0, nl, per_target, c, t, nev);
 	if (per_target) return;
 	// sum over lanes (FP64), then K(d_c - t) ~ K - J t + H:tt / 2 per target
@@ -1173,6 +1304,18 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 		__syncthreads();
 	}
 	const int lane = threadIdx.x & 31;
+	// the table path stages its records (EwaldStage after the warps' areas)
+	EwaldStage *st = MLP ? nullptr
+	                     : ((EwaldStage *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS)) + (threadIdx.x >> 5);
+	StageState ss = { 0u, 0, false, true };
+	if (st) {
+		if (lane == 0) {
+			mbar_init(&st->bar[0], 1);
+			mbar_init(&st->bar[1], 1);
+			asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		}
+		__syncwarp();
+	}
 	double ev_acc = 0;
 	const int64_t ngroups = p.dc->ngroups;
 	for (;;) {
@@ -1192,7 +1335,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 		Target t[TPL];
 		float nev = 0.f;
 		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, tay, mlp, w2b, first, cnt, active, t, nev,
-		                 status);
+		                 st, ss, status);
 		ev_acc += nev;
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
@@ -1360,7 +1503,8 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	static int nblk_dev[TVG_MAX_DEVICES] = { 0 };
 	TVG_CHECK(device_slot(ctx));
 	int &nblk = nblk_dev[ctx->device];
-	const size_t smem = sizeof(EwaldSmem) * GW_WARPS + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : 0);
+	const size_t smem = sizeof(EwaldSmem) * GW_WARPS
+	                  + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : sizeof(EwaldStage) * GW_WARPS);
 	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
 	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
@@ -1509,24 +1653,80 @@ int tvg_walk_group_results(tvg_context *ctx)
 // Autotuner of the group form: times the walks of the current tree and active
 // set with each group size (targets per lane) and keeps the fastest; the walk
 // of the chosen size runs last, so its accelerations are the ones left.
+// The autotuner's sample: the active particles (all particles without an
+// active list) that lie in every TUNE_STRIDE-th window of 128 particles, so
+// that groups of 32, 64 and 128 are all full windows of the sample.
+#define TUNE_WINDOW 128
+#define TUNE_STRIDE 8
+
+__global__ void k_tune_flags(int64_t n_src, const tvg_devcount *__restrict__ dc,
+                             const int32_t *__restrict__ src, int32_t *__restrict__ flag)
+{
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k >= n_src) return;
+	const int64_t m = src ? dc->n_active : n_src;
+	const int64_t i = src ? (int64_t) src[k] : k;
+	flag[k] = k < m && (i / TUNE_WINDOW) % TUNE_STRIDE == 0;
+}
+
+__global__ void k_tune_scatter(int64_t n_src, const int32_t *__restrict__ src, const int32_t *__restrict__ flag,
+                               const int32_t *__restrict__ off, int32_t *__restrict__ out)
+{
+	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (k < n_src && flag[k]) out[off[k]] = src ? src[k] : (int32_t) k;
+}
+
 extern "C" int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
                             int32_t *choice, double *ms)
 {
 	if (!ctx) return TVG_E_BADINPUT;
 	if (!ctx->have_tree) return tvg_fail(ctx, TVG_E_STATE, "autotune: no tree");
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	cudaStream_t s = ctx->stream;
+	// the active count as the walks read it, on the device
+	int64_t dev_n_active = 0;
+	TVG_CUDA(ctx, cudaMemcpyAsync(&dev_n_active, &ctx->dc->n_active, 8, cudaMemcpyDeviceToHost, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	// the sample as a temporary active list
+	const int64_t n_src = ctx->use_active ? dev_n_active : ctx->n;
+	if (!ctx->tune_active) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->tune_active, 4 * (size_t) ctx->cap));
+	if (!ctx->act_flag) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_flag, 4 * (size_t) ctx->cap));
+	if (!ctx->act_off) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->act_off, 4 * (size_t) ctx->cap));
+	const int32_t *src = ctx->use_active ? ctx->active : nullptr;
+	k_tune_flags<<<TVG_CNT(ctx, tvg_blocks(n_src, 256)), 256, 0, s>>>(n_src, ctx->dc, src, ctx->act_flag);
+	TVG_CUDA(ctx, cudaGetLastError());
+	int64_t n_tune = 0;
+	TVG_CHECK(tvg_device_scan_i32(ctx, ctx->act_flag, ctx->act_off, n_src, &n_tune));
+	k_tune_scatter<<<TVG_CNT(ctx, tvg_blocks(n_src, 256)), 256, 0, s>>>(n_src, src, ctx->act_flag,
+	                                                                    ctx->act_off, ctx->tune_active);
+	TVG_CUDA(ctx, cudaGetLastError());
+	const bool was_active = ctx->use_active;
+	int32_t *const saved_list = ctx->active;
+	const int64_t saved_n = ctx->n_active;
+	ctx->active = ctx->tune_active;
+	ctx->use_active = true;
+	ctx->n_active = n_tune;
+	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->dc->n_active, &n_tune, 8, cudaMemcpyHostToDevice, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
 	const int sizes[3] = { 1, 2, 4 };
 	double t[3] = { 0, 0, 0 };
-	int best = 0;
-	for (int c = 0; c < 3; c++) {
+	int best = 0, rc = TVG_OK;
+	for (int c = 0; c < 3 && rc == TVG_OK && n_tune > 0; c++) {
 		ctx->group_tpl = sizes[c];
-		TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
+		rc = tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind);
 		t[c] = ctx->phase_ms[4] + ctx->phase_ms[5];
 		if (t[c] < t[best]) best = c;
 	}
-	ctx->group_tpl = sizes[best];
-	if (best != 2) TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
-	if (choice) *choice = sizes[best];
+	// the caller's active set back, then the chosen walk over all of it
+	ctx->active = saved_list;
+	ctx->use_active = was_active;
+	ctx->n_active = saved_n;
+	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->dc->n_active, &dev_n_active, 8, cudaMemcpyHostToDevice, s));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	if (rc != TVG_OK) return rc;
+	ctx->group_tpl = n_tune > 0 ? sizes[best] : GW_DEFAULT_TPL;
+	TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
+	if (choice) *choice = ctx->group_tpl;
 	if (ms) for (int c = 0; c < 3; c++) ms[c] = t[c];
 	return tvg_sync_status(ctx, "autotune");
 }

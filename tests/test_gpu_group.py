@@ -119,3 +119,34 @@ def test_walk_limit_times_out_and_the_context_recovers():
         ctx.zero_accel()
         ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
         assert np.array_equal(ctx.download(G.F_GRAV_ACC)["grav_acc"], first)
+
+
+def test_autotune_on_a_sample_leaves_the_active_set_and_the_chosen_walk():
+    """tvg_autotune times the three group sizes on a sample (every 8th window
+    of 128 active particles), then walks the whole active set with the
+    fastest: the accelerations it leaves equal a later walk with the same
+    choice, for all particles and for an active list, whose length the
+    sample must not change."""
+    p = ics.zeldovich_box(n_side=32, seed=35)
+    parts = G.WALK_GRAVITY | G.WALK_EWALD
+    with G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box,
+                          softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.peano_keys()
+        ctx.sort_particles()
+        ctx.top_nodes()
+        ctx.tree_build()
+        ctx.ewald_init()
+        for active in (None, np.arange(0, p.n, 3, dtype=np.int32)):
+            ctx.set_active(active)
+            ctx.zero_accel()
+            choice, ms = ctx.autotune(use_bh=True, parts=parts)
+            assert choice in (1, 2, 4) and all(t > 0 for t in ms)
+            tuned = ctx.download(G.F_GRAV_ACC)["grav_acc"].copy()
+            ctx.zero_accel()
+            ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
+            again = ctx.download(G.F_GRAV_ACC)["grav_acc"]
+            assert np.array_equal(tuned, again)
+            sel = np.arange(p.n) if active is None else active
+            assert np.all(np.abs(again[:, sel]).sum(0) > 0)
