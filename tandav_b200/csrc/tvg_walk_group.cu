@@ -80,10 +80,11 @@
 #ifndef GW_EWALD_MINB
 #define GW_EWALD_MINB 1
 #endif
-// resident blocks per SM the gravity walk is compiled for, and the unroll of
-// its far-list loop (source pairs per iteration)
+// resident blocks per SM the gravity walk is compiled for (4: at most 128
+// registers; unbounded it took 138 and ran 3 blocks, 8 % slower), and the
+// unroll of its far-list loop (source pairs per iteration)
 #ifndef GW_WALK_MINB
-#define GW_WALK_MINB 1
+#define GW_WALK_MINB 4
 #endif
 #ifndef GW_FAR_UNROLL
 #define GW_FAR_UNROLL 2
@@ -312,13 +313,20 @@ struct EwaldSmem {
 	int2 bq[GW_BQ];
 };
 
-// Per-warp stage of the Ewald walk's Taylor records (table evaluation): a
-// full batch of 32 accepted sources has its 32 records (256 B each) copied
-// from the table in global memory into shared memory by the bulk-copy (TMA)
-// engine, cp.async.bulk completing on an mbarrier, while the warp goes on
-// walking; the batch is evaluated from shared memory when the next one is
-// issued. Two buffers: a new batch is issued before the pending one is
-// evaluated. Sources are this GPU's own memory; no multicast.
+// Per-warp stage of the Ewald walk's Taylor records (table evaluation),
+// compiled in with GW_EWALD_STAGE=1: a full batch of 32 accepted sources has
+// its 32 records (256 B each) copied from the table in global memory into
+// shared memory by the bulk-copy (TMA) engine, cp.async.bulk completing on an
+// mbarrier, while the warp goes on walking; the batch is evaluated from
+// shared memory when the next one is issued. Two buffers: a new batch is
+// issued before the pending one is evaluated. Sources are this GPU's own
+// memory; no multicast. The results are those of the direct loads bit for
+// bit, but the walk is slower (768 against 462 ms per 256^3 step): the
+// records of neighbouring groups are reused through L1, which bulk copies
+// bypass and the 92 KB stage per block shrinks. Off by default.
+#ifndef GW_EWALD_STAGE
+#define GW_EWALD_STAGE 0
+#endif
 struct EwaldStage {
 	float4 rec[2][32][16];     // the batches' records
 	float4 pend[2][32];        // the batches' sources
@@ -1304,8 +1312,10 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 		__syncthreads();
 	}
 	const int lane = threadIdx.x & 31;
-	// the table path stages its records (EwaldStage after the warps' areas)
-	EwaldStage *st = MLP ? nullptr
+	// with GW_EWALD_STAGE the table path stages its records (EwaldStage after
+	// the warps' areas)
+	EwaldStage *st = (MLP || !GW_EWALD_STAGE)
+	                     ? nullptr
 	                     : ((EwaldStage *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS)) + (threadIdx.x >> 5);
 	StageState ss = { 0u, 0, false, true };
 	if (st) {
@@ -1504,7 +1514,7 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	TVG_CHECK(device_slot(ctx));
 	int &nblk = nblk_dev[ctx->device];
 	const size_t smem = sizeof(EwaldSmem) * GW_WARPS
-	                  + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : sizeof(EwaldStage) * GW_WARPS);
+	                  + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : (GW_EWALD_STAGE ? sizeof(EwaldStage) * GW_WARPS : 0));
 	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
 	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,

@@ -89,10 +89,11 @@ def test_group_accuracy(kind):
 
 def test_walk_limit_times_out_and_the_context_recovers():
     """The group walks' traversal loops are bounded (tvg_set_walk_limit): with
-    a limit of a few iterations both the gravity and the Ewald walk stop,
-    tvg_walk returns TVG_E_TIMEOUT, and the context stays usable -- with the
-    limit restored the same walk gives the accelerations of a walk that never
-    timed out."""
+    a limit of two iterations the gravity and Ewald walks (which a periodic
+    group walk runs together) stop, tvg_walk returns TVG_E_TIMEOUT, and the
+    context stays usable -- with the limit restored the same walk gives the
+    accelerations of a walk that never timed out. An isolated context stops
+    its gravity walk the same way."""
     # 32^3: 512 particles per level-2 cell, so every top node has a subtree
     # and a group needs many node batches
     p = ics.zeldovich_box(n_side=32, seed=34)
@@ -109,16 +110,30 @@ def test_walk_limit_times_out_and_the_context_recovers():
         ctx.zero_accel()
         ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
         first = ctx.download(G.F_GRAV_ACC)["grav_acc"].copy()
-        for part in (G.WALK_GRAVITY, G.WALK_EWALD):
-            ctx.set_walk_limit(2)
-            ctx.zero_accel()
-            with pytest.raises(G.TvgError) as e:
-                ctx.walk(G.FORM_GROUP, use_bh=True, parts=part)
-            assert e.value.code == 4, e.value          # TVG_E_TIMEOUT
+        ctx.set_walk_limit(2)
+        ctx.zero_accel()
+        with pytest.raises(G.TvgError) as e:
+            ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
+        assert e.value.code == 4, e.value          # TVG_E_TIMEOUT
         ctx.set_walk_limit()
         ctx.zero_accel()
         ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
         assert np.array_equal(ctx.download(G.F_GRAV_ACC)["grav_acc"], first)
+    h = ics.hernquist(n=32768, seed=37)
+    c = np.median(h.pos, axis=1)
+    size = 2.001 * float(np.abs(h.pos - c[:, None]).max())
+    with G.GravityContext(h.n, float_bytes=4, softening=h.softening) as ctx:
+        ctx.upload(h.pos, h.mass)
+        ctx.set_domain(c - 0.5 * size, size)
+        ctx.peano_keys()
+        ctx.sort_particles()
+        ctx.top_nodes()
+        ctx.tree_build()
+        ctx.set_walk_limit(2)
+        ctx.zero_accel()
+        with pytest.raises(G.TvgError) as e:
+            ctx.walk(G.FORM_GROUP, use_bh=True, parts=G.WALK_GRAVITY)
+        assert e.value.code == 4, e.value
 
 
 def test_autotune_on_a_sample_leaves_the_active_set_and_the_chosen_walk():
