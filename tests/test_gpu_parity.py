@@ -182,6 +182,50 @@ def test_balanced_decomposition_matches_reference(golden_dir, case):
         assert np.array_equal(last.astype(np.float64), g["last_acc_mag"])
 
 
+def test_balanced_decomposition_vs_oracle_at_size():
+    """2^19 particles in clumps (FP32, periodic) balanced over 8 targets with
+    synthetic costs: ~5e4 interactions per particle in a slab of 12 % of the
+    box, 1-100 elsewhere, so the slab's cells are split down to level 7 (1177
+    top nodes). The bunch costs reach 10^9, far above 2^24, so the float
+    partial sums of the thread shares round, in the same order on both
+    sides. Top nodes, tree and Tree_Parent equal the oracle's
+    (oracle/decomposition.py and the restated build)."""
+    p = ics.random_box(1 << 19, box=1000.0, seed=45, clumps=11)
+    h = np.arange(p.n, dtype=np.uint64) * 2654435761
+    cost = np.where(p.pos[0] < 120.0, 50000 - (h % 1000), h % 100 + 1).astype(np.float64)
+    ew = oracle_ewald_tables(4, p.box)
+    o = oracle_pipeline(p.pos, p.mass, np.zeros(3), p.box, 4, box=p.box, softening=p.softening,
+                        passes=("bh",), ntask=8, cost=cost, ewald=ew)
+    assert len(o["top"]) > 1000
+    parts = G.WALK_GRAVITY | G.WALK_EWALD
+    with make_ctx(p.n, 4, box=p.box, softening=p.softening) as ctx:
+        ctx.set_domain_decomposition(8)
+        ctx.upload(p.pos, p.mass, cost=cost)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.peano_keys()
+        perm = ctx.sort_particles()
+        ctx.top_nodes()
+        ctx.tree_build(exact_moments=True)
+        tree, top = ctx.download_tree()
+        assert np.array_equal(perm, o["perm"])
+        assert_struct_equal(top, o["top"], TOP_FIELDS, "topnodes")
+        assert_struct_equal(tree, o["tree"], TREE_FIELDS, "tree")
+        assert np.array_equal(ctx.download(G.F_TREE_PARENT)["tree_parent"], o["tree_parent"])
+        # the plain walk over 1177 top nodes (read through L1, not staged)
+        ctx.upload_ewald_table(*reference_table(4))
+        ctx.zero_accel()
+        ctx.walk(G.FORM_PLAIN, use_bh=True, parts=parts)
+        got = ctx.download(G.F_GRAV_ACC | G.F_COST)
+        assert np.array_equal(got["cost"], o["bh_cost"])
+        assert np.array_equal(got["grav_acc"].astype(np.float64), o["bh_gacc"].astype(np.float64))
+        # the group walks push their roots in chunks of 256
+        ctx.ewald_init()
+        ctx.zero_accel()
+        ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
+        ga = ctx.download(G.F_GRAV_ACC)["grav_acc"].astype(np.float64)
+        assert np.all(np.isfinite(ga)) and np.all(np.abs(ga).sum(0) > 0)
+
+
 RANDOM_CASES = [
     ("hernquist", 8, 32768),
     ("hernquist", 4, 65536),
