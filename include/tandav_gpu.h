@@ -464,7 +464,8 @@ int tvg_step_graph_reset(tvg_context *ctx);
  * the active particles in every 8th window of 128 particles -- and keeps the
  * fastest for the later walks of this context. choice receives 1, 2 or 4,
  * ms[3] the three sample times. The chosen walk then runs over the whole
- * active set: the accelerations left are its result. */
+ * active set: Acc, Grav_Acc and Cost are left as that one walk leaves them
+ * (Acc as it was plus the walk's contribution). */
 int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
                  int32_t *choice, double *ms);
 

@@ -499,6 +499,21 @@ __device__ __forceinline__ int pop_nodes(const int32_t *stack, int &sp, int *sta
 	return node;
 }
 
+// GW_PREFETCH: the lanes that open an internal node also prefetch its
+// children's records (contiguous, nchild x 48 B) into L1; the next batch
+// pops them from the top of the stack
+#ifndef GW_PREFETCH
+#define GW_PREFETCH 0
+#endif
+
+__device__ __forceinline__ void prefetch_children(const tvg_wnode *wt, bool open_int, int nchild, int child)
+{
+	if (!GW_PREFETCH || !open_int) return;
+	const char *a = (const char *) (wt + child), *e = (const char *) (wt + child + nchild);
+	for (const char *q = (const char *) ((uintptr_t) a & ~(uintptr_t) 127); q < e; q += 128)
+		asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+}
+
 // pushes the children of the lanes' opened internal nodes
 __device__ __forceinline__ void push_children(int32_t *stack, int &sp, bool open_int, int nchild,
                                               int child)
@@ -701,6 +716,7 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 			if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
 			nl += __popc(bm);
 			nw += __popc(bw);
+			prefetch_children(wt, open_int, nchild, child);
 			push_children(S.stack, sp, open_int, nchild, child);
 			// opened bundles -> bundle queue
 			const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
@@ -1718,6 +1734,12 @@ extern "C" int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, in
 	ctx->n_active = n_tune;
 	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->dc->n_active, &n_tune, 8, cudaMemcpyHostToDevice, s));
 	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	// the walks add to Acc: keep it (in the sort's free second buffers) so
+	// that only the final walk's contribution remains
+	const size_t acc_bytes = tvg_fsize(ctx) * (size_t) ctx->n;
+	for (int k = 0; k < 3; k++)
+		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->falt[FS_ACC0 + k], ctx->f[FS_ACC0 + k], acc_bytes,
+		                              cudaMemcpyDeviceToDevice, s));
 	const int sizes[3] = { 1, 2, 4 };
 	double t[3] = { 0, 0, 0 };
 	int best = 0, rc = TVG_OK;
@@ -1732,6 +1754,9 @@ extern "C" int tvg_autotune(tvg_context *ctx, int32_t use_bh, uint32_t parts, in
 	ctx->use_active = was_active;
 	ctx->n_active = saved_n;
 	TVG_CUDA(ctx, cudaMemcpyAsync(&ctx->dc->n_active, &dev_n_active, 8, cudaMemcpyHostToDevice, s));
+	for (int k = 0; k < 3; k++)
+		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->f[FS_ACC0 + k], ctx->falt[FS_ACC0 + k], acc_bytes,
+		                              cudaMemcpyDeviceToDevice, s));
 	TVG_CUDA(ctx, cudaStreamSynchronize(s));
 	if (rc != TVG_OK) return rc;
 	ctx->group_tpl = n_tune > 0 ? sizes[best] : GW_DEFAULT_TPL;

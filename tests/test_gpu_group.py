@@ -158,10 +158,13 @@ def test_autotune_on_a_sample_leaves_the_active_set_and_the_chosen_walk():
             ctx.zero_accel()
             choice, ms = ctx.autotune(use_bh=True, parts=parts)
             assert choice in (1, 2, 4) and all(t > 0 for t in ms)
-            tuned = ctx.download(G.F_GRAV_ACC)["grav_acc"].copy()
+            tuned = ctx.download(G.F_GRAV_ACC | G.F_ACC)
             ctx.zero_accel()
             ctx.walk(G.FORM_GROUP, use_bh=True, parts=parts)
-            again = ctx.download(G.F_GRAV_ACC)["grav_acc"]
-            assert np.array_equal(tuned, again)
+            again = ctx.download(G.F_GRAV_ACC | G.F_ACC)
+            assert np.array_equal(tuned["grav_acc"], again["grav_acc"])
+            # Acc holds one walk's contribution, not the trial walks' too
+            assert np.array_equal(tuned["acc"], again["acc"])
+            again = again["grav_acc"]
             sel = np.arange(p.n) if active is None else active
             assert np.all(np.abs(again[:, sel]).sum(0) > 0)
