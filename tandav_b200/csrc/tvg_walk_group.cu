@@ -499,21 +499,6 @@ __device__ __forceinline__ int pop_nodes(const int32_t *stack, int &sp, int *sta
 	return node;
 }
 
-// GW_PREFETCH: the lanes that open an internal node also prefetch its
-// children's records (contiguous, nchild x 48 B) into L1; the next batch
-// pops them from the top of the stack
-#ifndef GW_PREFETCH
-#define GW_PREFETCH 0
-#endif
-
-__device__ __forceinline__ void prefetch_children(const tvg_wnode *wt, bool open_int, int nchild, int child)
-{
-	if (!GW_PREFETCH || !open_int) return;
-	const char *a = (const char *) (wt + child), *e = (const char *) (wt + child + nchild);
-	for (const char *q = (const char *) ((uintptr_t) a & ~(uintptr_t) 127); q < e; q += 128)
-		asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
-}
-
 // pushes the children of the lanes' opened internal nodes
 __device__ __forceinline__ void push_children(int32_t *stack, int &sp, bool open_int, int nchild,
                                               int child)
@@ -716,7 +701,6 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 			if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
 			nl += __popc(bm);
 			nw += __popc(bw);
-			prefetch_children(wt, open_int, nchild, child);
 			push_children(S.stack, sp, open_int, nchild, child);
 			// opened bundles -> bundle queue
 			const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
