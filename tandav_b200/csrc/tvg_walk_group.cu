@@ -62,6 +62,11 @@
 #define GW_WARPS 4
 #endif
 #define GW_THREADS (GW_WARPS * 32)
+// warps per block of the Ewald walk (its registers allow 9 warps per SM)
+#ifndef GE_WARPS
+#define GE_WARPS 4
+#endif
+#define GE_THREADS (GE_WARPS * 32)
 #define GW_STACK 1024
 #define GW_RESERVE (7 * (TVG_MAX_LEVEL - 2) + 8)
 #ifndef GW_LIST
@@ -1291,7 +1296,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 }
 
 template <int TPL, bool MLP, typename F>
-__global__ void __launch_bounds__(GW_THREADS, GW_EWALD_MINB)
+__global__ void __launch_bounds__(GE_THREADS, GW_EWALD_MINB)
 k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
               const tvg_wnode *__restrict__ wt,
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
@@ -1305,7 +1310,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 	EwaldSmem &S = ((EwaldSmem *) smem_raw)[threadIdx.x >> 5];
 	// the learned correction's parameters, once per block: the network BF16 ->
 	// FP32, the fitted cubic and scale FP32, and W2 as BF16 pairs for the MMAs
-	float *mlp = (float *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS);
+	float *mlp = (float *) (smem_raw + sizeof(EwaldSmem) * GE_WARPS);
 	uint32_t *w2b = (uint32_t *) (mlp + MLP_NPARAM);
 	if (MLP) {
 		mlp_load_shared(mlp_w, mlp_f32, mlp, w2b);
@@ -1316,7 +1321,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 	// the warps' areas)
 	EwaldStage *st = (MLP || !GW_EWALD_STAGE)
 	                     ? nullptr
-	                     : ((EwaldStage *) (smem_raw + sizeof(EwaldSmem) * GW_WARPS)) + (threadIdx.x >> 5);
+	                     : ((EwaldStage *) (smem_raw + sizeof(EwaldSmem) * GE_WARPS)) + (threadIdx.x >> 5);
 	StageState ss = { 0u, 0, false, true };
 	if (st) {
 		if (lane == 0) {
@@ -1475,12 +1480,12 @@ static int device_slot(tvg_context *ctx)
 }
 
 template <typename K>
-static int blocks_for(tvg_context *ctx, K kernel, size_t smem, int *cache)
+static int blocks_for(tvg_context *ctx, K kernel, size_t smem, int *cache, int threads = GW_THREADS)
 {
 	if (!*cache) {
 		TVG_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
 		int per_sm = 0, nsm = 0;
-		TVG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, GW_THREADS, smem));
+		TVG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
 		TVG_CUDA(ctx, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
 		*cache = (per_sm > 0 ? per_sm : 1) * nsm;
 	}
@@ -1513,10 +1518,10 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	static int nblk_dev[TVG_MAX_DEVICES] = { 0 };
 	TVG_CHECK(device_slot(ctx));
 	int &nblk = nblk_dev[ctx->device];
-	const size_t smem = sizeof(EwaldSmem) * GW_WARPS
-	                  + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : (GW_EWALD_STAGE ? sizeof(EwaldStage) * GW_WARPS : 0));
-	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk));
-	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
+	const size_t smem = sizeof(EwaldSmem) * GE_WARPS
+	                  + (MLP ? 4 * MLP_NPARAM + 2 * MLP_H * MLP_H : (GW_EWALD_STAGE ? sizeof(EwaldStage) * GE_WARPS : 0));
+	TVG_CHECK(blocks_for(ctx, k_ewald_group<TPL, MLP, F>, smem, &nblk, GE_THREADS));
+	k_ewald_group<TPL, MLP, F><<<TVG_CNT(ctx, nblk), GE_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
 	    ctx->wtree, ctx->ipos[0], ctx->ipos[1],
 	    ctx->ipos[2], mass_f, last_f, (const float4 *) ctx->ewald_ext,
