@@ -52,6 +52,10 @@ UNIT = "particles/s"
 # 8-corner trilinear interpolations
 FLOP_PER_GRAV = 20.0
 FLOP_PER_EWALD = 60.0
+# node quadrupole (group form, --quadrupole): 3 sub, 5 for r^2, rsqrt, 4 for
+# r^-3, r^-5, r^-7, mass, 15 for Q d, 5 for d.Q d, 3 for the radial factor,
+# 12 for the accumulation, 2 for the criterion
+FLOP_PER_QUAD = 51.0
 
 
 def parse():
@@ -76,6 +80,9 @@ def parse():
     ap.add_argument("--open-rel", type=float, default=7e-5,
                     help="TREE_OPEN_PARAM_REL of the group form (the loosest of a sweep that keeps "
                          "the 256^3 box below 1e-3 rms: 9.7e-4)")
+    ap.add_argument("--quadrupole", action="store_true",
+                    help="group form with node quadrupoles and the octupole-order criterion "
+                         "(TVG_CFG_QUADRUPOLE)")
     ap.add_argument("--ewald-alpha", type=float, default=4e-4,
                     help="opening of the group form's Ewald walk (relative to |a_old|)")
     ap.add_argument("--plain-open-rel", type=float, default=0.005,
@@ -385,7 +392,7 @@ def main():
     p = make_ics(args.nside, 1234 + rank, args.box_mpc)
     n = p.n
     ctx = G.GravityContext(n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
-                           device=local)
+                           device=local, flags=G.CFG_QUADRUPOLE if args.quadrupole else 0)
     parts = G.WALK_GRAVITY | G.WALK_EWALD
     ctx.upload(p.pos, p.mass)
     ctx.set_domain((0.0, 0.0, 0.0), p.box)
@@ -413,7 +420,7 @@ def main():
     clocks.start()
     l0 = ctx.launch_count()
     ctx.timer_start()
-    walk_ms, ew_ms, grav_i, ew_i, phases = 0.0, 0.0, 0.0, 0.0, []
+    walk_ms, ew_ms, grav_i, ew_i, quad_i, phases = 0.0, 0.0, 0.0, 0.0, 0.0, []
     for _ in range(args.steps):
         ctx.step_graph(parts)                  # the whole step: one CUDA graph launch
         ph = ctx.phase_times()
@@ -423,6 +430,7 @@ def main():
         g, e = ctx.walk_counters()
         grav_i += g
         ew_i += e
+        quad_i += ctx.walk_quad_interactions()
     total_ms = ctx.timer_stop()
     launches = ctx.launch_count() - l0
     clk = clocks.stop()
@@ -479,14 +487,18 @@ def main():
     d2h = n * 4 * 4        # grav_acc[3], id (the order of the result)
 
     # ---- roofline of the dominant kernel (the gravity walk)
-    achieved = FLOP_PER_GRAV * grav_i / (walk_ms * 1e-3) / 1e12
+    walk_flop = FLOP_PER_GRAV * (grav_i - quad_i) + FLOP_PER_QUAD * quad_i
+    achieved = walk_flop / (walk_ms * 1e-3) / 1e12
     roofline = {
-        "kernel": "k_walk_group<GM_CENTRE, 2, float> (gravity walk)", "bound": "fp32",
+        "kernel": ("k_walk_group<GM_CENTRE, 2, float, quadrupole> (gravity walk)" if args.quadrupole
+                   else "k_walk_group<GM_CENTRE, 2, float> (gravity walk)"), "bound": "fp32",
         "achieved": round(achieved, 3), "peak": round(fp32_peak, 3), "unit": "TFLOP/s",
         "frac": round(achieved / fp32_peak, 4) if fp32_peak > 0 else None,
         "peak_source": "measured FFMA loop on this GPU (1.5 s, sustained under the power cap)",
         "traffic": None,
-        "algorithmic": f"{FLOP_PER_GRAV:.0f} flop x {grav_i / args.steps / n:.0f} interactions/particle",
+        "algorithmic": (f"{FLOP_PER_GRAV:.0f} flop x {(grav_i - quad_i) / args.steps / n:.0f} monopole"
+                        f" + {FLOP_PER_QUAD:.0f} flop x {quad_i / args.steps / n:.0f} quadrupole"
+                        " interactions/particle"),
     }
     prof = ROOT / "profiles" / "walk_group_traffic.json"
     if prof.exists():
@@ -673,6 +685,7 @@ def main():
             "clocks": clk,
             "phases_ms": ph,
             "interactions_per_particle": {"gravity": round(grav_i / args.steps / n, 1),
+                                          "of_which_quadrupole": round(quad_i / args.steps / n, 1),
                                           "ewald_evaluations": round(ew_i / args.steps / n, 1)},
             "ewald_walk": {"kernel": f"k_ewald_group<{tune_choice}, false, float>",
                            "ms_per_step": round(ew_ms / args.steps, 2),

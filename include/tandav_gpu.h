@@ -79,7 +79,15 @@ enum {
 	 * (tvg_find_domain), as Domain_Decomposition does (domain.c:67-71);
 	 * tvg_step_graph then runs such steps directly. Without it the domain is
 	 * the one last set (tvg_set_domain / tvg_find_domain). */
-	TVG_CFG_FIND_DOMAIN = 8
+	TVG_CFG_FIND_DOMAIN = 8,
+	/* Group form (no reference counterpart; the reference's walks use node
+	 * monopoles): every accepted node also carries its traceless quadrupole
+	 * moment about its centre of mass, summed from its particles in FP64 for
+	 * each walk tree, and the relative criterion bounds the next (octupole)
+	 * term instead: a node of mass M and size s at distance r from the group
+	 * box is accepted when M s^3 <= r^5 |a_old|_min TREE_OPEN_PARAM_REL / G.
+	 * The plain form is unaffected. */
+	TVG_CFG_QUADRUPOLE = 16
 };
 
 /* Host view of struct Particle_Data (src/Gravity/../particles.h:17-37). Any
@@ -315,6 +323,9 @@ int tvg_sort_keys_noalloc(const uint64_t *key_hi, const uint64_t *key_lo, int64_
 
 /* Counters of the last walk: total gravity and Ewald interactions. */
 int tvg_walk_counters(tvg_context *ctx, double *grav_interactions, double *ewald_interactions);
+/* Of the last group walk's gravity interactions, those with a node's
+ * quadrupole (TVG_CFG_QUADRUPOLE; 0 otherwise). No reference counterpart. */
+int tvg_walk_quad_interactions(tvg_context *ctx, double *quad_interactions);
 
 /* Largest n_targets accepted by tvg_forcetest. */
 #define TVG_FORCETEST_MAX_TARGETS (1 << 20)

@@ -181,7 +181,7 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
 	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
 	                 ctx->d_toptab, ctx->top_of, ctx->dd_scratch, ctx->tu_first, ctx->tu_dp,
-	                 ctx->tune_active };
+	                 ctx->tune_active, ctx->wquad, ctx->wrange };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -444,6 +444,13 @@ extern "C" int tvg_walk_counters(tvg_context *ctx, double *g, double *e)
 	if (!ctx) return TVG_E_BADINPUT;
 	if (g) *g = ctx->last_counts[0];
 	if (e) *e = ctx->last_counts[1];
+	return TVG_OK;
+}
+
+extern "C" int tvg_walk_quad_interactions(tvg_context *ctx, double *q)
+{
+	if (!ctx || !q) return TVG_E_BADINPUT;
+	*q = ctx->last_counts[2];
 	return TVG_OK;
 }
 

@@ -84,6 +84,7 @@ struct tvg_devcount {
 	int32_t ntop;            // top nodes
 	int32_t max_active_bin;  // bins <= this are active
 	int32_t sort_skip[8];    // radix digit d is the same for all keys
+	int64_t nwchild;         // walk nodes below the top nodes (TVG_CFG_QUADRUPOLE)
 };
 
 // Per top node tables of the tree build, on the device (TVG_MAX_TOP
@@ -187,6 +188,8 @@ struct tvg_context {
 	// group walk data
 	uint32_t *ipos[3] = { nullptr, nullptr, nullptr };
 	tvg_wnode *wtree = nullptr;
+	float4 *wquad = nullptr;           // TVG_CFG_QUADRUPOLE: G Q of every walk node, 2 float4
+	int32_t *wrange = nullptr;         // first particle and count of every walk node (2 int32)
 	int64_t nw = 0;
 	int32_t *group_first = nullptr;
 	int64_t ngroups = 0;
@@ -238,7 +241,7 @@ struct tvg_context {
 	// timings
 	cudaEvent_t ev[16];
 	double phase_ms[8] = { 0 };
-	double last_counts[2] = { 0, 0 };
+	double last_counts[3] = { 0, 0, 0 };   // gravity, Ewald, of the gravity ones quadrupole
 };
 
 

@@ -179,7 +179,7 @@ __device__ __forceinline__ void wt_emit_one(int64_t g, int ntop, const GNode<F> 
                                             const int32_t *__restrict__ nch,
                                             const int32_t *__restrict__ choff, double ox, double oy,
                                             double oz, double fac, double dsize,
-                                            tvg_wnode *__restrict__ wt)
+                                            tvg_wnode *__restrict__ wt, int2 *__restrict__ wrange)
 {
 	const GNode<F> &nd = tree[g];
 	if (!is_local(nd.Bitfield)) return;
@@ -217,19 +217,27 @@ __device__ __forceinline__ void wt_emit_one(int64_t g, int ntop, const GNode<F> 
 		r.nchild = -nd.Npart;
 	}
 	wt[w] = r;
+	if (wrange) {
+		// particles of the node: Npart from its first particle, the first of
+		// the first bundle or leaf below it (pre-order: a first child follows
+		// its parent)
+		int64_t f = g;
+		while (tree[f].DNext > 0) f++;
+		wrange[w] = make_int2(-tree[f].DNext - 1, nd.Npart);
+	}
 }
 
 template <typename F>
 __global__ void k_wt_emit(const tvg_devcount *__restrict__ dc, int64_t tcap,
                           const GNode<F> *__restrict__ tree, const int32_t *__restrict__ nch,
                           const int32_t *__restrict__ choff, double ox, double oy, double oz, double fac,
-                          double dsize, tvg_wnode *__restrict__ wt)
+                          double dsize, tvg_wnode *__restrict__ wt, int2 *__restrict__ wrange)
 {
 	const int64_t nn = min(dc->nnodes, tcap);
 	const int ntop = dc->ntop;
 	for (int64_t g = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; g < nn;
 	     g += (int64_t) gridDim.x * blockDim.x)
-		wt_emit_one<F>(g, ntop, tree, nch, choff, ox, oy, oz, fac, dsize, wt);
+		wt_emit_one<F>(g, ntop, tree, nch, choff, ox, oy, oz, fac, dsize, wt, wrange);
 }
 
 // top nodes without subtree: one bundle record each (their First_Part; the
@@ -237,7 +245,7 @@ __global__ void k_wt_emit(const tvg_devcount *__restrict__ dc, int64_t tcap,
 // quirk Q3, which the group form does not repeat)
 __global__ void k_wt_small_top(const tvg_devcount *__restrict__ dc, const tvg_topnode *__restrict__ top,
                                int vsize, double ox, double oy, double oz, double fac, double dsize,
-                               tvg_wnode *__restrict__ wt)
+                               tvg_wnode *__restrict__ wt, int2 *__restrict__ wrange)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= dc->ntop || top[t].npart > vsize) return;
@@ -255,6 +263,64 @@ __global__ void k_wt_small_top(const tvg_devcount *__restrict__ dc, const tvg_to
 	r.child = top[t].first_part;
 	r.nchild = -top[t].npart;
 	wt[t] = r;
+	if (wrange) wrange[t] = make_int2(top[t].first_part, top[t].npart);
+}
+
+// TVG_CFG_QUADRUPOLE: G times the traceless quadrupole moment of every walk
+// node about its centre of mass (the integer one of its record),
+// Q_ab = sum m (3 y_a y_b - |y|^2 delta_ab), summed in FP64 over the node's
+// particles, one warp per node, stored negated: wq[2w] = -(Qxx, Qyy, Qzz,
+// Qxy), wq[2w + 1] = -(Qxz, Qyz, 0, 0).
+__device__ __forceinline__ void wt_quad_one(int64_t w, int lane, const tvg_wnode *__restrict__ wt,
+                                            const int2 *__restrict__ wrange, const uint32_t *__restrict__ ix,
+                                            const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
+                                            const float *__restrict__ mass_f, double scale, double gravity,
+                                            float4 *__restrict__ wq)
+{
+	const int2 r = wrange[w];
+	if (r.y <= 0) return;
+	const uint32_t cx = wt[w].cx, cy = wt[w].cy, cz = wt[w].cz;
+	double sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+	for (int64_t j = r.x + lane; j < (int64_t) r.x + r.y; j += 32) {
+		const double m = (double) mass_f[j];
+		const double x = (double) (int) (ix[j] - cx) * scale, y = (double) (int) (iy[j] - cy) * scale,
+		             z = (double) (int) (iz[j] - cz) * scale;
+		sxx += m * x * x;
+		syy += m * y * y;
+		szz += m * z * z;
+		sxy += m * x * y;
+		sxz += m * x * z;
+		syz += m * y * z;
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+		sxx += __shfl_xor_sync(0xFFFFFFFFu, sxx, o);
+		syy += __shfl_xor_sync(0xFFFFFFFFu, syy, o);
+		szz += __shfl_xor_sync(0xFFFFFFFFu, szz, o);
+		sxy += __shfl_xor_sync(0xFFFFFFFFu, sxy, o);
+		sxz += __shfl_xor_sync(0xFFFFFFFFu, sxz, o);
+		syz += __shfl_xor_sync(0xFFFFFFFFu, syz, o);
+	}
+	if (lane == 0) {
+		const double tr = sxx + syy + szz, g = -gravity;
+		wq[2 * w] = make_float4((float) (g * (3 * sxx - tr)), (float) (g * (3 * syy - tr)),
+		                        (float) (g * (3 * szz - tr)), (float) (g * 3 * sxy));
+		wq[2 * w + 1] = make_float4((float) (g * 3 * sxz), (float) (g * 3 * syz), 0.f, 0.f);
+	}
+}
+
+// every walk node (top nodes + the walk nodes below them, counted on the device)
+__global__ void k_wt_quad_dev(const tvg_devcount *__restrict__ dc, const tvg_wnode *__restrict__ wt,
+                              const int2 *__restrict__ wrange, const uint32_t *__restrict__ ix,
+                              const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
+                              const float *__restrict__ mass_f, double scale, double gravity,
+                              float4 *__restrict__ wq)
+{
+	const int64_t nw = (int64_t) dc->ntop + dc->nwchild;
+	const int lane = threadIdx.x & 31;
+	for (int64_t w = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5; w < nw;
+	     w += ((int64_t) gridDim.x * blockDim.x) >> 5)
+		wt_quad_one(w, lane, wt, wrange, ix, iy, iz, mass_f, scale, gravity, wq);
 }
 
 
@@ -274,6 +340,7 @@ struct GroupParams {
 	int use_bh;
 	int open_bundles;   // TVG_CFG_OPEN_BUNDLES
 	int max_iter;       // iteration limit of a group's traversal (tvg_set_walk_limit)
+	int quad;           // TVG_CFG_QUADRUPOLE: node quadrupoles, octupole-order criterion
 	float scale;        // length per integer unit
 	float box, half_box;
 	float theta2;       // TREE_OPEN_PARAM_BH
@@ -311,6 +378,7 @@ __device__ __forceinline__ void far_put(WarpSmem &S, int i, float4 e)
 	b[o] = e.z;
 	b[2 + o] = e.w;
 }
+
 
 struct EwaldSmem {
 	int32_t stack[GW_STACK];
@@ -387,6 +455,7 @@ struct Target {
 	float tx, ty, tz;       // offset from the group centre
 	double ax, ay, az;      // FP32 sums of each list flush, carried in FP64
 	float cost;
+	float qcost;            // of which quadrupole interactions (TVG_CFG_QUADRUPOLE)
 	bool valid;
 };
 
@@ -444,6 +513,7 @@ __device__ __forceinline__ void group_setup(const GroupParams &p, const uint32_t
 		t[k].tz = __fmul_rn((float) (int) (pz[k] - g.cz), p.scale);
 		t[k].ax = t[k].ay = t[k].az = 0.0;
 		t[k].cost = 0.f;
+		t[k].qcost = 0.f;
 	}
 	// group-wide relative criterion: the smallest |a_old| opens the most
 #pragma unroll
@@ -470,6 +540,7 @@ __device__ __forceinline__ bool gravity_opens(const GroupParams &p, const GroupB
 	r2 = qx * qx + qy * qy + qz * qz;
 	bool want;
 	if (p.use_bh) want = nd.size2 > r2 * p.theta2;
+	else if (p.quad) want = nd.mass * nd.size2 * nd.size > r2 * r2 * sqrtf(r2) * g.fac;
 	else want = nd.mass * nd.size2 > r2 * r2 * g.fac;
 	const float lim = 0.6f * nd.size;
 	if (fabsf(gx) < lim + g.hx && fabsf(gy) < lim + g.hy && fabsf(gz) < lim + g.hz) want = true;
@@ -586,6 +657,96 @@ __device__ __forceinline__ void flush_far(WarpSmem &S, int nl, Target (&t)[TPL])
 	__syncwarp();
 }
 
+// TVG_CFG_QUADRUPOLE: the accepted nodes with their quadrupoles (-G Q), in
+// pairs like the far list; in shared memory after the warps' WarpSmem
+#define GW_QLIST 64
+struct QuadList {
+	float4 xy[GW_QLIST / 2];   // x0 x1 y0 y1
+	float4 zw[GW_QLIST / 2];   // z0 z1 w0 w1 (w = G m)
+	float4 qa[GW_QLIST / 2];   // Qxx0 Qxx1 Qyy0 Qyy1
+	float4 qb[GW_QLIST / 2];   // Qzz0 Qzz1 Qxy0 Qxy1
+	float4 qc[GW_QLIST / 2];   // Qxz0 Qxz1 Qyz0 Qyz1
+};
+
+__device__ __forceinline__ void quad_put(QuadList &Q, int i, float4 e, float4 q0, float4 q1)
+{
+	const int h = i >> 1, o = i & 1;
+	float *a = (float *) &Q.xy[h], *b = (float *) &Q.zw[h], *c = (float *) &Q.qa[h],
+	      *d = (float *) &Q.qb[h], *f = (float *) &Q.qc[h];
+	a[o] = e.x;
+	a[2 + o] = e.y;
+	b[o] = e.z;
+	b[2 + o] = e.w;
+	c[o] = q0.x;
+	c[2 + o] = q0.y;
+	d[o] = q0.z;
+	d[2 + o] = q0.w;
+	f[o] = q1.x;
+	f[2 + o] = q1.y;
+}
+
+// Quadrupole flush: with d = source - target, r = |d| and the stored -G Q,
+// a = G M d / r^3 + (-G Q) d / r^5 - 5/2 (d . (-G Q) d) d / r^7, two sources
+// per packed step (31 f32x2 operations and two MUFU.RSQ per two
+// interactions). An odd count is padded with a massless source far away.
+template <int TPL>
+__device__ __forceinline__ void flush_quad(QuadList &Q, int nq, Target (&t)[TPL])
+{
+	if (nq & 1) {
+		if ((threadIdx.x & 31) == 0)
+			quad_put(Q, nq, make_float4(1.0e15f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f),
+			         make_float4(0.f, 0.f, 0.f, 0.f));
+		__syncwarp();
+	}
+	const int np = (nq + 1) >> 1;
+	const float2 m25 = make_float2(-2.5f, -2.5f);
+	float2 ax[TPL], ay[TPL], az[TPL], mx[TPL], my[TPL], mz[TPL];
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		ax[k] = ay[k] = az[k] = make_float2(0.f, 0.f);
+		mx[k] = make_float2(-t[k].tx, -t[k].tx);
+		my[k] = make_float2(-t[k].ty, -t[k].ty);
+		mz[k] = make_float2(-t[k].tz, -t[k].tz);
+	}
+#pragma unroll 1
+	for (int q = 0; q < np; q++) {
+		const float4 a = Q.xy[q], b = Q.zw[q], qa = Q.qa[q], qb = Q.qb[q], qc = Q.qc[q];
+		const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w),
+		             sz = make_float2(b.x, b.y), sw = make_float2(b.z, b.w);
+		const float2 qxx = make_float2(qa.x, qa.y), qyy = make_float2(qa.z, qa.w),
+		             qzz = make_float2(qb.x, qb.y), qxy = make_float2(qb.z, qb.w),
+		             qxz = make_float2(qc.x, qc.y), qyz = make_float2(qc.z, qc.w);
+#pragma unroll
+		for (int k = 0; k < TPL; k++) {
+			const float2 dx = __fadd2_rn(sx, mx[k]), dy = __fadd2_rn(sy, my[k]),
+			             dz = __fadd2_rn(sz, mz[k]);
+			const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+			const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+			const float2 ri2 = __fmul2_rn(ri, ri), ri3 = __fmul2_rn(ri2, ri);
+			const float2 fm = __fmul2_rn(sw, ri3);
+			const float2 qdx = __ffma2_rn(qxx, dx, __ffma2_rn(qxy, dy, __fmul2_rn(qxz, dz)));
+			const float2 qdy = __ffma2_rn(qxy, dx, __ffma2_rn(qyy, dy, __fmul2_rn(qyz, dz)));
+			const float2 qdz = __ffma2_rn(qxz, dx, __ffma2_rn(qyz, dy, __fmul2_rn(qzz, dz)));
+			const float2 dqd = __ffma2_rn(dx, qdx, __ffma2_rn(dy, qdy, __fmul2_rn(dz, qdz)));
+			const float2 ri5 = __fmul2_rn(ri3, ri2), ri7 = __fmul2_rn(ri5, ri2);
+			const float2 cd = __ffma2_rn(__fmul2_rn(dqd, ri7), m25, fm);
+			ax[k] = __ffma2_rn(cd, dx, __ffma2_rn(qdx, ri5, ax[k]));
+			ay[k] = __ffma2_rn(cd, dy, __ffma2_rn(qdy, ri5, ay[k]));
+			az[k] = __ffma2_rn(cd, dz, __ffma2_rn(qdz, ri5, az[k]));
+		}
+	}
+#pragma unroll
+	for (int k = 0; k < TPL; k++) {
+		t[k].ax += (double) ax[k].x + (double) ax[k].y;
+		t[k].ay += (double) ay[k].x + (double) ay[k].y;
+		t[k].az += (double) az[k].x + (double) az[k].y;
+		t[k].cost += (float) nq;
+		t[k].qcost += (float) nq;
+	}
+	__syncwarp();
+}
+
+
 __device__ __forceinline__ float wrap_half(float d, float box, float half)
 {
 	d = d > half ? d - box : d;
@@ -626,12 +787,13 @@ __device__ __forceinline__ void flush_slow(const GroupParams &p, const float4 *l
 
 // gravity walk of one group: 32 * TPL PH-contiguous active particles, lane l
 // holds the particles first + l + 32 k
-template <int MODE, int TPL>
+template <int MODE, int TPL, bool QUAD>
 __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *__restrict__ wt,
                            const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
                            const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
                            const float *__restrict__ last_acc, int64_t first, int cnt,
-                           const int32_t *__restrict__ active, Target (&t)[TPL], int *status)
+                           const int32_t *__restrict__ active, Target (&t)[TPL], QuadList *QL,
+                           const float4 *__restrict__ wq, int *status)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned lt = (1u << lane) - 1u;
@@ -645,7 +807,7 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	const float wlimx = p.half_box - 2.f * g.hx, wlimy = p.half_box - 2.f * g.hy,
 	            wlimz = p.half_box - 2.f * g.hz;
 
-	int sp = 0, nl = 0, nw = 0;
+	int sp = 0, nl = 0, nw = 0, nq = 0;
 	const int ntop = p.dc->ntop;
 	int guard = 0;
 	bool halt = false;
@@ -692,7 +854,15 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 			if (wrap) entry.w = -entry.w;
 			const unsigned bm = __ballot_sync(0xFFFFFFFFu, to_far);
 			const unsigned bw = __ballot_sync(0xFFFFFFFFu, to_slow);
-			if (nl + __popc(bm) > GW_LIST) {
+			// (with quadrupoles the accepted nodes go to the quadrupole list;
+			// the far list then holds the particles of opened bundles)
+			if (QUAD) {
+				if (nq + __popc(bm) > GW_QLIST) {
+					flush_quad<TPL>(*QL, nq, t);
+					nq = 0;
+					__syncwarp();
+				}
+			} else if (nl + __popc(bm) > GW_LIST) {
 				flush_far<TPL>(S, nl, t);
 				nl = 0;
 				__syncwarp();
@@ -702,9 +872,13 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 				nw = 0;
 				__syncwarp();
 			}
-			if (to_far) far_put(S, nl + __popc(bm & lt), entry);
+			if (to_far) {
+				if (QUAD) quad_put(*QL, nq + __popc(bm & lt), entry, wq[2 * node], wq[2 * node + 1]);
+				else far_put(S, nl + __popc(bm & lt), entry);
+			}
 			if (to_slow) S.wlist[nw + __popc(bw & lt)] = entry;
-			nl += __popc(bm);
+			if (QUAD) nq += __popc(bm);
+			else nl += __popc(bm);
 			nw += __popc(bw);
 			push_children(S.stack, sp, open_int, nchild, child);
 			// opened bundles -> bundle queue
@@ -756,15 +930,16 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	__syncwarp();
 	flush_far<TPL>(S, nl, t);
 	flush_slow<TPL>(p, S.wlist, nw, t);
+	if (QUAD) flush_quad<TPL>(*QL, nq, t);
 #pragma unroll
 	for (int k = 0; k < TPL; k++) t[k].cost -= 1.f;     // the self pair, which the reference skips
 	__syncwarp();
 }
 
-template <int MODE, int TPL, typename F>
+template <int MODE, int TPL, typename F, bool QUAD>
 __global__ void __launch_bounds__(GW_THREADS, GW_WALK_MINB)
 k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
-             const tvg_wnode *__restrict__ wt,
+             const tvg_wnode *__restrict__ wt, const float4 *__restrict__ wq,
              const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,
              const uint32_t *__restrict__ iz, const float *__restrict__ mass_f,
              const float *__restrict__ last_acc, F *acc0, F *acc1, F *acc2, F *gacc0, F *gacc1,
@@ -772,8 +947,10 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *_
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	WarpSmem &S = ((WarpSmem *) smem_raw)[threadIdx.x >> 5];
+	QuadList *QL = QUAD ? ((QuadList *) (smem_raw + sizeof(WarpSmem) * GW_WARPS)) + (threadIdx.x >> 5)
+	                    : nullptr;
 	const int lane = threadIdx.x & 31;
-	double cnt_acc = 0;
+	double cnt_acc = 0, qcnt_acc = 0;
 	const int64_t ngroups = p.dc->ngroups;
 	for (;;) {
 		int64_t g = 0;
@@ -790,7 +967,8 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *_
 			cnt = (int) min((int64_t) p.gsize, p.n - first);
 		}
 		Target t[TPL];
-		walk_group<MODE, TPL>(p, S, wt, ix, iy, iz, mass_f, last_acc, first, cnt, active, t, status);
+		walk_group<MODE, TPL, QUAD>(p, S, wt, ix, iy, iz, mass_f, last_acc, first, cnt, active, t, QL, wq,
+		                            status);
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
 			if (!t[k].valid) continue;
@@ -804,11 +982,16 @@ k_walk_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *_
 			gacc2[i] = (F) t[k].az;
 			cost_out[i] = (F) t[k].cost;
 			cnt_acc += t[k].cost;
+			qcnt_acc += t[k].qcost;
 		}
 	}
 #pragma unroll
-	for (int o = 16; o; o >>= 1) cnt_acc += __shfl_xor_sync(0xFFFFFFFFu, cnt_acc, o);
+	for (int o = 16; o; o >>= 1) {
+		cnt_acc += __shfl_xor_sync(0xFFFFFFFFu, cnt_acc, o);
+		qcnt_acc += __shfl_xor_sync(0xFFFFFFFFu, qcnt_acc, o);
+	}
 	if (lane == 0 && cnt_acc != 0) atomicAdd(counter, cnt_acc);
+	if (QUAD && lane == 0 && qcnt_acc != 0) atomicAdd(counter + 2, qcnt_acc);
 }
 
 // ------------------------------------------------------ the Ewald walk
@@ -1407,13 +1590,35 @@ static int prepare_typed(tvg_context *ctx)
 	const GNode<F> *tree = (const GNode<F> *) ctx->tree;
 	k_wt_nchild<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, lscan, tree, nch);
 	TVG_CUDA(ctx, cudaGetLastError());
-	TVG_CHECK(tvg_device_scan_i32(ctx, nch, choff, lscan, nullptr));
+	const bool quad = (ctx->cfg.flags & TVG_CFG_QUADRUPOLE) != 0;
+	int2 *wrange = nullptr;
+	if (quad) {
+		if (!ctx->wrange) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->wrange, sizeof(int2) * ctx->tcap));
+		if (!ctx->wquad) TVG_CUDA(ctx, cudaMalloc((void **) &ctx->wquad, 2 * sizeof(float4) * ctx->tcap));
+		wrange = (int2 *) ctx->wrange;
+		TVG_CUDA(ctx, cudaMemsetAsync(wrange, 0, sizeof(int2) * ctx->tcap, s));
+		TVG_CHECK(tvg_device_scan_i32_dev(ctx, nch, choff, lscan, &ctx->dc->nwchild));
+	} else {
+		TVG_CHECK(tvg_device_scan_i32(ctx, nch, choff, lscan, nullptr));
+	}
 	k_wt_emit<F><<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, tcap, tree, nch, choff, go[0], go[1],
-	                                                   go[2], fac, ctx->dsize, ctx->wtree);
+	                                                   go[2], fac, ctx->dsize, ctx->wtree, wrange);
 	TVG_CUDA(ctx, cudaGetLastError());
 	k_wt_small_top<<<TVG_CNT(ctx, TVG_MAX_TOP / 128), 128, 0, s>>>(ctx->dc, ctx->d_top, ctx->cfg.vector_size, go[0], go[1],
-	                                 go[2], fac, ctx->dsize, ctx->wtree);
+	                                 go[2], fac, ctx->dsize, ctx->wtree, wrange);
 	TVG_CUDA(ctx, cudaGetLastError());
+	if (quad) {
+		const float *mf = (const float *) ctx->f[FS_MASS];
+		if (ctx->cfg.float_bytes != 4) {   // the walks' FP32 masses (the FP64 build keeps a copy)
+			mf = (const float *) ctx->falt[FS_MASS];
+			k_to_float<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, (const F *) ctx->f[FS_MASS],
+			                                                                (float *) mf);
+		}
+		k_wt_quad_dev<<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, ctx->wtree, wrange, ctx->ipos[0],
+		                                                     ctx->ipos[1], ctx->ipos[2], mf,
+		                                                     1.0 / fac, ctx->cfg.gravity, ctx->wquad);
+		TVG_CUDA(ctx, cudaGetLastError());
+	}
 	ctx->have_walktree = true;
 	return TVG_OK;
 }
@@ -1492,23 +1697,31 @@ static int blocks_for(tvg_context *ctx, K kernel, size_t smem, int *cache, int t
 	return TVG_OK;
 }
 
-template <int MODE, int TPL, typename F>
-static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
-                       double *counter)
+template <int MODE, int TPL, typename F, bool QUAD>
+static int launch_walk_q(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
+                         double *counter)
 {
 	static int nblk_dev[TVG_MAX_DEVICES] = { 0 };
 	TVG_CHECK(device_slot(ctx));
 	int &nblk = nblk_dev[ctx->device];
-	const size_t smem = sizeof(WarpSmem) * GW_WARPS;
-	TVG_CHECK(blocks_for(ctx, k_walk_group<MODE, TPL, F>, smem, &nblk));
-	k_walk_group<MODE, TPL, F><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
+	const size_t smem = (sizeof(WarpSmem) + (QUAD ? sizeof(QuadList) : 0)) * GW_WARPS;
+	TVG_CHECK(blocks_for(ctx, k_walk_group<MODE, TPL, F, QUAD>, smem, &nblk));
+	k_walk_group<MODE, TPL, F, QUAD><<<TVG_CNT(ctx, nblk), GW_THREADS, smem, ctx->stream>>>(
 	    p, ctx->use_active ? ctx->active : nullptr, ctx->use_active ? ctx->group_first : nullptr,
-	    ctx->wtree, ctx->ipos[0], ctx->ipos[1],
+	    ctx->wtree, ctx->wquad, ctx->ipos[0], ctx->ipos[1],
 	    ctx->ipos[2], mass_f, last_f, (F *) ctx->f[FS_ACC0], (F *) ctx->f[FS_ACC1],
 	    (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1], (F *) ctx->f[FS_GACC2],
 	    (F *) ctx->f[FS_COST], ctx->work_counter, counter, ctx->status);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
+}
+
+template <int MODE, int TPL, typename F>
+static int launch_walk(tvg_context *ctx, GroupParams p, const float *mass_f, const float *last_f,
+                       double *counter)
+{
+	if (p.quad) return launch_walk_q<MODE, TPL, F, true>(ctx, p, mass_f, last_f, counter);
+	return launch_walk_q<MODE, TPL, F, false>(ctx, p, mass_f, last_f, counter);
 }
 
 template <int TPL, bool MLP, typename F>
@@ -1597,6 +1810,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 	p.n = n;
 	p.dc = ctx->dc;
 	p.max_iter = ctx->walk_limit;
+	p.quad = (ctx->cfg.flags & TVG_CFG_QUADRUPOLE) ? 1 : 0;
 	p.gsize = 32 * tpl;
 	if (ctx->use_active) {
 		TVG_CHECK(build_groups(ctx, p.gsize));
@@ -1636,7 +1850,7 @@ static int walk_group_typed(tvg_context *ctx, int use_bh, uint32_t parts, int ew
 		k_mass_total<<<TVG_CNT(ctx, 148 * 4), 256, 0, s>>>(n, mass_f, dm);
 		TVG_CUDA(ctx, cudaGetLastError());
 	}
-	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 16, s));
+	TVG_CUDA(ctx, cudaMemsetAsync(ctx->counters, 0, 24, s));
 	TVG_CUDA(ctx, cudaMemsetAsync(ctx->work_counter, 0, 8, s));
 	TVG_CUDA(ctx, tvg_record(ctx, ctx->ev[0]));
 	double *cnt = ctx->counters;
@@ -1658,10 +1872,11 @@ int tvg_walk_group_results(tvg_context *ctx)
 	TVG_CUDA(ctx, cudaEventElapsedTime(&ms_e, ctx->ev[1], ctx->ev[2]));
 	ctx->phase_ms[4] = ms;
 	ctx->phase_ms[5] = ms_e;
-	double c[2];
-	TVG_CUDA(ctx, cudaMemcpy(c, ctx->counters, 16, cudaMemcpyDeviceToHost));
+	double c[3];
+	TVG_CUDA(ctx, cudaMemcpy(c, ctx->counters, 24, cudaMemcpyDeviceToHost));
 	ctx->last_counts[0] = c[0];
 	ctx->last_counts[1] = c[1];
+	ctx->last_counts[2] = c[2];
 	return TVG_OK;
 }
 

@@ -26,6 +26,7 @@ CFG_FIX_SMALL_TOPNODES = 1
 CFG_OPEN_BUNDLES = 2
 CFG_POTENTIAL = 4              # the plain form computes Grav_Pot
 CFG_FIND_DOMAIN = 8            # isolated: the domain is found at every decomposition
+CFG_QUADRUPOLE = 16            # group form: node quadrupoles, octupole-order opening
 
 F_TYPE, F_TIME_BIN, F_IT_DRIFT, F_IT_KICK, F_KEY, F_ID, F_COST = (1 << k for k in range(7))
 F_POS, F_VEL, F_ACC, F_MASS, F_GRAV_ACC, F_LAST_ACC, F_TREE_PARENT = (1 << k for k in range(7, 14))
@@ -401,6 +402,14 @@ class GravityContext:
         g, e = C.c_double(), C.c_double()
         self._check(self.lib.tvg_walk_counters(self.ctx, C.byref(g), C.byref(e)), "walk_counters")
         return g.value, e.value
+
+    def walk_quad_interactions(self):
+        """Of the last group walk's gravity interactions, those with a
+        node's quadrupole (CFG_QUADRUPOLE); 0 otherwise."""
+        q = C.c_double()
+        self._check(self.lib.tvg_walk_quad_interactions(self.ctx, C.byref(q)),
+                    "walk_quad_interactions")
+        return q.value
 
     def set_opening(self, open_bh, open_rel):
         """TREE_OPEN_PARAM_BH (theta^2) and TREE_OPEN_PARAM_REL for later walks."""

@@ -16,8 +16,9 @@ PARTS = G.WALK_GRAVITY | G.WALK_EWALD
 FIELDS = G.F_ACC | G.F_GRAV_ACC | G.F_ID | G.F_POS | G.F_VEL | G.F_LAST_ACC
 
 
-def _ctx(p):
-    ctx = G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening)
+def _ctx(p, flags=0):
+    ctx = G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
+                           flags=flags)
     ctx.set_domain((0, 0, 0), p.box)
     ctx.ewald_init()
     ctx.set_opening(0.25, 2e-4)
@@ -29,9 +30,10 @@ def _same(a, b):
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
 
 
-def test_graph_step_equals_direct_step():
+@pytest.mark.parametrize("flags", [0, G.CFG_QUADRUPOLE])
+def test_graph_step_equals_direct_step(flags):
     p = ics.zeldovich_box(n_side=32, seed=41)
-    direct, graph = _ctx(p), _ctx(p)
+    direct, graph = _ctx(p, flags), _ctx(p, flags)
     try:
         for c in (direct, graph):
             c.upload(p.pos, p.mass)
@@ -42,6 +44,8 @@ def test_graph_step_equals_direct_step():
             graph.step_graph(PARTS)
             _same(direct.download(FIELDS), graph.download(FIELDS))
             assert direct.walk_counters() == graph.walk_counters()
+            assert direct.walk_quad_interactions() == graph.walk_quad_interactions()
+            assert (graph.walk_quad_interactions() > 0) == bool(flags)
             (tree_d, top_d), (tree_g, top_g) = direct.download_tree(), graph.download_tree()
             assert tree_d.tobytes() == tree_g.tobytes() and top_d.tobytes() == top_g.tobytes()
         # the captured steps' kernels are counted per launch
@@ -112,6 +116,8 @@ def test_graph_follows_parameter_changes():
                 graph.step_graph(PARTS)
                 _same(direct.download(FIELDS), graph.download(FIELDS))
                 assert direct.walk_counters() == graph.walk_counters()
+            assert direct.walk_quad_interactions() == graph.walk_quad_interactions()
+            assert (graph.walk_quad_interactions() > 0) == bool(flags)
     finally:
         direct.close()
         graph.close()

@@ -32,11 +32,11 @@ def rel_err(a, ref):
     return d / np.sqrt((ref ** 2).sum(0))
 
 
-def run_walks(p, origin, size, form, fsize=4):
+def run_walks(p, origin, size, form, fsize=4, flags=0):
     periodic = p.box > 0
     parts = G.WALK_GRAVITY | (G.WALK_EWALD if periodic else 0)
     with G.GravityContext(max(p.n, 1024), float_bytes=fsize, periodic=periodic, boxsize=p.box,
-                          softening=p.softening) as ctx:
+                          softening=p.softening, flags=flags) as ctx:
         ctx.upload(p.pos, p.mass)
         ctx.set_domain(origin, size)
         ctx.peano_keys()
@@ -48,27 +48,32 @@ def run_walks(p, origin, size, form, fsize=4):
         ctx.zero_accel()
         ctx.walk(form, use_bh=True, parts=parts)
         bh = ctx.download(G.F_GRAV_ACC | G.F_COST)
+        counts = {"bh": ctx.walk_counters() + (ctx.walk_quad_interactions(),)}
         ctx.save_last_accel()
         ctx.walk(form, use_bh=False, parts=parts)
         rel = ctx.download(G.F_GRAV_ACC | G.F_COST)
+        counts["rel"] = ctx.walk_counters() + (ctx.walk_quad_interactions(),)
     inv = np.empty_like(perm)
     inv[perm] = np.arange(len(perm))
-    return {k: (v["grav_acc"][:, inv].astype(np.float64), v["cost"][inv]) for k, v in
-            (("bh", bh), ("rel", rel))}
+    out = {k: (v["grav_acc"][:, inv].astype(np.float64), v["cost"][inv]) for k, v in
+           (("bh", bh), ("rel", rel))}
+    out["counts"] = counts
+    return out
 
 
-@pytest.mark.parametrize("kind", ["hernquist", "zeldovich"])
-def test_group_accuracy(kind):
+def _case(kind):
     if kind == "hernquist":
         p = ics.hernquist(n=32768, seed=31)
         c = np.median(p.pos, axis=1)
         size = 2.001 * np.abs(p.pos - c[:, None]).max()
-        origin = c - 0.5 * size
-        corr = None
-    else:
-        p = ics.zeldovich_box(n_side=32, seed=32)
-        origin, size = np.zeros(3), p.box
-        corr = fine_corr_table()
+        return p, c - 0.5 * size, size, None
+    p = ics.zeldovich_box(n_side=32, seed=32)
+    return p, np.zeros(3), p.box, fine_corr_table()
+
+
+@pytest.mark.parametrize("kind", ["hernquist", "zeldovich"])
+def test_group_accuracy(kind):
+    p, origin, size, corr = _case(kind)
     rng = np.random.default_rng(5)
     tgt = rng.choice(p.n, 1000, replace=False)
     ref = port.direct(p.pos, p.mass, tgt, ics.GRAVITY, p.softening, box=p.box,
@@ -85,6 +90,36 @@ def test_group_accuracy(kind):
         assert rms_g <= 1.2 * rms_p + 1e-6
         if rms_p < 1e-3:
             assert rms_g < 1e-3
+
+
+@pytest.mark.parametrize("kind,fsize", [("hernquist", 4), ("hernquist", 8), ("zeldovich", 4)])
+def test_quadrupole_accuracy(kind, fsize):
+    """TVG_CFG_QUADRUPOLE (no reference counterpart): under the BH criterion
+    the walk accepts the same nodes as the monopole walk, so the interaction
+    counts are equal, and every accepted node's quadrupole lowers the error;
+    under the relative criterion (octupole-order bound) the error at the same
+    TREE_OPEN_PARAM_REL is lower again with fewer interactions."""
+    p, origin, size, corr = _case(kind)
+    tgt = np.random.default_rng(5).choice(p.n, 1000, replace=False)
+    ref = port.direct(p.pos, p.mass, tgt, ics.GRAVITY, p.softening, box=p.box,
+                      corr_table=corr, corr_n=64)
+    mono = run_walks(p, origin, size, G.FORM_GROUP, fsize=fsize)
+    quad = run_walks(p, origin, size, G.FORM_GROUP, fsize=fsize, flags=G.CFG_QUADRUPOLE)
+    for crit in ("bh", "rel"):
+        em = rel_err(mono[crit][0][:, tgt], ref)
+        eq = rel_err(quad[crit][0][:, tgt], ref)
+        rms_m, rms_q = np.sqrt((em ** 2).mean()), np.sqrt((eq ** 2).mean())
+        (gm, ewm, qm), (gq, ewq, qq) = mono["counts"][crit], quad["counts"][crit]
+        print(f"{kind} f{fsize} {crit}: rms monopole {rms_m:.3e} quadrupole {rms_q:.3e}; "
+              f"interactions {gm / p.n:.0f} / {gq / p.n:.0f} (quadrupole {qq / p.n:.0f})")
+        assert qm == 0 and 0 < qq < gq
+        if crit == "bh":
+            assert gq == gm and ewq == ewm
+            # (in the periodic box the Ewald walk's own monopole error stays)
+            assert rms_q < (0.5 if p.box == 0 else 0.8) * rms_m
+        else:
+            assert gq < gm
+            assert rms_q < rms_m and rms_q < 1e-3
 
 
 def test_walk_limit_times_out_and_the_context_recovers():
