@@ -56,6 +56,12 @@ FLOP_PER_EWALD = 60.0
 # r^-3, r^-5, r^-7, mass, 15 for Q d, 5 for d.Q d, 3 for the radial factor,
 # 12 for the accumulation, 2 for the criterion
 FLOP_PER_QUAD = 51.0
+CFG_QUADRUPOLE = 16
+# operating points (TREE_OPEN_PARAM_REL, Ewald alpha_E) at 256^3, the fastest
+# of a sweep that keeps the rms force error below 1e-3 with margin:
+# quadrupoles (the headline) and the reference's monopoles (9.7e-4)
+QUAD_OPEN = (8e-3, 1e-2)
+MONO_OPEN = (7e-5, 4e-4)
 
 
 def parse():
@@ -77,14 +83,17 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-mlp", action="store_true", help="skip the learned-Ewald step")
     ap.add_argument("--no-peak", action="store_true", help="skip the FFMA peak loop (profiling runs)")
-    ap.add_argument("--open-rel", type=float, default=7e-5,
-                    help="TREE_OPEN_PARAM_REL of the group form (the loosest of a sweep that keeps "
-                         "the 256^3 box below 1e-3 rms: 9.7e-4)")
-    ap.add_argument("--quadrupole", action="store_true",
-                    help="group form with node quadrupoles and the octupole-order criterion "
-                         "(TVG_CFG_QUADRUPOLE)")
-    ap.add_argument("--ewald-alpha", type=float, default=4e-4,
-                    help="opening of the group form's Ewald walk (relative to |a_old|)")
+    ap.add_argument("--monopole", action="store_true",
+                    help="headline group form with node monopoles (the reference's moments) "
+                         "instead of quadrupoles (TVG_CFG_QUADRUPOLE)")
+    ap.add_argument("--open-rel", type=float, default=None,
+                    help="TREE_OPEN_PARAM_REL of the headline group form (default: the operating "
+                         "point of its form, QUAD_OPEN or MONO_OPEN)")
+    ap.add_argument("--ewald-alpha", type=float, default=None,
+                    help="opening of the group form's Ewald walk, relative to |a_old| (default: "
+                         "the operating point of its form)")
+    ap.add_argument("--no-monopole-run", action="store_true",
+                    help="skip the monopole group form's own run (quadrupole headline only)")
     ap.add_argument("--plain-open-rel", type=float, default=0.005,
                     help="TREE_OPEN_PARAM_REL of the plain form (the reference's value)")
     ap.add_argument("--domain-update-param", type=float, default=None,
@@ -96,7 +105,12 @@ def parse():
     ap.add_argument("--time-int-accuracy", type=float, default=0.025)
     ap.add_argument("--forcetest-targets", type=int, default=10000,
                     help="particles in the FP64 direct-sum error check (0: skip)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    rel, alpha = MONO_OPEN if args.monopole else QUAD_OPEN
+    args.open_rel = rel if args.open_rel is None else args.open_rel
+    args.ewald_alpha = alpha if args.ewald_alpha is None else args.ewald_alpha
+    args.flags = 0 if args.monopole else CFG_QUADRUPOLE
+    return args
 
 
 def dist_info():
@@ -290,7 +304,7 @@ def rung_run(args, p, G, device):
     Set_New_Timesteps, first kick, drift, Compute_Acceleration of the active
     particles, second kick; per-step active particles, time and rung counts."""
     ctx = G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
-                           device=device)
+                           device=device, flags=args.flags)
     try:
         n = p.n
         ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32),
@@ -354,6 +368,48 @@ def rung_run(args, p, G, device):
         ctx.close()
 
 
+def force_error(ctx, G, n, tgt_ids):
+    """rms / p99 / mean / max relative force error of the particles tgt_ids
+    (input order) against the FP64 direct Ewald sum on the GPU."""
+    try:
+        ids = ctx.download(G.F_ID)["id"]
+        inv = np.empty(n, np.int64)
+        inv[ids] = np.arange(n)
+        _, _, err = ctx.forcetest(np.sort(inv[tgt_ids]))
+        return {k: float(f"{v:.4e}") for k, v in err.items()}
+    except Exception as e:
+        return {"error": str(e)}
+
+
+def graph_steps(ctx, parts, steps, open_rel, dist, n, G, tgt_ids, prep_err=None):
+    """`steps` timed graph steps of ctx at TREE_OPEN_PARAM_REL open_rel (after a
+    direct step and the two captures), with the force error of the last one.
+    Every rank takes the same collective steps, failed or not."""
+    err, ms, g = prep_err, math.inf, 0.0
+    if err is None:
+        try:
+            ctx.set_opening(0.25, open_rel)
+            for _ in range(3):                     # direct step, then the two captures
+                ctx.step_graph(parts)
+            ms = 0.0
+            for _ in range(steps):
+                ctx.timer_start()
+                ctx.step_graph(parts)
+                ms += ctx.timer_stop()
+            g, _ = ctx.walk_counters()
+        except Exception as e:
+            err, ms = str(e), math.inf
+    t = dist.max(ms / steps) / 1e3
+    n_all = dist.sum(n)
+    if err is not None or not math.isfinite(t):
+        return {"error": err or "failed on another rank"}
+    out = {"open_rel": open_rel, "particles_per_s": n_all / t, "ms_per_step": round(t * 1e3, 2),
+           "steps": steps, "interactions_per_particle": round(g / n, 1)}
+    if tgt_ids is not None:
+        out["force_error"] = force_error(ctx, G, n, tgt_ids)
+    return out
+
+
 def workload_config(args, p, ws):
     return {
         "workload": f"zeldovich_{args.nside}^3_periodic_z50",
@@ -371,6 +427,10 @@ def workload_config(args, p, ws):
                   f"table, trilinear"),
         "form": ("group: warp per PH group of 32 x (targets per lane, autotuned) particles, FP32 on "
                  "32-bit integer box offsets"),
+        "moments": ("monopoles (the reference's)" if args.monopole else
+                    "quadrupoles (TVG_CFG_QUADRUPOLE): every accepted node's traceless quadrupole in "
+                    "the gravity walk, with the octupole-order relative criterion M s^3 <= r^5 "
+                    "|a_old| TREE_OPEN_PARAM_REL / G, and in the Ewald walk's expansion"),
         "step": ("Compute_Acceleration (keys, sort, top nodes, build, |a_old|, gravity and Ewald "
                  "walks) as one captured CUDA graph launch (tvg_step_graph); |a_old| from the "
                  "previous step"),
@@ -392,7 +452,7 @@ def main():
     p = make_ics(args.nside, 1234 + rank, args.box_mpc)
     n = p.n
     ctx = G.GravityContext(n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
-                           device=local, flags=G.CFG_QUADRUPOLE if args.quadrupole else 0)
+                           device=local, flags=args.flags)
     parts = G.WALK_GRAVITY | G.WALK_EWALD
     ctx.upload(p.pos, p.mass)
     ctx.set_domain((0.0, 0.0, 0.0), p.box)
@@ -490,8 +550,8 @@ def main():
     walk_flop = FLOP_PER_GRAV * (grav_i - quad_i) + FLOP_PER_QUAD * quad_i
     achieved = walk_flop / (walk_ms * 1e-3) / 1e12
     roofline = {
-        "kernel": ("k_walk_group<GM_CENTRE, 2, float, quadrupole> (gravity walk)" if args.quadrupole
-                   else "k_walk_group<GM_CENTRE, 2, float> (gravity walk)"), "bound": "fp32",
+        "kernel": (f"k_walk_group<GM_CENTRE, {tune_choice}, float, "
+                   f"{'monopole' if args.monopole else 'quadrupole'}> (gravity walk)"), "bound": "fp32",
         "achieved": round(achieved, 3), "peak": round(fp32_peak, 3), "unit": "TFLOP/s",
         "frac": round(achieved / fp32_peak, 4) if fp32_peak > 0 else None,
         "peak_source": "measured FFMA loop on this GPU (1.5 s, sustained under the power cap)",
@@ -507,41 +567,42 @@ def main():
         except (OSError, ValueError):
             pass
 
-    # ---- the group form at the plain form's opening parameter (same
-    # criterion, same particles): one pair of numbers at matched opening
-    matched = None
-    if not args.no_matched:
-        m_err = None
+    # ---- the monopole group form (the reference's node moments) at its own
+    # operating point, and at the plain form's opening parameter (the same
+    # criterion as the plain form, on the same particles)
+    monopole = matched = None
+    if args.monopole:
+        if not args.no_matched:
+            matched = graph_steps(ctx, parts, args.steps, args.plain_open_rel, dist, n, G, tgt_ids)
+            ctx.set_opening(0.25, args.open_rel)
+    elif not args.no_monopole_run:
+        cm, prep_err = None, None
         try:
-            ctx.set_opening(0.25, args.plain_open_rel)
-            for _ in range(3):                     # direct step, then the two captures
-                ctx.step_graph(parts)
-            m_ms = 0.0
-            for _ in range(args.steps):
-                ctx.timer_start()
-                ctx.step_graph(parts)
-                m_ms += ctx.timer_stop()
-            mg, _ = ctx.walk_counters()
+            cm = G.GravityContext(n, float_bytes=4, periodic=True, boxsize=p.box,
+                                  softening=p.softening, device=local)
+            cm.upload(p.pos, p.mass)
+            cm.set_domain((0.0, 0.0, 0.0), p.box)
+            cm.ewald_init()
+            cm.set_ewald_opening(MONO_OPEN[1])
+            cm.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
+            cm.save_last_accel()
+            cm.set_opening(0.25, MONO_OPEN[0])
+            cm.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
+            if not args.tpl:
+                cm.autotune(use_bh=False, parts=parts)
         except Exception as e:       # every rank still takes the collective steps below
-            m_err, m_ms = str(e), math.inf
-        t_m = dist.max(m_ms / args.steps) / 1e3
-        n_all_m = dist.sum(n)
-        if m_err is not None or not math.isfinite(t_m):
-            matched = {"error": m_err or "failed on another rank"}
-        else:
-            matched = {"open_rel": args.plain_open_rel, "particles_per_s": n_all_m / t_m,
-                       "ms_per_step": round(t_m * 1e3, 2),
-                       "interactions_per_particle": round(mg / n, 1)}
-            if tgt_ids is not None:
-                try:
-                    ids_m = ctx.download(G.F_ID)["id"]
-                    inv = np.empty(n, np.int64)
-                    inv[ids_m] = np.arange(n)
-                    _, _, err_m = ctx.forcetest(np.sort(inv[tgt_ids]))
-                    matched["force_error"] = {k: float(f"{v:.4e}") for k, v in err_m.items()}
-                except Exception as e:
-                    matched["force_error"] = {"error": str(e)}
-        ctx.set_opening(0.25, args.open_rel)
+            prep_err = str(e)
+        try:
+            monopole = graph_steps(cm, parts, min(args.steps, 2), MONO_OPEN[0], dist, n, G, tgt_ids,
+                                   prep_err)
+            if monopole.get("particles_per_s"):
+                monopole["ewald_alpha"] = MONO_OPEN[1]
+            if not args.no_matched:
+                matched = graph_steps(cm, parts, args.steps, args.plain_open_rel, dist, n, G, tgt_ids,
+                                      prep_err)
+        finally:
+            if cm is not None:
+                cm.close()
 
     # ---- the same step with the learned Ewald correction: trained here by the
     # library's own kernels, validated against the exact table, then run in the walk
@@ -692,6 +753,7 @@ def main():
                            "evaluations_per_group": round(ew_i / args.steps / (n / (32 * tune_choice)), 1),
                            "evaluation": "Taylor-table K, dK, d2K: 15 float4 loads, ~200 FP32 ops"},
             "plain_form": plain,
+            "group_form_monopole": monopole,
             "group_form_at_plain_opening": matched,
             "learned_ewald": learned,
             "device_memory_used_gb": hbm_gb,

@@ -86,7 +86,10 @@ enum {
 	 * each walk tree, and the relative criterion bounds the next (octupole)
 	 * term instead: a node of mass M and size s at distance r from the group
 	 * box is accepted when M s^3 <= r^5 |a_old|_min TREE_OPEN_PARAM_REL / G.
-	 * The plain form is unaffected. */
+	 * The Ewald walk (groups without per-target images) adds each accepted
+	 * node's quadrupole term to its correction and bounds the next term,
+	 * G M s^3 max|d3 T| / (48 L^5) <= alpha_E |a_old|_min
+	 * (tvg_set_ewald_opening). The plain form is unaffected. */
 	TVG_CFG_QUADRUPOLE = 16
 };
 

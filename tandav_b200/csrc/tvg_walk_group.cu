@@ -383,6 +383,7 @@ __device__ __forceinline__ void far_put(WarpSmem &S, int i, float4 e)
 struct EwaldSmem {
 	int32_t stack[GW_STACK];
 	float4 list[GW_ELIST];     // accepted sources: offset from the group centre, G m
+	int32_t lnode[GW_ELIST];   // TVG_CFG_QUADRUPOLE: their walk nodes (-1: a particle)
 	int2 bq[GW_BQ];
 };
 
@@ -530,17 +531,20 @@ __device__ __forceinline__ float ioff(uint32_t v, uint32_t c, float scale)
 // The gravity walk's opening decision for a node (shared by both walks, so
 // that the Ewald walk can repeat it bit for bit). d: centre of mass offset,
 // gx..: geometric centre offset. r2 receives the squared distance from the
-// centre of mass to the group box.
+// centre of mass to the group box. quad: the octupole-order criterion
+// (TVG_CFG_QUADRUPOLE, groups without per-target images), except for a node
+// within the softening length, which goes to the softened monopole list.
 __device__ __forceinline__ bool gravity_opens(const GroupParams &p, const GroupBox &g,
                                               const tvg_wnode &nd, int node, float dx, float dy,
-                                              float dz, float gx, float gy, float gz, float &r2)
+                                              float dz, float gx, float gy, float gz, float &r2,
+                                              bool quad)
 {
 	const float qx = fmaxf(fabsf(dx) - g.hx, 0.f), qy = fmaxf(fabsf(dy) - g.hy, 0.f),
 	            qz = fmaxf(fabsf(dz) - g.hz, 0.f);
 	r2 = qx * qx + qy * qy + qz * qz;
 	bool want;
 	if (p.use_bh) want = nd.size2 > r2 * p.theta2;
-	else if (p.quad) want = nd.mass * nd.size2 * nd.size > r2 * r2 * sqrtf(r2) * g.fac;
+	else if (quad && r2 >= p.near2) want = nd.mass * nd.size2 * nd.size > r2 * r2 * sqrtf(r2) * g.fac;
 	else want = nd.mass * nd.size2 > r2 * r2 * g.fac;
 	const float lim = 0.6f * nd.size;
 	if (fabsf(gx) < lim + g.hx && fabsf(gy) < lim + g.hy && fabsf(gz) < lim + g.hz) want = true;
@@ -806,6 +810,9 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 	    && (MODE == GM_NEAREST || fmaxf(g.hx, fmaxf(g.hy, g.hz)) >= p.taylor_h);
 	const float wlimx = p.half_box - 2.f * g.hx, wlimy = p.half_box - 2.f * g.hy,
 	            wlimz = p.half_box - 2.f * g.hz;
+	// per-target images go to the monopole list: their nodes keep the
+	// monopole criterion (the Ewald walk makes the same choice)
+	const bool quad_open = QUAD && !per_target;
 
 	int sp = 0, nl = 0, nw = 0, nq = 0;
 	const int ntop = p.dc->ntop;
@@ -832,7 +839,8 @@ __device__ void walk_group(const GroupParams &p, WarpSmem &S, const tvg_wnode *_
 				            dz = ioff(nd.cz, g.cz, p.scale);
 				float r2;
 				const bool open = gravity_opens(p, g, nd, node, dx, dy, dz, ioff(nd.gx, g.cx, p.scale),
-				                                ioff(nd.gy, g.cy, p.scale), ioff(nd.gz, g.cz, p.scale), r2);
+				                                ioff(nd.gy, g.cy, p.scale), ioff(nd.gz, g.cz, p.scale), r2,
+				                                quad_open);
 				if (!open) {
 					accept = true;
 					entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
@@ -1041,11 +1049,17 @@ __device__ __forceinline__ int taylor_record(const GroupParams &p, float4 e)
 	return (i * TVG_TAYLOR_NODES + j) * TVG_TAYLOR_NODES + l;
 }
 
-// STAGED: the record is `staged` (shared memory) instead of the table entry
-template <bool OVR, bool STAGED = false>
+// STAGED: the record is `staged` (shared memory) instead of the table entry.
+// SQ (TVG_CFG_QUADRUPOLE): srcq is the source node's stored -G Q (two float4,
+// null for a particle), and the value also takes the node's quadrupole term,
+// the second-order term of the expansion about its centre of mass:
+// sum_j m_j y_b y_c / 2 d2K_a/dd_b dd_c = Q_bc / 6 d2K_a/dd_b dd_c (d2K_a is
+// traceless: the lattice sum's divergence is constant away from the source).
+template <bool OVR, bool STAGED = false, bool SQ = false>
 __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const float4 *__restrict__ tay,
                                                  float4 e, CorrSum &c, const float *ovr,
-                                                 const float4 *staged = nullptr)
+                                                 const float4 *staged = nullptr,
+                                                 const float4 *__restrict__ srcq = nullptr)
 {
 	const float sg[3] = { e.x < 0.f ? -1.f : 1.f, e.y < 0.f ? -1.f : 1.f, e.z < 0.f ? -1.f : 1.f };
 	const float u = fabsf(e.x) * p.tay_grid, v = fabsf(e.y) * p.tay_grid, w = fabsf(e.z) * p.tay_grid;
@@ -1055,6 +1069,15 @@ __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const flo
 	const float du = u - (float) i, dv = v - (float) j, dw = w - (float) l;
 	const float4 *rec = STAGED ? staged : tay + 16 * ((i * TVG_TAYLOR_NODES + j) * TVG_TAYLOR_NODES + l);
 	const float m0 = -e.w * p.inv_box * p.inv_box, m1 = m0 * p.tay_grid, m2 = m1 * p.tay_grid;
+	float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0;
+	if (SQ && srcq) {
+		q0 = __ldg(srcq);
+		q1 = __ldg(srcq + 1);
+		q0.w *= 2.f * sg[0] * sg[1];      // both off-diagonal terms, with their signs
+		q1.x *= 2.f * sg[0] * sg[2];
+		q1.y *= 2.f * sg[1] * sg[2];
+	}
+	const float mq = p.tay_grid * p.tay_grid * p.inv_box * p.inv_box * (1.f / 6.f);
 #pragma unroll
 	for (int q = 0; q < 3; q++) {
 		float4 r0, r1, r2, r3, r4;
@@ -1090,6 +1113,13 @@ __device__ __forceinline__ void ewald_kjh_taylor(const GroupParams &p, const flo
 		                                                                    fmaf(0.5f, bz, r0.w) * dw));
 		const float sq = sg[q];
 		c.k[q] = fmaf(m0 * sq, val, c.k[q]);
+		if (SQ) {
+			// per unit G m, d2K_a/dd_b dd_c = -s_a s_b s_c h_bc tay_grid^2 / L^2;
+			// with G Q = -(stored), the term is mq s_a sum_bc stored_bc s_b s_c h_bc
+			const float hq = fmaf(q0.x, hxx, fmaf(q0.y, hyy, fmaf(q0.z, hzz,
+			                 fmaf(q0.w, hxy, fmaf(q1.x, hxz, q1.y * hyz)))));
+			c.k[q] = fmaf(mq * sq, hq, c.k[q]);
+		}
 		c.j[3 * q + 0] = fmaf(m1 * sq * sg[0], gx, c.j[3 * q + 0]);
 		c.j[3 * q + 1] = fmaf(m1 * sq * sg[1], gy, c.j[3 * q + 1]);
 		c.j[3 * q + 2] = fmaf(m1 * sq * sg[2], gz, c.j[3 * q + 2]);
@@ -1145,6 +1175,15 @@ __device__ __forceinline__ float ewald_h2(float r)
 	return 92.f * x * sqrtf(x);
 }
 
+// bound of |d3 T| (box units) within distance r of the source: 75 near the
+// source (the lattice sum's cubic term), 753 at the face centres; 77 + 680
+// (2 r)^4 bounds the table's third derivatives at every node
+__device__ __forceinline__ float ewald_h3(float r)
+{
+	const float x = fminf(2.f * r, 1.f), x2 = x * x;
+	return fmaf(680.f, x2 * x2, 77.f);
+}
+
 // Field of the uniform unit-density cube [-1/2, 1/2]^3 at tau (G = 1): the
 // closed form of the rectangular prism (the double antiderivative of 1/r,
 // F = Y ln(Z + r) + Z ln(Y + r) - X atan(Y Z / (X r)), over the corners;
@@ -1195,14 +1234,23 @@ __device__ __noinline__ void mlp_forward_warp_call(const float *mlp, const uint3
 // the lane (K at the target's nearest image; FP32 per batch, carried in
 // FP64). With the learned correction the value of K comes from the warp's
 // tensor-core evaluation of the network (one point per lane).
+// wq (TVG_CFG_QUADRUPOLE, groups without per-target images): the walk
+// nodes' stored quadrupoles, lnode the list entries' nodes
 template <int TPL, bool MLP>
 __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *tab, const float4 *tay,
                                             const float *mlp, const uint32_t *w2b, const float4 *list,
                                             int from, int cnt, bool per_target, CorrSum &c,
-                                            Target (&t)[TPL], float &nev)
+                                            Target (&t)[TPL], float &nev,
+                                            const int32_t *lnode = nullptr,
+                                            const float4 *__restrict__ wq = nullptr)
 {
 	const int lane = threadIdx.x & 31;
 	if (!per_target) {
+		const float4 *srcq = nullptr;
+		if (wq && lane < cnt) {
+			const int nd = lnode[from + lane];
+			srcq = nd >= 0 ? wq + 2 * (int64_t) nd : nullptr;
+		}
 		if (MLP) {
 			// lanes past cnt repeat the last entry and drop the result
 			const float4 e = list[from + min(lane, cnt - 1)];
@@ -1210,11 +1258,13 @@ __device__ __forceinline__ void ewald_batch(const GroupParams &p, const float4 *
 			float tv[3];
 			mlp_forward_warp(mlp, w2b, xs, tv);
 			if (lane < cnt) {
-				ewald_kjh_taylor<true>(p, tay, e, c, tv);
+				if (wq) ewald_kjh_taylor<true, false, true>(p, tay, e, c, tv, nullptr, srcq);
+				else ewald_kjh_taylor<true>(p, tay, e, c, tv);
 				nev += 1.f;
 			}
 		} else if (lane < cnt) {
-			ewald_kjh_taylor<false>(p, tay, list[from + lane], c, nullptr);
+			if (wq) ewald_kjh_taylor<false, false, true>(p, tay, list[from + lane], c, nullptr, nullptr, srcq);
+			else ewald_kjh_taylor<false>(p, tay, list[from + lane], c, nullptr);
 			nev += 1.f;
 		}
 	} else {
@@ -1320,7 +1370,8 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
                             const float *__restrict__ last_acc, const float4 *__restrict__ tab,
                             const float4 *__restrict__ tay, const float *mlp, const uint32_t *w2b,
                             int64_t first, int cnt, const int32_t *__restrict__ active,
-                            Target (&t)[TPL], float &nev, EwaldStage *st, StageState &ss, int *status)
+                            Target (&t)[TPL], float &nev, EwaldStage *st, StageState &ss, int *status,
+                            const float4 *__restrict__ wq_all)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned lt = (1u << lane) - 1u;
@@ -1329,6 +1380,10 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 	const float hmax = fmaxf(g.hx, fmaxf(g.hy, g.hz));
 	// the gravity walk makes the same choice (walk_group)
 	const bool per_target = hmax >= p.taylor_h;
+	// node quadrupoles (TVG_CFG_QUADRUPOLE) in the expansion about the group
+	// centre; per-target images evaluate K alone and keep monopoles
+	const float4 *wq = per_target ? nullptr : wq_all;
+	if (wq) st = nullptr;
 	// straddling: the node (and, with per-target images, the group box) reaches
 	// the half-box plane; then the gravity walk's decision is repeated
 	const float margin = 8.f * p.scale;
@@ -1342,102 +1397,133 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 #pragma unroll
 	for (int a = 0; a < 18; a++) c.h[a] = 0.f;
 
-	int sp = 0, nl = 0;
+	int sp = 0, nl = 0, r0 = 0;
 	const int ntop = p.dc->ntop;
 	int guard = 0;
-	bool halt = false;
-	// the roots in chunks of GW_ROOTS (a balanced decomposition can have
-	// thousands of top nodes, more than the stack holds at once)
-	for (int r0 = 0; r0 < ntop && !halt; r0 += GW_ROOTS) {
-		const int nr = min(GW_ROOTS, ntop - r0);
-		for (int r = lane; r < nr; r += 32) S.stack[r] = r0 + r;
-		sp = nr;
-		__syncwarp();
-		while (sp > 0) {
-			if (++guard > p.max_iter) { atomicOr(status, TVG_ST_TIMEOUT); halt = true; break; }
+	bool final = false;
+	// One loop step pops up to 32 nodes, lists the accepted ones and queues
+	// the opened bundles; then the drain below evaluates every full batch of
+	// 32 sources (at the end the rest too) and lists the next 32 particles of
+	// the queued bundles, so that the evaluation is inlined once in the loop.
+	for (;;) {
+		int nb = 0;
+		if (sp == 0 && !final) {
+			// the roots in chunks of GW_ROOTS (a balanced decomposition can have
+			// thousands of top nodes, more than the stack holds at once)
+			if (r0 < ntop) {
+				const int nr = min(GW_ROOTS, ntop - r0);
+				for (int r = lane; r < nr; r += 32) S.stack[r] = r0 + r;
+				sp = nr;
+				r0 += GW_ROOTS;
+				__syncwarp();
+			} else {
+				final = true;
+			}
+		}
+		if (!final && ++guard > p.max_iter) {
+			atomicOr(status, TVG_ST_TIMEOUT);
+			final = true;
+		}
+		if (!final) {
 			bool stop;
 			const int node = pop_nodes(S.stack, sp, status, stop);
-			if (stop) { halt = true; break; }
-			bool accept = false, open_int = false, open_bundle = false;
-			float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
-			int nchild = 0, child = 0;
-			if (node >= 0) {
-				const tvg_wnode nd = wt[node];
-				const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
-				            dz = ioff(nd.cz, g.cz, p.scale);
-				const float gx = ioff(nd.gx, g.cx, p.scale), gy = ioff(nd.gy, g.cy, p.scale),
-				            gz = ioff(nd.gz, g.cz, p.scale);
-				const float hs = 0.5f * nd.size + margin;
-				const bool straddle = fabsf(gx) + hs + ex > p.half_box || fabsf(gy) + hs + ey > p.half_box
-				                   || fabsf(gz) + hs + ez > p.half_box;
-				bool open;
-				if (straddle) {
-					float r2;
-					open = gravity_opens(p, g, nd, node, dx, dy, dz, gx, gy, gz, r2);
-				} else {
-					// monopole error of K: G M h2 s^2 / (8 L^4) (s^2 / 4: the mean square
-					// offset of a uniform cube's mass from its centre)
-					const float rfar = (sqrtf(gx * gx + gy * gy + gz * gz) + nd.size + hmax) * p.inv_box;
-					const float l2 = p.inv_box * p.inv_box;
-					const float hs2 = ewald_h2(rfar) * nd.size2 * l2;     // h2 s^2 / L^2
-					if (p.use_bh) open = hs2 > p.ew_bh;
-					else open = nd.mass * hs2 * 0.125f * l2 > p.ew_rel * g.fac;
-				}
-				if (!open) {
-					accept = true;
-					entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
-				} else if (nd.nchild > 0) {
-					open_int = true;
-					nchild = nd.nchild;
-					child = nd.child;
-				} else {
-					open_bundle = true;
-					nchild = -nd.nchild;
-					child = nd.child;
-				}
-			}
-			const unsigned bm = __ballot_sync(0xFFFFFFFFu, accept);
-			if (accept) S.list[nl + __popc(bm & lt)] = entry;
-			nl += __popc(bm);
-			__syncwarp();
-			if (nl >= 32) {
-				if (st && ss.ok && !per_target) stage_batch(p, tay, st, S.list, nl - 32, ss, c, nev, status);
-				else ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
-				nl -= 32;
-			}
-			push_children(S.stack, sp, open_int, nchild, child);
-			const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
-			if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
-			__syncwarp();
-			const int nb = __popc(bb);
-			for (int b = 0; b < nb; b++) {
-				const int2 q = S.bq[b];
-				for (int o = 0; o < q.y; o += 32) {
-					const int jj = o + lane;
-					const bool have = jj < q.y;
-					float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-					if (have) {
-						const int64_t jp = (int64_t) q.x + jj;
-						e = make_float4(ioff(ix[jp], g.cx, p.scale), ioff(iy[jp], g.cy, p.scale),
-						                ioff(iz[jp], g.cz, p.scale), p.gravity * mass_f[jp]);
+			if (stop) {
+				final = true;
+			} else {
+				bool accept = false, open_int = false, open_bundle = false;
+				float4 entry = make_float4(0.f, 0.f, 0.f, 0.f);
+				int nchild = 0, child = 0;
+				if (node >= 0) {
+					const tvg_wnode nd = wt[node];
+					const float dx = ioff(nd.cx, g.cx, p.scale), dy = ioff(nd.cy, g.cy, p.scale),
+					            dz = ioff(nd.cz, g.cz, p.scale);
+					const float gx = ioff(nd.gx, g.cx, p.scale), gy = ioff(nd.gy, g.cy, p.scale),
+					            gz = ioff(nd.gz, g.cz, p.scale);
+					const float hs = 0.5f * nd.size + margin;
+					const bool straddle = fabsf(gx) + hs + ex > p.half_box || fabsf(gy) + hs + ey > p.half_box
+					                   || fabsf(gz) + hs + ez > p.half_box;
+					bool open;
+					if (straddle) {
+						float r2;
+						open = gravity_opens(p, g, nd, node, dx, dy, dz, gx, gy, gz, r2, p.quad && !per_target);
+					} else {
+						// monopole error of K: G M h2 s^2 / (8 L^4) (s^2 / 4: the mean square
+						// offset of a uniform cube's mass from its centre); with the node's
+						// quadrupole the next term, G M h3 s^3 / (48 L^5) (s / 2 per axis)
+						const float rfar = (sqrtf(gx * gx + gy * gy + gz * gz) + nd.size + hmax) * p.inv_box;
+						const float l2 = p.inv_box * p.inv_box;
+						const float hs2 = ewald_h2(rfar) * nd.size2 * l2;     // h2 s^2 / L^2
+						if (p.use_bh) open = hs2 > p.ew_bh;
+						else if (wq) {
+							const float sl = nd.size * p.inv_box;
+							open = nd.mass * ewald_h3(rfar) * sl * sl * sl * (1.f / 48.f) * l2 > p.ew_rel * g.fac;
+						} else open = nd.mass * hs2 * 0.125f * l2 > p.ew_rel * g.fac;
 					}
-					const unsigned mb = __ballot_sync(0xFFFFFFFFu, have);
-					if (have) S.list[nl + __popc(mb & lt)] = e;
-					nl += __popc(mb);
-					__syncwarp();
-					if (nl >= 32) {
-						if (st && ss.ok && !per_target) stage_batch(p, tay, st, S.list, nl - 32, ss, c, nev, status);
-						else ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - 32, 32, per_target, c, t, nev);
-						nl -= 32;
+					if (!open) {
+						accept = true;
+						entry = make_float4(dx, dy, dz, p.gravity * nd.mass);
+					} else if (nd.nchild > 0) {
+						open_int = true;
+						nchild = nd.nchild;
+						child = nd.child;
+					} else {
+						open_bundle = true;
+						nchild = -nd.nchild;
+						child = nd.child;
 					}
 				}
+				const unsigned bm = __ballot_sync(0xFFFFFFFFu, accept);
+				if (accept) {
+					S.list[nl + __popc(bm & lt)] = entry;
+					S.lnode[nl + __popc(bm & lt)] = node;
+				}
+				nl += __popc(bm);       // below 64: the drain left fewer than 32
+				push_children(S.stack, sp, open_int, nchild, child);
+				const unsigned bb = __ballot_sync(0xFFFFFFFFu, open_bundle);
+				if (open_bundle) S.bq[__popc(bb & lt)] = make_int2(child, nchild);
+				nb = __popc(bb);
+				__syncwarp();
 			}
-			__syncwarp();
 		}
+		int b = 0, o = 0;
+		for (;;) {
+			const bool full = nl >= 32;
+			if (full || (final && nl > 0)) {
+				const int cnt = full ? 32 : nl;
+				if (full && st && ss.ok && !per_target) stage_batch(p, tay, st, S.list, nl - 32, ss, c, nev, status);
+				else ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, nl - cnt, cnt, per_target, c, t, nev,
+				                           S.lnode, wq);
+				nl -= cnt;
+				continue;
+			}
+			if (b >= nb) break;
+			// the next 32 particles of queued bundle b
+			const int2 q = S.bq[b];
+			const int jj = o + lane;
+			const bool have = jj < q.y;
+			float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+			if (have) {
+				const int64_t jp = (int64_t) q.x + jj;
+				e = make_float4(ioff(ix[jp], g.cx, p.scale), ioff(iy[jp], g.cy, p.scale),
+				                ioff(iz[jp], g.cz, p.scale), p.gravity * mass_f[jp]);
+			}
+			const unsigned mb = __ballot_sync(0xFFFFFFFFu, have);
+			if (have) {
+				S.list[nl + __popc(mb & lt)] = e;
+				S.lnode[nl + __popc(mb & lt)] = -1;
+			}
+			nl += __popc(mb);
+			__syncwarp();
+			o += 32;
+			if (o >= q.y) {
+				b++;
+				o = 0;
+			}
+		}
+		__syncwarp();
+		if (final) break;
 	}
-	__syncwarp();
 	if (st && ss.ok) stage_drain(p, st, ss, c, nev, status);
-	if (nl > 0) ewald_batch<TPL, MLP>(p, tab, tay, mlp, w2b, S.list, 0, nl, per_target, c, t, nev);
 	if (per_target) return;
 	// sum over lanes (FP64), then K(d_c - t) ~ K - J t + H:tt / 2 per target
 	double K[3], J[9], H[18];
@@ -1487,7 +1573,8 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
               const float *__restrict__ last_acc, const float4 *__restrict__ tab,
               const float4 *__restrict__ tay, const __nv_bfloat16 *__restrict__ mlp_w,
               const float *__restrict__ mlp_f32, F *acc0, F *acc1,
-              F *acc2, F *gacc0, F *gacc1, F *gacc2, int32_t *work, double *counter, int *status)
+              F *acc2, F *gacc0, F *gacc1, F *gacc2, int32_t *work, double *counter, int *status,
+              const float4 *__restrict__ wq)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	EwaldSmem &S = ((EwaldSmem *) smem_raw)[threadIdx.x >> 5];
@@ -1533,7 +1620,7 @@ k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *
 		Target t[TPL];
 		float nev = 0.f;
 		ewald_group<TPL, MLP>(p, S, wt, ix, iy, iz, mass_f, last_acc, tab, tay, mlp, w2b, first, cnt, active, t, nev,
-		                 st, ss, status);
+		                 st, ss, status, wq);
 		ev_acc += nev;
 #pragma unroll
 		for (int k = 0; k < TPL; k++) {
@@ -1741,7 +1828,8 @@ static int launch_ewald(tvg_context *ctx, GroupParams p, const float *mass_f, co
 	    (const float4 *) ctx->ewald_taylor, (const __nv_bfloat16 *) ctx->mlp_bf16, ctx->mlp_prm,
 	    (F *) ctx->f[FS_ACC0],
 	    (F *) ctx->f[FS_ACC1], (F *) ctx->f[FS_ACC2], (F *) ctx->f[FS_GACC0], (F *) ctx->f[FS_GACC1],
-	    (F *) ctx->f[FS_GACC2], ctx->work_counter + 1, counter, ctx->status);
+	    (F *) ctx->f[FS_GACC2], ctx->work_counter + 1, counter, ctx->status,
+	    p.quad ? (const float4 *) ctx->wquad : nullptr);
 	TVG_CUDA(ctx, cudaGetLastError());
 	return TVG_OK;
 }
