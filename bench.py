@@ -92,6 +92,9 @@ def parse():
     ap.add_argument("--ewald-alpha", type=float, default=None,
                     help="opening of the group form's Ewald walk, relative to |a_old| (default: "
                          "the operating point of its form)")
+    ap.add_argument("--vector-size", type=int, default=64,
+                    help="VECTOR_SIZE of the headline form's tree: particles per bundle (the "
+                         "reference's 64)")
     ap.add_argument("--no-monopole-run", action="store_true",
                     help="skip the monopole group form's own run (quadrupole headline only)")
     ap.add_argument("--plain-open-rel", type=float, default=0.005,
@@ -427,6 +430,7 @@ def workload_config(args, p, ws):
                   f"table, trilinear"),
         "form": ("group: warp per PH group of 32 x (targets per lane, autotuned) particles, FP32 on "
                  "32-bit integer box offsets"),
+        "vector_size": getattr(args, "vector_size", 64),
         "moments": ("monopoles (the reference's)" if args.monopole else
                     "quadrupoles (TVG_CFG_QUADRUPOLE): every accepted node's traceless quadrupole in "
                     "the gravity walk, with the octupole-order relative criterion M s^3 <= r^5 "
@@ -452,7 +456,7 @@ def main():
     p = make_ics(args.nside, 1234 + rank, args.box_mpc)
     n = p.n
     ctx = G.GravityContext(n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
-                           device=local, flags=args.flags)
+                           device=local, flags=args.flags, vector_size=args.vector_size)
     parts = G.WALK_GRAVITY | G.WALK_EWALD
     ctx.upload(p.pos, p.mass)
     ctx.set_domain((0.0, 0.0, 0.0), p.box)

@@ -40,7 +40,8 @@ def nvcc() -> str:
 
 def _compile(src: Path) -> Path:
     obj = OBJ / (src.stem + ".o")
-    deps = [src] + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "tandav_gpu.h"]
+    deps = ([src] + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc"))
+            + [ROOT / "include" / "tandav_gpu.h"])
     if obj.exists() and all(obj.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return obj
     flags = list(COMMON)
