@@ -72,8 +72,9 @@ def top_nodes(std_sorted, pos_sorted, origin, size, fsize=4):
     return out[:nt].copy()
 
 
-def tree_build(rev_sorted, pos_sorted, mass_sorted, domain_size, top, fsize=4):
-    """Returns (tree, top (updated), tree_parent)."""
+def tree_build(rev_sorted, pos_sorted, mass_sorted, domain_size, top, fsize=4, vector_size=64):
+    """Returns (tree, top (updated), tree_parent). vector_size: the reference's
+    compile-time VECTOR_SIZE (bundle size), 64 by default."""
     ft = ftype(fsize)
     x, y, z = (np.ascontiguousarray(pos_sorted[k], dtype=ft) for k in range(3))
     m = np.ascontiguousarray(mass_sorted, dtype=ft)
@@ -86,7 +87,7 @@ def tree_build(rev_sorted, pos_sorted, mass_sorted, domain_size, top, fsize=4):
     lib().tvo_tree_build.restype = C.c_int64
     nn = lib().tvo_tree_build(C.c_int64(n), C.c_int32(fsize), _p(rk), _p(x), _p(y), _p(z),
                               _p(m), C.c_double(domain_size), _p(top), C.c_int32(len(top)),
-                              _p(tree), C.c_int64(cap), _p(parent))
+                              _p(tree), C.c_int64(cap), _p(parent), C.c_int32(vector_size))
     if nn < 0:
         raise RuntimeError(f"tvo_tree_build failed: {nn}")
     return tree[:nn].copy(), top, parent

@@ -23,5 +23,9 @@ if [ "$prec" = "f64" ]; then echo "DOUBLE_PRECISION" >> "$tmp"; fi
 # suffix _pot: the gravitational potential (GRAVITY_POTENTIAL) and its
 # snapshot block (OUTPUT_GRAV_POTENTIAL, which changes nothing but the I/O)
 case "$variant" in *_pot*) printf 'GRAVITY_POTENTIAL\nOUTPUT_GRAV_POTENTIAL\n' >> "$tmp" ;; esac
+# suffix _v<N>: VECTOR_SIZE N (particles per tree leaf) instead of the Config's
+case "$variant" in
+  *_v[0-9]*) vs=${variant##*_v}; sed -i -e "s/^VECTOR_SIZE .*/VECTOR_SIZE $vs/" "$tmp" ;;
+esac
 sed '/^#/d; /^[[:space:]]*$/d; s/^/#define /g' "$tmp" > "$out"
 rm -f "$tmp"

@@ -114,15 +114,16 @@ int32_t tvo_top_nodes(int64_t n, int32_t fsize, const uint64_t *std_key, const v
 int64_t tvo_tree_build(int64_t n, int32_t fsize, const uint64_t *rev_key, const void *x,
                        const void *y, const void *z, const void *mass, double domain_size,
                        tvo_topnode *top, int32_t ntop, void *tree, int64_t tree_cap,
-                       int32_t *tree_parent)
+                       int32_t *tree_parent, int32_t vector_size)
 {
 	/* particles equal in all 42 levels would be dumped into a level-41 node
-	 * (tree_build.c:337-342); the restatement follows that path too */
+	 * (tree_build.c:337-342); the restatement follows that path too.
+	 * vector_size: the reference's compile-time VECTOR_SIZE (64 by default) */
 	if (fsize == 4)
 		return tree_build_f32(n, rev_key, x, y, z, mass, domain_size, top, ntop, tree, tree_cap,
-		                      tree_parent);
+		                      tree_parent, vector_size);
 	return tree_build_f64(n, rev_key, x, y, z, mass, domain_size, top, ntop, tree, tree_cap,
-	                      tree_parent);
+	                      tree_parent, vector_size);
 }
 
 void tvo_walk_gravity(int64_t n, int32_t fsize, const void *x, const void *y, const void *z,

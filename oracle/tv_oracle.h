@@ -67,7 +67,7 @@ int64_t tvo_tree_build(int64_t n, int32_t fsize, const uint64_t *rev_key,
                        const void *x, const void *y, const void *z,
                        const void *mass, double domain_size,
                        tvo_topnode *top, int32_t ntop, void *tree,
-                       int64_t tree_cap, int32_t *tree_parent);
+                       int64_t tree_cap, int32_t *tree_parent, int32_t vector_size);
 
 /* Gravity_Tree_Acceleration walk part for the active particles
  * (tree_accel.c:32-394): acc += per-particle sum (double), cost = count.

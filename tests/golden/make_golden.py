@@ -6,7 +6,8 @@ stores their outputs (keys, sort permutation, top nodes, tree, Tree_Parent,
 accelerations of the BH and relative passes, Ewald parts) as compressed .npz
 files. Re-run after changing the inputs: `python tests/golden/make_golden.py`
 (`... make_golden.py potential` for the potential fixtures only,
-`... make_golden.py decomposition` for the balanced decompositions only).
+`... make_golden.py decomposition` for the balanced decompositions only,
+`... make_golden.py vector_size` for the smaller-VECTOR_SIZE builds only).
 """
 from __future__ import annotations
 
@@ -47,10 +48,11 @@ def keys_case():
     np.savez_compressed(HERE / "keys_grid.npz", **out)
 
 
-def force_case(name, variant, p, flags=3):
+def force_case(name, variant, p, flags=3, vector_size=64):
     r = refrun.run(variant, "force", p.pos, p.vel, p.mass, box=p.box, softening=p.softening,
                    flags=flags)
     out = dict(pos_in=p.pos, mass_in=p.mass, box=np.array(p.box), softening=np.array(p.softening),
+               vector_size=np.array(vector_size),
                float_size=np.array(r["float_size"]), gravity=r["gravity"],
                domain_size=r["domain_size"], domain_origin=r["domain_origin"],
                perm=r["perm"], std_key=r["std_key"], rev_key=r["rev_key"],
@@ -98,6 +100,14 @@ def main():
     force_case("zeldovich_per_f64", "per_f64", ics.zeldovich_box(n_side=20, seed=9))
 
 
+def vector_size_cases():
+    """The reference built with a smaller VECTOR_SIZE (variants *_v<N>)."""
+    force_case("box_per_f32_v32", "per_f32_v32",
+               ics.random_box(3000, box=1000.0, seed=8, clumps=6), vector_size=32)
+    force_case("hernquist_iso_f64_v16", "iso_f64_v16", ics.hernquist(n=2048, seed=5),
+               vector_size=16)
+
+
 def potential_cases():
     """The same inputs through the reference built with GRAVITY_POTENTIAL
     (variants *_pot): forces and Grav_Pot of both passes."""
@@ -112,5 +122,7 @@ if __name__ == "__main__":
         potential_cases()
     elif sys.argv[1:] == ["decomposition"]:
         decomposition_cases()
+    elif sys.argv[1:] == ["vector_size"]:
+        vector_size_cases()
     else:
         main()

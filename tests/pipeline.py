@@ -26,10 +26,10 @@ def balanced_top_nodes(std_s, pos_s, cost_s, origin, size, ntask):
 
 
 def oracle_pipeline(pos, mass, origin, size, fsize, box=0.0, softening=0.01, gravity=43007.1,
-                    ewald=None, passes=("bh", "rel"), ntask=1, cost=None):
+                    ewald=None, passes=("bh", "rel"), ntask=1, cost=None, vector_size=64):
     """Keys -> sort -> top nodes -> tree -> walks, as the reference runs them
     (top nodes balanced over `ntask` targets by `cost`, in input order, when
-    ntask > 1)."""
+    ntask > 1; bundles of at most `vector_size` particles)."""
     ft = port.ftype(fsize)
     pos_f = np.asarray(pos).astype(ft)
     std, rev = port.peano_keys(pos_f, origin, size, fsize)
@@ -41,11 +41,12 @@ def oracle_pipeline(pos, mass, origin, size, fsize, box=0.0, softening=0.01, gra
         top = balanced_top_nodes(std_s, pos_s, np.asarray(cost, np.float64)[perm], origin, size, ntask)
     else:
         top = port.top_nodes(std_s, pos_s, origin, size, fsize)
-    tree, top, parent = port.tree_build(rev_s, pos_s, mass_s, size, top, fsize)
+    tree, top, parent = port.tree_build(rev_s, pos_s, mass_s, size, top, fsize,
+                                        vector_size=vector_size)
     out = dict(perm=perm, std_key=std_s, rev_key=rev_s, pos=pos_s, mass=mass_s, top=top,
                tree=tree, tree_parent=parent)
     prm = port.WalkParams(gravity=gravity, softening=softening, domain_size=size, boxsize=box,
-                          open_bh=0.25, open_rel=0.005, use_bh=1, vector_size=64)
+                          open_bh=0.25, open_rel=0.005, use_bh=1, vector_size=vector_size)
     last = np.zeros(len(mass_s), ft)
     for name in passes:
         prm.use_bh = 1 if name == "bh" else 0

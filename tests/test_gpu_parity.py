@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 
 TREE_FIELDS = ["DNext", "Bitfield", "DUp", "Npart", "Pos", "Mass", "CoM", "Dp"]
 TOP_FIELDS = ["Key", "Target", "Level", "First_Part", "Npart", "Pos", "Mass", "CoM"]
-FORCE_CASES = ["hernquist_iso_f64", "hernquist_iso_f32", "box_per_f32", "zeldovich_per_f64"]
+FORCE_CASES = ["hernquist_iso_f64", "hernquist_iso_f32", "box_per_f32", "zeldovich_per_f64",
+               "box_per_f32_v32", "hernquist_iso_f64_v16"]
 
 
 def make_ctx(n, fsize, box=0.0, softening=0.01, gravity=43007.1, **kw):
@@ -85,8 +86,9 @@ def test_pipeline_matches_reference_golden(golden_dir, case):
     fsize = int(g["float_size"])
     box = float(g["box"])
     n = len(g["mass_in"])
+    vsize = int(g["vector_size"]) if "vector_size" in g.files else 64
     with make_ctx(n, fsize, box=box, softening=float(g["softening"]),
-                  gravity=float(g["gravity"][0])) as ctx:
+                  gravity=float(g["gravity"][0]), vector_size=vsize) as ctx:
         perm, keys, tree, top = gpu_pipeline(ctx, g["pos_in"], g["mass_in"], g["domain_origin"],
                                              float(g["domain_size"][0]))
         assert np.array_equal(perm, g["perm"])
@@ -352,6 +354,35 @@ def test_keys_sort_and_tree_of_the_256_box():
     assert_struct_equal(top, top_o, TOP_FIELDS, "topnodes")
     assert_struct_equal(tree, tree_o, TREE_FIELDS, "tree")
     assert np.array_equal(parent, parent_o)
+
+
+@pytest.mark.parametrize("kind,fsize,n,vsize", [("zeldovich", 4, 64 ** 3, 32),
+                                               ("zeldovich", 4, 64 ** 3, 8),
+                                               ("hernquist", 8, 1 << 17, 32),
+                                               ("clumpy_box", 4, 1 << 17, 16)])
+def test_tree_vs_oracle_at_other_vector_sizes(kind, fsize, n, vsize):
+    """VECTOR_SIZE (bundle size) is a compile-time constant of the reference
+    (64 by default); the build takes it from the context's configuration.
+    Top nodes, every tree field and Tree_Parent at smaller bundle sizes equal
+    the oracle's build with the same VECTOR_SIZE, and the tree passes the
+    node audit."""
+    p, origin, size = make_case(kind, n)
+    ft = port.ftype(fsize)
+    pos_f = p.pos.astype(ft)
+    std, rev = port.peano_keys(pos_f, origin, size, fsize)
+    perm_o = port.sort_keys(std)
+    pos_s, mass_s = pos_f[:, perm_o], p.mass.astype(ft)[perm_o]
+    top_o = port.top_nodes(std[perm_o], pos_s, origin, size, fsize)
+    tree_o, top_o, parent_o = port.tree_build(rev[perm_o], pos_s, mass_s, size, top_o, fsize,
+                                              vector_size=vsize)
+    with make_ctx(p.n, fsize, box=p.box, softening=p.softening, vector_size=vsize) as ctx:
+        perm, keys, tree, top = gpu_pipeline(ctx, p.pos, p.mass, origin, size, exact=True)
+        parent = ctx.download(G.F_TREE_PARENT)["tree_parent"]
+    assert np.array_equal(perm, perm_o)
+    assert_struct_equal(top, top_o, TOP_FIELDS, "topnodes")
+    assert_struct_equal(tree, tree_o, TREE_FIELDS, "tree")
+    assert np.array_equal(parent, parent_o)
+    audit(tree, top, pos_s, mass_s, size, fsize, vector_size=vsize)
 
 
 @pytest.mark.parametrize("kind,fsize,n,exact", [("zeldovich", 4, 128 ** 3, True),

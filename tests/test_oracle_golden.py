@@ -9,7 +9,8 @@ import port
 from pipeline import oracle_pipeline, oracle_ewald_tables, assert_struct_equal
 from tree_audit import audit
 
-FORCE_CASES = ["hernquist_iso_f64", "hernquist_iso_f32", "box_per_f32", "zeldovich_per_f64"]
+FORCE_CASES = ["hernquist_iso_f64", "hernquist_iso_f32", "box_per_f32", "zeldovich_per_f64",
+               "box_per_f32_v32", "hernquist_iso_f64_v16"]
 TREE_FIELDS = ["DNext", "Bitfield", "DUp", "Npart", "Pos", "Mass", "CoM", "Dp"]
 TOP_FIELDS = ["Key", "Target", "Level", "First_Part", "Npart", "Pos", "Mass", "CoM"]
 
@@ -49,9 +50,10 @@ def test_pipeline_matches_reference(golden_dir, case, ewald_cache):
         if key not in ewald_cache:
             ewald_cache[key] = oracle_ewald_tables(fsize, box)
         ew = ewald_cache[key]
+    vsize = int(g["vector_size"]) if "vector_size" in g.files else 64
     o = oracle_pipeline(g["pos_in"], g["mass_in"], g["domain_origin"], float(g["domain_size"][0]),
                         fsize, box=box, softening=float(g["softening"]),
-                        gravity=float(g["gravity"][0]), ewald=ew)
+                        gravity=float(g["gravity"][0]), ewald=ew, vector_size=vsize)
     assert np.array_equal(o["perm"], g["perm"])
     assert np.array_equal(o["std_key"], g["std_key"])
     assert np.array_equal(o["rev_key"], g["rev_key"])
@@ -144,7 +146,8 @@ def test_tree_audit_on_reference_trees(golden_dir, case):
     pos = g["pos_in"].astype(ft)[:, g["perm"]]
     mass = g["mass_in"].astype(ft)[g["perm"]]
     size = float(g["domain_size"][0])
-    audit(g["tree"], g["topnodes"], pos, mass, size, fsize)
+    vsize = int(g["vector_size"]) if "vector_size" in g.files else 64
+    audit(g["tree"], g["topnodes"], pos, mass, size, fsize, vector_size=vsize)
     i = np.flatnonzero(g["tree"]["DNext"] > 0)[3]
     for field, k, delta in (("Npart", None, 1), ("DNext", None, 1), ("CoM", 0, 0.05 * size),
                             ("Pos", 1, 1e-4 * size)):
@@ -154,7 +157,7 @@ def test_tree_audit_on_reference_trees(golden_dir, case):
         else:
             bad[field][i + 1, k] += delta
         with pytest.raises(AssertionError):
-            audit(bad, g["topnodes"], pos, mass, size, fsize)
+            audit(bad, g["topnodes"], pos, mass, size, fsize, vector_size=vsize)
 
 
 @pytest.mark.parametrize("case", ["hernquist_iso_f32", "hernquist_iso_f64"])
