@@ -426,7 +426,8 @@ def workload_config(args, p, ws):
                            "learned correction runs the same step in learned_ewald"),
         "ewald": (f"group form: per-group Ewald walk, Taylor table of the lattice sum (33^3 nodes, "
                   f"third order; K, dK, d2K at node centres of mass, second-order expansion about "
-                  f"the group centre plus the exact uniform-cube remainder), opening "
+                  f"the group centre plus the uniform-cube remainder, a degree-7 fit of its closed "
+                  f"form), opening "
                   f"alpha_E {args.ewald_alpha:g}; plain form: the reference's Ewald walk, 65^3 "
                   f"table, trilinear"),
         "form": ("group: warp per PH group of 32 x (targets per lane, autotuned) particles, FP32 on "
