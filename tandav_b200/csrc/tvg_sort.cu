@@ -205,26 +205,32 @@ k_radix_scatter(int64_t n, int shift, const uint64_t *__restrict__ kin,
 	}
 }
 
-// order runs of equal key_hi by the low key word (stable)
-__global__ void k_fix_ties(int64_t n, const uint64_t *__restrict__ hi, const uint64_t *__restrict__ lo_orig,
-                           uint32_t *__restrict__ perm)
+// Orders runs of equal key_hi by the low key word, stably (the radix passes
+// sort the high words only): out = perm with each run reordered. Every
+// element of a run finds the run's ends and its rank by one pass over the run,
+// in parallel, so a run of r equal high words costs O(r) time on r threads;
+// elements outside runs are copied.
+__global__ void k_tie_rank(int64_t n, const uint64_t *__restrict__ hi, const uint64_t *__restrict__ lo_orig,
+                           const uint32_t *__restrict__ perm, uint32_t *__restrict__ out)
 {
-	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (i >= n - 1) return;
-	if (hi[i] != hi[i + 1]) return;
-	if (i > 0 && hi[i - 1] == hi[i]) return;      // not the first of the run
-	int64_t e = i + 1;
-	while (e < n && hi[e] == hi[i]) e++;
-	for (int64_t a = i + 1; a < e; a++) {
-		uint32_t pv = perm[a];
-		uint64_t kv = lo_orig[pv];
-		int64_t b = a - 1;
-		while (b >= i && lo_orig[perm[b]] > kv) {
-			perm[b + 1] = perm[b];
-			b--;
-		}
-		perm[b + 1] = pv;
+	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint64_t h = hi[i];
+	const uint32_t pv = perm[i];
+	if (!((i > 0 && hi[i - 1] == h) || (i + 1 < n && hi[i + 1] == h))) {
+		out[i] = pv;
+		return;
 	}
+	int64_t a = i, e = i + 1;
+	while (a > 0 && hi[a - 1] == h) a--;
+	while (e < n && hi[e] == h) e++;
+	const uint64_t kv = lo_orig[pv];
+	int64_t r = 0;
+	for (int64_t j = a; j < e; j++) {
+		const uint64_t kj = lo_orig[perm[j]];
+		r += (kj < kv || (kj == kv && j < i)) ? 1 : 0;
+	}
+	out[a + r] = pv;
 }
 
 __global__ void k_gather_u64(int64_t n, const uint32_t *__restrict__ perm, const uint64_t *__restrict__ in,
@@ -336,8 +342,9 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 		uint32_t *vt = vin; vin = vout; vout = vt;
 	}
 	ctx->key_hi = kin; ctx->key_tmp = kout;
-	ctx->perm = vin; ctx->perm_tmp = vout;
-	k_fix_ties<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->key_hi, ctx->key_lo, ctx->perm);
+	// runs of equal high words by the low words, into the other buffer
+	k_tie_rank<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, kin, ctx->key_lo, vin, vout);
+	ctx->perm = vout; ctx->perm_tmp = vin;
 	k_gather_u64<<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, ctx->perm, ctx->key_lo, ctx->key_tmp);
 	{ uint64_t *t = ctx->key_lo; ctx->key_lo = ctx->key_tmp; ctx->key_tmp = t; }
 	GatherList g;
@@ -425,12 +432,6 @@ __global__ void __launch_bounds__(1024) k_scan_small(const uint32_t *__restrict_
 	}
 }
 
-__global__ void k_copy_u32(int64_t n, const uint32_t *__restrict__ in, uint32_t *__restrict__ out)
-{
-	int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (i < n) out[i] = in[i];
-}
-
 // Device address of the scratch array, looked up once per device with that
 // device current (the host-side symbol is not a device address).
 static NoallocScratch *noalloc_scratch(int device)
@@ -477,8 +478,7 @@ extern "C" int tvg_sort_keys_noalloc(const uint64_t *key_hi, const uint64_t *key
 		kin = kout;
 		cur ^= 1;
 	}
-	k_fix_ties<<<tvg_blocks(n, 256), 256, 0, s>>>(n, kin, key_lo, S->idx[cur]);
-	k_copy_u32<<<tvg_blocks(n, 256), 256, 0, s>>>(n, S->idx[cur], perm);
+	k_tie_rank<<<tvg_blocks(n, 256), 256, 0, s>>>(n, kin, key_lo, S->idx[cur], perm);
 	cudaError_t e = cudaGetLastError();
 	if (e == cudaSuccess) e = cudaStreamSynchronize(s);
 	return e == cudaSuccess ? TVG_OK : TVG_E_CUDA;

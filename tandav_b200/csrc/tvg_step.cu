@@ -169,9 +169,9 @@ extern "C" int tvg_compute_acceleration(tvg_context *ctx, int32_t form, uint32_t
 //
 // The step's launch sequence has no host round trip (every count stays on the
 // device), so it is captured once and replayed. Captured kernels keep the
-// buffer pointers they were given; the sort leaves the particle fields and
-// the low key words in the other buffer of their pair (and the radix passes,
-// always eight, leave the high words and the permutation where they were), so
+// buffer pointers they were given; the sort leaves the particle fields, the
+// low key words and the permutation in the other buffer of their pair (and
+// the radix passes, always eight, leave the high words where they were), so
 // the buffers alternate between two states from step to step. One graph is
 // kept per state, with the pointer set it starts from and the one it leaves.
 

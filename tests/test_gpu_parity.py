@@ -426,6 +426,33 @@ def test_ewald_table_vs_oracle(fsize):
         assert err.max() <= tol, f"{name}: max err {err.max()} > {tol}"
 
 
+def test_sort_long_runs_of_equal_high_key_words():
+    """Particles packed into cells of the 21st level share the high 64 bits of
+    their Peano-Hilbert keys: the radix passes leave such runs (here of 20000,
+    5000 and 300 particles) in input order, and the tie pass orders each by
+    the low words. The permutation is the oracle's full 128-bit sort."""
+    rng = np.random.default_rng(17)
+    L = 1.0
+    pos = [rng.uniform(0, L, (3, 150000))]
+    for n_run in (20000, 5000, 300):
+        cell = L / 2 ** 21
+        corner = np.floor(rng.uniform(0.1, 0.9, 3) / cell) * cell
+        pos.append(corner[:, None] + rng.uniform(0.1, 0.9, (3, n_run)) * cell)
+    pos = np.concatenate(pos, axis=1)
+    n = pos.shape[1]
+    std, _ = port.peano_keys(pos, (0.0, 0.0, 0.0), L, 8)
+    perm_o = port.sort_keys(std)
+    assert len(np.unique(std[:, 0])) < n - 25000            # the runs are there
+    with make_ctx(n, 8) as ctx:
+        ctx.upload(pos, np.ones(n))
+        ctx.set_domain((0.0, 0.0, 0.0), L)
+        ctx.peano_keys()
+        perm = ctx.sort_particles()
+        keys = ctx.download(G.F_KEY)["key"]
+    assert np.array_equal(perm, perm_o)
+    assert np.array_equal(keys, std[perm_o])
+
+
 def test_coincident_particles_reported():
     # enough particles that every top node gets a subtree (> 64 particles)
     p = ics.random_box(20000, box=100.0, seed=3)

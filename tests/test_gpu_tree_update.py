@@ -74,8 +74,12 @@ def _assert_tree(ctx, expected, what):
     assert_struct_equal(top, expected[1], TOP_FIELDS, f"top nodes {what}")
 
 
-@pytest.mark.parametrize("kind,fsize", [("hernquist", 4), ("hernquist", 8), ("clumps", 4)])
-def test_tree_updates_in_the_step_loop(kind, fsize):
+@pytest.mark.parametrize("kind,fsize,flags", [("hernquist", 4, 0), ("hernquist", 8, 0), ("clumps", 4, 0),
+                                              ("hernquist", 4, G.CFG_QUADRUPOLE)])
+def test_tree_updates_in_the_step_loop(kind, fsize, flags):
+    # (flags: with TVG_CFG_QUADRUPOLE the group form's node quadrupoles are
+    # summed again from the drifted particles of the kept tree; the plain
+    # form is unaffected)
     p, origin, size, timeline = _case(kind)
     ft = port.ftype(fsize)
     n = p.n
@@ -84,7 +88,7 @@ def test_tree_updates_in_the_step_loop(kind, fsize):
     group_check = fsize == 4 and p.box == 0
     seen = dict(kick=0, drift=0, walk=0, group=0)
     with G.GravityContext(n, float_bytes=fsize, periodic=p.box > 0, boxsize=p.box,
-                          softening=p.softening) as ctx:
+                          softening=p.softening, flags=flags) as ctx:
         ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32),
                    time_bin=np.zeros(n, np.int32), it_drift=np.zeros(n, np.uint32),
                    it_kick=np.zeros(n, np.uint32))
