@@ -77,13 +77,15 @@
 #define GW_ROOTS 256        // top nodes pushed at a time
 #define GW_ELIST 64
 #define GW_DEFAULT_TPL 2
-// resident blocks per SM the Ewald walk is compiled for; capping its
-// registers for 3 or 4 blocks made it slower, with the tricubic lookup
-// (1340, 1442 ms against 1252 ms per step at 256^3) and with the Taylor table
-// (3 blocks at 168 registers: 140.4 against 136.9 ms at 128^3): the loads in
-// flight need the registers more than the SM needs the warps
+// resident blocks per SM the table-evaluating Ewald walk is compiled for:
+// 3 (168 registers) since the uniform remainder is a polynomial (15.8 against
+// 18.4 ms per step at 256^3 with 2 blocks of 206 registers). Before that,
+// capping the registers had made it slower, with the tricubic lookup (1340,
+// 1442 ms against 1252 ms per step) and with the Taylor table and the closed
+// form (140.4 against 136.9 ms at 128^3). The learned correction's walk keeps
+// 1 (its network needs the registers).
 #ifndef GW_EWALD_MINB
-#define GW_EWALD_MINB 1
+#define GW_EWALD_MINB 3
 #endif
 // resident blocks per SM the gravity walk is compiled for (4: at most 128
 // registers; unbounded it took 138 and ran 3 blocks, 8 % slower), and the
@@ -712,7 +714,9 @@ __device__ __forceinline__ void flush_quad(QuadList &Q, int nq, Target (&t)[TPL]
 		my[k] = make_float2(-t[k].ty, -t[k].ty);
 		mz[k] = make_float2(-t[k].tz, -t[k].tz);
 	}
-#pragma unroll 1
+	// two source pairs per iteration: four independent chains per lane
+	// (150.7 against 152.7 ms per 256^3 step with one pair)
+#pragma unroll 2
 	for (int q = 0; q < np; q++) {
 		const float4 a = Q.xy[q], b = Q.zw[q], qa = Q.qa[q], qb = Q.qb[q], qc = Q.qc[q];
 		const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w),
@@ -1565,7 +1569,7 @@ __device__ void ewald_group(const GroupParams &p, EwaldSmem &S, const tvg_wnode 
 }
 
 template <int TPL, bool MLP, typename F>
-__global__ void __launch_bounds__(GE_THREADS, GW_EWALD_MINB)
+__global__ void __launch_bounds__(GE_THREADS, MLP ? 1 : GW_EWALD_MINB)
 k_ewald_group(GroupParams p, const int32_t *__restrict__ active, const int32_t *__restrict__ gfirst,
               const tvg_wnode *__restrict__ wt,
               const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy,

@@ -55,8 +55,8 @@ def test_graph_step_equals_direct_step(flags):
         graph.close()
 
 
-def _loop_ctx(p):
-    ctx = _ctx(p)
+def _loop_ctx(p, flags=0):
+    ctx = _ctx(p, flags)
     n = p.n
     ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32), time_bin=np.zeros(n, np.int32),
                it_drift=np.zeros(n, np.uint32), it_kick=np.zeros(n, np.uint32))
@@ -68,9 +68,10 @@ def _loop_ctx(p):
     return ctx
 
 
-def test_graph_step_in_the_step_loop():
+@pytest.mark.parametrize("flags", [0, G.CFG_QUADRUPOLE])
+def test_graph_step_in_the_step_loop(flags):
     p = ics.zeldovich_box(n_side=32, seed=42)
-    direct, graph = _loop_ctx(p), _loop_ctx(p)
+    direct, graph = _loop_ctx(p, flags), _loop_ctx(p, flags)
     try:
         actives = set()
         for _ in range(8):
