@@ -130,11 +130,13 @@ def test_quadrupole_accuracy(kind, fsize):
             assert rms_q < rms_m
 
 
-def _periodic_walk(p, flags, open_rel, ewald_alpha, tgt):
+def _periodic_walk(p, flags, open_rel, ewald_alpha, tgt, ntask=1, cost=None, tops=None):
     parts = G.WALK_GRAVITY | G.WALK_EWALD
     with G.GravityContext(p.n, float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
                           flags=flags) as ctx:
-        ctx.upload(p.pos, p.mass)
+        if ntask > 1:
+            ctx.set_domain_decomposition(ntask)
+        ctx.upload(p.pos, p.mass, cost=cost)
         ctx.set_domain((0.0, 0.0, 0.0), p.box)
         ctx.ewald_init()
         ctx.set_ewald_opening(ewald_alpha)
@@ -143,6 +145,8 @@ def _periodic_walk(p, flags, open_rel, ewald_alpha, tgt):
         ctx.set_opening(0.25, open_rel)
         ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
         counts = ctx.walk_counters() + (ctx.walk_quad_interactions(),)
+        if tops is not None:
+            tops.append(len(ctx.download_tree()[1]))
         ids = ctx.download(G.F_ID)["id"]
         inv = np.empty(p.n, np.int64)
         inv[ids] = np.arange(p.n)
@@ -249,3 +253,47 @@ def test_autotune_on_a_sample_leaves_the_active_set_and_the_chosen_walk():
             again = again["grav_acc"]
             sel = np.arange(p.n) if active is None else active
             assert np.all(np.abs(again[:, sel]).sum(0) > 0)
+
+
+def test_quadrupole_with_many_top_nodes():
+    """A cost-balanced decomposition over 8 targets gives a clumped box
+    hundreds of top nodes, which the walks push in chunks of 256; their
+    quadrupoles come from the top nodes' own particle ranges. With the same
+    |a_old| (from one Barnes-Hut pass) the relative walk's force error
+    against the FP64 direct Ewald sum stays that of the default top nodes."""
+    p = ics.random_box(1 << 17, box=1000.0, seed=45, clumps=11)
+    h = np.arange(p.n, dtype=np.uint64) * 2654435761
+    cost = np.where(p.pos[0] < 120.0, 50000 - (h % 1000), h % 100 + 1).astype(np.float64)
+    tgt = np.random.default_rng(7).choice(p.n, 3000, replace=False)
+    parts = G.WALK_GRAVITY | G.WALK_EWALD
+    kw = dict(float_bytes=4, periodic=True, boxsize=p.box, softening=p.softening,
+              flags=G.CFG_QUADRUPOLE)
+    with G.GravityContext(p.n, **kw) as ctx:
+        ctx.upload(p.pos, p.mass)
+        ctx.set_domain((0.0, 0.0, 0.0), p.box)
+        ctx.force_step(form=G.FORM_GROUP, use_bh=True, parts=parts)
+        d = ctx.download(G.F_GRAV_ACC | G.F_ID)
+    last = np.empty(p.n)
+    last[d["id"]] = np.sqrt((d["grav_acc"].astype(np.float64) ** 2).sum(0))
+    out = []
+    for ntask in (1, 8):
+        with G.GravityContext(p.n, **kw) as ctx:
+            if ntask > 1:
+                ctx.set_domain_decomposition(ntask)
+            ctx.upload(p.pos, p.mass, cost=cost, last_acc=last)
+            ctx.set_domain((0.0, 0.0, 0.0), p.box)
+            ctx.set_opening(0.25, 8e-3)
+            ctx.set_ewald_opening(1e-2)
+            ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
+            q = ctx.walk_quad_interactions()
+            ntop = len(ctx.download_tree()[1])
+            ids = ctx.download(G.F_ID)["id"]
+            inv = np.empty(p.n, np.int64)
+            inv[ids] = np.arange(p.n)
+            _, _, err = ctx.forcetest(np.sort(inv[tgt]))
+        out.append((ntop, err["rms"], q))
+    print(f"top nodes, rms, quadrupole interactions per particle: "
+          f"{[(t, f'{e:.3e}', round(q / p.n)) for t, e, q in out]}")
+    (t1, e1, _), (t8, e8, q8) = out
+    assert t8 > 256 and t8 > 4 * t1 and q8 > 0
+    assert e8 < 1.3 * e1 and e8 < 2e-3
