@@ -271,47 +271,45 @@ __global__ void k_wt_small_top(const tvg_devcount *__restrict__ dc, const tvg_to
 // TVG_CFG_QUADRUPOLE: G times the traceless quadrupole moment of every walk
 // node about its centre of mass (the integer one of its record),
 // Q_ab = sum m (3 y_a y_b - |y|^2 delta_ab), summed in FP64 over the node's
-// particles, one warp per node, stored negated: wq[2w] = -(Qxx, Qyy, Qzz,
-// Qxy), wq[2w + 1] = -(Qxz, Qyz, 0, 0).
-__device__ __forceinline__ void wt_quad_one(int64_t w, int lane, const tvg_wnode *__restrict__ wt,
-                                            const int2 *__restrict__ wrange, const uint32_t *__restrict__ ix,
-                                            const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
-                                            const float *__restrict__ mass_f, double scale, double gravity,
-                                            float4 *__restrict__ wq)
+// particles, stored negated: wq[2w] = -(Qxx, Qyy, Qzz, Qxy),
+// wq[2w + 1] = -(Qxz, Qyz, 0, 0).
+struct QuadSums {
+	double xx, yy, zz, xy, xz, yz;
+};
+
+__device__ __forceinline__ void quad_add(QuadSums &q, const uint32_t *__restrict__ ix,
+                                         const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
+                                         const float *__restrict__ mass_f, int64_t j, uint32_t cx,
+                                         uint32_t cy, uint32_t cz, double scale)
 {
-	const int2 r = wrange[w];
-	if (r.y <= 0) return;
-	const uint32_t cx = wt[w].cx, cy = wt[w].cy, cz = wt[w].cz;
-	double sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-	for (int64_t j = r.x + lane; j < (int64_t) r.x + r.y; j += 32) {
-		const double m = (double) mass_f[j];
-		const double x = (double) (int) (ix[j] - cx) * scale, y = (double) (int) (iy[j] - cy) * scale,
-		             z = (double) (int) (iz[j] - cz) * scale;
-		sxx += m * x * x;
-		syy += m * y * y;
-		szz += m * z * z;
-		sxy += m * x * y;
-		sxz += m * x * z;
-		syz += m * y * z;
-	}
-#pragma unroll
-	for (int o = 16; o; o >>= 1) {
-		sxx += __shfl_xor_sync(0xFFFFFFFFu, sxx, o);
-		syy += __shfl_xor_sync(0xFFFFFFFFu, syy, o);
-		szz += __shfl_xor_sync(0xFFFFFFFFu, szz, o);
-		sxy += __shfl_xor_sync(0xFFFFFFFFu, sxy, o);
-		sxz += __shfl_xor_sync(0xFFFFFFFFu, sxz, o);
-		syz += __shfl_xor_sync(0xFFFFFFFFu, syz, o);
-	}
-	if (lane == 0) {
-		const double tr = sxx + syy + szz, g = -gravity;
-		wq[2 * w] = make_float4((float) (g * (3 * sxx - tr)), (float) (g * (3 * syy - tr)),
-		                        (float) (g * (3 * szz - tr)), (float) (g * 3 * sxy));
-		wq[2 * w + 1] = make_float4((float) (g * 3 * sxz), (float) (g * 3 * syz), 0.f, 0.f);
-	}
+	const double m = (double) mass_f[j];
+	const double x = (double) (int) (ix[j] - cx) * scale, y = (double) (int) (iy[j] - cy) * scale,
+	             z = (double) (int) (iz[j] - cz) * scale;
+	q.xx += m * x * x;
+	q.yy += m * y * y;
+	q.zz += m * z * z;
+	q.xy += m * x * y;
+	q.xz += m * x * z;
+	q.yz += m * y * z;
 }
 
-// every walk node (top nodes + the walk nodes below them, counted on the device)
+__device__ __forceinline__ void quad_store(const QuadSums &q, double gravity, float4 *__restrict__ wq,
+                                           int64_t w)
+{
+	const double tr = q.xx + q.yy + q.zz, g = -gravity;
+	wq[2 * w] = make_float4((float) (g * (3 * q.xx - tr)), (float) (g * (3 * q.yy - tr)),
+	                        (float) (g * (3 * q.zz - tr)), (float) (g * 3 * q.xy));
+	wq[2 * w + 1] = make_float4((float) (g * 3 * q.xz), (float) (g * 3 * q.yz), 0.f, 0.f);
+}
+
+// Every walk node (top nodes + the walk nodes below them, counted on the
+// device), in two passes: a lane sums a node of at most GW_QUAD_LANE
+// particles by itself (most nodes: bundles and the levels just above them),
+// 32 consecutive nodes to a warp; then each larger node takes a warp of its
+// own with a butterfly reduction. (Larger nodes come in runs, the top levels
+// first, so a warp of 32 consecutive nodes summing its large ones in turn
+// would leave one warp with the top nodes: 75 ms per 256^3 step.)
+#define GW_QUAD_LANE 64
 __global__ void k_wt_quad_dev(const tvg_devcount *__restrict__ dc, const tvg_wnode *__restrict__ wt,
                               const int2 *__restrict__ wrange, const uint32_t *__restrict__ ix,
                               const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
@@ -320,9 +318,35 @@ __global__ void k_wt_quad_dev(const tvg_devcount *__restrict__ dc, const tvg_wno
 {
 	const int64_t nw = (int64_t) dc->ntop + dc->nwchild;
 	const int lane = threadIdx.x & 31;
-	for (int64_t w = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5; w < nw;
-	     w += ((int64_t) gridDim.x * blockDim.x) >> 5)
-		wt_quad_one(w, lane, wt, wrange, ix, iy, iz, mass_f, scale, gravity, wq);
+	const int64_t warp = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5;
+	const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
+	for (int64_t w = warp * 32 + lane; w - lane < nw; w += nwarps * 32) {
+		if (w >= nw) continue;
+		const int2 r = wrange[w];
+		if (r.y <= 0 || r.y > GW_QUAD_LANE) continue;
+		QuadSums q = { 0, 0, 0, 0, 0, 0 };
+		const uint32_t cx = wt[w].cx, cy = wt[w].cy, cz = wt[w].cz;
+		for (int64_t j = r.x; j < (int64_t) r.x + r.y; j++) quad_add(q, ix, iy, iz, mass_f, j, cx, cy, cz, scale);
+		quad_store(q, gravity, wq, w);
+	}
+	for (int64_t w = warp; w < nw; w += nwarps) {
+		const int2 r = wrange[w];
+		if (r.y <= GW_QUAD_LANE) continue;
+		const uint32_t cx = wt[w].cx, cy = wt[w].cy, cz = wt[w].cz;
+		QuadSums q = { 0, 0, 0, 0, 0, 0 };
+		for (int64_t j = r.x + lane; j < (int64_t) r.x + r.y; j += 32)
+			quad_add(q, ix, iy, iz, mass_f, j, cx, cy, cz, scale);
+#pragma unroll
+		for (int o = 16; o; o >>= 1) {
+			q.xx += __shfl_xor_sync(0xFFFFFFFFu, q.xx, o);
+			q.yy += __shfl_xor_sync(0xFFFFFFFFu, q.yy, o);
+			q.zz += __shfl_xor_sync(0xFFFFFFFFu, q.zz, o);
+			q.xy += __shfl_xor_sync(0xFFFFFFFFu, q.xy, o);
+			q.xz += __shfl_xor_sync(0xFFFFFFFFu, q.xz, o);
+			q.yz += __shfl_xor_sync(0xFFFFFFFFu, q.yz, o);
+		}
+		if (lane == 0) quad_store(q, gravity, wq, w);
+	}
 }
 
 
