@@ -72,3 +72,19 @@ def test_noalloc_rejects_oversized_input():
     rc = tandav_b200.lib().tvg_sort_keys_noalloc(C.c_void_p(buf.data_ptr()), C.c_void_p(buf.data_ptr()),
                                                  C.c_int64(MAX_KEYS + 1), C.c_void_p(buf.data_ptr()))
     assert rc == 5                                    # TVG_E_BADINPUT
+
+
+def test_noalloc_sort_orders_long_runs_of_equal_high_words():
+    """Keys whose high words repeat in runs of thousands (particles packed in
+    one cell of the 21st level share them): each run comes out ordered by the
+    low word and stable for equal keys, as numpy's lexicographic sort gives."""
+    rng = np.random.default_rng(43)
+    n = 200000
+    hi = rng.integers(0, 2 ** 63, size=n, dtype=np.uint64)
+    runs = rng.choice(n, 30000, replace=False)
+    hi[runs] = rng.choice(np.array([3, 17, 2 ** 40 + 5, 2 ** 62 + 1], dtype=np.uint64), size=len(runs),
+                          p=[0.5, 0.3, 0.15, 0.05])
+    lo = rng.integers(0, 2 ** 20, size=n, dtype=np.uint64)   # with repeats
+    keys = np.stack([hi, lo], axis=1)
+    perm, _, _ = noalloc_perm(keys)
+    assert np.array_equal(perm, np.lexsort((lo, hi)).astype(np.uint32))
