@@ -326,20 +326,79 @@ __global__ void k_bin_hist(int64_t n, const int32_t *__restrict__ bin, int32_t *
 }
 
 // per-type sums of |v|^2 (Float squares summed in Float, added in FP64),
-// minimum mass and count (Comoving_VelDisp_Timestep_Constraint, comoving.c:195-223)
+// minimum mass and count (Comoving_VelDisp_Timestep_Constraint, comoving.c:195-223).
+// Like the reference's per-thread partial sums, each thread sums its
+// particles in registers; the warp and then the block combine them, and one
+// atomic per block and type adds the block's share (one atomic per particle
+// on six addresses serialises: 43 ms at 256^3). The FP64 sum's order is not
+// the reference's either way (its threads' partial sums meet in a critical
+// section in any order).
+#define VD_THREADS 256
 template <typename F>
-__global__ void k_veldisp(int64_t n, const int32_t *__restrict__ type, const F *v0, const F *v1,
-                          const F *v2, const F *mass, double *vel2, uint32_t *min_mass_bits,
-                          unsigned long long *npart)
+__global__ void __launch_bounds__(VD_THREADS) k_veldisp(int64_t n, const int32_t *__restrict__ type,
+                                                        const F *__restrict__ v0, const F *__restrict__ v1,
+                                                        const F *__restrict__ v2, const F *__restrict__ mass,
+                                                        double *vel2, uint32_t *min_mass_bits,
+                                                        unsigned long long *npart)
 {
-	const int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (i >= n) return;
-	const int t = type[i];
-	if (t < 0 || t >= 6) return;
-	const F a = v0[i], b = v1[i], c = v2[i];
-	atomicAdd(&vel2[t], (double) (a * a + b * b + c * c));
-	atomicMin(&min_mass_bits[t], __float_as_uint((float) mass[i]));     // masses > 0
-	atomicAdd(&npart[t], 1ull);
+	__shared__ double s_v[VD_THREADS / 32][6];
+	__shared__ uint32_t s_m[VD_THREADS / 32][6];
+	__shared__ unsigned long long s_n[VD_THREADS / 32][6];
+	double sv[6];
+	uint32_t sm[6];
+	unsigned long long sn[6];
+#pragma unroll
+	for (int t = 0; t < 6; t++) {
+		sv[t] = 0.0;
+		sm[t] = 0xFFFFFFFFu;
+		sn[t] = 0ull;
+	}
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n;
+	     i += (int64_t) gridDim.x * blockDim.x) {
+		const int ty = type[i];
+		const F a = v0[i], b = v1[i], c = v2[i];
+		const double q = (double) (a * a + b * b + c * c);
+		const uint32_t m = __float_as_uint((float) mass[i]);     // masses > 0
+#pragma unroll
+		for (int t = 0; t < 6; t++)
+			if (ty == t) {
+				sv[t] += q;
+				sm[t] = min(sm[t], m);
+				sn[t] += 1ull;
+			}
+	}
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+	for (int t = 0; t < 6; t++) {
+#pragma unroll
+		for (int o = 16; o; o >>= 1) {
+			sv[t] += __shfl_xor_sync(0xFFFFFFFFu, sv[t], o);
+			sm[t] = min(sm[t], __shfl_xor_sync(0xFFFFFFFFu, sm[t], o));
+			sn[t] += __shfl_xor_sync(0xFFFFFFFFu, sn[t], o);
+		}
+		if (lane == 0) {
+			s_v[w][t] = sv[t];
+			s_m[w][t] = sm[t];
+			s_n[w][t] = sn[t];
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x < 6) {
+		const int t = threadIdx.x;
+		double v = 0.0;
+		uint32_t m = 0xFFFFFFFFu;
+		unsigned long long c = 0ull;
+		for (int k = 0; k < VD_THREADS / 32; k++) {
+			v += s_v[k][t];
+			m = min(m, s_m[k][t]);
+			c += s_n[k][t];
+		}
+		if (c) {
+			atomicAdd(&vel2[t], v);
+			atomicMin(&min_mass_bits[t], m);
+			atomicAdd(&npart[t], c);
+		}
+	}
 }
 
 // Make_Active_Particle_List (timestep.c:280-299): flags, scan, scatter
@@ -549,7 +608,8 @@ static int velocity_constraint(tvg_context *ctx, double *dt_out)
 	TVG_CUDA(ctx, cudaMemsetAsync(mmin, 0x7F, 24, s));
 	TVG_CUDA(ctx, cudaMemsetAsync(np, 0, 48, s));
 	const int64_t n = ctx->n;
-	k_veldisp<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(
+	const unsigned nb = tvg_blocks(n, VD_THREADS * 8) < 148u * 8u ? tvg_blocks(n, VD_THREADS * 8) : 148u * 8u;
+	k_veldisp<F><<<TVG_CNT(ctx, nb), VD_THREADS, 0, s>>>(
 	    n, (const int32_t *) ctx->f[FS_TYPE], (const F *) ctx->f[FS_VEL0], (const F *) ctx->f[FS_VEL1],
 	    (const F *) ctx->f[FS_VEL2], (const F *) ctx->f[FS_MASS], vel2, mmin, np);
 	TVG_CUDA(ctx, cudaGetLastError());
