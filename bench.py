@@ -337,21 +337,34 @@ def rung_run(args, p, G, device):
             st = ctx.timeline()
             if st.current >= st.end:
                 break
+            # each phase in its own device-timed region (events on the
+            # library stream); the step's time is their sum
             ctx.timer_start()
             ctx.set_new_timesteps()
+            bins_ms = ctx.timer_stop()
             st = ctx.timeline()
+            ctx.timer_start()
             ctx.kick_first_halfstep()
+            kick1_ms = ctx.timer_stop()
+            ctx.timer_start()
             ctx.drift_to_sync_point()
+            drift_ms = ctx.timer_stop()
             rebuilt = ctx.time_for_domain_update(dup) if dup is not None else True
+            ctx.timer_start()
             ctx.step_graph(parts)              # Compute_Acceleration, one graph launch
+            force_ms = ctx.timer_stop()
+            ctx.timer_start()
             ctx.kick_second_halfstep()
-            ms = ctx.timer_stop()
+            kick2_ms = ctx.timer_stop()
+            ms = bins_ms + kick1_ms + drift_ms + force_ms + kick2_ms
             h = ctx.rung_histogram()
             ph = ctx.phase_times()
             g_i, e_i = ctx.walk_counters()
             steps.append({"a": round(st.time_current, 6), "n_active": int(st.n_active),
                           "max_active_bin": int(st.max_active_bin), "rebuilt": bool(rebuilt),
                           "ms": round(ms, 2),
+                          "timesteps_ms": round(bins_ms, 3), "kick_ms": round(kick1_ms + kick2_ms, 3),
+                          "drift_ms": round(drift_ms, 3), "force_ms": round(force_ms, 2),
                           "walk_ms": round(ph["walk"], 1), "ewald_ms": round(ph["ewald"], 1),
                           "interactions_per_active": round(g_i / max(st.n_active, 1)),
                           "ewald_evals_per_active": round(e_i / max(st.n_active, 1), 1),
@@ -359,6 +372,22 @@ def rung_run(args, p, G, device):
                           "rungs": {int(b): int(c) for b, c in enumerate(h) if c}})
         tot_ms = sum(s["ms"] for s in steps)
         tot_act = sum(s["n_active"] for s in steps)
+        # kick and drift against the copy bandwidth, over the steps that move
+        # every particle: 36 B per particle and kick or drift (Vel += dt Acc;
+        # Pos += dt Vel, FP32), the kernels' own traffic 48 B per kick (also
+        # Time_Bin and It_Kick_Pos) and 44 B per drift (It_Drift_Pos)
+        full = [s for s in steps if s["n_active"] == n and s["rebuilt"]]
+        hbm = None
+        if full:
+            k_ms = min(s["kick_ms"] for s in full) / 2.0
+            d_ms = min(s["drift_ms"] for s in full)
+            hbm = {"steps": len(full), "n_particles": n,
+                   "kick_ms": round(k_ms, 4), "drift_ms": round(d_ms, 4),
+                   "kick_gbs_algorithmic": round(36.0 * n / (k_ms * 1e6), 1),
+                   "drift_gbs_algorithmic": round(36.0 * n / (d_ms * 1e6), 1),
+                   "kick_gbs_touched": round(48.0 * n / (k_ms * 1e6), 1),
+                   "drift_gbs_touched": round(44.0 * n / (d_ms * 1e6), 1),
+                   "timing": "fastest full step; one half kick is half the step's two kicks"}
         return {"workload": f"zeldovich_{args.nside}^3 from z = 50, hierarchical steps, "
                             f"TimeIntAccuracy {args.time_int_accuracy}",
                 "tree": ("rebuilt every step" if dup is None else
@@ -367,6 +396,7 @@ def rung_run(args, p, G, device):
                 "steps": len(steps), "total_ms": round(tot_ms, 1),
                 "active_particles_per_s": round(tot_act / (tot_ms * 1e-3)) if tot_ms else None,
                 "rungs_populated_max": max(len(s["rungs"]) for s in steps) if steps else 0,
+                "kick_drift_hbm": hbm,
                 "per_step": steps}
     finally:
         ctx.close()
