@@ -181,16 +181,18 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
 	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
 	                 ctx->d_toptab, ctx->top_of, ctx->dd_scratch, ctx->tu_first, ctx->tu_dp,
-	                 ctx->tune_active, ctx->wquad, ctx->wrange };
+	                 ctx->tu_big, ctx->tune_active, ctx->wquad, ctx->wrange };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+	for (int i = 0; i < 3; i++) if (ctx->xev[i]) cudaEventDestroy(ctx->xev[i]);
+	if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
 	if (ctx->stream) cudaStreamDestroy(ctx->stream);
 	delete ctx;
 }
 
 // host field pointer for a slot
-static void *host_field(const tvg_particles *p, int slot)
+void *tvg_host_field(const tvg_particles *p, int slot)
 {
 	switch (slot) {
 	case FS_TYPE: return p->type;
@@ -211,7 +213,7 @@ static void *host_field(const tvg_particles *p, int slot)
 	return nullptr;
 }
 
-static uint32_t slot_bit(int slot)
+uint32_t tvg_slot_bit(int slot)
 {
 	switch (slot) {
 	case FS_TYPE: return TVG_F_TYPE;
@@ -252,8 +254,8 @@ extern "C" int tvg_upload(tvg_context *ctx, int64_t n, const tvg_particles *p, u
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	ctx->n = n;
 	for (int s = 0; s < FS_NFIELDS; s++) {
-		if (!(fields & slot_bit(s))) continue;
-		const void *h = host_field(p, s);
+		if (!(fields & tvg_slot_bit(s))) continue;
+		const void *h = tvg_host_field(p, s);
 		if (!h) return tvg_fail(ctx, TVG_E_BADINPUT, "upload: field slot %d is NULL", s);
 		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->f[s], h, tvg_field_bytes(ctx, s) * n,
 		                              cudaMemcpyHostToDevice, ctx->stream));
@@ -282,8 +284,8 @@ extern "C" int tvg_download(tvg_context *ctx, tvg_particles *p, uint32_t fields)
 	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	const int64_t n = ctx->n;
 	for (int s = 0; s < FS_NFIELDS; s++) {
-		if (!(fields & slot_bit(s))) continue;
-		void *h = host_field(p, s);
+		if (!(fields & tvg_slot_bit(s))) continue;
+		void *h = tvg_host_field(p, s);
 		if (!h) return tvg_fail(ctx, TVG_E_BADINPUT, "download: field slot %d is NULL", s);
 		TVG_CUDA(ctx, cudaMemcpyAsync(h, ctx->f[s], tvg_field_bytes(ctx, s) * n,
 		                              cudaMemcpyDeviceToHost, ctx->stream));

@@ -113,6 +113,13 @@ struct tvg_context {
 	int device = 0;
 	tvg_config cfg{};
 	cudaStream_t stream = nullptr;
+	// tvg_force_step_host: copies that overlap the step's kernels, and the
+	// events that order them against the context stream (created on first use)
+	cudaStream_t copy_stream = nullptr;
+	cudaEvent_t xev[3] = { nullptr, nullptr, nullptr };
+	// when set, the sort's field gather waits for this event (inputs still
+	// uploading on copy_stream)
+	cudaEvent_t gather_wait = nullptr;
 	int64_t cap = 0;          // particle capacity
 	int64_t n = 0;            // active particle count
 	double origin[3] = { 0, 0, 0 };
@@ -226,6 +233,7 @@ struct tvg_context {
 	bool domain_update = true;         // Sig.Domain_Update (= Sig.Tree_Update)
 	int64_t npart_updates = 0;         // Local_NPart_Updates (signal.c:80)
 	int32_t *tu_first = nullptr;       // first particle of every tree node
+	int32_t *tu_big = nullptr;         // [0]: count, then the nodes the node kick leaves to a warp each
 	void *tu_dp = nullptr;             // dp of the active particles by slot, 3 x cap Float
 
 	// device-resident counts and top-node tables of the step
@@ -326,6 +334,10 @@ static inline size_t tvg_field_bytes(const tvg_context *ctx, int slot)
 		return tvg_fsize(ctx);
 	}
 }
+
+// host pointer of a field slot in a tvg_particles, and the TVG_F_* bit of a slot
+void *tvg_host_field(const tvg_particles *p, int slot);
+uint32_t tvg_slot_bit(int slot);
 
 static inline unsigned tvg_blocks(int64_t n, int threads)
 {

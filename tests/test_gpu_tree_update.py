@@ -146,3 +146,41 @@ def test_tree_updates_in_the_step_loop(kind, fsize, flags):
     print(seen)
     assert seen["kick"] >= 6 and seen["drift"] >= 3 and seen["walk"] >= 2
     assert seen["group"] == (1 if group_check else 0)
+
+
+@pytest.mark.parametrize("fsize", [4, 8])
+def test_tree_kick_of_every_particle(fsize):
+    """The first kick at a sync point that follows kept-tree steps adds every
+    particle's momentum to the kept tree (the reference decides on the domain
+    update only after that kick, main.c:49-67). There the top nodes and every
+    node with more than 128 active particles are summed by a warp each; the
+    tree must still equal the restatement bit for bit. A domain update
+    parameter too large to trigger keeps the tree until the sync point."""
+    p, origin, size, timeline = _case("hernquist")
+    n = p.n
+    with G.GravityContext(n, float_bytes=fsize, periodic=False, softening=p.softening) as ctx:
+        ctx.upload(p.pos, p.mass, vel=p.vel, types=np.ones(n, np.int32),
+                   time_bin=np.zeros(n, np.int32), it_drift=np.zeros(n, np.uint32),
+                   it_kick=np.zeros(n, np.uint32))
+        ctx.set_domain(origin, size)
+        ctx.timeline_init(**timeline)
+        ctx.compute_acceleration(form=G.FORM_PLAIN, parts=G.WALK_GRAVITY, prepare=True)
+        dom = ctx.time_for_domain_update(1e6)
+        kept = 0
+        for _ in range(600):
+            ctx.set_new_timesteps()
+            st = ctx.timeline()
+            if st.current >= st.end:
+                break
+            if not dom and st.n_active == n:
+                exp = _expected_kick(ctx, fsize)
+                ctx.kick_first_halfstep()
+                _assert_tree(ctx, exp, "after a kick of every particle")
+                return
+            ctx.kick_first_halfstep()
+            ctx.drift_to_sync_point()
+            dom = ctx.time_for_domain_update(1e6)
+            kept += int(not dom)
+            ctx.compute_acceleration(form=G.FORM_PLAIN, parts=G.WALK_GRAVITY)
+            ctx.kick_second_halfstep()
+    pytest.fail(f"no sync point after {kept} kept-tree steps")
