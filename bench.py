@@ -571,10 +571,10 @@ def main():
     dist.barrier()
     ctx.timer_start()
     for _ in range(args.steps):
-        ctx.upload_fields(n, pos=h_pos.array, mass=h_mass.array, last_acc=h_last.array,
-                          ids=h_ids.array)
-        ctx.force_step(form=G.FORM_GROUP, use_bh=False, parts=parts)
-        ctx.download_into(grav_acc=h_acc.array, ids=h_oid.array)
+        # tvg_force_step_host: the copies overlap the keys, sort and walks
+        ctx.force_step_host(n, h_pos.array, h_mass.array, last_acc=h_last.array, ids=h_ids.array,
+                            grav_acc=h_acc.array, ids_out=h_oid.array, form=G.FORM_GROUP,
+                            use_bh=False, parts=parts)
     e2e_ms = ctx.timer_stop()
     dist.barrier()
     t_e2e = dist.max(e2e_ms / args.steps) / 1e3

@@ -260,6 +260,20 @@ int tvg_zero_accel(tvg_context *ctx);
 int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
                    int32_t ewald_kind);
 
+/* tvg_force_step end to end from host buffers, for a host code whose
+ * particles live in host memory (the reference's P, Gravity_Tree_Acceleration
+ * after Domain_Decomposition, accel.c:15-71): uploads the `in_fields` of n
+ * particles (positions required), runs the same keys, sort, top nodes, build
+ * and walks, and downloads the `out_fields` (in the new PH order, like the
+ * reference's reordered P). The copies overlap the kernels: the positions go
+ * first, the other inputs while the keys and radix passes run (the field
+ * gather waits for them), and outputs that the walks do not write (ID, ...)
+ * while the walks run. Returns when `out` holds the results. Page-locked
+ * host memory (tvg_host_alloc / tvg_host_register) gives full copy speed. */
+int tvg_force_step_host(tvg_context *ctx, int64_t n, const tvg_particles *in, uint32_t in_fields,
+                        tvg_particles *out, uint32_t out_fields, int32_t form, int32_t use_bh,
+                        uint32_t parts, int32_t ewald_kind);
+
 /* Active_Particle_List / NActive_Particles (src/timestep.c:280-299): the walks
  * compute forces for these particles only (indices into the current, sorted
  * order, ascending). NULL selects all particles. Sorting resets it to all. */

@@ -21,7 +21,7 @@ EXPORTS = (
     "tvg_set_domain", "tvg_peano_keys", "tvg_sort_particles", "tvg_reverse_keys",
     "tvg_top_nodes", "tvg_set_domain_decomposition", "tvg_decomposition_rounds", "tvg_tree_build", "tvg_download_tree", "tvg_ewald_init",
     "tvg_download_ewald_table", "tvg_upload_ewald_table", "tvg_walk", "tvg_save_last_accel", "tvg_zero_accel",
-    "tvg_force_step", "tvg_phase_times", "tvg_walk_counters", "tvg_walk_quad_interactions", "tvg_set_active", "tvg_timer",
+    "tvg_force_step", "tvg_force_step_host", "tvg_phase_times", "tvg_walk_counters", "tvg_walk_quad_interactions", "tvg_set_active", "tvg_timer",
     "tvg_launch_count", "tvg_host_alloc", "tvg_host_free",
     "tvg_host_register", "tvg_host_unregister", "tvg_fp32_peak",
     "tvg_sort_keys_noalloc", "tvg_forcetest", "tvg_set_opening",

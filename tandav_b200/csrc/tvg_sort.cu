@@ -355,6 +355,7 @@ int tvg_impl_sort(tvg_context *ctx, uint32_t *perm_out)
 		g.bytes[g.nf] = (int) tvg_field_bytes(ctx, f);
 		g.nf++;
 	}
+	if (ctx->gather_wait) TVG_CUDA(ctx, cudaStreamWaitEvent(s, ctx->gather_wait, 0));
 	k_gather_fields<<<TVG_CNT(ctx, tvg_blocks((n + 3) / 4, 256)), 256, 0, s>>>(n, ctx->perm, g);
 	TVG_CUDA(ctx, cudaGetLastError());
 	for (int f = 0; f < FS_NFIELDS; f++) { void *t = ctx->f[f]; ctx->f[f] = ctx->falt[f]; ctx->falt[f] = t; }

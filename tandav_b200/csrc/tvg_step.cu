@@ -1,6 +1,7 @@
 // tvg_step.cu -- one tree-force evaluation on device-resident particles, with
-// per-phase CUDA-event timing on the context stream; and the same evaluation
-// captured as a CUDA graph (tvg_step_graph).
+// per-phase CUDA-event timing on the context stream; the same evaluation from
+// and to host buffers with the copies overlapped (tvg_force_step_host); and
+// the evaluation captured as a CUDA graph (tvg_step_graph).
 #include <string.h>
 
 #include "tvg_internal.cuh"
@@ -11,13 +12,12 @@ static bool find_domain_each_step(const tvg_context *ctx)
 	return (ctx->cfg.flags & TVG_CFG_FIND_DOMAIN) && !ctx->cfg.periodic;
 }
 
-extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
-                              int32_t ewald_kind)
+// keys, sort, top nodes, tree build and walks of one force step, enqueued on
+// the context stream between the phase events ev[8..13]; `sorted`, when set,
+// is recorded right after the sort
+static int force_phases(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts, int32_t ewald_kind,
+                        cudaEvent_t sorted)
 {
-	if (!ctx) return TVG_E_BADINPUT;
-	if (!ctx->have_domain && !find_domain_each_step(ctx))
-		return tvg_fail(ctx, TVG_E_STATE, "force_step: domain not set");
-	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
 	cudaStream_t s = ctx->stream;
 	cudaEvent_t *ev = ctx->ev;
 	if (find_domain_each_step(ctx)) {
@@ -31,6 +31,7 @@ extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, ui
 	TVG_CHECK(tvg_impl_sort(ctx, nullptr));
 	ctx->sorted = true;
 	ctx->use_active = false;
+	if (sorted) TVG_CUDA(ctx, cudaEventRecord(sorted, s));
 	TVG_CUDA(ctx, cudaEventRecord(ev[10], s));
 	TVG_CHECK(tvg_impl_top_nodes(ctx));
 	ctx->have_top = true;
@@ -50,7 +51,13 @@ extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, ui
 	else
 		TVG_CHECK(tvg_impl_walk_group(ctx, use_bh, parts, ewald_kind));
 	TVG_CUDA(ctx, cudaEventRecord(ev[13], s));
-	TVG_CUDA(ctx, cudaEventSynchronize(ev[13]));
+	return TVG_OK;
+}
+
+// the phase times of the last force step, once ev[13] has completed
+static int force_times(tvg_context *ctx)
+{
+	cudaEvent_t *ev = ctx->ev;
 	float ms[5];
 	TVG_CUDA(ctx, cudaEventElapsedTime(&ms[0], ev[8], ev[9]));
 	TVG_CUDA(ctx, cudaEventElapsedTime(&ms[1], ev[9], ev[10]));
@@ -62,7 +69,95 @@ extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, ui
 	ctx->phase_ms[2] = ms[2];
 	ctx->phase_ms[3] = ms[3];
 	ctx->phase_ms[6] = ms[4];
+	return TVG_OK;
+}
+
+extern "C" int tvg_force_step(tvg_context *ctx, int32_t form, int32_t use_bh, uint32_t parts,
+                              int32_t ewald_kind)
+{
+	if (!ctx) return TVG_E_BADINPUT;
+	if (!ctx->have_domain && !find_domain_each_step(ctx))
+		return tvg_fail(ctx, TVG_E_STATE, "force_step: domain not set");
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	TVG_CHECK(force_phases(ctx, form, use_bh, parts, ewald_kind, nullptr));
+	TVG_CUDA(ctx, cudaEventSynchronize(ctx->ev[13]));
+	TVG_CHECK(force_times(ctx));
 	return tvg_sync_status(ctx, "force_step");
+}
+
+// Fields that the steps after the sort never write: a force step from host
+// buffers downloads them while the walks run.
+static const uint32_t kWrittenByStep = TVG_F_ACC | TVG_F_GRAV_ACC | TVG_F_COST | TVG_F_TREE_PARENT
+                                     | TVG_F_GRAV_POT;
+
+extern "C" int tvg_force_step_host(tvg_context *ctx, int64_t n, const tvg_particles *in, uint32_t in_fields,
+                                   tvg_particles *out, uint32_t out_fields, int32_t form, int32_t use_bh,
+                                   uint32_t parts, int32_t ewald_kind)
+{
+	if (!ctx || !in || !out) return TVG_E_BADINPUT;
+	if (n < 0 || n > ctx->cap)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "force_step_host: n=%lld > capacity %lld", (long long) n,
+		                (long long) ctx->cap);
+	if (!(in_fields & TVG_F_POS)) return tvg_fail(ctx, TVG_E_BADINPUT, "force_step_host: positions are an input");
+	if ((in_fields | out_fields) & TVG_F_KEY)
+		return tvg_fail(ctx, TVG_E_BADINPUT, "force_step_host: keys are no field of this call");
+	if (!ctx->have_domain && !find_domain_each_step(ctx))
+		return tvg_fail(ctx, TVG_E_STATE, "force_step_host: domain not set");
+	for (int f = 0; f < FS_NFIELDS; f++) {
+		if ((in_fields & tvg_slot_bit(f)) && !tvg_host_field(in, f))
+			return tvg_fail(ctx, TVG_E_BADINPUT, "force_step_host: input field slot %d is NULL", f);
+		if ((out_fields & tvg_slot_bit(f)) && !tvg_host_field(out, f))
+			return tvg_fail(ctx, TVG_E_BADINPUT, "force_step_host: output field slot %d is NULL", f);
+		if (((in_fields | out_fields) & tvg_slot_bit(f)) && !ctx->f[f])
+			return tvg_fail(ctx, TVG_E_STATE, "force_step_host: field slot %d is not kept by this context", f);
+	}
+	TVG_CUDA(ctx, cudaSetDevice(ctx->device));
+	if (!ctx->copy_stream) TVG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+	for (int i = 0; i < 3; i++)
+		if (!ctx->xev[i]) TVG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->xev[i], cudaEventDisableTiming));
+	cudaStream_t s = ctx->stream, cs = ctx->copy_stream;
+	ctx->n = n;
+	ctx->sorted = false;
+	ctx->have_tree = false;
+	ctx->have_top = false;
+	ctx->use_active = false;
+	// positions first, on the context stream: the keys need them
+	for (int f = FS_POS0; f <= FS_POS2; f++)
+		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->f[f], tvg_host_field(in, f), tvg_field_bytes(ctx, f) * n,
+		                              cudaMemcpyHostToDevice, s));
+	// then the other inputs on the copy stream, while the keys and the radix
+	// passes run; the field gather of the sort waits for them
+	TVG_CUDA(ctx, cudaEventRecord(ctx->xev[0], s));
+	TVG_CUDA(ctx, cudaStreamWaitEvent(cs, ctx->xev[0], 0));
+	for (int f = 0; f < FS_NFIELDS; f++) {
+		if (f >= FS_POS0 && f <= FS_POS2) continue;
+		if (!(in_fields & tvg_slot_bit(f))) continue;
+		TVG_CUDA(ctx, cudaMemcpyAsync(ctx->f[f], tvg_host_field(in, f), tvg_field_bytes(ctx, f) * n,
+		                              cudaMemcpyHostToDevice, cs));
+	}
+	TVG_CUDA(ctx, cudaEventRecord(ctx->xev[1], cs));
+	// the isolated domain search reads the particles before the sort
+	if (find_domain_each_step(ctx)) TVG_CUDA(ctx, cudaStreamWaitEvent(s, ctx->xev[1], 0));
+	ctx->gather_wait = ctx->xev[1];
+	const int rc = force_phases(ctx, form, use_bh, parts, ewald_kind, ctx->xev[2]);
+	ctx->gather_wait = nullptr;
+	if (rc != TVG_OK) {
+		cudaStreamSynchronize(cs);
+		return rc;
+	}
+	// outputs the walks do not write leave as soon as the sort is done, the
+	// others after the walks
+	TVG_CUDA(ctx, cudaStreamWaitEvent(cs, ctx->xev[2], 0));
+	for (int f = 0; f < FS_NFIELDS; f++) {
+		const uint32_t bit = tvg_slot_bit(f);
+		if (!(out_fields & bit)) continue;
+		TVG_CUDA(ctx, cudaMemcpyAsync(tvg_host_field(out, f), ctx->f[f], tvg_field_bytes(ctx, f) * n,
+		                              cudaMemcpyDeviceToHost, (bit & kWrittenByStep) ? s : cs));
+	}
+	TVG_CUDA(ctx, cudaStreamSynchronize(cs));
+	TVG_CUDA(ctx, cudaStreamSynchronize(s));
+	TVG_CHECK(force_times(ctx));
+	return tvg_sync_status(ctx, "force_step_host");
 }
 
 // The launches of Compute_Acceleration (accel.c:15-71) after the single-rank

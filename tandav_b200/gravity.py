@@ -641,6 +641,35 @@ class GravityContext:
             fields |= F_ID
         self._check(self.lib.tvg_download(self.ctx, C.byref(p), C.c_uint32(fields)), "download")
 
+    def force_step_host(self, n, pos, mass, last_acc=None, ids=None, grav_acc=None, ids_out=None,
+                        form=FORM_GROUP, use_bh=False, parts=WALK_GRAVITY, ewald_kind=EWALD_TABLE):
+        """tvg_force_step_host: one force step from pre-allocated (e.g.
+        pinned) Float arrays, results (PH order) into grav_acc / ids_out."""
+        src, dst = Particles(), Particles()
+        fin = F_POS | F_MASS
+        for k in range(3):
+            src.pos[k] = pos[k].ctypes.data
+        src.mass = mass.ctypes.data
+        if last_acc is not None:
+            src.last_acc_mag = last_acc.ctypes.data
+            fin |= F_LAST_ACC
+        if ids is not None:
+            src.id = ids.ctypes.data
+            fin |= F_ID
+        fout = 0
+        if grav_acc is not None:
+            for k in range(3):
+                dst.grav_acc[k] = grav_acc[k].ctypes.data
+            fout |= F_GRAV_ACC
+        if ids_out is not None:
+            dst.id = ids_out.ctypes.data
+            fout |= F_ID
+        self._check(self.lib.tvg_force_step_host(self.ctx, C.c_int64(n), C.byref(src), C.c_uint32(fin),
+                                                 C.byref(dst), C.c_uint32(fout), C.c_int32(form),
+                                                 C.c_int32(int(use_bh)), C.c_uint32(parts),
+                                                 C.c_int32(ewald_kind)), "force_step_host")
+        self.n = n
+
 
 def read_snapshot_header(path):
     """The header of a snapshot (or of path.0 of a split one) and the number
