@@ -134,6 +134,7 @@ extern "C" int tvg_init(int device, const tvg_config *cfg, tvg_context **out)
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->pref, 8 * 4 * (cap + 1)));
 	for (int k = 0; k < 3; k++) TVG_CHECK(dalloc(ctx, (void **) &ctx->ipos[k], 4 * cap));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->wtree, sizeof(tvg_wnode) * ctx->tcap));
+	TVG_CHECK(dalloc(ctx, (void **) &ctx->big_list, 4 * (ctx->tcap + 1)));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->group_first, 4 * (cap / 8 + 1024)));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->work_counter, 64));
 	TVG_CHECK(dalloc(ctx, (void **) &ctx->counters, 8 * 8));
@@ -181,7 +182,7 @@ extern "C" void tvg_finalize(tvg_context *ctx)
 	                 ctx->kd_m2k, ctx->kd_m2d, ctx->kd_work, ctx->tl_scratch, ctx->act_flag,
 	                 ctx->act_off, ctx->mlp_prm, ctx->mlp_bf16, ctx->ewald_taylor, ctx->dc,
 	                 ctx->d_toptab, ctx->top_of, ctx->dd_scratch, ctx->tu_first, ctx->tu_dp,
-	                 ctx->tu_big, ctx->tune_active, ctx->wquad, ctx->wrange };
+	                 ctx->tu_big, ctx->big_list, ctx->tune_active, ctx->wquad, ctx->wrange };
 	for (void *b : bufs) if (b) cudaFree(b);
 	if (ctx->h_status) cudaFreeHost(ctx->h_status);
 	for (int i = 0; i < 16; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

@@ -234,6 +234,7 @@ struct tvg_context {
 	int64_t npart_updates = 0;         // Local_NPart_Updates (signal.c:80)
 	int32_t *tu_first = nullptr;       // first particle of every tree node
 	int32_t *tu_big = nullptr;         // [0]: count, then the nodes the node kick leaves to a warp each
+	int32_t *big_list = nullptr;       // [0]: count, then the nodes whose moments a block each sums
 	void *tu_dp = nullptr;             // dp of the active particles by slot, 3 x cap Float
 
 	// device-resident counts and top-node tables of the step

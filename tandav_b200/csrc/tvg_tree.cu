@@ -514,7 +514,11 @@ __global__ void k_moments_seq(const tvg_devcount *__restrict__ dc, int64_t tcap,
 	}
 }
 
-// fast mode: one warp per internal node, FP64 sums relative to the node centre
+// fast mode: one warp per internal node, FP64 sums relative to the node
+// centre; nodes of more than MOM_BLOCK_MIN particles are left to a block each
+// (k_moments_block: the subtree roots below the top nodes hold about N / 64
+// particles, and one warp over one of them set the kernel's length)
+#define MOM_BLOCK_MIN 8192
 template <typename F>
 __device__ void moments_warp_one(int64_t G, int lane, TNode<F> *tree, const int32_t *__restrict__ tree_u,
                                  const int32_t *__restrict__ u_start, const F *__restrict__ x,
@@ -522,7 +526,7 @@ __device__ void moments_warp_one(int64_t G, int lane, TNode<F> *tree, const int3
                                  const F *__restrict__ m)
 {
 	const TNode<F> &nd = tree[G];
-	if (!(nd.Bitfield & (1u << 9)) || nd.DNext <= 0) return;
+	if (!(nd.Bitfield & (1u << 9)) || nd.DNext <= 0 || nd.Npart > MOM_BLOCK_MIN) return;
 	const int64_t s = u_start[tree_u[G]], cnt = nd.Npart;
 	const double c0 = (double) nd.Pos[0], c1 = (double) nd.Pos[1], c2 = (double) nd.Pos[2];
 	double a0 = 0, a1 = 0, a2 = 0, am = 0;
@@ -560,6 +564,77 @@ __global__ void k_moments_warp(const tvg_devcount *__restrict__ dc, int64_t tcap
 	for (int64_t G = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5; G < nnodes;
 	     G += ((int64_t) gridDim.x * blockDim.x) >> 5)
 		moments_warp_one<F>(G, lane, tree, tree_u, u_start, x, y, z, m);
+}
+
+// the internal nodes of more than MOM_BLOCK_MIN particles, listed for
+// k_moments_block (list[0] counts them; at most one entry per node)
+template <typename F>
+__global__ void k_list_big_nodes(const tvg_devcount *__restrict__ dc, int64_t tcap, const TNode<F> *tree,
+                                 int32_t *list)
+{
+	const int64_t nnodes = min(dc->nnodes, tcap);
+	for (int64_t G = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; G < nnodes;
+	     G += (int64_t) gridDim.x * blockDim.x) {
+		const TNode<F> &nd = tree[G];
+		if ((nd.Bitfield & (1u << 9)) && nd.DNext > 0 && nd.Npart > MOM_BLOCK_MIN)
+			list[1 + atomicAdd(&list[0], 1)] = (int32_t) G;
+	}
+}
+
+// the listed nodes, a block each, with the FP64 sums of moments_warp_one
+#define MOM_BLOCK_THREADS 256
+template <typename F>
+__global__ void __launch_bounds__(MOM_BLOCK_THREADS) k_moments_block(TNode<F> *tree,
+                                                                     const int32_t *__restrict__ tree_u,
+                                                                     const int32_t *__restrict__ u_start,
+                                                                     const F *__restrict__ x, const F *__restrict__ y,
+                                                                     const F *__restrict__ z, const F *__restrict__ m,
+                                                                     const int32_t *__restrict__ list)
+{
+	__shared__ double red[MOM_BLOCK_THREADS / 32][4];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int nl = list[0];
+	for (int k = blockIdx.x; k < nl; k += gridDim.x) {
+		const int64_t H = list[1 + k];
+		const TNode<F> &nd = tree[H];
+		const int64_t s = u_start[tree_u[H]], cnt = nd.Npart;
+		const double c0x = (double) nd.Pos[0], c0y = (double) nd.Pos[1], c0z = (double) nd.Pos[2];
+		double a0 = 0, a1 = 0, a2 = 0, am = 0;
+		for (int64_t j = s + threadIdx.x; j < s + cnt; j += MOM_BLOCK_THREADS) {
+			const double mj = (double) m[j];
+			am += mj;
+			a0 += mj * ((double) x[j] - c0x);
+			a1 += mj * ((double) y[j] - c0y);
+			a2 += mj * ((double) z[j] - c0z);
+		}
+#pragma unroll
+		for (int o = 16; o; o >>= 1) {
+			am += __shfl_xor_sync(0xFFFFFFFFu, am, o);
+			a0 += __shfl_xor_sync(0xFFFFFFFFu, a0, o);
+			a1 += __shfl_xor_sync(0xFFFFFFFFu, a1, o);
+			a2 += __shfl_xor_sync(0xFFFFFFFFu, a2, o);
+		}
+		if (lane == 0) {
+			red[w][0] = am;
+			red[w][1] = a0;
+			red[w][2] = a1;
+			red[w][3] = a2;
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			for (int v = 1; v < MOM_BLOCK_THREADS / 32; v++) {
+				am += red[v][0];
+				a0 += red[v][1];
+				a1 += red[v][2];
+				a2 += red[v][3];
+			}
+			tree[H].Mass = (F) am;
+			tree[H].CoM[0] = (F) (c0x + a0 / am);
+			tree[H].CoM[1] = (F) (c0y + a1 / am);
+			tree[H].CoM[2] = (F) (c0z + a2 / am);
+		}
+		__syncthreads();
+	}
 }
 
 // top node Mass/CoM (finalise_subtree copies the subtree root, as float),
@@ -645,8 +720,13 @@ static int build_typed(tvg_context *ctx, uint32_t flags)
 	const int exact = (flags & TVG_BUILD_EXACT_MOMENTS) ? 1 : 0;
 	k_moments_seq<F><<<TVG_CNT(ctx, gs), 128, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z, m,
 	                                                 exact);
-	if (!exact)
+	if (!exact) {
+		TVG_CUDA(ctx, cudaMemsetAsync(ctx->big_list, 0, 4, s));
+		k_list_big_nodes<F><<<TVG_CNT(ctx, gs), 256, 0, s>>>(dc, tcap, tree, ctx->big_list);
 		k_moments_warp<F><<<TVG_CNT(ctx, gs), 256, 0, s>>>(dc, tcap, tree, ctx->tree_u, ctx->u_start, x, y, z, m);
+		k_moments_block<F><<<TVG_CNT(ctx, 148 * 4), MOM_BLOCK_THREADS, 0, s>>>(tree, ctx->tree_u, ctx->u_start,
+		                                                                      x, y, z, m, ctx->big_list);
+	}
 	TVG_CUDA(ctx, cudaGetLastError());
 	k_finish_top<F><<<TVG_CNT(ctx, TVG_MAX_TOP / 128), 128, 0, s>>>(dc, ctx->d_top, tree, tp, tcap, x, y,
 	                                                                 z, m, vsize);

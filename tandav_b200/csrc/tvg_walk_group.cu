@@ -310,6 +310,9 @@ __device__ __forceinline__ void quad_store(const QuadSums &q, double gravity, fl
 // first, so a warp of 32 consecutive nodes summing its large ones in turn
 // would leave one warp with the top nodes: 75 ms per 256^3 step.)
 #define GW_QUAD_LANE 64
+// nodes of more particles than this (the top nodes, about N / 64 each, and
+// the levels just below them) are summed by a block each, k_wt_quad_block
+#define GW_QUAD_BLOCK 8192
 __global__ void k_wt_quad_dev(const tvg_devcount *__restrict__ dc, const tvg_wnode *__restrict__ wt,
                               const int2 *__restrict__ wrange, const uint32_t *__restrict__ ix,
                               const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
@@ -331,7 +334,7 @@ __global__ void k_wt_quad_dev(const tvg_devcount *__restrict__ dc, const tvg_wno
 	}
 	for (int64_t w = warp; w < nw; w += nwarps) {
 		const int2 r = wrange[w];
-		if (r.y <= GW_QUAD_LANE) continue;
+		if (r.y <= GW_QUAD_LANE || r.y > GW_QUAD_BLOCK) continue;
 		const uint32_t cx = wt[w].cx, cy = wt[w].cy, cz = wt[w].cz;
 		QuadSums q = { 0, 0, 0, 0, 0, 0 };
 		for (int64_t j = r.x + lane; j < (int64_t) r.x + r.y; j += 32)
@@ -346,6 +349,69 @@ __global__ void k_wt_quad_dev(const tvg_devcount *__restrict__ dc, const tvg_wno
 			q.yz += __shfl_xor_sync(0xFFFFFFFFu, q.yz, o);
 		}
 		if (lane == 0) quad_store(q, gravity, wq, w);
+	}
+}
+
+// the walk nodes of more than GW_QUAD_BLOCK particles, listed for
+// k_wt_quad_block (list[0] counts them). The top nodes come first in the
+// walk tree, so a block per chunk of consecutive nodes would leave one
+// block with all of them.
+__global__ void k_wt_list_big(const tvg_devcount *__restrict__ dc, const int2 *__restrict__ wrange, int32_t *list)
+{
+	const int64_t nw = (int64_t) dc->ntop + dc->nwchild;
+	for (int64_t w = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; w < nw;
+	     w += (int64_t) gridDim.x * blockDim.x)
+		if (wrange[w].y > GW_QUAD_BLOCK) list[1 + atomicAdd(&list[0], 1)] = (int32_t) w;
+}
+
+// the listed walk nodes, a block each
+#define GW_QUAD_BLOCK_THREADS 256
+__global__ void __launch_bounds__(GW_QUAD_BLOCK_THREADS)
+k_wt_quad_block(const tvg_wnode *__restrict__ wt, const int2 *__restrict__ wrange,
+                const uint32_t *__restrict__ ix, const uint32_t *__restrict__ iy, const uint32_t *__restrict__ iz,
+                const float *__restrict__ mass_f, double scale, double gravity, float4 *__restrict__ wq,
+                const int32_t *__restrict__ list)
+{
+	__shared__ double red[GW_QUAD_BLOCK_THREADS / 32][6];
+	const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+	const int nl = list[0];
+	for (int k = blockIdx.x; k < nl; k += gridDim.x) {
+		const int64_t v = list[1 + k];
+		const int2 r = wrange[v];
+		const uint32_t cx = wt[v].cx, cy = wt[v].cy, cz = wt[v].cz;
+		QuadSums q = { 0, 0, 0, 0, 0, 0 };
+		for (int64_t j = r.x + threadIdx.x; j < (int64_t) r.x + r.y; j += GW_QUAD_BLOCK_THREADS)
+			quad_add(q, ix, iy, iz, mass_f, j, cx, cy, cz, scale);
+#pragma unroll
+		for (int o = 16; o; o >>= 1) {
+			q.xx += __shfl_xor_sync(0xFFFFFFFFu, q.xx, o);
+			q.yy += __shfl_xor_sync(0xFFFFFFFFu, q.yy, o);
+			q.zz += __shfl_xor_sync(0xFFFFFFFFu, q.zz, o);
+			q.xy += __shfl_xor_sync(0xFFFFFFFFu, q.xy, o);
+			q.xz += __shfl_xor_sync(0xFFFFFFFFu, q.xz, o);
+			q.yz += __shfl_xor_sync(0xFFFFFFFFu, q.yz, o);
+		}
+		if (lane == 0) {
+			red[wp][0] = q.xx;
+			red[wp][1] = q.yy;
+			red[wp][2] = q.zz;
+			red[wp][3] = q.xy;
+			red[wp][4] = q.xz;
+			red[wp][5] = q.yz;
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			for (int u = 1; u < GW_QUAD_BLOCK_THREADS / 32; u++) {
+				q.xx += red[u][0];
+				q.yy += red[u][1];
+				q.zz += red[u][2];
+				q.xy += red[u][3];
+				q.xz += red[u][4];
+				q.yz += red[u][5];
+			}
+			quad_store(q, gravity, wq, v);
+		}
+		__syncthreads();
 	}
 }
 
@@ -739,7 +805,8 @@ __device__ __forceinline__ void flush_quad(QuadList &Q, int nq, Target (&t)[TPL]
 		mz[k] = make_float2(-t[k].tz, -t[k].tz);
 	}
 	// two source pairs per iteration: four independent chains per lane
-	// (150.7 against 152.7 ms per 256^3 step with one pair)
+	// (150.7 against 152.7 ms per 256^3 step with one pair; three pairs:
+	// 151.7 against 149.7 ms of walk)
 #pragma unroll 2
 	for (int q = 0; q < np; q++) {
 		const float4 a = Q.xy[q], b = Q.zw[q], qa = Q.qa[q], qb = Q.qb[q], qc = Q.qc[q];
@@ -1729,9 +1796,14 @@ static int prepare_typed(tvg_context *ctx)
 			k_to_float<F><<<TVG_CNT(ctx, tvg_blocks(n, 256)), 256, 0, s>>>(n, (const F *) ctx->f[FS_MASS],
 			                                                                (float *) mf);
 		}
+		TVG_CUDA(ctx, cudaMemsetAsync(ctx->big_list, 0, 4, s));
+		k_wt_list_big<<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, wrange, ctx->big_list);
 		k_wt_quad_dev<<<TVG_CNT(ctx, 148 * 16), 256, 0, s>>>(ctx->dc, ctx->wtree, wrange, ctx->ipos[0],
 		                                                     ctx->ipos[1], ctx->ipos[2], mf,
 		                                                     1.0 / fac, ctx->cfg.gravity, ctx->wquad);
+		k_wt_quad_block<<<TVG_CNT(ctx, 148 * 4), GW_QUAD_BLOCK_THREADS, 0, s>>>(
+		    ctx->wtree, wrange, ctx->ipos[0], ctx->ipos[1], ctx->ipos[2], mf, 1.0 / fac, ctx->cfg.gravity,
+		    ctx->wquad, ctx->big_list);
 		TVG_CUDA(ctx, cudaGetLastError());
 	}
 	ctx->have_walktree = true;
