@@ -78,14 +78,15 @@
 #define GW_ELIST 64
 #define GW_DEFAULT_TPL 2
 // resident blocks per SM the table-evaluating Ewald walk is compiled for:
-// 3 (168 registers) since the uniform remainder is a polynomial (15.8 against
-// 18.4 ms per step at 256^3 with 2 blocks of 206 registers). Before that,
+// 4 (128 registers, 8 B of spill: 15.2 against 15.8 ms per step at 256^3
+// with 3 blocks of 168 registers, and 18.4 ms with 2 blocks of 206, since
+// the uniform remainder is a polynomial). Before that,
 // capping the registers had made it slower, with the tricubic lookup (1340,
 // 1442 ms against 1252 ms per step) and with the Taylor table and the closed
 // form (140.4 against 136.9 ms at 128^3). The learned correction's walk keeps
 // 1 (its network needs the registers).
 #ifndef GW_EWALD_MINB
-#define GW_EWALD_MINB 3
+#define GW_EWALD_MINB 4
 #endif
 // resident blocks per SM the gravity walk is compiled for (4: at most 128
 // registers; unbounded it took 138 and ran 3 blocks, 8 % slower), and the
