@@ -12,8 +12,8 @@ the curve is a finite automaton: a state (an orientation of the sub-cube)
 maps the octant of the next level, o = x << 2 | y << 1 | z, to the digit of
 that level and to the state of the child cube.
 
-This script restates the transpose (the same steps as hilbert_transpose in
-tvg_keys.cu), discovers the states by their digit maps over all suffixes of
+This script restates the transpose (Skilling's published steps), discovers
+the states by their digit maps over all suffixes of
 three levels, checks that the automaton reproduces the transpose on random
 64-bit coordinates, and writes a table of 64 entries per state indexed by
 the octants of two levels (o1 << 3 | o2):
@@ -28,9 +28,6 @@ import sys
 from pathlib import Path
 
 import numpy as np
-
-M64 = np.uint64(0xFFFFFFFFFFFFFFFF)
-
 
 def transpose(x0, x1, x2):
     """Skilling's axes-to-transpose step, Gray encoding and the parity undo,
@@ -125,7 +122,7 @@ def discover():
 
 
 def check(trans, n=20000, seed=7):
-    """The automaton against the transpose on random 63-bit coordinates."""
+    """The automaton against the transpose on random 64-bit coordinates."""
     rng = np.random.default_rng(seed)
     x = [rng.integers(0, 1 << 64, n, dtype=np.uint64) for _ in range(3)]
     x[0][: n // 2] >>= np.uint64(1)           # half of them below 2^63 in every axis
