@@ -177,22 +177,64 @@ __device__ __forceinline__ double drift_step(const TimeParams &p, uint32_t c, ui
 	return spline_eval(p.tab, p.tab.drift, p.tab.m2d, a1) - spline_eval(p.tab, p.tab.drift, p.tab.m2d, a0);
 }
 
-// Kick_First_Halfstep / Kick_Second_Halfstep (kick.c:9-70)
-template <typename F>
-__global__ void k_kick(int64_t n_act, const int32_t *__restrict__ active, TimeParams p,
-                       const int32_t *__restrict__ bin, uint32_t *it_kick, const F *a0, const F *a1,
-                       const F *a2, F *v0, F *v1, F *v2)
+// Kick_First_Halfstep / Kick_Second_Halfstep (kick.c:9-70). The kick factor
+// (an exponential and a spline in FP64) depends only on It_Kick_Pos and the
+// time bin, and the particles of one bin share their It_Kick_Pos in a step.
+// So a block keeps one slot per bin: the first thread that claims a bin's
+// slot for its particle's It_Kick_Pos evaluates the factor there, and every
+// particle of the block with that bin and position takes it (the same
+// function, so the same bits); a particle whose position differs evaluates
+// its own. KD_IPT particles per thread.
+#define KD_THREADS 256
+#define KD_IPT 4
+#define KD_EMPTY 0xFFFFFFFFu          // no integer time reaches it (the timeline ends at 2^31)
+
+// claims the bin's slot for it_curr; true for the thread that must evaluate
+__device__ __forceinline__ bool kd_claim(uint32_t *s_curr, int b, uint32_t it_curr)
 {
-	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (k >= n_act) return;
-	const int64_t i = active ? active[k] : k;
-	const uint32_t it_step = 1u << bin[i];
-	const uint32_t it_curr = it_kick[i], it_next = it_curr + (it_step >> 1);
-	const F dt = (F) kick_step(p, it_curr, it_next);
-	v0[i] += dt * a0[i];
-	v1[i] += dt * a1[i];
-	v2[i] += dt * a2[i];
-	it_kick[i] += it_step >> 1;
+	return b >= 0 && b < N_INT_BINS && atomicCAS(&s_curr[b], KD_EMPTY, it_curr) == KD_EMPTY;
+}
+
+template <typename F>
+__global__ void __launch_bounds__(KD_THREADS) k_kick(int64_t n_act, const int32_t *__restrict__ active,
+                                                     TimeParams p, const int32_t *__restrict__ bin,
+                                                     uint32_t *it_kick, const F *a0, const F *a1, const F *a2,
+                                                     F *v0, F *v1, F *v2)
+{
+	__shared__ uint32_t s_curr[N_INT_BINS];
+	__shared__ double s_dt[N_INT_BINS];
+	if (threadIdx.x < N_INT_BINS) s_curr[threadIdx.x] = KD_EMPTY;
+	__syncthreads();
+	const int64_t k0 = (int64_t) blockIdx.x * (KD_THREADS * KD_IPT);
+	int64_t idx[KD_IPT];
+	int b[KD_IPT];
+	uint32_t cur[KD_IPT];
+#pragma unroll
+	for (int u = 0; u < KD_IPT; u++) {
+		const int64_t k = k0 + u * KD_THREADS + threadIdx.x;
+		idx[u] = -1;
+		if (k < n_act) {
+			idx[u] = active ? active[k] : k;
+			b[u] = bin[idx[u]];
+			cur[u] = it_kick[idx[u]];
+			if (kd_claim(s_curr, b[u], cur[u]))
+				s_dt[b[u]] = kick_step(p, cur[u], cur[u] + ((1u << b[u]) >> 1));
+		}
+	}
+	__syncthreads();
+#pragma unroll
+	for (int u = 0; u < KD_IPT; u++) {
+		if (idx[u] < 0) continue;
+		const int64_t i = idx[u];
+		const uint32_t it_step = 1u << b[u];
+		const uint32_t it_curr = cur[u], it_next = it_curr + (it_step >> 1);
+		const bool hit = b[u] >= 0 && b[u] < N_INT_BINS && s_curr[b[u]] == it_curr;
+		const F dt = (F) (hit ? s_dt[b[u]] : kick_step(p, it_curr, it_next));
+		v0[i] += dt * a0[i];
+		v1[i] += dt * a1[i];
+		v2[i] += dt * a2[i];
+		it_kick[i] += it_step >> 1;
+	}
 }
 
 // the momentum change of each active particle for the tree updates
@@ -217,25 +259,53 @@ __global__ void k_kick_dp(int64_t n, const int32_t *__restrict__ flag, const int
 	dp2[k] = d[2];
 }
 
-// Drift_To_Sync_Point (drift.c:12-40): the active particles only
+// Drift_To_Sync_Point (drift.c:12-40): the active particles only. The drift
+// factor depends only on It_Drift_Pos (it_next is the step's); as in k_kick,
+// a block evaluates it once per distinct position of each time bin.
 template <typename F>
-__global__ void k_drift(int64_t n_act, const int32_t *__restrict__ active, TimeParams p,
-                        uint32_t it_next, uint32_t it_end, uint32_t *it_drift, const F *v0,
-                        const F *v1, const F *v2, F *x0, F *x1, F *x2, int *status)
+__global__ void __launch_bounds__(KD_THREADS) k_drift(int64_t n_act, const int32_t *__restrict__ active,
+                                                      TimeParams p, uint32_t it_next, uint32_t it_end,
+                                                      const int32_t *__restrict__ bin, uint32_t *it_drift,
+                                                      const F *v0, const F *v1, const F *v2, F *x0, F *x1, F *x2,
+                                                      int *status)
 {
-	const int64_t k = blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
-	if (k >= n_act) return;
-	const int64_t i = active ? active[k] : k;
-	const uint32_t it_curr = it_drift[i];
-	if (it_next > it_end || it_next < it_curr) {            // drift.c:22-27
-		atomicOr(status, TVG_ST_BADPOS);
-		return;
+	__shared__ uint32_t s_curr[N_INT_BINS];
+	__shared__ double s_dt[N_INT_BINS];
+	if (threadIdx.x < N_INT_BINS) s_curr[threadIdx.x] = KD_EMPTY;
+	__syncthreads();
+	const int64_t k0 = (int64_t) blockIdx.x * (KD_THREADS * KD_IPT);
+	int64_t idx[KD_IPT];
+	int b[KD_IPT];
+	uint32_t cur[KD_IPT];
+#pragma unroll
+	for (int u = 0; u < KD_IPT; u++) {
+		const int64_t k = k0 + u * KD_THREADS + threadIdx.x;
+		idx[u] = -1;
+		if (k < n_act) {
+			idx[u] = active ? active[k] : k;
+			b[u] = bin[idx[u]];
+			cur[u] = it_drift[idx[u]];
+			const bool valid = !(it_next > it_end || it_next < cur[u]);
+			if (valid && kd_claim(s_curr, b[u], cur[u])) s_dt[b[u]] = drift_step(p, cur[u], it_next);
+		}
 	}
-	const double dt = drift_step(p, it_curr, it_next);
-	x0[i] = (F) ((double) x0[i] + dt * (double) v0[i]);
-	x1[i] = (F) ((double) x1[i] + dt * (double) v1[i]);
-	x2[i] = (F) ((double) x2[i] + dt * (double) v2[i]);
-	it_drift[i] += it_next - it_curr;
+	__syncthreads();
+#pragma unroll
+	for (int u = 0; u < KD_IPT; u++) {
+		if (idx[u] < 0) continue;
+		const int64_t i = idx[u];
+		const uint32_t it_curr = cur[u];
+		if (it_next > it_end || it_next < it_curr) {            // drift.c:22-27
+			atomicOr(status, TVG_ST_BADPOS);
+			continue;
+		}
+		const bool hit = b[u] >= 0 && b[u] < N_INT_BINS && s_curr[b[u]] == it_curr;
+		const double dt = hit ? s_dt[b[u]] : drift_step(p, it_curr, it_next);
+		x0[i] = (F) ((double) x0[i] + dt * (double) v0[i]);
+		x1[i] = (F) ((double) x1[i] + dt * (double) v1[i]);
+		x2[i] = (F) ((double) x2[i] + dt * (double) v2[i]);
+		it_drift[i] += it_next - it_curr;
+	}
 }
 
 // Periodic_Constrain_Particles_To_Box (periodic.c:30-55), all particles; the
@@ -732,7 +802,7 @@ static int kick_typed(tvg_context *ctx)
 		    (const F *) ctx->f[FS_ACC1], (const F *) ctx->f[FS_ACC2], dp, dp + cap, dp + 2 * cap);
 		TVG_CUDA(ctx, cudaGetLastError());
 	}
-	k_kick<F><<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, ctx->stream>>>(
+	k_kick<F><<<TVG_CNT(ctx, tvg_blocks(na, KD_THREADS * KD_IPT)), KD_THREADS, 0, ctx->stream>>>(
 	    na, ctx->use_active ? ctx->active : nullptr, time_params(ctx),
 	    (const int32_t *) ctx->f[FS_TIME_BIN], (uint32_t *) ctx->f[FS_IT_KICK],
 	    (const F *) ctx->f[FS_ACC0], (const F *) ctx->f[FS_ACC1], (const F *) ctx->f[FS_ACC2],
@@ -773,9 +843,9 @@ static int drift_typed(tvg_context *ctx)
 	cudaStream_t s = ctx->stream;
 	const int64_t na = ctx->use_active ? ctx->n_active : ctx->n;
 	if (na > 0) {
-		k_drift<F><<<TVG_CNT(ctx, tvg_blocks(na, 256)), 256, 0, s>>>(
+		k_drift<F><<<TVG_CNT(ctx, tvg_blocks(na, KD_THREADS * KD_IPT)), KD_THREADS, 0, s>>>(
 		    na, ctx->use_active ? ctx->active : nullptr, time_params(ctx), st.next, st.end,
-		    (uint32_t *) ctx->f[FS_IT_DRIFT], (const F *) ctx->f[FS_VEL0], (const F *) ctx->f[FS_VEL1],
+		    (const int32_t *) ctx->f[FS_TIME_BIN], (uint32_t *) ctx->f[FS_IT_DRIFT], (const F *) ctx->f[FS_VEL0], (const F *) ctx->f[FS_VEL1],
 		    (const F *) ctx->f[FS_VEL2], (F *) ctx->f[FS_POS0], (F *) ctx->f[FS_POS1],
 		    (F *) ctx->f[FS_POS2], ctx->status);
 		TVG_CUDA(ctx, cudaGetLastError());
