@@ -66,3 +66,25 @@ def test_host_register_rejects_null_or_empty_ranges():
     assert lib.tvg_host_register(None, C.c_size_t(64)) == 5
     assert lib.tvg_host_register(buf, C.c_size_t(0)) == 5
     assert lib.tvg_host_unregister(None) == 5
+
+
+def test_step_entry_points_reject_a_null_context():
+    """The whole-step calls check their arguments before any CUDA call, so
+    they answer TVG_E_BADINPUT without a GPU."""
+    lib = tandav_b200.lib()
+    p = gravity.Particles()
+    i32, u32, i64 = C.c_int32, C.c_uint32, C.c_int64
+    assert lib.tvg_force_step(None, i32(1), i32(0), u32(1), i32(0)) == 5
+    assert lib.tvg_force_step_host(None, i64(10), C.byref(p), u32(gravity.F_POS), C.byref(p), u32(0),
+                                   i32(1), i32(0), u32(1), i32(0)) == 5
+    # a context is required, and so are the input and output descriptions
+    fake = C.c_void_p(1)
+    assert lib.tvg_force_step_host(fake, i64(10), None, u32(gravity.F_POS), C.byref(p), u32(0),
+                                   i32(1), i32(0), u32(1), i32(0)) == 5
+    assert lib.tvg_force_step_host(fake, i64(10), C.byref(p), u32(gravity.F_POS), None, u32(0),
+                                   i32(1), i32(0), u32(1), i32(0)) == 5
+    assert lib.tvg_kick_first_halfstep(None) == 5
+    assert lib.tvg_kick_second_halfstep(None) == 5
+    assert lib.tvg_drift_to_sync_point(None) == 5
+    assert lib.tvg_set_new_timesteps(None) == 5
+    assert lib.tvg_time_for_domain_update(None, C.c_double(0.1), None) == 5
