@@ -10,15 +10,18 @@ build, the gravity walk with the relative opening criterion (|a_old| from an
 untimed Barnes-Hut prepare pass, as src/accel.c:51-71 does) and the Ewald
 periodic correction.
 
-Our arm: the group form (FP32 integer-offset walk, warp per PH group, a
-per-group Ewald walk) at the opening parameter that brings the rms force
-error below 1e-3 (TREE_OPEN_PARAM_REL 7e-5 on this box; the error is measured
-in every run against an FP64 Ewald-summed direct sum over all particles for
-10^4 random particles), particles resident in HBM (`value`), and the same
-step through the C ABI with host buffers (`e2e`). The plain GPU form (the
-reference algorithm, one thread per particle, FP64, exact moments, the
-reference's TREE_OPEN_PARAM_REL 0.005) is timed on a strided subset of the
-particles and reported beside it with its own measured error.
+Our arm: the group form (FP32 integer-offset walk, warp per PH group, node
+quadrupoles with the octupole-order relative criterion, a per-group Ewald
+walk on a Taylor table) at TREE_OPEN_PARAM_REL 8e-3, which keeps the rms
+force error below 1e-3 with a quarter in reserve (measured in every run
+against an FP64 Ewald-summed direct sum over all particles for 10^4 random
+particles); the step is one captured CUDA graph with the particles resident
+in HBM (`value`), and the same step through the C ABI from and to pinned host
+buffers with the copies overlapped (`e2e`, tvg_force_step_host). Beside it:
+the plain GPU form (the reference algorithm, one thread per particle, FP64,
+exact moments, the reference's TREE_OPEN_PARAM_REL 0.005) over all particles
+with its own measured error, the group form at the plain form's opening, the
+group form with monopoles, and the learned Ewald correction.
 `--impl reference`: the unmodified reference C code (oracle/_ref timing
 build) on the host cores, the walk timed on a strided subset.
 
